@@ -1,0 +1,126 @@
+/*
+ * zdemx.h -- C ABI of libzdemx.so, the B200 implementation of the ZDEM-X polyhedral contact step.
+ *
+ * The reference has no plugin or FFI layer; its surfaces are the zdem_cpu program (src/main.cpp), its
+ * file formats, and the Python pair-contact module polyline.py.  Each entry point below says which
+ * reference code it replaces (file:line, paths inside the reference project).
+ *
+ * Conventions
+ *   - Every call returns a status (ZDX_OK == 0).  zdx_last_error() describes the last failure of a context.
+ *   - Buffers belong to the caller.  In a pair call, zdx_pair_opts.mem says whether every pointer of that
+ *     call is host memory (copies are made inside the call) or device memory on the context's GPU.
+ *   - One context = one GPU and one CUDA stream.  A context is not thread-safe; use one per thread.
+ *   - All geometry is FP64.  Integer results (segment lists, components, snapped topology, loops,
+ *     contact ids) are bit-exact with the reference's own C++ path on the same inputs.
+ *   - There is no CPU fallback: without a usable GPU, calls that compute return ZDX_ERR_NO_DEVICE.
+ */
+#ifndef ZDEMX_H
+#define ZDEMX_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ------------------------------------------------------------------------------------- */
+#define ZDX_OK 0
+#define ZDX_ERR_INVALID 1    /* bad argument                                                        */
+#define ZDX_ERR_CUDA 2       /* a CUDA call failed                                                  */
+#define ZDX_ERR_CAPACITY 3   /* a fixed-capacity buffer would overflow; totals report what is needed */
+#define ZDX_ERR_IO 4         /* a file could not be read or written                                 */
+#define ZDX_ERR_NO_DEVICE 5  /* no usable CUDA device                                               */
+#define ZDX_ERR_CONFIG 6     /* config file rejected (src/main.cpp:1879-1881, 1940-1953)              */
+#define ZDX_ERR_STATE 7      /* call out of order (e.g. stepping before a scene is loaded)         */
+
+typedef struct zdx_ctx zdx_ctx;
+
+/* Create a context on CUDA device `device` (its own stream and workspaces).  No reference counterpart. */
+int zdx_create(zdx_ctx** out, int device);
+int zdx_destroy(zdx_ctx* ctx);
+const char* zdx_status_string(int status);
+const char* zdx_last_error(const zdx_ctx* ctx);
+/* Library version string, e.g. "zdemx 0.1 sm_100a". */
+const char* zdx_version(void);
+
+/* ---- meshes (host) -------------------------------------------------------------------------------
+ * zdx_stl_load replaces load_stl (src/main.cpp:308-371; polyline.py:59-96): binary when the file size
+ * is exactly 84 + 50 n, ASCII otherwise.  Returns the triangle count (may exceed cap; only cap are
+ * written) or a negative status.  tris: 9 doubles per triangle. */
+int64_t zdx_stl_load(const char* path, double* tris, int64_t cap);
+
+/* zdx_mesh_build replaces build_mesh (src/main.cpp:445-497) with compute_mass_properties (:373-443)
+ * and unique_vertices (:287-306).  tris_out receives the (optionally centred) triangles; props17 =
+ * volume, center(3), radius, mean_edge, bbox_diag, inertia_unit(9 row-major), unique vertex count. */
+int zdx_mesh_build(const double* tris, int64_t ntri, int center_mesh, double* tris_out, double* props17);
+
+/* ---- batched pair contacts ------------------------------------------------------------------------
+ * Replaces the per-pair body of the zdem_cpu step (src/main.cpp:2062-2219: transform_tris, plane and
+ * AABB set-up, the nA x nB triangle loop with tri_tri_intersection_segment, label_segments_by_contact_
+ * greedy, snap_endpoints, split_t_junctions, extract_loops, accumulate_Sn_Gn_from_polyline,
+ * contact_point_xc0 and the loop filters) and the pair call of polyline.py (main, polyline.py:743-822,
+ * with build_contacts_from_loops, :655-701), for many pairs at once. */
+#define ZDX_MODE_ZDEM 0      /* zdem_cpu semantics: tol from mesh A, |Sn| filters, nA flipped toward B   */
+#define ZDX_MODE_POLYLINE 1  /* polyline.py semantics: tol given, bbox filter, stable orders, no flip    */
+#define ZDX_MEM_HOST 0
+#define ZDX_MEM_DEVICE 1
+#define ZDX_SCHED_BATCHED 0  /* one launch per stage over the whole batch, cost-ordered work queue       */
+#define ZDX_SCHED_PLAIN 1    /* one launch per stage per pair (the unbatched form, for comparison)      */
+
+typedef struct zdx_pair_opts {
+    int mode;             /* ZDX_MODE_*                                                               */
+    int split_contacts;   /* split segments into components first (src/main.cpp:2154; --split-contacts) */
+    double tol;           /* > 0: snap tolerance (polyline --tol); <= 0: 0.1 mean_edge(A) (:2118)      */
+    double k;             /* stiffness of the minimal law Fn = k/2 |Sn| (polyline.py:677)               */
+    int mem;              /* ZDX_MEM_*: where every pointer of the call lives                          */
+    int sched;            /* ZDX_SCHED_*                                                              */
+    int want_loop_points; /* also return each contact's loop polyline                                 */
+    int max_seg_per_pair; /* segment capacity per pair (0: 16384); a larger pair reports CAPACITY     */
+} zdx_pair_opts;
+
+typedef struct zdx_mesh_set {
+    int32_t n_mesh;
+    const double* tris;       /* mesh-local triangles, 9 doubles each, meshes back to back             */
+    const int64_t* tri_off;   /* n_mesh + 1 triangle offsets                                          */
+    const double* mean_edge;  /* n_mesh, Mesh::mean_edge (sets tol and area_eps in zdem mode)          */
+    const double* bbox_diag;  /* n_mesh, Mesh::bbox_diag (tol when mean_edge is 0)                     */
+} zdx_mesh_set;
+
+typedef struct zdx_pair_batch {
+    int64_t n_pairs;
+    const int32_t* mesh;  /* 2 per pair: mesh of A, mesh of B                                          */
+    const double* pose;   /* 14 per pair: posA(3) quatA(w,x,y,z) posB(3) quatB(w,x,y,z)               */
+} zdx_pair_batch;
+
+/* Per contact (one accepted loop), 20 doubles in contact_geom:
+ *   Sn(3) Gn(3) xc0(3) nA(3) area Fn F_A(3) F_B(3)
+ * zdem mode: nA is flipped to point from A toward B (src/main.cpp:2209-2219), F_A = -Fn nA pushes A
+ * away from B as the zdem_cpu scatter does (:2281).  polyline mode: nA = -Sn/|Sn|, F_A = Fn nA,
+ * F_B = -F_A exactly as build_contacts_from_loops (polyline.py:672-679); a loop with |Sn| < 1e-14 is
+ * still a contact with xc0 = 0, nA = 0, area = 0 (xc0 None in Python).
+ * contact_info, 4 int32 per contact: pair index, contact_id (running count within the pair over
+ * components in size order, then loops in trace order), loop vertex count, component index. */
+typedef struct zdx_pair_result {
+    int32_t* pair_ncontact;    /* n_pairs                                                           */
+    int64_t* pair_contact_off; /* n_pairs + 1: contacts of pair p are [off[p], off[p+1])             */
+    int32_t* pair_stats;       /* n_pairs x 4: segments, components, raw loops, status (0 = ok)      */
+    int64_t contact_cap;
+    double* contact_geom;      /* contact_cap x 20                                                   */
+    int32_t* contact_info;     /* contact_cap x 4                                                    */
+    int64_t loop_point_cap;    /* used when want_loop_points                                        */
+    double* loop_points;       /* loop_point_cap x 3, loop vertices of every contact in order        */
+    int64_t* contact_point_off;/* contact_cap + 1                                                   */
+    int64_t totals[4];         /* out: contacts, segments, triangle AABB checks (the step log's
+                                  tri_checks, src/main.cpp:2129), loop points                        */
+} zdx_pair_result;
+
+int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* meshes,
+                      const zdx_pair_batch* pairs, zdx_pair_result* out);
+
+/* Per-stage device times of the last pair call, in milliseconds (CUDA events on the context stream):
+ * [0] mesh bounds, [1] cull + triangle tests, [2] contact rebuild, [3] gather, [4] whole call. */
+int zdx_pair_timings(const zdx_ctx* ctx, double* ms5);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
