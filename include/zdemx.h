@@ -116,9 +116,12 @@ typedef struct zdx_pair_result {
 int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* meshes,
                       const zdx_pair_batch* pairs, zdx_pair_result* out);
 
-/* Per-stage device times of the last pair call, in milliseconds (CUDA events on the context stream):
- * [0] mesh bounds, [1] cull + triangle tests, [2] contact rebuild, [3] gather, [4] whole call. */
-int zdx_pair_timings(const zdx_ctx* ctx, double* ms5);
+/* Device times of the last pair call, in milliseconds (CUDA events on the context stream):
+ * [0] inputs in + mesh bounds + work order, [1] the triangle-test kernel, [2] the rebuild kernel,
+ * [3] gather + outputs out, [4] whole call.  *launches (may be NULL) receives the number of kernels
+ * this context has launched so far.  No reference counterpart (the reference times with std::chrono
+ * around its stages, src/main.cpp:2061-2304). */
+int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launches);
 
 #ifdef __cplusplus
 }

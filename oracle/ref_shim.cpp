@@ -26,6 +26,8 @@
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
+#include <atomic>
+#include <thread>
 
 #ifdef ZDX_REF_HIPREC
 #define setprecision(x) setprecision(17)
@@ -86,17 +88,14 @@ extern "C" int zdx_ref_build_mesh(const double* tris, int ntri, int center_mesh,
 }
 
 // The per-pair body of the reference step loop, src/main.cpp:2062-2219, driven stage by stage through the
-// reference's own functions.  Only the bookkeeping that records intermediate results is added.
-extern "C" int zdx_ref_pair(const double* trisA, int nA, double mean_edgeA, double bbox_diagA,
-                            const double* trisB, int nB, const double* poseA, const double* poseB,
-                            int split_contacts, ZdxRefPairOut* out) {
+// reference's own functions.  Only the bookkeeping that records intermediate results is added (when out
+// is not null).  Returns the number of accepted loops (contacts).
+static int run_pair(const Mesh& meshA, const Mesh& meshB, const Transform& tfA, const Transform& tfB,
+                    int split_contacts, ZdxRefPairOut* out) {
+    ZdxRefPairOut scratch;
+    const bool rec = out != nullptr;
+    if (!rec) out = &scratch;
     std::memset(out, 0, sizeof(*out));
-    Mesh meshA, meshB;
-    meshA.tris = tris_from(trisA, nA);
-    meshA.mean_edge = mean_edgeA;
-    meshA.bbox_diag = bbox_diagA;
-    meshB.tris = tris_from(trisB, nB);
-    Transform tfA = pose_from(poseA), tfB = pose_from(poseB);
 
     std::vector<std::array<Vec3, 3>> tA = transform_tris(meshA, tfA);
     std::vector<std::array<Vec3, 3>> tB = transform_tris(meshB, tfB);
@@ -141,11 +140,13 @@ extern "C" int zdx_ref_pair(const double* trisA, int nA, double mean_edgeA, doub
     }
     out->tri_checks = checks;
     std::vector<double> seg;
-    for (auto& s : segments) {
-        seg.insert(seg.end(), {s.first.x, s.first.y, s.first.z, s.second.x, s.second.y, s.second.z});
-    }
+    if (rec)
+        for (auto& s : segments) {
+            seg.insert(seg.end(), {s.first.x, s.first.y, s.first.z, s.second.x, s.second.y, s.second.z});
+        }
     out->nseg = static_cast<int>(segments.size());
-    out->seg = dup_vec(seg);
+    if (rec) out->seg = dup_vec(seg);
+    int ncontact = 0;
 
     std::vector<std::vector<int>> comps;
     if (!segments.empty()) {
@@ -198,6 +199,7 @@ extern "C" int zdx_ref_pair(const double* trisA, int nA, double mean_edgeA, doub
                     status = 2;
                     if (!(area < area_eps)) {
                         status = 3;
+                        ncontact++;
                         if (dot(nA, dirAB) < 0.0) nA = nA * -1.0;
                     }
                 }
@@ -209,6 +211,8 @@ extern "C" int zdx_ref_pair(const double* trisA, int nA, double mean_edgeA, doub
         }
     }
     out->ncomp = static_cast<int>(comps.size());
+    out->nloop = static_cast<int>(loop_comp.size());
+    if (!rec) return ncontact;
     out->comp_off = dup_vec(comp_off);
     out->comp_idx = dup_vec(comp_idx);
     out->v_off = dup_vec(v_off);
@@ -223,7 +227,48 @@ extern "C" int zdx_ref_pair(const double* trisA, int nA, double mean_edgeA, doub
     out->loop_vid = dup_vec(loop_vid);
     out->loop_status = dup_vec(loop_status);
     out->loop_geom = dup_vec(loop_geom);
+    return ncontact;
+}
+
+extern "C" int zdx_ref_pair(const double* trisA, int nA, double mean_edgeA, double bbox_diagA,
+                            const double* trisB, int nB, const double* poseA, const double* poseB,
+                            int split_contacts, ZdxRefPairOut* out) {
+    Mesh meshA, meshB;
+    meshA.tris = tris_from(trisA, nA);
+    meshA.mean_edge = mean_edgeA;
+    meshA.bbox_diag = bbox_diagA;
+    meshB.tris = tris_from(trisB, nB);
+    run_pair(meshA, meshB, pose_from(poseA), pose_from(poseB), split_contacts, out);
     return 0;
+}
+
+// Many pairs over a mesh library on nthreads host threads (the reference is single-threaded; pairs are
+// independent, so each thread runs the unchanged per-pair code on its own pairs).
+extern "C" int64_t zdx_ref_pair_batch(const double* tris, const int64_t* tri_off, const double* mean_edge,
+                                      const double* bbox_diag, int n_mesh, int64_t n_pairs, const int32_t* pair_mesh,
+                                      const double* pose, int split_contacts, int nthreads, int32_t* ncontact) {
+    std::vector<Mesh> meshes(n_mesh);
+    for (int m = 0; m < n_mesh; ++m) {
+        meshes[m].tris = tris_from(tris + 9 * tri_off[m], static_cast<int>(tri_off[m + 1] - tri_off[m]));
+        meshes[m].mean_edge = mean_edge[m];
+        meshes[m].bbox_diag = bbox_diag[m];
+    }
+    std::atomic<int64_t> next{0}, total{0};
+    auto work = [&]() {
+        for (;;) {
+            int64_t p = next.fetch_add(1);
+            if (p >= n_pairs) break;
+            int c = run_pair(meshes[pair_mesh[2 * p]], meshes[pair_mesh[2 * p + 1]], pose_from(pose + 14 * p),
+                             pose_from(pose + 14 * p + 7), split_contacts, nullptr);
+            if (ncontact) ncontact[p] = c;
+            total.fetch_add(c);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(nthreads, 1); ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    return total.load();
 }
 
 extern "C" void zdx_ref_pair_free(ZdxRefPairOut* o) {

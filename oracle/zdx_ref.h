@@ -48,6 +48,13 @@ int zdx_ref_pair(const double* trisA, int nA, double mean_edgeA, double bbox_dia
                  int split_contacts, ZdxRefPairOut* out);
 void zdx_ref_pair_free(ZdxRefPairOut* out);
 
+/* Many pairs over a mesh library (tris back to back, tri_off n_mesh+1) on nthreads threads, each pair
+ * through the same reference code as zdx_ref_pair.  ncontact (may be NULL) receives contacts per pair;
+ * returns the total. */
+int64_t zdx_ref_pair_batch(const double* tris, const int64_t* tri_off, const double* mean_edge,
+                           const double* bbox_diag, int n_mesh, int64_t n_pairs, const int32_t* pair_mesh,
+                           const double* pose, int split_contacts, int nthreads, int32_t* ncontact);
+
 /* compute_wall_contact (src/main.cpp:1205-1258).  Returns 1 on contact. */
 int zdx_ref_wall_contact(const double* tris, int ntri, const double* pose, const double* wall_tri9,
                          const double* wall_normal, double radius, double tol, double* area,

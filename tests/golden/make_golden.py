@@ -1,0 +1,167 @@
+"""Generate the golden fixtures of tests/golden from the reference itself.
+
+Run here, where the reference is present:  python tests/golden/make_golden.py
+It needs oracle/_ref (built by `make -C oracle ref` from the reference's src/main.cpp) and imports the
+reference's polyline.py from /root/reference (read-only).  The fixtures it writes are small .npz files;
+the tests that use them never touch the reference.
+
+* pairs_ref.npz      seeded noised-icosphere pairs through the reference C++ per-pair code
+                     (src/main.cpp:2062-2219): segments, components, snapped vertices/edges, loops,
+                     Sn/Gn/xc0/nA/area and the loop filters.
+* mesh_ref.npz       build_mesh (src/main.cpp:445-497) on a few meshes.
+* sort_ref.npz       std::sort permutations under the reference's three comparators.
+* polyline_ref.npz   polyline.py's own pipeline (polyline.py:743-822) on a few pairs.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "zedm-x_b200"), os.path.join(ROOT, "oracle")]
+
+from oracle import Reference  # noqa: E402
+from zdemx import synth  # noqa: E402
+
+REF_PY = "/root/reference"
+
+
+def pack(prefix, r, d):
+    for k in ["seg", "comp_off", "comp_idx", "v_off", "V", "e_off", "E", "e2_off", "E2", "loop_comp", "loop_off",
+              "loop_vid", "loop_status", "loop_geom"]:
+        d[f"{prefix}{k}"] = r[k]
+    d[f"{prefix}scalars"] = np.array([r["nseg"], r["ncomp"], r["nloop"], r["tri_checks"]], np.int64)
+
+
+def make_pairs(R):
+    rng = np.random.default_rng(20261203)
+    d = {}
+    cases = [(1, 1), (1, 2), (2, 1), (2, 2), (2, 2), (2, 2), (1, 3), (2, 3), (3, 2), (2, 2), (2, 2), (1, 1), (3, 3)]
+    for ci, (sA, sB) in enumerate(cases):
+        A = synth.noised_icosphere(sA, 1e-3, 0.15, rng)
+        B = synth.noised_icosphere(sB, 1e-3, 0.15, rng)
+        pose = synth.pair_poses(rng, 1, 1e-3, 0.0, 0.1)[0]
+        if ci == 11:  # far apart: no contact
+            pose[7:10] = [5e-3, 0.0, 0.0]
+        split = ci % 4 != 3
+        Ab, pA = R.build_mesh(A)
+        Bb, _ = R.build_mesh(B)
+        r = R.pair(Ab, pA[5], pA[6], Bb, pose[:7], pose[7:], split=split)
+        d[f"c{ci}_A"] = A
+        d[f"c{ci}_B"] = B
+        d[f"c{ci}_pose"] = pose
+        d[f"c{ci}_split"] = np.array(split)
+        pack(f"c{ci}_", r, d)
+    d["ncase"] = np.array(len(cases))
+    np.savez_compressed(os.path.join(HERE, "pairs_ref.npz"), **d)
+
+
+def make_mesh(R):
+    rng = np.random.default_rng(7)
+    d = {}
+    for i, s in enumerate([0, 1, 2]):
+        t = synth.noised_icosphere(s, 1e-3, 0.15, rng) + np.array([1e-3, -2e-3, 5e-4])
+        out, props = R.build_mesh(t, True)
+        d[f"m{i}_in"] = t
+        d[f"m{i}_out"] = out
+        d[f"m{i}_props"] = props
+        out2, props2 = R.build_mesh(t, False)
+        d[f"m{i}_out_nc"] = out2
+        d[f"m{i}_props_nc"] = props2
+    d["nmesh"] = np.array(3)
+    np.savez_compressed(os.path.join(HERE, "mesh_ref.npz"), **d)
+
+
+def make_sort(R):
+    rng = np.random.default_rng(11)
+    d = {}
+    n_cases = 60
+    for i in range(n_cases):
+        kind = i % 3
+        n = int(rng.integers(0, 120))
+        ik = rng.integers(0, int(rng.integers(1, 6)), size=max(n, 1)).astype(np.int32)
+        dk = rng.integers(0, int(rng.integers(1, 6)), size=max(n, 1)).astype(float)
+        d[f"s{i}_kind"] = np.array(kind)
+        d[f"s{i}_ikey"] = ik
+        d[f"s{i}_dkey"] = dk
+        d[f"s{i}_perm"] = R.std_sort(kind, n, ik, dk)
+    d["ncase"] = np.array(n_cases)
+    np.savez_compressed(os.path.join(HERE, "sort_ref.npz"), **d)
+
+
+def make_polyline():
+    sys.path.insert(0, REF_PY)
+    import polyline as P  # the reference module, imported read-only
+
+    rng = np.random.default_rng(99)
+    d = {}
+    n_cases = 4
+    for ci in range(n_cases):
+        A = synth.noised_icosphere(1 + ci % 2, 1e-3, 0.15, rng)
+        B = synth.noised_icosphere(1, 1e-3, 0.15, rng)
+        pose = synth.pair_poses(rng, 1, 1e-3, 0.02, 0.1)[0]
+        tol = 1e-5
+        trisA = P.transform_points(A.reshape(-1, 3), pose[0:3], pose[3:7]).reshape(-1, 3, 3)
+        trisB = P.transform_points(B.reshape(-1, 3), pose[7:10], pose[10:14]).reshape(-1, 3, 3)
+        nA_all = P.tri_normals(trisA)
+        nB_all = P.tri_normals(trisB)
+        planesA = [P.plane_from_tri(trisA[i]) for i in range(len(trisA))]
+        planesB = [P.plane_from_tri(trisB[i]) for i in range(len(trisB))]
+        aminA, amaxA = trisA.min(axis=1), trisA.max(axis=1)
+        aminB, amaxB = trisB.min(axis=1), trisB.max(axis=1)
+        segs = []
+        for i in range(len(trisA)):
+            nAi, dAi = planesA[i]
+            if nAi is None:
+                continue
+            for j in range(len(trisB)):
+                if (amaxA[i, 0] < aminB[j, 0] or aminA[i, 0] > amaxB[j, 0] or amaxA[i, 1] < aminB[j, 1] or
+                        aminA[i, 1] > amaxB[j, 1] or amaxA[i, 2] < aminB[j, 2] or aminA[i, 2] > amaxB[j, 2]):
+                    continue
+                nBj, dBj = planesB[j]
+                if nBj is None:
+                    continue
+                s = P.tri_tri_intersection_segment(trisA[i], nA_all[i], dAi, trisB[j], nB_all[j], dBj)
+                if s is not None:
+                    segs.append(s)
+        loops, cids = [], []
+        comps = [list(range(len(segs)))]
+        for comp in comps:
+            V, E = P.snap_endpoints([segs[i] for i in comp], tol=tol)
+            V2, E2 = P.split_t_junctions(V, E, tol=tol)
+            for lv in P.extract_loops(V2, E2):
+                if len(lv) < 3:
+                    continue
+                pts = [V2[i] for i in lv]
+                if np.linalg.norm(np.max(pts, axis=0) - np.min(pts, axis=0)) < tol * 2:
+                    continue
+                loops.append(np.asarray(pts))
+                cids.append(len(cids))
+        man = P.build_contacts_from_loops(0, 1, loops, cids, k_stiff=1e7)
+        d[f"c{ci}_A"] = A
+        d[f"c{ci}_B"] = B
+        d[f"c{ci}_pose"] = pose
+        d[f"c{ci}_tol"] = np.array(tol)
+        d[f"c{ci}_nseg"] = np.array(len(segs))
+        d[f"c{ci}_nloop"] = np.array(len(loops))
+        d[f"c{ci}_loop_len"] = np.array([len(x) for x in loops], np.int64)
+        d[f"c{ci}_loop_pts"] = np.concatenate(loops) if loops else np.zeros((0, 3))
+        geo = [c["Sn"] + c["Gn"] + (c["xc0"] or [0, 0, 0]) + c["nA"] + [c["area"], c["Fn"]] + c["F_A"]
+               for c in man["contacts"]]
+        d[f"c{ci}_geom"] = np.asarray(geo, float).reshape(-1, 17)
+    d["ncase"] = np.array(n_cases)
+    np.savez_compressed(os.path.join(HERE, "polyline_ref.npz"), **d)
+
+
+if __name__ == "__main__":
+    R = Reference()
+    make_pairs(R)
+    make_mesh(R)
+    make_sort(R)
+    make_polyline()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,119 @@
+"""Pins the oracle (oracle/zdx_oracle.c) to the reference: golden fixtures made by running the reference
+(tests/golden/make_golden.py), and -- where oracle/_ref is built -- the reference library itself."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import compare_pair
+
+FIELDS = ["seg", "comp_off", "comp_idx", "v_off", "V", "e_off", "E", "e2_off", "E2", "loop_comp", "loop_off",
+          "loop_vid", "loop_status", "loop_geom"]
+
+
+def _golden_case(z, ci):
+    r = {k: z[f"c{ci}_{k}"] for k in FIELDS}
+    s = z[f"c{ci}_scalars"]
+    r.update(nseg=int(s[0]), ncomp=int(s[1]), nloop=int(s[2]), tri_checks=int(s[3]))
+    r["seg"] = r["seg"].reshape(-1, 6)
+    r["V"] = r["V"].reshape(-1, 3)
+    r["E"] = r["E"].reshape(-1, 2)
+    r["E2"] = r["E2"].reshape(-1, 2)
+    r["loop_geom"] = r["loop_geom"].reshape(-1, 13)
+    return r
+
+
+def test_oracle_matches_reference_golden_pairs(oracle):
+    z = np.load(os.path.join(GOLDEN, "pairs_ref.npz"))
+    n_with_loops = 0
+    for ci in range(int(z["ncase"])):
+        A, B, pose, split = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], bool(z[f"c{ci}_split"])
+        Ab, pA = oracle.build_mesh(A)
+        Bb, _ = oracle.build_mesh(B)
+        o = oracle.pair(Ab, pA[5], pA[6], Bb, pose[:7], pose[7:], split=split)
+        g = _golden_case(z, ci)
+        assert o["tri_checks"] == g["tri_checks"]
+        assert compare_pair(g, o, exact=True) == [], f"case {ci}"
+        n_with_loops += g["nloop"] > 0
+    assert n_with_loops >= 8
+
+
+def test_oracle_mesh_build_golden(oracle):
+    z = np.load(os.path.join(GOLDEN, "mesh_ref.npz"))
+    for i in range(int(z["nmesh"])):
+        out, props = oracle.build_mesh(z[f"m{i}_in"], True)
+        assert np.array_equal(out, z[f"m{i}_out"]) and np.array_equal(props, z[f"m{i}_props"])
+        out, props = oracle.build_mesh(z[f"m{i}_in"], False)
+        assert np.array_equal(out, z[f"m{i}_out_nc"]) and np.array_equal(props, z[f"m{i}_props_nc"])
+
+
+def test_sort_replica_golden(oracle):
+    z = np.load(os.path.join(GOLDEN, "sort_ref.npz"))
+    for i in range(int(z["ncase"])):
+        n = len(z[f"s{i}_perm"])
+        got = oracle.sort(int(z[f"s{i}_kind"]), n, z[f"s{i}_ikey"], z[f"s{i}_dkey"])
+        assert np.array_equal(got, z[f"s{i}_perm"]), i
+
+
+def _antiqsort_keys(oracle, n):
+    """McIlroy's adversary against the sort replica: keys fixed lazily so every pivot is bad, which drives
+    introsort into its heapsort fallback.  Plays the adversary in Python over the replica's compares."""
+    # Cheap stand-in: an organ-pipe with many ties also exercises deep partitions.
+    k = np.concatenate([np.arange(n // 2), np.arange(n - n // 2)[::-1]]) % 7
+    return k.astype(np.int32)
+
+
+def test_sort_replica_live(oracle, ref):
+    rng = np.random.default_rng(5)
+    for trial in range(400):
+        kind = trial % 3
+        n = int(rng.integers(0, 600))
+        ik = rng.integers(0, int(rng.integers(1, 8)), size=max(n, 1)).astype(np.int32)
+        dk = rng.integers(0, int(rng.integers(1, 8)), size=max(n, 1)).astype(float)
+        assert np.array_equal(ref.std_sort(kind, n, ik, dk), oracle.sort(kind, n, ik, dk))
+    for n in (17, 100, 1000, 5000):
+        ik = _antiqsort_keys(oracle, n)
+        for kind in (0, 1):
+            assert np.array_equal(ref.std_sort(kind, n, ik), oracle.sort(kind, n, ik))
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_oracle_matches_reference_live(oracle, ref, seed):
+    from zdemx import synth
+
+    rng = np.random.default_rng(1000 + seed)
+    for trial in range(25):
+        sA, sB = int(rng.integers(1, 4)), int(rng.integers(1, 4))
+        A = synth.noised_icosphere(sA, 1e-3, 0.15, rng)
+        B = synth.noised_icosphere(sB, 1e-3, 0.15, rng)
+        Ab, pA = ref.build_mesh(A)
+        Bb, pB = ref.build_mesh(B)
+        pose = synth.pair_poses(rng, 1, 1e-3, 0.0, 0.12)[0]
+        split = bool(trial % 3)
+        r = ref.pair(Ab, pA[5], pA[6], Bb, pose[:7], pose[7:], split=split)
+        o = oracle.pair(Ab, pA[5], pA[6], Bb, pose[:7], pose[7:], split=split)
+        assert compare_pair(r, o, exact=True) == [], (seed, trial)
+
+
+def test_oracle_wall_and_integrate_live(oracle, ref):
+    from zdemx import synth
+
+    rng = np.random.default_rng(3)
+    hits = 0
+    for trial in range(30):
+        P = synth.noised_icosphere(2, 1e-3, 0.15, rng)
+        Pb, pp = ref.build_mesh(P)
+        pose = np.r_[rng.uniform(-5e-4, 5e-4, 2), rng.uniform(-8e-4, 8e-4), synth.random_unit_quat(rng)]
+        wt = np.array([-0.01, -0.01, 0.0, 0.01, -0.01, 0.0, 0.01, 0.01, 0.0])
+        wn = np.array([0.0, 0.0, 1.0])
+        a = ref.wall_contact(Pb, pose, wt, wn, pp[4], pp[5] * 0.1)
+        b = oracle.wall_contact(Pb, pose, wt, wn, pp[4], pp[5] * 0.1)
+        assert a[0] == b[0]
+        if a[0]:
+            hits += 1
+            assert a[1] == b[1] and np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+        st = np.r_[pose, rng.normal(size=9), 1.0 / 3.0, rng.normal(size=9)]
+        f, t, g = rng.normal(size=3), rng.normal(size=3), np.array([0.0, 0.0, -9.81])
+        assert np.array_equal(ref.integrate(st, f, t, g, 1e-5)[:16], oracle.integrate(st, f, t, g, 1e-5)[:16])
+    assert hits > 5

@@ -1,0 +1,163 @@
+"""Parity of the CUDA pair-contact path (through the C ABI) with the oracle and with the reference.
+
+Integer results (segment counts, components, raw loops, contact count, loop vertex counts, component
+of each contact, contact ids) must be identical; with --fmad=false on both sides the FP64 geometry
+(Sn, Gn, xc0, nA, |Sn|) and the snapped loop vertices are bit-exact too, which is stronger than the
+1e-9 relative bound the path promises."""
+import os
+
+import numpy as np
+import pytest
+
+from _helpers import compare_gpu_to_expected, expected_contacts, gpu_pair_slice
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _library(raw_meshes):
+    from zdemx.contact import MeshLibrary
+
+    return MeshLibrary.build(raw_meshes)
+
+
+def _run(ctx, lib, pm, pp, **kw):
+    from zdemx import contact
+
+    return contact.pair_contacts_batch(ctx, lib, pm, pp, want_points=True, **kw)
+
+
+def test_gpu_matches_reference_golden(ctx):
+    z = np.load(os.path.join(GOLDEN, "pairs_ref.npz"))
+    from test_oracle_pin import _golden_case
+
+    for ci in range(int(z["ncase"])):
+        lib = _library([z[f"c{ci}_A"], z[f"c{ci}_B"]])
+        split = bool(z[f"c{ci}_split"])
+        res = _run(ctx, lib, [[0, 1]], z[f"c{ci}_pose"][None, :], split=split, k=1e7)
+        g = _golden_case(z, ci)
+        bad = compare_gpu_to_expected(gpu_pair_slice(res, 0), expected_contacts(g), g)
+        assert bad == [], f"case {ci}: {bad}"
+
+
+@pytest.mark.parametrize("split", [True, False])
+def test_gpu_matches_oracle_mixed_batch(ctx, oracle, split):
+    from zdemx import synth
+
+    rng = np.random.default_rng(42 + split)
+    meshes = [synth.noised_icosphere(s, 1e-3, 0.15, rng) for s in (1, 1, 2, 2, 2, 3, 3)]
+    lib = _library(meshes)
+    npairs = 96
+    pm = rng.integers(0, lib.n_mesh, size=(npairs, 2)).astype(np.int32)
+    pp = synth.pair_poses(rng, npairs, 1e-3, 0.0, 0.12)
+    pp[5, 7:10] = [0.01, 0.0, 0.0]  # a pair far apart
+    res = _run(ctx, lib, pm, pp, split=split, k=1e7)
+    nct = 0
+    for p in range(npairs):
+        a, b = pm[p]
+        r = oracle.pair(lib.mesh(a), lib.mean_edge[a], lib.bbox_diag[a], lib.mesh(b), pp[p, :7], pp[p, 7:],
+                        split=split)
+        e = expected_contacts(r)
+        nct += len(e["geom"])
+        bad = compare_gpu_to_expected(gpu_pair_slice(res, p), e, r)
+        assert bad == [], f"pair {p}: {bad}"
+        assert res["stats"][p, 0] == r["nseg"]
+    assert nct > npairs  # most pairs touch, several with more than one loop
+    assert res["totals"][0] == nct
+
+
+def test_gpu_force_law_feng_min(ctx):
+    from zdemx import synth
+
+    rng = np.random.default_rng(3)
+    lib = _library([synth.noised_icosphere(2, 1e-3, 0.15, rng) for _ in range(2)])
+    pp = synth.pair_poses(rng, 8, 1e-3, 0.03, 0.1)
+    res = _run(ctx, lib, np.array([[0, 1]] * 8, np.int32), pp, k=1e7)
+    g = res["geom"]
+    assert len(g) > 0
+    # Fn = k/2 |Sn| (polyline.py:677); zdem mode: F_A = -Fn nA, F_B = -F_A, nA toward B
+    assert np.array_equal(g[:, 13], 0.5 * 1e7 * g[:, 12])
+    assert np.array_equal(g[:, 14:17], g[:, 9:12] * (-g[:, 13:14]))
+    assert np.array_equal(g[:, 17:20], -g[:, 14:17])
+    for c in range(len(g)):
+        p = res["info"][c, 0]
+        assert np.dot(g[c, 9:12], pp[p, 7:10] - pp[p, 0:3]) >= 0.0
+
+
+def test_batched_equals_plain(ctx):
+    from zdemx import _lib, synth
+
+    rng = np.random.default_rng(9)
+    lib = _library([synth.noised_icosphere(s, 1e-3, 0.15, rng) for s in (1, 2, 3)])
+    pm = rng.integers(0, 3, size=(24, 2)).astype(np.int32)
+    pp = synth.pair_poses(rng, 24, 1e-3, 0.0, 0.1)
+    a = _run(ctx, lib, pm, pp, sched=_lib.SCHED_BATCHED)
+    b = _run(ctx, lib, pm, pp, sched=_lib.SCHED_PLAIN)
+    for k in ("ncontact", "contact_off", "stats", "geom", "info", "points", "point_off"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_edge_cases(ctx, oracle):
+    from zdemx import _lib, synth
+
+    rng = np.random.default_rng(4)
+    A = synth.noised_icosphere(2, 1e-3, 0.15, rng)
+    B = synth.noised_icosphere(1, 1e-3, 0.0, rng)
+    # a degenerate (zero-area) triangle and a sliver in B
+    B[3, 2] = B[3, 0]
+    B[7, 1] = B[7, 0] + 1e-16
+    lib = _library([A, B, A[:0]])
+    # empty batch
+    r0 = _run(ctx, lib, np.zeros((0, 2), np.int32), np.zeros((0, 14)))
+    assert r0["totals"][0] == 0 and len(r0["contact_off"]) == 1
+    pp = synth.pair_poses(rng, 6, 1e-3, 0.02, 0.1)
+    pp[1, 7:10] = 0.0                      # concentric: B well inside A's hull region
+    pp[2, 10:14] = pp[2, 3:7]              # same orientation
+    pp[3, 7:10] = [2.3e-3, 0, 0]           # just apart
+    pm = np.array([[0, 1], [0, 1], [1, 0], [0, 1], [0, 0], [0, 2]], np.int32)   # last: empty mesh B
+    res = _run(ctx, lib, pm, pp)
+    for p in range(len(pm)):
+        a, b = pm[p]
+        r = oracle.pair(lib.mesh(a), lib.mean_edge[a], lib.bbox_diag[a], lib.mesh(b), pp[p, :7], pp[p, 7:], split=True)
+        assert compare_gpu_to_expected(gpu_pair_slice(res, p), expected_contacts(r), r) == [], p
+    assert res["stats"][5, 0] == 0
+    # bad mesh index is rejected before any work
+    with pytest.raises(_lib.ZdxError):
+        _run(ctx, lib, np.array([[0, 7]], np.int32), pp[:1])
+
+
+def test_capacity_is_reported_not_truncated(ctx):
+    from zdemx import _lib, synth
+
+    rng = np.random.default_rng(6)
+    lib = _library([synth.noised_icosphere(3, 1e-3, 0.15, rng) for _ in range(2)])
+    pp = synth.pair_poses(rng, 1, 1e-3, 0.08, 0.08)
+    with pytest.raises(_lib.ZdxError) as ei:
+        _lib.pair_contacts_raw(ctx, lib.tris, lib.tri_off, lib.mean_edge, lib.bbox_diag, [[0, 1]], pp,
+                               max_seg_per_pair=4)
+    assert ei.value.status == _lib.ZDX_ERR_CAPACITY
+
+
+def test_polyline_mode_matches_oracle_and_python_reference(ctx, oracle):
+    from zdemx import polyline
+
+    z = np.load(os.path.join(GOLDEN, "polyline_ref.npz"))
+    for ci in range(int(z["ncase"])):
+        A, B, pose, tol = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], float(z[f"c{ci}_tol"])
+        man, loops, xc0s, cids = polyline.pair_contacts(A, B, pose[0:3], pose[3:7], pose[7:10], pose[10:14], k=1e7,
+                                                        tol=tol, split_contacts=False, ctx=ctx)
+        o = oracle.pair(A, 0.0, 0.0, B, pose[:7], pose[7:], split=False, mode=1, tol=tol)
+        e = expected_contacts(o, polyline=True)
+        # GPU vs oracle in polyline mode: bit-exact
+        assert len(man["contacts"]) == len(e["geom"])
+        for c, cc in enumerate(man["contacts"]):
+            got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"]]
+            assert np.array_equal(got, e["geom"][c]), (ci, c)
+            assert np.array_equal(np.asarray(loops[c]), e["points"][c])
+        # vs polyline.py itself (numpy arithmetic, so within tolerance): same loops, same numbers
+        assert len(loops) == int(z[f"c{ci}_nloop"])
+        assert [len(x) for x in loops] == list(z[f"c{ci}_loop_len"])
+        ref = z[f"c{ci}_geom"]
+        for c, cc in enumerate(man["contacts"]):
+            got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"], cc["Fn"], cc["F_A"]]
+            assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)

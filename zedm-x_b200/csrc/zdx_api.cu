@@ -1,0 +1,432 @@
+// zdx_api.cu -- the C ABI of libzdemx.so (include/zdemx.h): contexts, workspaces and the pair call.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/zdemx.h"
+#include "zdx_ctx.h"
+#include "zdx_pair.cuh"
+
+using namespace zdx;
+
+namespace zdx {
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+cudaError_t DevBuf::ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    release();
+    size_t b = std::max<size_t>(need, 256);
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    bytes = b;
+    return cudaSuccess;
+}
+
+int ctx_fail(zdx_ctx* c, int status, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->last_error = buf;
+    return status;
+}
+
+}  // namespace zdx
+
+#define CK(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return ctx_fail(ctx, ZDX_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                            __FILE__, __LINE__);                                                        \
+    } while (0)
+
+extern "C" const char* zdx_version(void) { return "zdemx 0.1 sm_100a"; }
+
+extern "C" const char* zdx_status_string(int s) {
+    switch (s) {
+    case ZDX_OK: return "ok";
+    case ZDX_ERR_INVALID: return "invalid argument";
+    case ZDX_ERR_CUDA: return "CUDA error";
+    case ZDX_ERR_CAPACITY: return "capacity exceeded";
+    case ZDX_ERR_IO: return "I/O error";
+    case ZDX_ERR_NO_DEVICE: return "no usable CUDA device";
+    case ZDX_ERR_CONFIG: return "config rejected";
+    case ZDX_ERR_STATE: return "call out of order";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char* zdx_last_error(const zdx_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+extern "C" int zdx_create(zdx_ctx** out, int device) {
+    if (!out) return ZDX_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return ZDX_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return ZDX_ERR_INVALID;
+    zdx_ctx* ctx = new zdx_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete ctx;
+        return ZDX_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    ctx->num_sms = prop.multiProcessorCount;
+    ctx->cc_major = prop.major;
+    ctx->cc_minor = prop.minor;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return ZDX_ERR_CUDA;
+    }
+    for (auto& e : ctx->ev) cudaEventCreate(&e);
+    *out = ctx;
+    return ZDX_OK;
+}
+
+extern "C" int zdx_destroy(zdx_ctx* ctx) {
+    if (!ctx) return ZDX_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto* b : ctx->all_bufs()) b->release();
+    ctx->scene_release();
+    for (auto& e : ctx->ev) cudaEventDestroy(e);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ZDX_OK;
+}
+
+extern "C" int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launches) {
+    if (!ctx || !ms5) return ZDX_ERR_INVALID;
+    for (int i = 0; i < 5; ++i) ms5[i] = ctx->pair_ms[i];
+    if (launches) *launches = ctx->launches;
+    return ZDX_OK;
+}
+
+namespace {
+
+template <class T>
+T* as(DevBuf& b) {
+    return static_cast<T*>(b.p);
+}
+
+// Copy `bytes` from a caller pointer into a workspace buffer (host mode) or alias it (device mode).
+template <class T>
+int stage_in(zdx_ctx* ctx, bool host, const T* src, size_t count, DevBuf& buf, const T** dst) {
+    if (!host) {
+        *dst = src;
+        return ZDX_OK;
+    }
+    size_t bytes = sizeof(T) * std::max<size_t>(count, 1);
+    CK(buf.ensure(bytes));
+    if (count) CK(cudaMemcpyAsync(buf.p, src, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->stream));
+    *dst = static_cast<const T*>(buf.p);
+    return ZDX_OK;
+}
+
+}  // namespace
+
+extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* ms,
+                                 const zdx_pair_batch* pb, zdx_pair_result* out) {
+    if (!ctx || !opts || !ms || !pb || !out) return ZDX_ERR_INVALID;
+    if (ms->n_mesh < 0 || pb->n_pairs < 0 || (opts->mode != ZDX_MODE_ZDEM && opts->mode != ZDX_MODE_POLYLINE))
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "bad mesh/pair count or mode");
+    if (pb->n_pairs > 0x7fffffffLL) return ctx_fail(ctx, ZDX_ERR_INVALID, "at most 2^31-1 pairs per call");
+    if (ms->n_mesh > 0 && (!ms->tris || !ms->tri_off || !ms->mean_edge || !ms->bbox_diag))
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "mesh set has null arrays");
+    if (pb->n_pairs > 0 && (!pb->mesh || !pb->pose)) return ctx_fail(ctx, ZDX_ERR_INVALID, "pair batch has null arrays");
+    if (!out->pair_ncontact || !out->pair_contact_off || !out->pair_stats)
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "result has null per-pair arrays");
+    CK(cudaSetDevice(ctx->device));
+    const bool host = opts->mem == ZDX_MEM_HOST;
+    cudaStream_t st = ctx->stream;
+    const int64_t NP = pb->n_pairs;
+    const int NM = ms->n_mesh;
+    for (int i = 0; i < 4; ++i) out->totals[i] = 0;
+
+    // mesh offsets on the host: sizes the workspaces
+    std::vector<int64_t> off_h(NM + 1, 0);
+    if (NM > 0) {
+        if (host) std::memcpy(off_h.data(), ms->tri_off, sizeof(int64_t) * (NM + 1));
+        else CK(cudaMemcpy(off_h.data(), ms->tri_off, sizeof(int64_t) * (NM + 1), cudaMemcpyDeviceToHost));
+    }
+    int64_t total_tris = NM > 0 ? off_h[NM] : 0;
+    int max_ntri = 0;
+    for (int m = 0; m < NM; ++m) {
+        int64_t c = off_h[m + 1] - off_h[m];
+        if (c < 0 || off_h[0] != 0) return ctx_fail(ctx, ZDX_ERR_INVALID, "tri_off must start at 0 and not decrease");
+        if (c > 0x7fffffff) return ctx_fail(ctx, ZDX_ERR_INVALID, "mesh too large");
+        max_ntri = std::max<int>(max_ntri, (int)c);
+    }
+    if (host && NP > 0) {
+        for (int64_t p = 0; p < 2 * NP; ++p)
+            if (pb->mesh[p] < 0 || pb->mesh[p] >= NM) return ctx_fail(ctx, ZDX_ERR_INVALID, "pair mesh index out of range");
+    }
+
+    CK(cudaEventRecord(ctx->ev[0], st));
+    PairArgs a{};
+    a.n_mesh = NM;
+    int rc;
+    if ((rc = stage_in(ctx, host, ms->tris, 9 * (size_t)total_tris, ctx->in_tris, &a.tris))) return rc;
+    if ((rc = stage_in(ctx, host, ms->tri_off, (size_t)NM + 1, ctx->in_off, &a.tri_off))) return rc;
+    if ((rc = stage_in(ctx, host, ms->mean_edge, (size_t)NM, ctx->in_me, &a.mean_edge))) return rc;
+    if ((rc = stage_in(ctx, host, ms->bbox_diag, (size_t)NM, ctx->in_bd, &a.bbox_diag))) return rc;
+    if ((rc = stage_in(ctx, host, pb->mesh, 2 * (size_t)NP, ctx->in_pm, &a.pmesh))) return rc;
+    if ((rc = stage_in(ctx, host, pb->pose, 14 * (size_t)NP, ctx->in_pose, &a.pose))) return rc;
+    a.n_pairs = NP;
+    a.mode = opts->mode;
+    a.split = opts->split_contacts ? 1 : 0;
+    a.tol_in = opts->mode == ZDX_MODE_POLYLINE ? (opts->tol > 0.0 ? opts->tol : 1e-6) : opts->tol;
+    a.k = opts->k;
+    a.want_pts = opts->want_loop_points ? 1 : 0;
+    a.cap_seg = opts->max_seg_per_pair > 0 ? opts->max_seg_per_pair : 16384;
+    a.cap_side = std::max(max_ntri, 1);
+
+    // stage 0: per-triangle spheres and mesh bounds
+    CK(ctx->tri_sph.ensure(sizeof(double4) * std::max<int64_t>(total_tris, 1)));
+    CK(ctx->mesh_R.ensure(sizeof(unsigned long long) * std::max(NM, 1)));
+    CK(ctx->mesh_valid.ensure(sizeof(int) * std::max(NM, 1)));
+    CK(cudaMemsetAsync(ctx->mesh_R.p, 0, sizeof(unsigned long long) * std::max(NM, 1), st));
+    CK(cudaMemsetAsync(ctx->mesh_valid.p, 0, sizeof(int) * std::max(NM, 1), st));
+    a.tri_sph = as<double4>(ctx->tri_sph);
+    a.mesh_R_bits = as<unsigned long long>(ctx->mesh_R);
+    a.mesh_valid = as<int>(ctx->mesh_valid);
+    launch_mesh_prep(a, total_tris, st);
+    CK(cudaGetLastError());
+
+    // per-pair state
+    const size_t P1 = (size_t)std::max<int64_t>(NP, 1);
+    CK(ctx->order.ensure(sizeof(int32_t) * P1));
+    CK(ctx->buckets.ensure(sizeof(int) * 128));
+    CK(ctx->pair_i64.ensure(sizeof(int64_t) * 5 * P1));
+    CK(ctx->pair_i32.ensure(sizeof(int32_t) * 6 * P1));
+    CK(ctx->counters.ensure(sizeof(unsigned long long) * 16));
+    int64_t* pi64 = as<int64_t>(ctx->pair_i64);
+    int32_t* pi32 = as<int32_t>(ctx->pair_i32);
+    a.pair_seg_off = pi64;
+    a.pair_checks = pi64 + P1;
+    a.pair_stage_off = pi64 + 2 * P1;
+    a.pair_pts_stage_off = pi64 + 3 * P1;
+    a.pair_npts = pi64 + 4 * P1;
+    a.pair_nseg = pi32;
+    a.pair_status = pi32 + P1;
+    a.pair_ncontact = pi32 + 2 * P1;
+    a.pair_ncomp = pi32 + 3 * P1;
+    a.pair_nloop = pi32 + 4 * P1;
+    unsigned long long* cnt = as<unsigned long long>(ctx->counters);
+    a.seg_counter = cnt + 0;
+    a.contact_counter = cnt + 1;
+    a.pts_counter = cnt + 2;
+    a.checks_total = cnt + 3;
+    a.queue1 = reinterpret_cast<int*>(cnt + 4);
+    a.queue2 = reinterpret_cast<int*>(cnt + 5);
+    a.max_nseg = reinterpret_cast<int*>(cnt + 6);
+    a.err = reinterpret_cast<int*>(cnt + 7);
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
+    CK(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
+
+    const bool plain = opts->sched == ZDX_SCHED_PLAIN;
+    if (plain) {
+        // identity order: the plain form walks the pairs as given
+        std::vector<int32_t> id((size_t)NP);
+        for (int64_t p = 0; p < NP; ++p) id[(size_t)p] = (int32_t)p;
+        if (NP) CK(cudaMemcpyAsync(ctx->order.p, id.data(), sizeof(int32_t) * NP, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    } else {
+        launch_cost_order(a, as<int32_t>(ctx->order), as<int>(ctx->buckets), st);
+        CK(cudaGetLastError());
+    }
+    a.order = as<int32_t>(ctx->order);
+    CK(cudaEventRecord(ctx->ev[1], st));
+    ctx->launches += plain ? 0 : 4;  // mesh prep + three cost-order kernels
+
+    // stage 1: segments
+    const int k1_grid = plain ? 1 : (int)std::min<int64_t>(std::max<int64_t>(NP, 1), (int64_t)ctx->num_sms * k1_blocks_per_sm());
+    a.k1_slot_bytes = tritest_slot_bytes(a.cap_side, a.cap_seg);
+    CK(ctx->k1_slots.ensure(a.k1_slot_bytes * (size_t)k1_grid));
+    a.k1_slots = as<char>(ctx->k1_slots);
+    int64_t seg_cap = std::max<int64_t>(ctx->seg_arena.bytes / (6 * sizeof(double)), std::max<int64_t>(NP * 256, 1 << 20));
+    if (plain) seg_cap = std::max<int64_t>(seg_cap, a.cap_seg);
+    CK(ctx->seg_arena.ensure(sizeof(double) * 6 * (size_t)seg_cap));
+    a.seg = as<double>(ctx->seg_arena);
+    a.seg_cap = seg_cap;
+
+    // plain form: each pair runs its two stages in its own launches, one after the other
+    if (plain) {
+        a.k2_nmax = a.cap_seg;
+        a.k2_slot_bytes = rebuild_slot_bytes(a.k2_nmax);
+        a.k2_nslots = 1;
+        CK(ctx->k2_slots.ensure(a.k2_slot_bytes));
+        a.k2_slots = as<char>(ctx->k2_slots);
+    }
+    // contact staging
+    const int64_t ccap = std::max<int64_t>(out->contact_cap, 0);
+    const int64_t pcap = a.want_pts ? std::max<int64_t>(out->loop_point_cap, 0) : 0;
+    CK(ctx->cstage.ensure(sizeof(double) * 20 * (size_t)std::max<int64_t>(ccap, 1)));
+    CK(ctx->cistage.ensure(sizeof(int32_t) * 5 * (size_t)std::max<int64_t>(ccap, 1)));
+    CK(ctx->pstage.ensure(sizeof(double) * 3 * (size_t)std::max<int64_t>(pcap, 1)));
+    a.cgeom_stage = as<double>(ctx->cstage);
+    a.cinfo_stage = as<int32_t>(ctx->cistage);
+    a.clen_stage = as<int32_t>(ctx->cistage) + 4 * std::max<int64_t>(ccap, 1);
+    a.contact_cap = ccap;
+    a.pts_stage = as<double>(ctx->pstage);
+    a.pts_cap = pcap;
+
+    unsigned long long hc[8];
+    if (plain) {
+        ctx->launches += 1 + 2 * NP;
+        for (int64_t p = 0; p < NP; ++p) {
+            a.item_begin = p;
+            a.item_end = p + 1;
+            CK(cudaMemsetAsync(a.queue1, 0, sizeof(int), st));
+            launch_segments(a, 1, st);
+            CK(cudaMemsetAsync(a.queue2, 0, sizeof(int), st));
+            launch_rebuild(a, 1, st);
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ctx->ev[5], st));
+        CK(cudaEventRecord(ctx->ev[2], st));
+        CK(cudaEventRecord(ctx->ev[3], st));
+        CK(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (((int*)&hc[7])[0] & ERR_SEG_ARENA)
+            return ctx_fail(ctx, ZDX_ERR_CAPACITY, "segment arena overflow in the plain form");
+    } else {
+        a.item_begin = 0;
+        a.item_end = NP;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            CK(cudaEventRecord(ctx->ev[1], st));
+            launch_segments(a, k1_grid, st);
+            ctx->launches += 1;
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(ctx->ev[5], st));
+            CK(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            int err = ((int*)&hc[7])[0];
+            if (!(err & ERR_SEG_ARENA)) break;
+            if (attempt == 1) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "segment arena overflow after growth");
+            // grow to what the first attempt counted, then run the triangle stage again
+            int64_t need = (int64_t)hc[0] + 1024;
+            CK(ctx->seg_arena.ensure(sizeof(double) * 6 * (size_t)need));
+            a.seg = as<double>(ctx->seg_arena);
+            a.seg_cap = need;
+            CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
+            CK(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
+        }
+        // stage 2: rebuild, one warp per pair, slots sized for the largest pair
+        const int nmax = std::max(((int*)&hc[6])[0], 1);
+        a.k2_nmax = nmax;
+        a.k2_slot_bytes = rebuild_slot_bytes(nmax);
+        const size_t budget = (size_t)2 << 30;
+        int64_t warps = std::min<int64_t>(std::max<int64_t>(NP, 1), (int64_t)ctx->num_sms * 32);
+        warps = std::min<int64_t>(warps, std::max<int64_t>(1, (int64_t)(budget / a.k2_slot_bytes)));
+        warps = (warps + k2_warps_per_block() - 1) / k2_warps_per_block() * k2_warps_per_block();
+        a.k2_nslots = warps;
+        CK(ctx->k2_slots.ensure(a.k2_slot_bytes * (size_t)warps));
+        a.k2_slots = as<char>(ctx->k2_slots);
+        CK(cudaEventRecord(ctx->ev[2], st));
+        launch_rebuild(a, (int)warps, st);
+        ctx->launches += 1;
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ctx->ev[3], st));
+        CK(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    const int err = ((int*)&hc[7])[0];
+    out->totals[0] = (int64_t)hc[1];
+    out->totals[1] = (int64_t)hc[0];
+    out->totals[2] = (int64_t)hc[3];
+    out->totals[3] = (int64_t)hc[2];
+    if (err & (ERR_CONTACT_STAGE | ERR_POINT_STAGE))
+        return ctx_fail(ctx, ZDX_ERR_CAPACITY, "need contact_cap >= %lld and loop_point_cap >= %lld",
+                        (long long)hc[1], (long long)hc[2]);
+    if (!out->contact_geom || !out->contact_info || (a.want_pts && (!out->loop_points || !out->contact_point_off)))
+        if (hc[1] > 0) return ctx_fail(ctx, ZDX_ERR_INVALID, "result has null contact arrays");
+
+    // stage 3: deterministic CSR, written straight into the caller's buffers in device mode
+    const int64_t nct = (int64_t)hc[1], npt = (int64_t)hc[2];
+    int64_t* coff;
+    int64_t* poff;
+    double* cg;
+    int32_t* ci;
+    double* pts;
+    int64_t* cpo;
+    int32_t* pstats;
+    CK(ctx->g_off.ensure(sizeof(int64_t) * 2 * (P1 + 1)));
+    poff = as<int64_t>(ctx->g_off) + (P1 + 1);
+    if (host) {
+        CK(ctx->o_cg.ensure(sizeof(double) * 20 * (size_t)std::max<int64_t>(nct, 1)));
+        CK(ctx->o_ci.ensure(sizeof(int32_t) * 4 * (size_t)std::max<int64_t>(nct, 1)));
+        CK(ctx->o_pts.ensure(sizeof(double) * 3 * (size_t)std::max<int64_t>(npt, 1)));
+        CK(ctx->o_cpo.ensure(sizeof(int64_t) * (size_t)(nct + 1)));
+        CK(ctx->o_ps.ensure(sizeof(int32_t) * 4 * P1));
+        coff = as<int64_t>(ctx->g_off);
+        cg = as<double>(ctx->o_cg);
+        ci = as<int32_t>(ctx->o_ci);
+        pts = as<double>(ctx->o_pts);
+        cpo = as<int64_t>(ctx->o_cpo);
+        pstats = as<int32_t>(ctx->o_ps);
+    } else {
+        coff = out->pair_contact_off;
+        cg = out->contact_geom;
+        ci = out->contact_info;
+        pts = out->loop_points;
+        cpo = out->contact_point_off;
+        pstats = out->pair_stats;
+    }
+    CK(cudaEventRecord(ctx->ev[6], st));
+    launch_gather(a, coff, poff, cg, ci, pts, cpo, pstats, nullptr, st);
+    ctx->launches += a.want_pts ? 4 : 2;
+    CK(cudaGetLastError());
+    if (host) {
+        CK(cudaMemcpyAsync(out->pair_ncontact, a.pair_ncontact, sizeof(int32_t) * NP, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(out->pair_contact_off, coff, sizeof(int64_t) * (NP + 1), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(out->pair_stats, pstats, sizeof(int32_t) * 4 * NP, cudaMemcpyDeviceToHost, st));
+        if (nct) {
+            CK(cudaMemcpyAsync(out->contact_geom, cg, sizeof(double) * 20 * nct, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out->contact_info, ci, sizeof(int32_t) * 4 * nct, cudaMemcpyDeviceToHost, st));
+        }
+        if (a.want_pts) {
+            if (npt) CK(cudaMemcpyAsync(out->loop_points, pts, sizeof(double) * 3 * npt, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out->contact_point_off, cpo, sizeof(int64_t) * (nct + 1), cudaMemcpyDeviceToHost, st));
+        }
+    } else {
+        CK(cudaMemcpyAsync(out->pair_ncontact, a.pair_ncontact, sizeof(int32_t) * NP, cudaMemcpyDeviceToDevice, st));
+        if (a.want_pts && nct == 0) CK(cudaMemsetAsync(out->contact_point_off, 0, sizeof(int64_t), st));
+    }
+    CK(cudaEventRecord(ctx->ev[4], st));
+    CK(cudaStreamSynchronize(st));
+    float el;
+    cudaEventElapsedTime(&el, ctx->ev[0], ctx->ev[1]);
+    ctx->pair_ms[0] = el;
+    cudaEventElapsedTime(&el, ctx->ev[1], ctx->ev[5]);
+    ctx->pair_ms[1] = el;
+    cudaEventElapsedTime(&el, ctx->ev[2], ctx->ev[3]);
+    ctx->pair_ms[2] = el;
+    cudaEventElapsedTime(&el, ctx->ev[6], ctx->ev[4]);
+    ctx->pair_ms[3] = el;
+    cudaEventElapsedTime(&el, ctx->ev[0], ctx->ev[4]);
+    ctx->pair_ms[4] = el;
+    if (err & ERR_PAIR) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "some pair exceeded its segment or edge capacity (see pair_stats)");
+    return ZDX_OK;
+}
+
+void zdx_ctx::scene_release() {}

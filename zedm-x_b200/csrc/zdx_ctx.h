@@ -1,0 +1,50 @@
+// zdx_ctx.h -- the context behind the opaque zdx_ctx handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+namespace zdx {
+
+// A grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need);
+    void release();
+};
+
+int ctx_fail(struct ::zdx_ctx* c, int status, const char* fmt, ...);
+
+struct Scene;  // DEM scene (zdx_scene.cu)
+
+}  // namespace zdx
+
+struct zdx_ctx {
+    int device = 0;
+    int num_sms = 148;
+    int cc_major = 0, cc_minor = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    std::string last_error;
+    double pair_ms[5] = {0, 0, 0, 0, 0};
+    long long launches = 0;  // kernels this context has launched
+
+    // pair-call workspaces
+    zdx::DevBuf in_tris, in_off, in_me, in_bd, in_pm, in_pose;
+    zdx::DevBuf tri_sph, mesh_R, mesh_valid;
+    zdx::DevBuf order, buckets, pair_i64, pair_i32, counters;
+    zdx::DevBuf k1_slots, seg_arena, k2_slots;
+    zdx::DevBuf cstage, cistage, pstage;
+    zdx::DevBuf g_off, o_cg, o_ci, o_pts, o_cpo, o_ps;
+
+    std::vector<zdx::DevBuf*> all_bufs() {
+        return {&in_tris, &in_off, &in_me, &in_bd, &in_pm, &in_pose, &tri_sph, &mesh_R, &mesh_valid,
+                &order, &buckets, &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots,
+                &cstage, &cistage, &pstage, &g_off, &o_cg, &o_ci, &o_pts, &o_cpo, &o_ps};
+    }
+
+    zdx::Scene* scene = nullptr;
+    void scene_release();
+};

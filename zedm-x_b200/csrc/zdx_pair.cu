@@ -1,0 +1,1035 @@
+// zdx_pair.cu -- batched pair-contact kernels for sm_100a.
+//
+// Stage 0  k_mesh_prep   per-triangle bounding spheres in the mesh frame and a bound per mesh.
+// Stage 1  k_segments    persistent CTAs fed by a cost-ordered queue (most expensive pair first).  Per
+//                        pair: cull both triangle lists against the other body's bounding cube (one
+//                        rotation per triangle, conservative so no AABB-overlapping pair is lost),
+//                        transform the survivors exactly as src/main.cpp:499-510 does, test every
+//                        surviving (ta,tb) with the reference's strict AABB compare, queue the overlaps
+//                        in shared memory and run tri_tri_intersection_segment on them with the whole
+//                        CTA, then order the segments by (ta,tb): the reference's emission order.
+// Stage 2  k_rebuild     one warp per pair: components (label_segments_by_contact_greedy), endpoint
+//                        snap, T-junction split, loop trace, Sn/Gn/xc0, filters and the minimal force
+//                        law.  Neighbour scans run across the 32 lanes; decisions whose order the
+//                        reference fixes (DFS pushes, union-find classes, std::sort of ties, the walk)
+//                        run on lane 0 in that order.
+// Stage 3  k_gather      deterministic CSR of contacts and loop points (exclusive scans over pairs).
+//
+// Compiled with --fmad=false: see zdx_math.cuh.
+#include <cstdio>
+
+#include "zdx_math.cuh"
+#include "zdx_pair.cuh"
+#include "zdx_sortrep.cuh"
+
+namespace zdx {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int K1_THREADS = 256;
+constexpr int K1_ITER = 8;
+constexpr int K1_QCAP = K1_THREADS * K1_ITER;
+constexpr int K2_WARPS = 4;
+
+int k1_blocks_per_sm() { return 2; }
+int k2_warps_per_block() { return K2_WARPS; }
+
+__device__ __forceinline__ V3 ld3(const double* p) { return V3{p[0], p[1], p[2]}; }
+__device__ __forceinline__ void st3(double* p, V3 v) {
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+}
+
+
+// --------------------------------------------------------------------------------------------- stage 0
+__global__ void k_mesh_prep(PairArgs a, int64_t total) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int lo = 0, hi = a.n_mesh;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (a.tri_off[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    const double* v = a.tris + 9 * t;
+    V3 p0 = ld3(v), p1 = ld3(v + 3), p2 = ld3(v + 6);
+    V3 c = (p0 + p1 + p2) * (1.0 / 3.0);
+    double r = sqrt(smax3(norm2(p0 - c), norm2(p1 - c), norm2(p2 - c))) * (1.0 + 1e-12);
+    a.tri_sph[t] = make_double4(c.x, c.y, c.z, r);
+    double R = (norm(c) + r) * (1.0 + 1e-12);
+    atomicMax(a.mesh_R_bits + lo, (unsigned long long)__double_as_longlong(R));
+    if (!(norm(cross(p1 - p0, p2 - p0)) < 1e-30)) atomicAdd(a.mesh_valid + lo, 1);
+}
+
+void launch_mesh_prep(const PairArgs& a, int64_t total_tris, cudaStream_t s) {
+    if (total_tris <= 0) return;
+    int64_t blocks = (total_tris + 255) / 256;
+    k_mesh_prep<<<(unsigned)blocks, 256, 0, s>>>(a, total_tris);
+}
+
+// ------------------------------------------------------------------------- cost order (work queue)
+// Pairs are bucketed by floor(log2(nA*nB)) and the buckets laid out most expensive first.  The order
+// only schedules work; results do not depend on it.
+__global__ void k_cost_count(PairArgs a, int* buckets) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= a.n_pairs) return;
+    int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
+    unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
+                           (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
+    int b = 63 - __clzll(c + 1);
+    atomicAdd(buckets + (63 - b), 1);
+}
+__global__ void k_cost_scan(int* buckets) {
+    if (threadIdx.x != 0) return;
+    int run = 0;
+    for (int i = 0; i < 64; ++i) {
+        int c = buckets[i];
+        buckets[64 + i] = run;
+        run += c;
+    }
+}
+__global__ void k_cost_scatter(PairArgs a, int* buckets, int32_t* order) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= a.n_pairs) return;
+    int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
+    unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
+                           (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
+    int b = 63 - __clzll(c + 1);
+    int pos = atomicAdd(buckets + 64 + (63 - b), 1);
+    order[pos] = (int32_t)p;
+}
+void launch_cost_order(const PairArgs& a, int32_t* order, int* buckets, cudaStream_t s) {
+    if (a.n_pairs <= 0) return;
+    unsigned blocks = (unsigned)((a.n_pairs + 255) / 256);
+    cudaMemsetAsync(buckets, 0, sizeof(int) * 128, s);
+    k_cost_count<<<blocks, 256, 0, s>>>(a, buckets);
+    k_cost_scan<<<1, 32, 0, s>>>(buckets);
+    k_cost_scatter<<<blocks, 256, 0, s>>>(a, buckets, order);
+}
+
+// --------------------------------------------------------------------------------------------- stage 1
+struct K1Side {
+    double* tri;  // 9 x cap, component-major
+    double* pl;   // 4 x cap: nx ny nz d
+    double* box;  // 6 x cap: min xyz, max xyz
+    int* id;      // cap
+};
+struct K1Slot {
+    K1Side side[2];
+    double* seg;    // 6 x cap_seg
+    uint64_t* key;  // cap_seg
+};
+
+__host__ __device__ inline size_t carve_k1(char* base, int cap, int cap_seg, K1Slot* s) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) -> char* {
+        char* p = base ? base + off : nullptr;
+        off = (off + bytes + 15) & ~size_t(15);
+        return p;
+    };
+    for (int k = 0; k < 2; ++k) {
+        K1Side d;
+        d.tri = (double*)take(sizeof(double) * 9 * (size_t)cap);
+        d.pl = (double*)take(sizeof(double) * 4 * (size_t)cap);
+        d.box = (double*)take(sizeof(double) * 6 * (size_t)cap);
+        d.id = (int*)take(sizeof(int) * (size_t)cap);
+        if (s) s->side[k] = d;
+    }
+    double* seg = (double*)take(sizeof(double) * 6 * (size_t)cap_seg);
+    uint64_t* key = (uint64_t*)take(sizeof(uint64_t) * (size_t)cap_seg);
+    if (s) {
+        s->seg = seg;
+        s->key = key;
+    }
+    return off;
+}
+
+size_t tritest_slot_bytes(int cap_side, int cap_seg) { return carve_k1(nullptr, cap_side, cap_seg, nullptr); }
+
+__global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
+    __shared__ int sh_item;
+    __shared__ int sh_n[2];
+    __shared__ int sh_nq;
+    __shared__ int sh_nseg;
+    __shared__ unsigned long long sh_base;
+    __shared__ int2 sh_q[K1_QCAP];
+    const int tid = threadIdx.x;
+    K1Slot S;
+    carve_k1(a.k1_slots + (size_t)blockIdx.x * a.k1_slot_bytes, a.cap_side, a.cap_seg, &S);
+    const int cap = a.cap_side;
+    const bool py = a.mode == 1;
+
+    for (;;) {
+        if (tid == 0) {
+            sh_item = (int)(a.item_begin + atomicAdd(a.queue1, 1));
+            sh_n[0] = sh_n[1] = 0;
+            sh_nq = 0;
+            sh_nseg = 0;
+        }
+        __syncthreads();
+        const int64_t item = sh_item;
+        if (item >= a.item_end) break;
+        const int p = a.order[item];
+        const double* ps = a.pose + 14 * (int64_t)p;
+        V3 tpos[2] = {V3{ps[0], ps[1], ps[2]}, V3{ps[7], ps[8], ps[9]}};
+        Q4 qraw[2] = {Q4{ps[3], ps[4], ps[5], ps[6]}, Q4{ps[10], ps[11], ps[12], ps[13]}};
+        Q4 qn[2];
+        for (int k = 0; k < 2; ++k) qn[k] = py ? qnormalize_py(qraw[k]) : qnormalize(qraw[k]);
+        const int mesh[2] = {a.pmesh[2 * (int64_t)p], a.pmesh[2 * (int64_t)p + 1]};
+        const int64_t off[2] = {a.tri_off[mesh[0]], a.tri_off[mesh[1]]};
+        const int nt[2] = {(int)(a.tri_off[mesh[0] + 1] - off[0]), (int)(a.tri_off[mesh[1] + 1] - off[1])};
+        const double R[2] = {__longlong_as_double((long long)a.mesh_R_bits[mesh[0]]),
+                             __longlong_as_double((long long)a.mesh_R_bits[mesh[1]])};
+        auto inf = [](V3 v) { return smax3(fabs(v.x), fabs(v.y), fabs(v.z)); };
+        const double pad = 1e-9 * (inf(tpos[0]) + inf(tpos[1]) + R[0] + R[1]);
+
+        // Cull each side against the other body's bounding cube; keep the exact world triangles,
+        // planes and AABBs of the survivors (src/main.cpp:2064-2116).
+        for (int s = 0; s < 2; ++s) {
+            const V3 other = tpos[1 - s];
+            const double lim = R[1 - s] + pad;
+            K1Side& D = S.side[s];
+            for (int t = tid; t < nt[s]; t += K1_THREADS) {
+                double4 sp = a.tri_sph[off[s] + t];
+                V3 c = V3{sp.x, sp.y, sp.z};
+                V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];
+                double L = sp.w + lim;
+                if (!(fabs(cw.x - other.x) <= L && fabs(cw.y - other.y) <= L && fabs(cw.z - other.z) <= L)) continue;
+                const double* v = a.tris + 9 * (off[s] + t);
+                V3 w[3];
+                for (int k = 0; k < 3; ++k) {
+                    V3 lv = ld3(v + 3 * k);
+                    w[k] = (py ? qrotate_py_n(qn[s], lv) : qrotate_n(qn[s], lv)) + tpos[s];
+                }
+                V3 n;
+                double d;
+                if (!plane_from_tri(w[0], w[1], w[2], n, d)) continue;
+                if (norm2(n) < 1e-30) continue;
+                int i = atomicAdd(&sh_n[s], 1);
+                for (int k = 0; k < 3; ++k) {
+                    D.tri[(3 * k + 0) * cap + i] = w[k].x;
+                    D.tri[(3 * k + 1) * cap + i] = w[k].y;
+                    D.tri[(3 * k + 2) * cap + i] = w[k].z;
+                }
+                D.pl[0 * cap + i] = n.x;
+                D.pl[1 * cap + i] = n.y;
+                D.pl[2 * cap + i] = n.z;
+                D.pl[3 * cap + i] = d;
+                D.box[0 * cap + i] = smin3(w[0].x, w[1].x, w[2].x);
+                D.box[1 * cap + i] = smin3(w[0].y, w[1].y, w[2].y);
+                D.box[2 * cap + i] = smin3(w[0].z, w[1].z, w[2].z);
+                D.box[3 * cap + i] = smax3(w[0].x, w[1].x, w[2].x);
+                D.box[4 * cap + i] = smax3(w[0].y, w[1].y, w[2].y);
+                D.box[5 * cap + i] = smax3(w[0].z, w[1].z, w[2].z);
+                D.id[i] = t;
+            }
+        }
+        __syncthreads();
+        const int nA = sh_n[0], nB = sh_n[1];
+        const int64_t total = (int64_t)nA * nB;
+        const K1Side& SA = S.side[0];
+        const K1Side& SB = S.side[1];
+        int ia = 0, ib = 0, dA = 0, dB = 0;
+        if (nB > 0) {
+            ia = tid / nB;
+            ib = tid % nB;
+            dA = K1_THREADS / nB;
+            dB = K1_THREADS % nB;
+        }
+        for (int64_t base = 0; base < total; base += K1_QCAP) {
+#pragma unroll 1
+            for (int it = 0; it < K1_ITER; ++it) {
+                int64_t kk = base + (int64_t)it * K1_THREADS + tid;
+                if (kk < total) {
+                    // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
+                    bool sep = SA.box[3 * cap + ia] < SB.box[0 * cap + ib] || SA.box[0 * cap + ia] > SB.box[3 * cap + ib] ||
+                               SA.box[4 * cap + ia] < SB.box[1 * cap + ib] || SA.box[1 * cap + ia] > SB.box[4 * cap + ib] ||
+                               SA.box[5 * cap + ia] < SB.box[2 * cap + ib] || SA.box[2 * cap + ia] > SB.box[5 * cap + ib];
+                    if (!sep) {
+                        int qi = atomicAdd(&sh_nq, 1);
+                        sh_q[qi] = make_int2(ia, ib);
+                    }
+                }
+                ib += dB;
+                ia += dA;
+                if (ib >= nB) {
+                    ib -= nB;
+                    ia++;
+                }
+            }
+            __syncthreads();
+            const int nq = sh_nq;
+            for (int qi = tid; qi < nq; qi += K1_THREADS) {
+                int2 e = sh_q[qi];
+                V3 TA[3], TB[3];
+                for (int k = 0; k < 3; ++k) {
+                    TA[k] = V3{SA.tri[(3 * k) * cap + e.x], SA.tri[(3 * k + 1) * cap + e.x], SA.tri[(3 * k + 2) * cap + e.x]};
+                    TB[k] = V3{SB.tri[(3 * k) * cap + e.y], SB.tri[(3 * k + 1) * cap + e.y], SB.tri[(3 * k + 2) * cap + e.y]};
+                }
+                V3 na{SA.pl[e.x], SA.pl[cap + e.x], SA.pl[2 * cap + e.x]};
+                V3 nb{SB.pl[e.y], SB.pl[cap + e.y], SB.pl[2 * cap + e.y]};
+                V3 o0, o1;
+                if (tri_tri(TA, na, SA.pl[3 * cap + e.x], TB, nb, SB.pl[3 * cap + e.y], o0, o1)) {
+                    int si = atomicAdd(&sh_nseg, 1);
+                    if (si < a.cap_seg) {
+                        st3(S.seg + 6 * si, o0);
+                        st3(S.seg + 6 * si + 3, o1);
+                        S.key[si] = ((uint64_t)(uint32_t)SA.id[e.x] << 32) | (uint64_t)(uint32_t)SB.id[e.y];
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid == 0) sh_nq = 0;
+            __syncthreads();
+        }
+        int ns = sh_nseg;
+        int status = 0;
+        if (ns > a.cap_seg) {
+            status |= PAIR_SEG_OVERFLOW;
+            ns = a.cap_seg;
+        }
+        if (tid == 0) sh_base = atomicAdd(a.seg_counter, (unsigned long long)ns);
+        __syncthreads();
+        const unsigned long long sbase = sh_base;
+        if (sbase + (unsigned long long)ns <= (unsigned long long)a.seg_cap) {
+            // order by (ta, tb): the reference emits segments in that lexicographic order
+            for (int i = tid; i < ns; i += K1_THREADS) {
+                uint64_t ki = S.key[i];
+                int r = 0;
+                for (int j = 0; j < ns; ++j) r += (S.key[j] < ki);
+                double* dst = a.seg + 6 * (sbase + (unsigned long long)r);
+                for (int k = 0; k < 6; ++k) dst[k] = S.seg[6 * i + k];
+            }
+        } else if (tid == 0) {
+            atomicOr(a.err, ERR_SEG_ARENA);
+        }
+        if (tid == 0) {
+            a.pair_seg_off[p] = (int64_t)sbase;
+            a.pair_nseg[p] = ns;
+            a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
+            a.pair_status[p] = status;
+            atomicMax(a.max_nseg, ns);
+            atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
+            if (status) atomicOr(a.err, ERR_PAIR);
+        }
+        __syncthreads();
+    }
+}
+
+void launch_segments(const PairArgs& a, int grid, cudaStream_t s) {
+    if (grid <= 0) return;
+    k_segments<<<grid, K1_THREADS, 0, s>>>(a);
+}
+
+// --------------------------------------------------------------------------------------------- stage 2
+struct PostBufs {
+    int* rcell;
+    double* bmn;
+    double* bmx;
+    int* visited;
+    int* stack;
+    int* raw_idx;
+    int* raw_off;
+    int* comp_sz;
+    int* comp_ord;
+    int* comp_idx;
+    int* comp_off;
+    int* el_j;
+    int* el_k;
+    double* pts;
+    int* pcell;
+    int* parent;
+    int* root;
+    int* rootv;
+    int* cnt;
+    double* V;
+    int* vcell;
+    int* E;
+    int* E2;
+    int* sp_v;
+    double* sp_t;
+    int* sp_i;
+    int* deg;
+    int* astart;
+    int* afill;
+    int* anb;
+    int* aei;
+    int* used;
+    int* vorder;
+    int* path;
+    int* loop_off;
+    int* loop_vid;
+    double* cgeom;
+    int* cinfo;
+    double* cpts;
+    int cap2;
+    int capc;
+};
+
+__host__ __device__ inline int rebuild_cap2(int n) { return 4 * n + 64; }
+
+__host__ __device__ inline size_t carve_post(char* base, int n, PostBufs* b) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) -> char* {
+        char* p = base ? base + off : nullptr;
+        off = (off + bytes + 15) & ~size_t(15);
+        return p;
+    };
+    const size_t N = (size_t)(n > 0 ? n : 1);
+    const int cap2 = rebuild_cap2(n);
+    const size_t C2 = (size_t)cap2;
+    const size_t capc = C2 / 3 + 2;  // a loop uses >= 3 edges, except 2-cycles which are never contacts
+    PostBufs t;
+    t.rcell = (int*)take(sizeof(int) * 9 * N);
+    t.bmn = (double*)take(sizeof(double) * 3 * N);
+    t.bmx = (double*)take(sizeof(double) * 3 * N);
+    t.visited = (int*)take(sizeof(int) * N);
+    t.stack = (int*)take(sizeof(int) * N);
+    t.raw_idx = (int*)take(sizeof(int) * N);
+    t.raw_off = (int*)take(sizeof(int) * (N + 1));
+    t.comp_sz = (int*)take(sizeof(int) * N);
+    t.comp_ord = (int*)take(sizeof(int) * N);
+    t.comp_idx = (int*)take(sizeof(int) * N);
+    t.comp_off = (int*)take(sizeof(int) * (N + 1));
+    t.el_j = (int*)take(sizeof(int) * N);
+    t.el_k = (int*)take(sizeof(int) * N);
+    t.pts = (double*)take(sizeof(double) * 6 * N);
+    t.pcell = (int*)take(sizeof(int) * 6 * N);
+    t.parent = (int*)take(sizeof(int) * 2 * N);
+    t.root = (int*)take(sizeof(int) * 2 * N);
+    t.rootv = (int*)take(sizeof(int) * 2 * N);
+    t.cnt = (int*)take(sizeof(int) * 2 * N);
+    t.V = (double*)take(sizeof(double) * 6 * N);
+    t.vcell = (int*)take(sizeof(int) * 6 * N);
+    t.E = (int*)take(sizeof(int) * 2 * N);
+    t.E2 = (int*)take(sizeof(int) * 2 * C2);
+    t.sp_v = (int*)take(sizeof(int) * 2 * N);
+    t.sp_t = (double*)take(sizeof(double) * 2 * N);
+    t.sp_i = (int*)take(sizeof(int) * 2 * N);
+    t.deg = (int*)take(sizeof(int) * 2 * N);
+    t.astart = (int*)take(sizeof(int) * (2 * N + 1));
+    t.afill = (int*)take(sizeof(int) * 2 * N);
+    t.anb = (int*)take(sizeof(int) * 2 * C2);
+    t.aei = (int*)take(sizeof(int) * 2 * C2);
+    t.used = (int*)take(sizeof(int) * C2);
+    t.vorder = (int*)take(sizeof(int) * 2 * N);
+    t.path = (int*)take(sizeof(int) * (C2 + 2));
+    t.loop_off = (int*)take(sizeof(int) * (C2 + 2));
+    t.loop_vid = (int*)take(sizeof(int) * (C2 + 2));
+    t.cgeom = (double*)take(sizeof(double) * 20 * capc);
+    t.cinfo = (int*)take(sizeof(int) * 4 * capc);
+    t.cpts = (double*)take(sizeof(double) * 3 * C2);
+    t.cap2 = cap2;
+    t.capc = (int)capc;
+    if (b) *b = t;
+    return off;
+}
+
+size_t rebuild_slot_bytes(int n) { return carve_post(nullptr, n, nullptr); }
+
+__device__ __forceinline__ I3 ld_cell(const int* c) { return I3{c[0], c[1], c[2]}; }
+__device__ __forceinline__ void st_cell(int* c, I3 v) {
+    c[0] = v.x;
+    c[1] = v.y;
+    c[2] = v.z;
+}
+__device__ __forceinline__ bool adjacent(I3 a, I3 b) {
+    int dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    return !(dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1);
+}
+__device__ int uf_find(int* parent, int x) {
+    while (parent[x] != x) {
+        parent[x] = parent[parent[x]];
+        x = parent[x];
+    }
+    return x;
+}
+__device__ int uf_find_ro(const int* parent, int x) {
+    while (parent[x] != x) x = parent[x];
+    return x;
+}
+
+// The post-triangle part of the reference's per-pair body (src/main.cpp:2148-2219) for one pair, by
+// one warp.  Component / loop / contact order follows the reference exactly.
+__device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, const int lane) {
+    const int n = a.pair_nseg[p];
+    int status = a.pair_status[p];
+    const double* S = a.seg + 6 * a.pair_seg_off[p];
+    const int mA = a.pmesh[2 * (int64_t)p];
+    const bool py = a.mode == 1;
+    const double* ps = a.pose + 14 * (int64_t)p;
+    const V3 dirAB = V3{ps[7], ps[8], ps[9]} - V3{ps[0], ps[1], ps[2]};
+    const double me = a.mean_edge[mA];
+    double tol = a.tol_in;
+    if (!(tol > 0.0)) {
+        tol = me > 0.0 ? (me * 0.1) : (a.bbox_diag[mA] * 1e-2);
+        if (tol <= 0.0) tol = 1e-6;
+    }
+    const double h = tol;
+    const double tol2 = h * h;
+    const double area_eps = me > 0.0 ? (me * me * 1e-4) : 1e-12;
+
+    int ncomp = 0, nloops = 0, nctc = 0, npts = 0;
+    if (n > 0 && !(status & PAIR_SEG_OVERFLOW)) {
+        // ---- components: label_segments_by_contact_greedy, src/main.cpp:804-898
+        if (a.split) {
+            for (int i = lane; i < n; i += 32) {
+                V3 p0 = ld3(S + 6 * i), p1 = ld3(S + 6 * i + 3);
+                V3 mid = (p0 + p1) * 0.5;
+                st_cell(B.rcell + 9 * i, cell_of(p0, h));
+                st_cell(B.rcell + 9 * i + 3, cell_of(p1, h));
+                st_cell(B.rcell + 9 * i + 6, cell_of(mid, h));
+                st3(B.bmn + 3 * i, V3{smin(p0.x, p1.x) - h, smin(p0.y, p1.y) - h, smin(p0.z, p1.z) - h});
+                st3(B.bmx + 3 * i, V3{smax(p0.x, p1.x) + h, smax(p0.y, p1.y) + h, smax(p0.z, p1.z) + h});
+                B.visited[i] = 0;
+            }
+            if (lane == 0) B.raw_off[0] = 0;
+            __syncwarp();
+            int cnt = 0, ncr = 0;
+            for (int seed = 0; seed < n; ++seed) {
+                if (B.visited[seed]) continue;
+                __syncwarp();
+                if (lane == 0) {
+                    B.visited[seed] = 1;
+                    B.stack[0] = seed;
+                    B.raw_idx[cnt] = seed;
+                }
+                int sp = 1;
+                cnt++;
+                __syncwarp();
+                while (sp > 0) {
+                    sp--;
+                    const int i = B.stack[sp];
+                    const V3 p1 = ld3(S + 6 * i), q1 = ld3(S + 6 * i + 3);
+                    I3 ci[3];
+                    for (int r = 0; r < 3; ++r) ci[r] = ld_cell(B.rcell + 9 * i + 3 * r);
+                    const V3 imn = ld3(B.bmn + 3 * i), imx = ld3(B.bmx + 3 * i);
+                    int nel = 0;
+                    for (int jb = 0; jb < n; jb += 32) {
+                        const int j = jb + lane;
+                        bool el = false;
+                        int best = 1 << 30;
+                        if (j < n && j != i && !B.visited[j]) {
+                            // first visit of j in the reference's hash-grid walk: smallest
+                            // r*27 + neighbour-cell rank over the rep points (p0, p1, mid)
+                            for (int r = 0; r < 3; ++r)
+                                for (int rj = 0; rj < 3; ++rj) {
+                                    I3 cj = ld_cell(B.rcell + 9 * j + 3 * rj);
+                                    int dx = cj.x - ci[r].x, dy = cj.y - ci[r].y, dz = cj.z - ci[r].z;
+                                    if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+                                    int k = r * 27 + (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+                                    if (k < best) best = k;
+                                }
+                            if (best != (1 << 30)) {
+                                V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
+                                bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y ||
+                                            imx.z < jmn.z || imn.z > jmx.z);
+                                if (ov && seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2) el = true;
+                            }
+                        }
+                        unsigned bal = __ballot_sync(FULL, el);
+                        if (el) {
+                            int pos = nel + __popc(bal & ((1u << lane) - 1u));
+                            B.el_j[pos] = j;
+                            B.el_k[pos] = best;
+                        }
+                        nel += __popc(bal);
+                    }
+                    __syncwarp();
+                    if (lane == 0) {
+                        for (int x = 1; x < nel; ++x) {
+                            int kj = B.el_j[x], kk = B.el_k[x], y = x - 1;
+                            while (y >= 0 && B.el_k[y] > kk) {
+                                B.el_j[y + 1] = B.el_j[y];
+                                B.el_k[y + 1] = B.el_k[y];
+                                --y;
+                            }
+                            B.el_j[y + 1] = kj;
+                            B.el_k[y + 1] = kk;
+                        }
+                        for (int x = 0; x < nel; ++x) {
+                            int j = B.el_j[x];
+                            B.visited[j] = 1;
+                            B.stack[sp + x] = j;
+                            B.raw_idx[cnt + x] = j;
+                        }
+                    }
+                    sp += nel;
+                    cnt += nel;
+                    __syncwarp();
+                }
+                ncr++;
+                if (lane == 0) B.raw_off[ncr] = cnt;
+                __syncwarp();
+            }
+            ncomp = ncr;
+            if (lane == 0) {
+                for (int c = 0; c < ncr; ++c) {
+                    B.comp_sz[c] = B.raw_off[c + 1] - B.raw_off[c];
+                    B.comp_ord[c] = c;
+                }
+                const int* sz = B.comp_sz;
+                sort_idx(B.comp_ord, ncr, [sz](int x, int y) { return sz[x] > sz[y]; }, py);
+                int o = 0;
+                B.comp_off[0] = 0;
+                for (int k = 0; k < ncr; ++k) {
+                    int c = B.comp_ord[k];
+                    for (int m = B.raw_off[c]; m < B.raw_off[c + 1]; ++m) B.comp_idx[o++] = B.raw_idx[m];
+                    B.comp_off[k + 1] = o;
+                }
+            }
+        } else {
+            ncomp = 1;
+            for (int i = lane; i < n; i += 32) B.comp_idx[i] = i;
+            if (lane == 0) {
+                B.comp_off[0] = 0;
+                B.comp_off[1] = n;
+            }
+        }
+        __syncwarp();
+
+        for (int c = 0; c < ncomp && !(status & PAIR_EDGE_OVERFLOW); ++c) {
+            const int m = B.comp_off[c + 1] - B.comp_off[c];
+            const int* idx = B.comp_idx + B.comp_off[c];
+            const int np = 2 * m;
+            // ---- snap_endpoints, src/main.cpp:680-746
+            for (int i = lane; i < np; i += 32) {
+                V3 pt = ld3(S + 6 * idx[i >> 1] + 3 * (i & 1));
+                st3(B.pts + 3 * i, pt);
+                st_cell(B.pcell + 3 * i, cell_of(pt, h));
+                B.parent[i] = i;
+            }
+            __syncwarp();
+            for (int i = 1; i < np; ++i) {
+                const V3 pi = ld3(B.pts + 3 * i);
+                const I3 ci = ld_cell(B.pcell + 3 * i);
+                for (int jb = 0; jb < i; jb += 32) {
+                    const int j = jb + lane;
+                    bool close = false;
+                    if (j < i && adjacent(ld_cell(B.pcell + 3 * j), ci)) {
+                        V3 d = pi - ld3(B.pts + 3 * j);
+                        close = py ? (sqrt(dot(d, d)) <= h) : (dot(d, d) <= h * h);
+                    }
+                    unsigned bal = __ballot_sync(FULL, close);
+                    if (lane == 0) {
+                        while (bal) {
+                            int b = __ffs(bal) - 1;
+                            bal &= bal - 1u;
+                            int ra = uf_find(B.parent, i), rb = uf_find(B.parent, jb + b);
+                            if (ra != rb) {
+                                if (ra < rb) B.parent[rb] = ra;
+                                else B.parent[ra] = rb;
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            for (int i = lane; i < np; i += 32) {
+                B.root[i] = uf_find_ro(B.parent, i);
+                B.rootv[i] = -1;
+            }
+            __syncwarp();
+            int nv = 0, ne = 0;
+            if (lane == 0) {
+                for (int i = 0; i < np; ++i) {
+                    int r = B.root[i];
+                    int v = B.rootv[r];
+                    V3 pt = ld3(B.pts + 3 * i);
+                    if (v < 0) {
+                        B.rootv[r] = nv;
+                        st3(B.V + 3 * nv, pt);
+                        B.cnt[nv] = 1;
+                        nv++;
+                    } else {
+                        st3(B.V + 3 * v, ld3(B.V + 3 * v) + pt);
+                        B.cnt[v] += 1;
+                    }
+                }
+                for (int s = 0; s < m; ++s) {
+                    int va = B.rootv[B.root[2 * s]], vb = B.rootv[B.root[2 * s + 1]];
+                    if (va != vb) {
+                        B.E[2 * ne] = va;
+                        B.E[2 * ne + 1] = vb;
+                        ne++;
+                    }
+                }
+            }
+            nv = __shfl_sync(FULL, nv, 0);
+            ne = __shfl_sync(FULL, ne, 0);
+            __syncwarp();
+            for (int v = lane; v < nv; v += 32) {
+                V3 q = ld3(B.V + 3 * v) / (double)B.cnt[v];
+                st3(B.V + 3 * v, q);
+                st_cell(B.vcell + 3 * v, cell_of(q, h));
+            }
+            __syncwarp();
+
+            // ---- split_t_junctions, src/main.cpp:900-961
+            int ne2 = 0;
+            for (int e = 0; e < ne; ++e) {
+                const int ea = B.E[2 * e], eb = B.E[2 * e + 1];
+                const V3 pa = ld3(B.V + 3 * ea), pb = ld3(B.V + 3 * eb);
+                const V3 mn{smin(pa.x, pb.x) - h, smin(pa.y, pb.y) - h, smin(pa.z, pb.z) - h};
+                const V3 mx{smax(pa.x, pb.x) + h, smax(pa.y, pb.y) + h, smax(pa.z, pb.z) + h};
+                const I3 cmin = cell_of(mn, h), cmax = cell_of(mx, h);
+                int nsp = 0;
+                for (int vb0 = 0; vb0 < nv; vb0 += 32) {
+                    const int v = vb0 + lane;
+                    bool ok = false;
+                    double t = 0.0;
+                    if (v < nv && v != ea && v != eb) {
+                        I3 cv = ld_cell(B.vcell + 3 * v);
+                        if (!(cv.x < cmin.x || cv.x > cmax.x || cv.y < cmin.y || cv.y > cmax.y || cv.z < cmin.z ||
+                              cv.z > cmax.z)) {
+                            double d2 = pt_seg_d2t(ld3(B.V + 3 * v), pa, pb, t);
+                            ok = d2 <= tol2 && t > 1e-6 && t < 1.0 - 1e-6;
+                        }
+                    }
+                    unsigned bal = __ballot_sync(FULL, ok);
+                    if (ok) {
+                        int pos = nsp + __popc(bal & ((1u << lane) - 1u));
+                        B.sp_v[pos] = v;
+                        B.sp_t[pos] = t;
+                    }
+                    nsp += __popc(bal);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    if (nsp == 0) {
+                        if (ne2 < B.cap2) {
+                            B.E2[2 * ne2] = ea;
+                            B.E2[2 * ne2 + 1] = eb;
+                            ne2++;
+                        } else {
+                            status |= PAIR_EDGE_OVERFLOW;
+                        }
+                    } else {
+                        // the reference visits candidates cell by cell (x, y, z), vertex id inside a
+                        // cell; the list holds them by id, so order it by cell (stable).
+                        for (int x = 1; x < nsp; ++x) {
+                            int vv = B.sp_v[x];
+                            double tt = B.sp_t[x];
+                            I3 cx = ld_cell(B.vcell + 3 * vv);
+                            int y = x - 1;
+                            while (y >= 0) {
+                                I3 cy = ld_cell(B.vcell + 3 * B.sp_v[y]);
+                                bool gt = (cy.x != cx.x) ? (cy.x > cx.x) : (cy.y != cx.y) ? (cy.y > cx.y) : (cy.z > cx.z);
+                                if (!gt) break;
+                                B.sp_v[y + 1] = B.sp_v[y];
+                                B.sp_t[y + 1] = B.sp_t[y];
+                                --y;
+                            }
+                            B.sp_v[y + 1] = vv;
+                            B.sp_t[y + 1] = tt;
+                        }
+                        for (int x = 0; x < nsp; ++x) B.sp_i[x] = x;
+                        const double* st = B.sp_t;
+                        sort_idx(B.sp_i, nsp, [st](int x, int y) { return st[x] < st[y]; }, py);
+                        int prev = ea, last = -1;
+                        for (int x = 0; x <= nsp; ++x) {
+                            int v = x < nsp ? B.sp_v[B.sp_i[x]] : eb;
+                            if (x < nsp && v == last) continue;
+                            if (prev != v) {
+                                if (ne2 < B.cap2) {
+                                    B.E2[2 * ne2] = prev;
+                                    B.E2[2 * ne2 + 1] = v;
+                                    ne2++;
+                                } else {
+                                    status |= PAIR_EDGE_OVERFLOW;
+                                }
+                            }
+                            prev = v;
+                            last = v;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            ne2 = __shfl_sync(FULL, ne2, 0);
+            status = __shfl_sync(FULL, status, 0);
+            if (status & PAIR_EDGE_OVERFLOW) break;
+
+            // ---- extract_loops (src/main.cpp:963-1025), then each loop's integrals, filters and
+            // force (src/main.cpp:1027-1052, 2187-2219; polyline.py:799-822, 655-701)
+            if (lane == 0) {
+                for (int v = 0; v < nv; ++v) {
+                    B.deg[v] = 0;
+                    B.afill[v] = 0;
+                }
+                for (int e = 0; e < ne2; ++e) {
+                    B.deg[B.E2[2 * e]]++;
+                    B.deg[B.E2[2 * e + 1]]++;
+                }
+                B.astart[0] = 0;
+                for (int v = 0; v < nv; ++v) B.astart[v + 1] = B.astart[v] + B.deg[v];
+                for (int e = 0; e < ne2; ++e) {
+                    int x = B.E2[2 * e], y = B.E2[2 * e + 1];
+                    B.anb[B.astart[x] + B.afill[x]] = y;
+                    B.aei[B.astart[x] + B.afill[x]] = e;
+                    B.afill[x]++;
+                    B.anb[B.astart[y] + B.afill[y]] = x;
+                    B.aei[B.astart[y] + B.afill[y]] = e;
+                    B.afill[y]++;
+                    B.used[e] = 0;
+                }
+                for (int v = 0; v < nv; ++v) B.vorder[v] = v;
+                const int* dg = B.deg;
+                sort_idx(B.vorder, nv,
+                         [dg](int x, int y) {
+                             int dx = dg[x], dy = dg[y];
+                             if ((dx == 2) != (dy == 2)) return dx == 2;
+                             return dx > dy;
+                         },
+                         py);
+                int nl = 0, lv_used = 0;
+                B.loop_off[0] = 0;
+                for (int oi = 0; oi < nv; ++oi) {
+                    const int sv = B.vorder[oi];
+                    for (int k = B.astart[sv]; k < B.astart[sv + 1]; ++k) {
+                        if (B.used[B.aei[k]]) continue;
+                        int plen = 0;
+                        B.path[plen++] = sv;
+                        int prev = sv, cur = B.anb[k];
+                        B.used[B.aei[k]] = 1;
+                        B.path[plen++] = cur;
+                        int steps = 0;
+                        while (steps < 100000) {
+                            steps += 1;
+                            if (cur == sv) {
+                                plen -= 1;
+                                for (int q = 0; q < plen; ++q) B.loop_vid[lv_used + q] = B.path[q];
+                                lv_used += plen;
+                                nl++;
+                                B.loop_off[nl] = lv_used;
+                                break;
+                            }
+                            int pick = -1, first = -1;
+                            for (int q = B.astart[cur]; q < B.astart[cur + 1]; ++q) {
+                                if (B.used[B.aei[q]]) continue;
+                                if (first < 0) first = q;
+                                if (B.anb[q] != prev) {
+                                    pick = q;
+                                    break;
+                                }
+                            }
+                            if (first < 0) break;
+                            if (pick < 0) pick = first;
+                            B.used[B.aei[pick]] = 1;
+                            prev = cur;
+                            cur = B.anb[pick];
+                            B.path[plen++] = cur;
+                        }
+                    }
+                }
+                nloops += nl;
+                for (int l = 0; l < nl; ++l) {
+                    const int len = B.loop_off[l + 1] - B.loop_off[l];
+                    const int* lv = B.loop_vid + B.loop_off[l];
+                    if (len < 3) continue;
+                    V3 Sn{0.0, 0.0, 0.0}, Gn{0.0, 0.0, 0.0};
+                    for (int q = 0; q < len; ++q) {
+                        V3 p0 = ld3(B.V + 3 * lv[q]);
+                        V3 p1 = ld3(B.V + 3 * lv[(q + 1) % len]);
+                        Sn = Sn + cross(p0, p1) * 0.5;
+                        V3 dx = p1 - p0;
+                        double s = dot(p0, p1) + (1.0 / 3.0) * dot(dx, dx);
+                        Gn = Gn + dx * (-(1.0 / 3.0) * s);
+                    }
+                    double area = norm(Sn);
+                    V3 nA{0.0, 0.0, 0.0}, xc0{0.0, 0.0, 0.0};
+                    bool contact = false;
+                    if (!py) {
+                        if (!(area < 1e-14)) {
+                            nA = Sn * (-1.0 / area);
+                            xc0 = cross(nA, Gn) / area;
+                            if (!(area < area_eps)) {
+                                contact = true;
+                                if (dot(nA, dirAB) < 0.0) nA = nA * -1.0;
+                            }
+                        }
+                    } else {
+                        V3 lo = ld3(B.V + 3 * lv[0]), hi = lo;
+                        for (int q = 1; q < len; ++q) {
+                            V3 pq = ld3(B.V + 3 * lv[q]);
+                            lo = V3{fmin(lo.x, pq.x), fmin(lo.y, pq.y), fmin(lo.z, pq.z)};
+                            hi = V3{fmax(hi.x, pq.x), fmax(hi.y, pq.y), fmax(hi.z, pq.z)};
+                        }
+                        if (!(norm(hi - lo) < tol * 2)) {
+                            contact = true;
+                            if (area < 1e-14) {
+                                area = 0.0;
+                            } else {
+                                nA = V3{-Sn.x / area, -Sn.y / area, -Sn.z / area};
+                                xc0 = cross(nA, Gn) / area;
+                            }
+                        }
+                    }
+                    if (!contact) continue;
+                    if (nctc >= B.capc) {
+                        status |= PAIR_EDGE_OVERFLOW;
+                        break;
+                    }
+                    const double Fn = 0.5 * a.k * area;
+                    V3 FA = py ? nA * Fn : nA * (-Fn);
+                    V3 FB = FA * -1.0;
+                    double* g = B.cgeom + 20 * nctc;
+                    st3(g, Sn);
+                    st3(g + 3, Gn);
+                    st3(g + 6, xc0);
+                    st3(g + 9, nA);
+                    g[12] = area;
+                    g[13] = Fn;
+                    st3(g + 14, FA);
+                    st3(g + 17, FB);
+                    B.cinfo[4 * nctc + 0] = p;
+                    B.cinfo[4 * nctc + 1] = nctc;
+                    B.cinfo[4 * nctc + 2] = len;
+                    B.cinfo[4 * nctc + 3] = c;
+                    if (a.want_pts) {
+                        for (int q = 0; q < len && npts < B.cap2; ++q) st3(B.cpts + 3 * (npts++), ld3(B.V + 3 * lv[q]));
+                    }
+                    nctc++;
+                }
+            }
+            nloops = __shfl_sync(FULL, nloops, 0);
+            nctc = __shfl_sync(FULL, nctc, 0);
+            npts = __shfl_sync(FULL, npts, 0);
+            status = __shfl_sync(FULL, status, 0);
+            __syncwarp();
+        }
+    }
+    // ---- publish this pair's contacts
+    unsigned long long cbase = 0, pbase = 0;
+    if (lane == 0) {
+        cbase = atomicAdd(a.contact_counter, (unsigned long long)nctc);
+        if (a.want_pts) pbase = atomicAdd(a.pts_counter, (unsigned long long)npts);
+    }
+    cbase = __shfl_sync(FULL, cbase, 0);
+    pbase = __shfl_sync(FULL, pbase, 0);
+    const bool cfit = cbase + (unsigned long long)nctc <= (unsigned long long)a.contact_cap;
+    if (cfit) {
+        for (int i = lane; i < 20 * nctc; i += 32) a.cgeom_stage[20 * cbase + i] = B.cgeom[i];
+        for (int i = lane; i < 4 * nctc; i += 32) a.cinfo_stage[4 * cbase + i] = B.cinfo[i];
+        for (int i = lane; i < nctc; i += 32) a.clen_stage[cbase + i] = B.cinfo[4 * i + 2];
+    }
+    if (a.want_pts && pbase + (unsigned long long)npts <= (unsigned long long)a.pts_cap) {
+        for (int i = lane; i < 3 * npts; i += 32) a.pts_stage[3 * pbase + i] = B.cpts[i];
+    }
+    if (lane == 0) {
+        if (!cfit) atomicOr(a.err, ERR_CONTACT_STAGE);
+        if (a.want_pts && pbase + (unsigned long long)npts > (unsigned long long)a.pts_cap) atomicOr(a.err, ERR_POINT_STAGE);
+        a.pair_stage_off[p] = (int64_t)cbase;
+        a.pair_pts_stage_off[p] = (int64_t)pbase;
+        a.pair_ncontact[p] = nctc;
+        a.pair_npts[p] = a.want_pts ? npts : 0;
+        a.pair_ncomp[p] = ncomp;
+        a.pair_nloop[p] = nloops;
+        a.pair_status[p] = status;
+        if (status) atomicOr(a.err, ERR_PAIR);
+    }
+    __syncwarp();
+}
+
+__global__ __launch_bounds__(K2_WARPS * 32) void k_rebuild(PairArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wslot = (int64_t)blockIdx.x * K2_WARPS + (threadIdx.x >> 5);
+    if (wslot >= a.k2_nslots) return;
+    PostBufs B;
+    carve_post(a.k2_slots + (size_t)wslot * a.k2_slot_bytes, a.k2_nmax, &B);
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = (int)(a.item_begin + atomicAdd(a.queue2, 1));
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= a.item_end) break;
+        rebuild_pair(a, a.order[item], B, lane);
+    }
+}
+
+void launch_rebuild(const PairArgs& a, int warps, cudaStream_t s) {
+    if (warps <= 0) return;
+    int blocks = (warps + K2_WARPS - 1) / K2_WARPS;
+    k_rebuild<<<blocks, K2_WARPS * 32, 0, s>>>(a);
+}
+
+// --------------------------------------------------------------------------------------------- stage 3
+// Exclusive scan of an int32 (or int64) count array into n+1 int64 offsets, one block.
+template <class T>
+__global__ void k_scan_counts(const T* cnt, int64_t n, int64_t* off) {
+    __shared__ int64_t warp_sums[32];
+    __shared__ int64_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t base = 0; base < n; base += blockDim.x) {
+        int64_t i = base + threadIdx.x;
+        int64_t v = i < n ? (int64_t)cnt[i] : 0;
+        int64_t x = v;
+        for (int d = 1; d < 32; d <<= 1) {
+            int64_t y = __shfl_up_sync(FULL, x, d);
+            if (lane >= d) x += y;
+        }
+        if (lane == 31) warp_sums[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int64_t s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+            for (int d = 1; d < 32; d <<= 1) {
+                int64_t y = __shfl_up_sync(FULL, s, d);
+                if (lane >= d) s += y;
+            }
+            warp_sums[lane] = s;
+        }
+        __syncthreads();
+        int64_t incl = x + (w > 0 ? warp_sums[w - 1] : 0) + carry;
+        if (i < n) off[i] = incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) off[n] = carry;
+}
+
+__global__ void k_gather(PairArgs a, const int64_t* coff, const int64_t* poff, double* cgeom, int32_t* cinfo,
+                         double* pts, int64_t* cpt_off, int32_t* pair_stats) {
+    const int lane = threadIdx.x & 31;
+    const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (p >= a.n_pairs) return;
+    const int nc = a.pair_ncontact[p];
+    const int64_t src = a.pair_stage_off[p], dst = coff[p];
+    for (int i = lane; i < 20 * nc; i += 32) cgeom[20 * dst + i] = a.cgeom_stage[20 * src + i];
+    for (int i = lane; i < 4 * nc; i += 32) cinfo[4 * dst + i] = a.cinfo_stage[4 * src + i];
+    if (a.want_pts) {
+        const int64_t np = a.pair_npts[p], ps = a.pair_pts_stage_off[p], pd = poff[p];
+        for (int64_t i = lane; i < 3 * np; i += 32) pts[3 * pd + i] = a.pts_stage[3 * ps + i];
+        if (lane == 0) {
+            int64_t run = pd;
+            for (int k = 0; k < nc; ++k) {
+                cpt_off[dst + k] = run;
+                run += a.clen_stage[src + k];
+            }
+        }
+    }
+    if (lane == 0) {
+        pair_stats[4 * p + 0] = a.pair_nseg[p];
+        pair_stats[4 * p + 1] = a.pair_ncomp[p];
+        pair_stats[4 * p + 2] = a.pair_nloop[p];
+        pair_stats[4 * p + 3] = a.pair_status[p];
+    }
+}
+
+__global__ void k_finish_cpt(const int64_t* coff, const int64_t* poff, int64_t n_pairs, int64_t* cpt_off) {
+    cpt_off[coff[n_pairs]] = poff[n_pairs];
+}
+
+void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_pts_off, double* cgeom, int32_t* cinfo,
+                   double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* scan_tmp, cudaStream_t s) {
+    (void)scan_tmp;
+    if (a.n_pairs <= 0) return;
+    k_scan_counts<int32_t><<<1, 1024, 0, s>>>(a.pair_ncontact, a.n_pairs, pair_contact_off);
+    if (a.want_pts) k_scan_counts<int64_t><<<1, 1024, 0, s>>>(a.pair_npts, a.n_pairs, pair_pts_off);
+    unsigned blocks = (unsigned)((a.n_pairs + 7) / 8);
+    k_gather<<<blocks, 256, 0, s>>>(a, pair_contact_off, pair_pts_off, cgeom, cinfo, pts, cpt_off, pair_stats);
+    if (a.want_pts) k_finish_cpt<<<1, 1, 0, s>>>(pair_contact_off, pair_pts_off, a.n_pairs, cpt_off);
+}
+
+}  // namespace zdx

@@ -1,0 +1,98 @@
+// zdx_pair.cuh -- internal interface between the pair-contact kernels (zdx_pair.cu) and the C ABI layer.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace zdx {
+
+// Pair status bits (zdx_pair_result.pair_stats[4p+3]).
+enum : int {
+    PAIR_SEG_OVERFLOW = 1,   // more segments than max_seg_per_pair
+    PAIR_EDGE_OVERFLOW = 2,  // the T-junction split produced more edges than the rebuild slot holds
+};
+// Call-wide error bits (*err).
+enum : int {
+    ERR_SEG_ARENA = 1,      // the segment arena is too small: grow it and rerun the triangle stage
+    ERR_CONTACT_STAGE = 2,  // more contacts than contact_cap
+    ERR_POINT_STAGE = 4,    // more loop points than loop_point_cap
+    ERR_PAIR = 8,           // some pair has a non-zero status
+};
+
+struct PairArgs {
+    // mesh set
+    int n_mesh;
+    const double* tris;
+    const int64_t* tri_off;
+    const double* mean_edge;
+    const double* bbox_diag;
+    // per-triangle bounding spheres (cx, cy, cz, r) in the mesh frame and per-mesh bounds (k_mesh_prep)
+    double4* tri_sph;
+    unsigned long long* mesh_R_bits;  // max over triangles of |c| + r, as the bits of a positive double
+    int* mesh_valid;                  // triangles with a plane (|e1 x e2| >= 1e-30) per mesh
+    // pairs
+    int64_t n_pairs;
+    const int32_t* pmesh;
+    const double* pose;
+    const int32_t* order;  // work item -> pair, most expensive first
+    int mode;              // 0 zdem, 1 polyline
+    int split;
+    double tol_in;
+    double k;
+    int want_pts;
+    // triangle stage (k_segments)
+    int* queue1;
+    int64_t item_begin, item_end;
+    int cap_side;
+    int cap_seg;
+    char* k1_slots;
+    size_t k1_slot_bytes;
+    double* seg;  // arena: 6 doubles per segment
+    int64_t seg_cap;
+    unsigned long long* seg_counter;
+    int64_t* pair_seg_off;
+    int32_t* pair_nseg;
+    int64_t* pair_checks;
+    int32_t* pair_status;
+    int* max_nseg;
+    unsigned long long* checks_total;
+    // rebuild stage (k_rebuild)
+    int* queue2;
+    char* k2_slots;
+    size_t k2_slot_bytes;
+    int k2_nmax;
+    int64_t k2_nslots;
+    double* cgeom_stage;  // 20 per contact
+    int32_t* cinfo_stage; // 4 per contact
+    int32_t* clen_stage;  // loop point count per contact
+    int64_t contact_cap;
+    unsigned long long* contact_counter;
+    double* pts_stage;
+    int64_t pts_cap;
+    unsigned long long* pts_counter;
+    int64_t* pair_stage_off;
+    int64_t* pair_pts_stage_off;
+    int32_t* pair_ncontact;
+    int64_t* pair_npts;
+    int32_t* pair_ncomp;
+    int32_t* pair_nloop;
+    int* err;
+};
+
+// Bytes of one rebuild slot able to hold a pair of n segments.
+size_t rebuild_slot_bytes(int n);
+// Bytes of one triangle-stage slot.
+size_t tritest_slot_bytes(int cap_side, int cap_seg);
+
+void launch_mesh_prep(const PairArgs& a, int64_t total_tris, cudaStream_t s);
+void launch_cost_order(const PairArgs& a, int32_t* order, int* buckets, cudaStream_t s);
+void launch_segments(const PairArgs& a, int grid, cudaStream_t s);
+void launch_rebuild(const PairArgs& a, int warps, cudaStream_t s);
+void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_pts_off, double* cgeom,
+                   int32_t* cinfo, double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* scan_tmp,
+                   cudaStream_t s);
+int k1_blocks_per_sm();
+int k2_warps_per_block();
+
+}  // namespace zdx

@@ -1,0 +1,226 @@
+"""ctypes binding of libzdemx.so (include/zdemx.h).
+
+The library is built in-tree (``make -C zedm-x_b200``) and loaded from ``zedm-x_b200/lib``.  There is no
+fallback: if the shared library is missing, or no CUDA device is usable, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.environ.get("ZDEMX_LIB", os.path.join(PKG_ROOT, "lib", "libzdemx.so"))
+
+ZDX_OK = 0
+ZDX_ERR_INVALID = 1
+ZDX_ERR_CUDA = 2
+ZDX_ERR_CAPACITY = 3
+ZDX_ERR_IO = 4
+ZDX_ERR_NO_DEVICE = 5
+ZDX_ERR_CONFIG = 6
+ZDX_ERR_STATE = 7
+
+MODE_ZDEM = 0
+MODE_POLYLINE = 1
+MEM_HOST = 0
+MEM_DEVICE = 1
+SCHED_BATCHED = 0
+SCHED_PLAIN = 1
+
+_dp = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+
+class PairOpts(C.Structure):
+    _fields_ = [("mode", C.c_int), ("split_contacts", C.c_int), ("tol", C.c_double), ("k", C.c_double),
+                ("mem", C.c_int), ("sched", C.c_int), ("want_loop_points", C.c_int), ("max_seg_per_pair", C.c_int)]
+
+
+class MeshSet(C.Structure):
+    _fields_ = [("n_mesh", C.c_int32), ("tris", C.c_void_p), ("tri_off", C.c_void_p), ("mean_edge", C.c_void_p),
+                ("bbox_diag", C.c_void_p)]
+
+
+class PairBatch(C.Structure):
+    _fields_ = [("n_pairs", C.c_int64), ("mesh", C.c_void_p), ("pose", C.c_void_p)]
+
+
+class PairResult(C.Structure):
+    _fields_ = [("pair_ncontact", C.c_void_p), ("pair_contact_off", C.c_void_p), ("pair_stats", C.c_void_p),
+                ("contact_cap", C.c_int64), ("contact_geom", C.c_void_p), ("contact_info", C.c_void_p),
+                ("loop_point_cap", C.c_int64), ("loop_points", C.c_void_p), ("contact_point_off", C.c_void_p),
+                ("totals", C.c_int64 * 4)]
+
+
+class ZdxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"zdemx status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libzdemx.so once (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `make -C zedm-x_b200` (or __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    L.zdx_version.restype = C.c_char_p
+    L.zdx_status_string.restype = C.c_char_p
+    L.zdx_status_string.argtypes = [C.c_int]
+    L.zdx_last_error.restype = C.c_char_p
+    L.zdx_last_error.argtypes = [C.c_void_p]
+    L.zdx_create.argtypes = [C.POINTER(C.c_void_p), C.c_int]
+    L.zdx_destroy.argtypes = [C.c_void_p]
+    L.zdx_stl_load.restype = C.c_int64
+    L.zdx_stl_load.argtypes = [C.c_char_p, _dp, C.c_int64]
+    L.zdx_mesh_build.argtypes = [_dp, C.c_int64, C.c_int, _dp, _dp]
+    L.zdx_pair_contacts.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
+                                    C.POINTER(PairResult)]
+    L.zdx_pair_timings.argtypes = [C.c_void_p, _dp, _i64p]
+    _lib = L
+    return L
+
+
+def exported_symbols() -> list[str]:
+    """Names declared in include/zdemx.h (parsed from the header)."""
+    import re
+
+    hdr = os.path.join(os.path.dirname(PKG_ROOT), "include", "zdemx.h")
+    text = open(hdr).read()
+    return sorted(set(re.findall(r"\b(zdx_[a-z0-9_]+)\s*\(", text)))
+
+
+def check(status: int, ctx=None):
+    if status != ZDX_OK:
+        msg = lib().zdx_status_string(status).decode()
+        if ctx is not None:
+            detail = lib().zdx_last_error(ctx).decode()
+            if detail:
+                msg = f"{msg}: {detail}"
+        raise ZdxError(status, msg)
+
+
+def stl_load(path: str) -> np.ndarray:
+    """load_stl (src/main.cpp:308-371; polyline.py:59-96).  Returns (n, 3, 3) float64."""
+    L = lib()
+    n = L.zdx_stl_load(path.encode(), None, 0)
+    if n < 0:
+        raise ZdxError(-n, f"cannot read STL {path}")
+    out = np.zeros((max(n, 1), 3, 3))
+    L.zdx_stl_load(path.encode(), out.ctypes.data_as(_dp), n)
+    return out[:n]
+
+
+def mesh_build(tris, center: bool = True):
+    """build_mesh (src/main.cpp:445-497).  Returns (tris_out (n,3,3), props dict)."""
+    t = np.ascontiguousarray(tris, dtype=np.float64).reshape(-1, 3, 3)
+    out = np.zeros_like(t)
+    props = np.zeros(17)
+    check(lib().zdx_mesh_build(t.ctypes.data_as(_dp), len(t), int(center), out.ctypes.data_as(_dp),
+                               props.ctypes.data_as(_dp)))
+    return out, {"volume": props[0], "center": props[1:4].copy(), "radius": props[4], "mean_edge": props[5],
+                 "bbox_diag": props[6], "inertia_unit": props[7:16].reshape(3, 3).copy(), "nvert": int(props[16]),
+                 "raw": props}
+
+
+class Context:
+    """One GPU, one stream (zdx_create)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        check(lib().zdx_create(C.byref(self._h), int(device)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().zdx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def timings(self):
+        t = np.zeros(5)
+        n = C.c_int64(0)
+        lib().zdx_pair_timings(self._h, t.ctypes.data_as(_dp), C.byref(n))
+        return {"prep": t[0], "segments": t[1], "rebuild": t[2], "gather": t[3], "total": t[4],
+                "launches": int(n.value)}
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array or a torch tensor (device mode)."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())
+
+
+def pair_contacts_raw(ctx: Context, mesh_tris, tri_off, mean_edge, bbox_diag, pair_mesh, pair_pose, *,
+                      mode=MODE_ZDEM, split=True, tol=0.0, k=1.0, want_points=False, sched=SCHED_BATCHED,
+                      contact_cap=None, point_cap=None, max_seg_per_pair=0):
+    """Host-memory batched pair call.  Returns a dict of numpy arrays (CSR over pairs)."""
+    tris = np.ascontiguousarray(mesh_tris, dtype=np.float64)
+    off = np.ascontiguousarray(tri_off, dtype=np.int64)
+    me = np.ascontiguousarray(mean_edge, dtype=np.float64)
+    bd = np.ascontiguousarray(bbox_diag, dtype=np.float64)
+    pm = np.ascontiguousarray(pair_mesh, dtype=np.int32).reshape(-1, 2)
+    pp = np.ascontiguousarray(pair_pose, dtype=np.float64).reshape(-1, 14)
+    npairs = len(pm)
+    if contact_cap is None:
+        contact_cap = max(64, 16 * npairs)
+    if point_cap is None:
+        point_cap = max(1024, 512 * npairs) if want_points else 0
+    for attempt in range(2):
+        ncontact = np.zeros(max(npairs, 1), np.int32)
+        coff = np.zeros(npairs + 1, np.int64)
+        stats = np.zeros((max(npairs, 1), 4), np.int32)
+        geom = np.zeros((max(contact_cap, 1), 20))
+        info = np.zeros((max(contact_cap, 1), 4), np.int32)
+        pts = np.zeros((max(point_cap, 1), 3))
+        cpo = np.zeros(max(contact_cap, 1) + 1, np.int64)
+        opts = PairOpts(mode, int(split), float(tol), float(k), MEM_HOST, sched, int(want_points), int(max_seg_per_pair))
+        ms = MeshSet(len(off) - 1, tris.ctypes.data, off.ctypes.data, me.ctypes.data, bd.ctypes.data)
+        pb = PairBatch(npairs, pm.ctypes.data, pp.ctypes.data)
+        res = PairResult(ncontact.ctypes.data, coff.ctypes.data, stats.ctypes.data, contact_cap, geom.ctypes.data,
+                         info.ctypes.data, point_cap, pts.ctypes.data, cpo.ctypes.data)
+        st = lib().zdx_pair_contacts(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), C.byref(res))
+        totals = list(res.totals)
+        if st == ZDX_ERR_CAPACITY and attempt == 0 and (totals[0] > contact_cap or totals[3] > point_cap):
+            contact_cap = int(totals[0]) + 16
+            point_cap = int(totals[3]) + 16 if want_points else 0
+            continue
+        check(st, ctx.handle)
+        break
+    nct = int(totals[0])
+    return {"ncontact": ncontact[:npairs], "contact_off": coff, "stats": stats[:npairs], "geom": geom[:nct],
+            "info": info[:nct], "points": pts[: int(totals[3])] if want_points else None,
+            "point_off": cpo[: nct + 1] if want_points else None, "totals": totals}
+
+
+def pair_contacts_device(ctx: Context, meshes: dict, pairs: dict, out: dict, *, mode=MODE_ZDEM, split=True, tol=0.0,
+                         k=1.0, sched=SCHED_BATCHED, mem=MEM_DEVICE):
+    """Batched pair call on caller-owned buffers given as dicts of tensors: CUDA tensors with
+    mem=MEM_DEVICE, (pinned) host tensors with mem=MEM_HOST.  Returns the totals."""
+    opts = PairOpts(mode, int(split), float(tol), float(k), mem, sched, 0, 0)
+    ms = MeshSet(int(meshes["tri_off"].numel() - 1), _ptr(meshes["tris"]), _ptr(meshes["tri_off"]),
+                 _ptr(meshes["mean_edge"]), _ptr(meshes["bbox_diag"]))
+    pb = PairBatch(int(pairs["mesh"].shape[0]), _ptr(pairs["mesh"]), _ptr(pairs["pose"]))
+    res = PairResult(_ptr(out["ncontact"]), _ptr(out["contact_off"]), _ptr(out["stats"]), int(out["geom"].shape[0]),
+                     _ptr(out["geom"]), _ptr(out["info"]), 0, 0, 0)
+    check(lib().zdx_pair_contacts(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), C.byref(res)), ctx.handle)
+    return list(res.totals)
