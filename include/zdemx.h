@@ -123,6 +123,30 @@ int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_se
  * around its stages, src/main.cpp:2061-2304). */
 int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launches);
 
+/* ---- pair contacts without device allocation ------------------------------------------------------
+ * No counterpart in the reference.  For callers that may not allocate GPU memory (a host program whose
+ * pool allocator owns the whole device, a real-time loop that cannot take the device-wide
+ * synchronisation of cudaMalloc/cudaFree): the same computation as zdx_pair_contacts, with every scratch
+ * buffer carved from one file-scope __device__ array of ZDX_NOALLOC_SCRATCH_BYTES that each GPU loading
+ * the library holds until exit.  It calls no cudaMalloc, cudaFree or other allocating routine.
+ *   - opts->mem must be ZDX_MEM_DEVICE (inputs and outputs are the caller's device buffers),
+ *     opts->sched ZDX_SCHED_BATCHED, opts->want_loop_points 0.
+ *   - Limits (larger inputs are rejected with ZDX_ERR_INVALID and a message): ZDX_NOALLOC_MAX_* below;
+ *     more than 65536 segments in one call reports ZDX_ERR_CAPACITY.
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
+ *     device current; make that first call before any stream capture.
+ *   - Every call on a device shares the one array and leaves its contents there (what must start at zero
+ *     is cleared by each call); calls that overlap on the GPU race on it. */
+#define ZDX_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define ZDX_NOALLOC_MAX_PAIRS 4096
+#define ZDX_NOALLOC_MAX_MESHES 1024
+#define ZDX_NOALLOC_MAX_TRIS 65536
+#define ZDX_NOALLOC_MAX_TRIS_PER_MESH 5120
+#define ZDX_NOALLOC_MAX_SEG_PER_PAIR 1024
+#define ZDX_NOALLOC_MAX_CONTACTS 16384
+int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* meshes,
+                              const zdx_pair_batch* pairs, zdx_pair_result* out);
+
 #ifdef __cplusplus
 }
 #endif

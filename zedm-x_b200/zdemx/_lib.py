@@ -85,6 +85,8 @@ def lib() -> C.CDLL:
     L.zdx_pair_contacts.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                     C.POINTER(PairResult)]
     L.zdx_pair_timings.argtypes = [C.c_void_p, _dp, _i64p]
+    L.zdx_pair_contacts_noalloc.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
+                                            C.POINTER(PairResult)]
     _lib = L
     return L
 
@@ -223,4 +225,19 @@ def pair_contacts_device(ctx: Context, meshes: dict, pairs: dict, out: dict, *, 
     res = PairResult(_ptr(out["ncontact"]), _ptr(out["contact_off"]), _ptr(out["stats"]), int(out["geom"].shape[0]),
                      _ptr(out["geom"]), _ptr(out["info"]), 0, 0, 0)
     check(lib().zdx_pair_contacts(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), C.byref(res)), ctx.handle)
+    return list(res.totals)
+
+
+def pair_contacts_noalloc(ctx: Context, meshes: dict, pairs: dict, out: dict, *, mode=MODE_ZDEM, split=True, tol=0.0,
+                          k=1.0):
+    """zdx_pair_contacts_noalloc on caller-owned CUDA tensors (the library allocates no device memory;
+    limits and sharing rules in include/zdemx.h).  Returns the totals."""
+    opts = PairOpts(mode, int(split), float(tol), float(k), MEM_DEVICE, SCHED_BATCHED, 0, 0)
+    ms = MeshSet(int(meshes["tri_off"].numel() - 1), _ptr(meshes["tris"]), _ptr(meshes["tri_off"]),
+                 _ptr(meshes["mean_edge"]), _ptr(meshes["bbox_diag"]))
+    pb = PairBatch(int(pairs["mesh"].shape[0]), _ptr(pairs["mesh"]), _ptr(pairs["pose"]))
+    res = PairResult(_ptr(out["ncontact"]), _ptr(out["contact_off"]), _ptr(out["stats"]), int(out["geom"].shape[0]),
+                     _ptr(out["geom"]), _ptr(out["info"]), 0, 0, 0)
+    check(lib().zdx_pair_contacts_noalloc(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), C.byref(res)),
+          ctx.handle)
     return list(res.totals)
