@@ -123,6 +123,29 @@ int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_se
  * around its stages, src/main.cpp:2061-2304). */
 int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launches);
 
+/* ---- the DEM scene (the zdem_cpu step loop) ------------------------------------------------------
+ * zdx_scene_load replaces parse_config_file (src/main.cpp:1531-1689), load_mesh_for and the particle
+ * and wall set-up (src/main.cpp:1883-2022): same grammar, defaults and acceptance rule; the scene then
+ * lives on the context's GPU.  ZDX_ERR_CONFIG with zdx_last_error() for what the reference prints.
+ * zdx_scene_step runs nsteps of the step loop body (src/main.cpp:2034-2468): broad phase, pair
+ * contacts, P-P force law with tangential history, walls, deterministic force/torque scatter,
+ * integrate_particle, history prune. */
+int zdx_scene_load(zdx_ctx* ctx, const char* config_path);
+int zdx_scene_step(zdx_ctx* ctx, int nsteps);
+/* info[12]: particles, walls, steps done, and for the last step: contacts, tri_checks, segments,
+ * components, loops (the step log's fields, src/main.cpp:2489-2499), candidate pairs, wall contacts,
+ * pair history entries, wall history entries. */
+int zdx_scene_info(zdx_ctx* ctx, int64_t* info);
+/* Host copies (any pointer may be NULL): state np x 16 = pos(3) quat(w,x,y,z) vel(3) omega(3) L(3);
+ * force/torque np x 3 and contact_count np as used by the last step's integration. */
+int zdx_scene_get_state(zdx_ctx* ctx, double* state16, double* force3, double* torque3, int32_t* contact_count);
+int zdx_scene_set_state(zdx_ctx* ctx, const double* state16);
+/* write_vtk_particles + write_particle_state_txt (src/main.cpp:1710-1870, 2470-2483) for `step`. */
+int zdx_scene_write_output(zdx_ctx* ctx, int64_t step);
+/* The whole zdem_cpu run after argument parsing (src/main.cpp:1879-2503) on CUDA device `device`:
+ * returns the process exit code (0, or 1 on a bad config / STL, as the reference). */
+int zdx_run_config(const char* config_path, int device);
+
 /* ---- pair contacts without device allocation ------------------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate GPU memory (a host program whose
  * pool allocator owns the whole device, a real-time loop that cannot take the device-wide

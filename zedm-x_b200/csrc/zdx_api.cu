@@ -429,4 +429,3 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     return ZDX_OK;
 }
 
-void zdx_ctx::scene_release() {}

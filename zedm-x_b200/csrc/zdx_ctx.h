@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+struct zdx_ctx;
+
 namespace zdx {
 
 // A grow-only device buffer.
@@ -15,7 +17,7 @@ struct DevBuf {
     void release();
 };
 
-int ctx_fail(struct ::zdx_ctx* c, int status, const char* fmt, ...);
+int ctx_fail(::zdx_ctx* c, int status, const char* fmt, ...);
 
 struct Scene;  // DEM scene (zdx_scene.cu)
 

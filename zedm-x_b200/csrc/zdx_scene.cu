@@ -1,0 +1,922 @@
+// zdx_scene.cu -- one DEM step of the zdem_cpu loop (src/main.cpp:2034-2468) on the device.
+//
+//   1. broad phase: particles binned by a hashed cell key (cell = 2 r_max), stable radix sort, bucket
+//      bounds; each particle scans the 27 neighbour cells for j > i with the reference's exact sphere
+//      test (src/main.cpp:2054-2059).  The candidate list is bit-identical to the O(N^2) loop, in (i,j)
+//      order.
+//   2. pair contacts: the batched pair kernels (zdx_pair.cu) over the candidate pairs.
+//   3. particle-particle force law and tangential history (src/main.cpp:2220-2278): one thread per
+//      pair, its contacts in loop order (all loops of a pair share one history entry).
+//   4. walls (src/main.cpp:2308-2447): one warp per (particle, wall) candidate, wall triangles in order.
+//   5. scatter (src/main.cpp:2280-2287, 2429-2433): one thread per particle adds its contributions in the
+//      reference's order -- pairs (i,p) by i, then pairs (p,j) by j, then walls -- with no atomics, so
+//      forces and torques are summed in exactly the reference's order.
+//   6. integrate_particle (src/main.cpp:1494-1510), then the history keeps this step's active keys only
+//      (src/main.cpp:2453-2468).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/zdemx.h"
+#include "zdx_math.cuh"
+#include "zdx_radix.cuh"
+#include "zdx_scene.h"
+
+namespace zdx {
+
+namespace {
+
+constexpr unsigned FULLM = 0xffffffffu;
+constexpr double PI_D = 3.141592653589793;
+
+__device__ __forceinline__ V3 L3(const double* p) { return V3{p[0], p[1], p[2]}; }
+__device__ __forceinline__ void S3(double* p, V3 v) {
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+}
+
+__device__ __forceinline__ uint32_t cell_hash(int x, int y, int z, uint32_t mask) {
+    return ((uint32_t)x * 73856093u ^ (uint32_t)y * 19349663u ^ (uint32_t)z * 83492791u) & mask;
+}
+
+// ---------------------------------------------------------------- broad phase
+__global__ void k_bp_cells(const double* state, int np, double inv_h, uint32_t mask, int4* cell, uint32_t* key,
+                           int32_t* idx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const double* s = state + 16 * (int64_t)i;
+    int cx = (int)floor(s[0] * inv_h), cy = (int)floor(s[1] * inv_h), cz = (int)floor(s[2] * inv_h);
+    cell[i] = make_int4(cx, cy, cz, 0);
+    key[i] = cell_hash(cx, cy, cz, mask);
+    idx[i] = i;
+}
+
+__global__ void k_bp_bounds(const uint32_t* key, int np, int* start, int* end) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= np) return;
+    uint32_t b = key[k];
+    if (k == 0 || key[k - 1] != b) start[b] = k;
+    if (k == np - 1 || key[k + 1] != b) end[b] = k + 1;
+}
+
+// Candidate j of particle i: j > i and the reference's sphere test passes.
+template <bool WRITE>
+__global__ void k_bp_pairs(const double* state, const double* mat, int np, const int4* cell, const int32_t* sidx,
+                           const int* start, const int* end, uint32_t mask, int32_t* cnt, const int64_t* off,
+                           int2* pairs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const double* si = state + 16 * (int64_t)i;
+    const V3 pi{si[0], si[1], si[2]};
+    const double ri = mat[17 * (int64_t)i + 2];
+    const int4 c = cell[i];
+    int n = 0;
+    int64_t o = WRITE ? off[i] : 0;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int nx = c.x + dx, ny = c.y + dy, nz = c.z + dz;
+                const uint32_t b = cell_hash(nx, ny, nz, mask);
+                for (int k = start[b]; k < end[b]; ++k) {
+                    int j = sidx[k];
+                    if (j <= i) continue;
+                    int4 cj = cell[j];
+                    if (cj.x != nx || cj.y != ny || cj.z != nz) continue;
+                    const double* sj = state + 16 * (int64_t)j;
+                    V3 d = V3{sj[0], sj[1], sj[2]} - pi;
+                    double dist2 = dot(d, d);
+                    double rsum = ri + mat[17 * (int64_t)j + 2];
+                    if (dist2 > rsum * rsum) continue;
+                    if (WRITE) pairs[o + n] = make_int2(i, j);
+                    n++;
+                }
+            }
+    if (!WRITE) {
+        cnt[i] = n;
+    } else {
+        // the reference visits j in increasing order
+        for (int a = 1; a < n; ++a) {
+            int2 v = pairs[o + a];
+            int b = a - 1;
+            while (b >= 0 && pairs[o + b].y > v.y) {
+                pairs[o + b + 1] = pairs[o + b];
+                --b;
+            }
+            pairs[o + b + 1] = v;
+        }
+    }
+}
+
+__global__ void k_pair_inputs(const int2* pairs, int64_t npair, const double* state, const int32_t* pmesh,
+                              int32_t* pr_mesh, double* pr_pose, uint32_t* tkey, int32_t* tval) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= npair) return;
+    int2 ij = pairs[p];
+    const double* a = state + 16 * (int64_t)ij.x;
+    const double* b = state + 16 * (int64_t)ij.y;
+    double* o = pr_pose + 14 * p;
+    for (int k = 0; k < 7; ++k) {
+        o[k] = a[k];
+        o[7 + k] = b[k];
+    }
+    pr_mesh[2 * p] = pmesh[ij.x];
+    pr_mesh[2 * p + 1] = pmesh[ij.y];
+    tkey[p] = (uint32_t)ij.y;
+    tval[p] = (int32_t)p;
+}
+
+__device__ int64_t find_key(const int64_t* keys, int64_t n, int64_t k) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && keys[lo] == k) ? lo : -1;
+}
+
+// ---------------------------------------------------------------- particle-particle force law
+// src/main.cpp:2220-2278 (normal damping is commented out in the reference for this law).
+__global__ void k_pp_force(const int2* pairs, int64_t npair, const int64_t* coff, const double* geom, const double* state,
+                           const double* mat, double dt, const int64_t* hkey, const double* hds, int64_t nh,
+                           double* contrib, int32_t* active, double* ds_out) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= npair) return;
+    const int64_t c0 = coff[p], c1 = coff[p + 1];
+    if (c0 == c1) {
+        active[p] = 0;
+        return;
+    }
+    const int2 ij = pairs[p];
+    const double* sa = state + 16 * (int64_t)ij.x;
+    const double* sb = state + 16 * (int64_t)ij.y;
+    const double* ma = mat + 17 * (int64_t)ij.x;
+    const double* mb = mat + 17 * (int64_t)ij.y;
+    const int64_t key = ((int64_t)ij.x << 32) | (int64_t)(uint32_t)ij.y;
+    int64_t h = find_key(hkey, nh, key);
+    V3 ds = h >= 0 ? L3(hds + 3 * h) : V3{0.0, 0.0, 0.0};
+    const V3 xa = L3(sa), xb = L3(sb);
+    for (int64_t c = c0; c < c1; ++c) {
+        const double* g = geom + 20 * c;
+        const V3 xc0 = L3(g + 6), nA = L3(g + 9);
+        const double A_n = g[12];
+        V3 rA = xc0 - xa, rB = xc0 - xb;
+        V3 vA = L3(sa + 7) + cross(L3(sa + 10), rA);
+        V3 vB = L3(sb + 7) + cross(L3(sb + 10), rB);
+        V3 vrel = vB - vA;
+        double vn = dot(vrel, nA);
+        double R1 = smax(ma[3], 1e-12), R2 = smax(mb[3], 1e-12);
+        double E1 = smax(ma[4], 1e-12), E2 = smax(mb[4], 1e-12);
+        double nu1 = ma[5], nu2 = mb[5];
+        double kn = (E1 / R1 + E2 / R2) * A_n;
+        double kt = (E1 / (2.0 * (1.0 + nu1) * R1) + E2 / (2.0 * (1.0 + nu2) * R2)) * A_n;
+        double m_eff = 1.0 / (ma[1] + mb[1]);
+        double e = smin(ma[7], mb[7]);
+        e = smin(0.9999, smax(1e-6, e));
+        double loge = log(e);
+        double ct = 2.0 * loge * sqrt(kt * m_eff) / sqrt(loge * loge + PI_D * PI_D);
+        ct = fabs(ct);
+        double deltaV = pow(A_n, 1.5);
+        double fn = kn * cbrt(deltaV);
+        if (fn < 0.0) fn = 0.0;
+        V3 fn_vec = nA * fn;
+        V3 vt = vrel - nA * vn;
+        ds = ds + vt * dt;
+        ds = ds - nA * dot(ds, nA);
+        V3 ft = ds * (-kt) + vt * (-ct);
+        double mu = smin(ma[6], mb[6]);
+        double ft_norm = norm(ft);
+        double ft_max = mu * fn;
+        if (ft_norm > ft_max && ft_norm > 1e-14) {
+            ft = ft * (ft_max / ft_norm);
+            if (kt > 1e-12) ds = ft * (-1.0 / kt);
+        }
+        V3 f = fn_vec + ft;
+        double* o = contrib + 9 * c;
+        S3(o, f);
+        S3(o + 3, cross(rA, f * -1.0));
+        S3(o + 6, cross(rB, f));
+    }
+    active[p] = 1;
+    S3(ds_out + 3 * p, ds);
+}
+
+// ---------------------------------------------------------------- walls
+__global__ void k_wall_cand(const double* state, const double* mat, int np, const double* wpose, const double* wrad,
+                            int nw, int32_t* cnt, const int64_t* off, int2* cand) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const double* s = state + 16 * (int64_t)i;
+    int n = 0;
+    for (int w = 0; w < nw; ++w) {
+        V3 d = V3{s[0], s[1], s[2]} - L3(wpose + 7 * w);
+        double dist2 = dot(d, d);
+        double rsum = mat[17 * (int64_t)i + 2] + wrad[w];
+        if (dist2 > rsum * rsum) continue;
+        if (off) cand[off[i] + n] = make_int2(i, w);
+        n++;
+    }
+    if (!off) cnt[i] = n;
+}
+
+struct V2d {
+    double x, y;
+};
+__device__ __forceinline__ double cr2(V2d a, V2d b) { return a.x * b.y - a.y * b.x; }
+__device__ __forceinline__ V2d sub2(V2d a, V2d b) { return V2d{a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ bool inside_clip(V2d p, V2d c1, V2d c2) { return cr2(sub2(c2, c1), sub2(p, c1)) >= 0.0; }
+__device__ V2d clip_isect(V2d s, V2d e, V2d c1, V2d c2) {
+    V2d dc = sub2(c1, c2), dp = sub2(s, e);
+    double n1 = cr2(c1, c2), n2 = cr2(s, e), n3 = cr2(dc, dp);
+    if (fabs(n3) < 1e-30) return s;
+    return V2d{(n1 * dp.x - n2 * dc.x) / n3, (n1 * dp.y - n2 * dc.y) / n3};
+}
+
+struct WallArgs {
+    const double* state;
+    const double* mat;
+    const int32_t* pmesh;
+    const double* mtris;
+    const int64_t* moff;
+    const double* mprops;  // me, bd per mesh (2 per mesh)
+    const double* wtris;
+    const double* wnorm;
+    const int64_t* wtri_off;
+    const double* wmat;
+    const int2* cand;
+    int64_t ncand;
+    int max_wtri;
+    double dt;
+    const int64_t* hkey;
+    const double* hds;
+    int64_t nh;
+    double* contrib;  // ncand x max_wtri x 6 (force, torque)
+    int32_t* valid;   // ncand x max_wtri
+    int32_t* active;  // ncand
+    double* ds_out;   // ncand x 3
+    double* scratch;  // per warp: section points (3 doubles each), polygons
+    int64_t scratch_pts;
+    int nwarps;
+};
+
+// compute_wall_contact (src/main.cpp:1205-1258) for one wall triangle, by one warp: lanes collect the
+// edge-plane crossings of the particle's triangles in (triangle, edge) order, lane 0 dedups, projects,
+// clips (Sutherland-Hodgman), and returns area and centroid.
+__device__ bool wall_contact_warp(const WallArgs& a, int lane, Q4 qn, V3 tpos, const double* ptris, int pnt,
+                                  const double* wt, V3 n, double tol, double* pts, double& area, V3& cp) {
+    const double d = -dot(n, L3(wt));
+    int ns = 0;
+    for (int b = 0; b < pnt; b += 32) {
+        int t = b + lane;
+        V3 q[3];
+        int c = 0;
+        V3 out[3];
+        if (t < pnt) {
+            for (int k = 0; k < 3; ++k) q[k] = qrotate_n(qn, L3(ptris + 9 * t + 3 * k)) + tpos;
+            for (int i = 0; i < 3; ++i) {
+                V3 p0 = q[i], p1 = q[(i + 1) % 3];
+                double d0 = dot(n, p0) + d, d1 = dot(n, p1) + d;
+                if (d0 * d1 < 0.0) {
+                    double tt = d0 / (d0 - d1);
+                    tt = smin(1.0, smax(0.0, tt));
+                    out[c++] = p0 + (p1 - p0) * tt;
+                }
+            }
+        }
+        int incl = c;
+        for (int s = 1; s < 32; s <<= 1) {
+            int y = __shfl_up_sync(FULLM, incl, s);
+            if (lane >= s) incl += y;
+        }
+        int pos = ns + incl - c;
+        for (int k = 0; k < c; ++k)
+            if (pos + k < a.scratch_pts) S3(pts + 3 * (pos + k), out[k]);
+        ns += __shfl_sync(FULLM, incl, 31);
+    }
+    __syncwarp();
+    bool ok = false;
+    if (lane == 0 && ns <= a.scratch_pts) {
+        // unique_points(section, tol), src/main.cpp:561-577
+        int nu = 0;
+        double tol2 = tol * tol;
+        for (int i = 0; i < ns; ++i) {
+            V3 p = L3(pts + 3 * i);
+            bool keep = true;
+            for (int k = 0; k < nu; ++k)
+                if (norm2(p - L3(pts + 3 * k)) <= tol2) {
+                    keep = false;
+                    break;
+                }
+            if (keep) S3(pts + 3 * (nu++), p);
+        }
+        if (nu >= 3) {
+            V3 bu = fabs(n.x) < 0.9 ? normalize(cross(n, V3{1.0, 0.0, 0.0})) : normalize(cross(n, V3{0.0, 1.0, 0.0}));
+            V3 bv = cross(n, bu);
+            V3 o = L3(wt);
+            // polygon buffers after the points: each clip stage at most doubles the vertex count
+            const int pcap = 8 * (int)a.scratch_pts + 16;
+            V2d* poly = reinterpret_cast<V2d*>(pts + 3 * (size_t)a.scratch_pts);
+            V2d* tmp = poly + pcap;
+            int np = nu;
+            for (int i = 0; i < nu; ++i) {
+                V3 dd = L3(pts + 3 * i) - o;
+                poly[i] = V2d{dot(dd, bu), dot(dd, bv)};
+            }
+            V2d clip[3];
+            for (int i = 0; i < 3; ++i) {
+                V3 dd = L3(wt + 3 * i) - o;
+                clip[i] = V2d{dot(dd, bu), dot(dd, bv)};
+            }
+            V2d c1 = clip[2];
+            for (int ci = 0; ci < 3; ++ci) {
+                V2d c2 = clip[ci];
+                if (np == 0) break;
+                int nin = np;
+                for (int k = 0; k < nin; ++k) tmp[k] = poly[k];
+                np = 0;
+                V2d s = tmp[nin - 1];
+                for (int k = 0; k < nin && np + 2 <= pcap; ++k) {
+                    V2d e = tmp[k];
+                    if (inside_clip(e, c1, c2)) {
+                        if (!inside_clip(s, c1, c2)) poly[np++] = clip_isect(s, e, c1, c2);
+                        poly[np++] = e;
+                    } else if (inside_clip(s, c1, c2)) {
+                        poly[np++] = clip_isect(s, e, c1, c2);
+                    }
+                    s = e;
+                }
+                c1 = c2;
+            }
+            if (np >= 3) {
+                double ar = 0.0;
+                for (int i = 0; i < np; ++i) ar += cr2(poly[i], poly[(i + 1) % np]);
+                ar = fabs(ar) * 0.5;
+                if (!(ar < tol * tol * 0.01)) {
+                    double cx = 0.0, cy = 0.0;
+                    for (int i = 0; i < np; ++i) {
+                        cx += poly[i].x;
+                        cy += poly[i].y;
+                    }
+                    double fnp = (double)np;
+                    cx = cx / fnp;
+                    cy = cy / fnp;
+                    cp = (o + bu * cx) + bv * cy;
+                    area = ar;
+                    ok = true;
+                }
+            }
+        }
+    }
+    return ok;
+}
+
+__global__ void k_walls(WallArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (warp >= a.nwarps) return;
+    double* pts = a.scratch + warp * (3 * a.scratch_pts + 4 * (8 * a.scratch_pts + 16));
+    for (int64_t k = warp; k < a.ncand; k += a.nwarps) {
+        const int2 iw = a.cand[k];
+        const int i = iw.x, w = iw.y;
+        const double* sp = a.state + 16 * (int64_t)i;
+        const double* mp = a.mat + 17 * (int64_t)i;
+        const int pm = a.pmesh[i];
+        const double* ptris = a.mtris + 9 * a.moff[pm];
+        const int pnt = (int)(a.moff[pm + 1] - a.moff[pm]);
+        double tol = a.mprops[2 * pm] > 0.0 ? (a.mprops[2 * pm] * 0.1) : (a.mprops[2 * pm + 1] * 1e-2);
+        if (tol <= 0.0) tol = 1e-6;
+        const int64_t key = ((int64_t)i << 16) | (int64_t)w;
+        int64_t h = find_key(a.hkey, a.nh, key);
+        V3 ds = h >= 0 ? L3(a.hds + 3 * h) : V3{0.0, 0.0, 0.0};
+        const Q4 qn = qnormalize(Q4{sp[3], sp[4], sp[5], sp[6]});
+        const V3 xp = L3(sp);
+        int touched = 0;
+        const int64_t t0 = a.wtri_off[w], t1 = a.wtri_off[w + 1];
+        for (int64_t t = t0; t < t1; ++t) {
+            const int slot = (int)(t - t0);
+            if (lane == 0) a.valid[k * a.max_wtri + slot] = 0;
+            const double* wt = a.wtris + 9 * t;
+            V3 w0 = L3(wt), w1 = L3(wt + 3), w2 = L3(wt + 6);
+            V3 wmn{smin3(w0.x, w1.x, w2.x), smin3(w0.y, w1.y, w2.y), smin3(w0.z, w1.z, w2.z)};
+            V3 wmx{smax3(w0.x, w1.x, w2.x), smax3(w0.y, w1.y, w2.y), smax3(w0.z, w1.z, w2.z)};
+            const double r = mp[2];
+            V3 pmn = xp - V3{r, r, r}, pmx = xp + V3{r, r, r};
+            if (pmx.x < wmn.x || pmn.x > wmx.x || pmx.y < wmn.y || pmn.y > wmx.y || pmx.z < wmn.z || pmn.z > wmx.z)
+                continue;
+            const V3 n = L3(a.wnorm + 3 * t);
+            double area = 0.0;
+            V3 cpt{0.0, 0.0, 0.0};
+            bool ok = wall_contact_warp(a, lane, qn, xp, ptris, pnt, wt, n, tol, pts, area, cpt);
+            ok = __shfl_sync(FULLM, ok ? 1 : 0, 0) != 0;
+            if (ok && lane == 0) {
+                V3 cn = n;
+                V3 to_p = xp - cpt;
+                if (dot(cn, to_p) < 0.0) cn = cn * -1.0;
+                V3 rP = cpt - xp;
+                V3 vrel = L3(sp + 7) + cross(L3(sp + 10), rP);
+                double vn = dot(vrel, cn);
+                double Rp = smax(mp[3], 1e-12), Ep = smax(mp[4], 1e-12), nup = mp[5];
+                double kn = (Ep / Rp) * area;
+                double kt = (Ep / (2.0 * (1.0 + nup) * Rp)) * area;
+                double m_eff = mp[0];
+                double e = mp[7];
+                e = smin(0.9999, smax(1e-6, e));
+                double loge = log(e);
+                double cnd = 2.0 * loge * sqrt(kn * m_eff) / sqrt(loge * loge + PI_D * PI_D);
+                double ctd = 2.0 * loge * sqrt(kt * m_eff) / sqrt(loge * loge + PI_D * PI_D);
+                cnd = fabs(cnd);
+                ctd = fabs(ctd);
+                double deltaV = pow(area, 1.5);
+                double fn = kn * cbrt(deltaV) + -cnd * vn;
+                if (fn < 0.0) fn = 0.0;
+                V3 fn_vec = cn * fn;
+                V3 vt = vrel - cn * vn;
+                ds = ds + vt * a.dt;
+                ds = ds - cn * dot(ds, cn);
+                V3 ft = ds * (-kt) + vt * (-ctd);
+                double mu = smin(mp[6], a.wmat[2 * w]);
+                double ftn = norm(ft), ftmax = mu * fn;
+                if (ftn > ftmax && ftn > 1e-14) {
+                    ft = ft * (ftmax / ftn);
+                    if (kt > 1e-12) ds = ft * (-1.0 / kt);
+                }
+                V3 f = fn_vec + ft;
+                double* o = a.contrib + 6 * (k * a.max_wtri + slot);
+                S3(o, f);
+                S3(o + 3, cross(rP, f));
+                a.valid[k * a.max_wtri + slot] = 1;
+                touched = 1;
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            a.active[k] = touched;
+            S3(a.ds_out + 3 * k, ds);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- scatter + integrate
+__global__ void k_scatter_integrate(int np, const int2* pairs, const int64_t* pstart, const int32_t* tidx,
+                                    const int64_t* tstart, const int64_t* coff, const double* pcontrib,
+                                    const int64_t* wstart, const double* wcontrib, const int32_t* wvalid, int max_wtri,
+                                    double* state, const double* mat, const double* g3, double dt, double* force,
+                                    double* torque, int32_t* count) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    V3 F{0.0, 0.0, 0.0}, T{0.0, 0.0, 0.0};
+    int cnt = 0;
+    // pairs (i, p), i < p, in increasing i: p receives +f and cross(rB, f)
+    for (int64_t k = tstart[p]; k < tstart[p + 1]; ++k) {
+        int64_t q = tidx[k];
+        for (int64_t c = coff[q]; c < coff[q + 1]; ++c) {
+            const double* o = pcontrib + 9 * c;
+            F = F + L3(o);
+            T = T + L3(o + 6);
+            cnt++;
+        }
+    }
+    // pairs (p, j), j > p, in increasing j: p receives -f and cross(rA, -f)
+    for (int64_t q = pstart[p]; q < pstart[p + 1]; ++q) {
+        for (int64_t c = coff[q]; c < coff[q + 1]; ++c) {
+            const double* o = pcontrib + 9 * c;
+            F = F - L3(o);
+            T = T + L3(o + 3);
+            cnt++;
+        }
+    }
+    // walls in (wall, triangle) order
+    for (int64_t k = wstart[p]; k < wstart[p + 1]; ++k)
+        for (int t = 0; t < max_wtri; ++t) {
+            if (!wvalid[k * max_wtri + t]) continue;
+            const double* o = wcontrib + 6 * (k * max_wtri + t);
+            F = F + L3(o);
+            T = T + L3(o + 3);
+            cnt++;
+        }
+    S3(force + 3 * p, F);
+    S3(torque + 3 * p, T);
+    count[p] = cnt;
+    // integrate_particle, src/main.cpp:1494-1510
+    double* s = state + 16 * (int64_t)p;
+    const double* m = mat + 17 * (int64_t)p;
+    V3 acc = F * m[1] + L3(g3);
+    V3 vel = L3(s + 7) + acc * dt;
+    V3 pos = L3(s) + vel * dt;
+    Q4 q{s[3], s[4], s[5], s[6]};
+    Q4 qn = qnormalize(q);
+    double w = qn.w, x = qn.x, y = qn.y, z = qn.z;
+    double R[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
+                   2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
+                   2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)};
+    const double* Ib = m + 8;
+    double RI[9], Iinv[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double acc2 = 0.0;
+            for (int k = 0; k < 3; ++k) acc2 += R[3 * r + k] * Ib[3 * k + c];
+            RI[3 * r + c] = acc2;
+        }
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double acc2 = 0.0;
+            for (int k = 0; k < 3; ++k) acc2 += RI[3 * r + k] * R[3 * c + k];
+            Iinv[3 * r + c] = acc2;
+        }
+    V3 L = L3(s + 13) + T * dt;
+    V3 om{Iinv[0] * L.x + Iinv[1] * L.y + Iinv[2] * L.z, Iinv[3] * L.x + Iinv[4] * L.y + Iinv[5] * L.z,
+          Iinv[6] * L.x + Iinv[7] * L.y + Iinv[8] * L.z};
+    Q4 qd = qmul(Q4{0.0, om.x, om.y, om.z}, q);
+    q.w += 0.5 * qd.w * dt;
+    q.x += 0.5 * qd.x * dt;
+    q.y += 0.5 * qd.y * dt;
+    q.z += 0.5 * qd.z * dt;
+    q = qnormalize(q);
+    S3(s, pos);
+    s[3] = q.w;
+    s[4] = q.x;
+    s[5] = q.y;
+    s[6] = q.z;
+    S3(s + 7, vel);
+    S3(s + 10, om);
+    S3(s + 13, L);
+}
+
+__global__ void k_range_bounds(const int2* pairs, int64_t npair, int np, int64_t* pstart) {
+    // pstart[i] = first pair with first index >= i (pairs sorted by i)
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > np) return;
+    int64_t lo = 0, hi = npair;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (pairs[mid].x < i) lo = mid + 1;
+        else hi = mid;
+    }
+    pstart[i] = lo;
+}
+
+__global__ void k_key_bounds(const uint32_t* keys, int64_t n, int np, int64_t* start) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > np) return;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)keys[mid] < i) lo = mid + 1;
+        else hi = mid;
+    }
+    start[i] = lo;
+}
+
+// history compaction: keep active entries in order
+__global__ void k_hist_write(const int32_t* active, const int64_t* pos, int64_t n, const int2* items, int shift,
+                             const double* ds, int64_t* key_out, double* ds_out) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= n || !active[k]) return;
+    int64_t o = pos[k];
+    int2 it = items[k];
+    key_out[o] = shift == 32 ? (((int64_t)it.x << 32) | (int64_t)(uint32_t)it.y) : (((int64_t)it.x << 16) | (int64_t)it.y);
+    ds_out[3 * o] = ds[3 * k];
+    ds_out[3 * o + 1] = ds[3 * k + 1];
+    ds_out[3 * o + 2] = ds[3 * k + 2];
+}
+
+__global__ void k_count_valid(const int32_t* v, int64_t n, unsigned long long* out) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int c = (k < n && v[k]) ? 1 : 0;
+    c = __reduce_add_sync(FULLM, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
+
+template <class T>
+T* as(DevBuf& b) {
+    return static_cast<T*>(b.p);
+}
+
+unsigned grid(int64_t n, int b = 256) { return (unsigned)std::max<int64_t>(1, (n + b - 1) / b); }
+
+}  // namespace
+
+#define CKS(call)                                                                                     \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return ctx_fail(ctx, ZDX_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                            __FILE__, __LINE__);                                                      \
+    } while (0)
+
+int scene_upload(zdx_ctx* ctx, Scene& s) {
+    cudaStream_t st = ctx->stream;
+    auto up = [&](DevBuf& b, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = b.ensure(std::max<size_t>(bytes, 16));
+        if (e != cudaSuccess) return e;
+        if (bytes) return cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st);
+        return cudaSuccess;
+    };
+    const int nm = (int)s.mesh_off.size() - 1;
+    std::vector<double> me(nm), bd(nm), mpr(2 * (size_t)nm), wrad(s.nw);
+    for (int m = 0; m < nm; ++m) {
+        me[m] = s.mesh_props[17 * (size_t)m + 5];
+        bd[m] = s.mesh_props[17 * (size_t)m + 6];
+        mpr[2 * m] = me[m];
+        mpr[2 * m + 1] = bd[m];
+    }
+    for (int w = 0; w < s.nw; ++w) wrad[w] = s.mesh_props[17 * (size_t)s.wmesh[w] + 4];
+    CKS(up(s.d_state, s.state.data(), sizeof(double) * s.state.size()));
+    CKS(up(s.d_mat, s.mat.data(), sizeof(double) * s.mat.size()));
+    CKS(up(s.d_pmesh, s.pmesh.data(), sizeof(int32_t) * s.pmesh.size()));
+    CKS(up(s.d_mtris, s.mesh_tris.data(), sizeof(double) * s.mesh_tris.size()));
+    CKS(up(s.d_moff, s.mesh_off.data(), sizeof(int64_t) * s.mesh_off.size()));
+    CKS(up(s.d_mme, me.data(), sizeof(double) * me.size()));
+    CKS(up(s.d_mbd, bd.data(), sizeof(double) * bd.size()));
+    CKS(up(s.d_mrad, mpr.data(), sizeof(double) * mpr.size()));
+    CKS(up(s.d_wtris, s.wtris.data(), sizeof(double) * s.wtris.size()));
+    CKS(up(s.d_wnorm, s.wnormals.data(), sizeof(double) * s.wnormals.size()));
+    CKS(up(s.d_wtri_off, s.wtri_off.data(), sizeof(int64_t) * s.wtri_off.size()));
+    CKS(up(s.d_wpose, s.wpose.data(), sizeof(double) * s.wpose.size()));
+    CKS(up(s.d_wmat, s.wmat.data(), sizeof(double) * s.wmat.size()));
+    CKS(up(s.d_wrad, wrad.data(), sizeof(double) * wrad.size()));
+    CKS(s.d_force.ensure(sizeof(double) * 3 * std::max(s.np, 1)));
+    CKS(s.d_torque.ensure(sizeof(double) * 3 * std::max(s.np, 1)));
+    CKS(s.d_count.ensure(sizeof(int32_t) * std::max(s.np, 1)));
+    s.nhist = s.nwhist = 0;
+    CKS(s.d_hist_key.ensure(16));
+    CKS(s.d_hist_ds.ensure(16));
+    CKS(s.d_whist_key.ensure(16));
+    CKS(s.d_whist_ds.ensure(16));
+    CKS(cudaStreamSynchronize(st));
+    return ZDX_OK;
+}
+
+int scene_download(zdx_ctx* ctx, Scene& s) {
+    cudaStream_t st = ctx->stream;
+    if (s.np) {
+        CKS(cudaMemcpyAsync(s.state.data(), s.d_state.p, sizeof(double) * s.state.size(), cudaMemcpyDeviceToHost, st));
+        if (s.have_forces) {
+            CKS(cudaMemcpyAsync(s.force.data(), s.d_force.p, sizeof(double) * s.force.size(), cudaMemcpyDeviceToHost, st));
+            CKS(cudaMemcpyAsync(s.torque.data(), s.d_torque.p, sizeof(double) * s.torque.size(), cudaMemcpyDeviceToHost, st));
+            CKS(cudaMemcpyAsync(s.contact_count.data(), s.d_count.p, sizeof(int32_t) * s.np, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    CKS(cudaStreamSynchronize(st));
+    s.host_dirty = false;
+    return ZDX_OK;
+}
+
+int scene_step(zdx_ctx* ctx, Scene& s) {
+    cudaStream_t st = ctx->stream;
+    const int np = s.np;
+    StepStats stats;
+    auto t_step0 = std::chrono::steady_clock::now();
+    double* state = as<double>(s.d_state);
+    const double* mat = as<double>(s.d_mat);
+
+    // ---- 1. broad phase
+    double rmax = 0.0;
+    for (int i = 0; i < np; ++i) rmax = std::max(rmax, s.mat[17 * (size_t)i + 2]);
+    double h = 2.0 * rmax * (1.0 + 1e-9);
+    if (!(h > 0.0)) h = 1.0;
+    uint32_t T = 1;
+    while (T < (uint32_t)std::max(2 * np, 2)) T <<= 1;
+    const size_t N1 = (size_t)std::max(np, 1);
+    CKS(s.bp_cell.ensure(sizeof(int4) * N1));
+    CKS(s.bp_key.ensure(sizeof(uint32_t) * N1));
+    CKS(s.bp_idx.ensure(sizeof(int32_t) * N1));
+    CKS(s.bp_key2.ensure(sizeof(uint32_t) * N1));
+    CKS(s.bp_idx2.ensure(sizeof(int32_t) * N1));
+    CKS(s.bp_start.ensure(sizeof(int) * T));
+    CKS(s.bp_end.ensure(sizeof(int) * T));
+    CKS(s.bp_cnt.ensure(sizeof(int32_t) * N1));
+    CKS(s.bp_off.ensure(sizeof(int64_t) * (N1 + 1)));
+    CKS(s.bp_tmp.ensure(std::max(radix_scratch_bytes(std::max<int64_t>(np, 1)), radix_scratch_bytes(1 << 22))));
+    int bits = 0;
+    while ((1u << bits) < T) bits++;
+    if (np > 0) {
+        k_bp_cells<<<grid(np), 256, 0, st>>>(state, np, 1.0 / h, T - 1, as<int4>(s.bp_cell), as<uint32_t>(s.bp_key),
+                                             as<int32_t>(s.bp_idx));
+        CKS(radix_sort_u32(as<uint32_t>(s.bp_key), as<int32_t>(s.bp_idx), as<uint32_t>(s.bp_key2), as<int32_t>(s.bp_idx2),
+                           np, bits, s.bp_tmp.p, st));
+        CKS(cudaMemsetAsync(s.bp_start.p, 0, sizeof(int) * T, st));
+        CKS(cudaMemsetAsync(s.bp_end.p, 0, sizeof(int) * T, st));
+        k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(s.bp_key), np, as<int>(s.bp_start), as<int>(s.bp_end));
+        k_bp_pairs<false><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
+                                                    as<int>(s.bp_start), as<int>(s.bp_end), T - 1, as<int32_t>(s.bp_cnt),
+                                                    nullptr, nullptr);
+        CKS(scan_counts_i32(as<int32_t>(s.bp_cnt), np, as<int64_t>(s.bp_off), st));
+        ctx->launches += 5 + 3 * ((bits + 7) / 8);
+    }
+    int64_t npair = 0;
+    if (np > 0) {
+        CKS(cudaMemcpyAsync(&npair, as<int64_t>(s.bp_off) + np, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+    }
+    const size_t P1 = (size_t)std::max<int64_t>(npair, 1);
+    CKS(s.bp_pairs.ensure(sizeof(int2) * P1));
+    if (np > 0) {
+        k_bp_pairs<true><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
+                                                   as<int>(s.bp_start), as<int>(s.bp_end), T - 1, nullptr,
+                                                   as<int64_t>(s.bp_off), as<int2>(s.bp_pairs));
+        ctx->launches += 1;
+    }
+    stats.pairs = npair;
+
+    // ---- 2. pair contacts
+    CKS(s.pr_mesh.ensure(sizeof(int32_t) * 2 * P1));
+    CKS(s.pr_pose.ensure(sizeof(double) * 14 * P1));
+    CKS(s.tr_key.ensure(sizeof(uint32_t) * P1));
+    CKS(s.tr_idx.ensure(sizeof(int32_t) * P1));
+    CKS(s.tr_key2.ensure(sizeof(uint32_t) * P1));
+    CKS(s.tr_idx2.ensure(sizeof(int32_t) * P1));
+    CKS(s.tr_start.ensure(sizeof(int64_t) * (N1 + 1)));
+    CKS(s.pr_ncontact.ensure(sizeof(int32_t) * P1));
+    CKS(s.pr_coff.ensure(sizeof(int64_t) * (P1 + 1)));
+    CKS(s.pr_stats.ensure(sizeof(int32_t) * 4 * P1));
+    CKS(s.pr_active.ensure(sizeof(int32_t) * P1));
+    CKS(s.pr_ds.ensure(sizeof(double) * 3 * P1));
+    CKS(s.pr_scan.ensure(sizeof(int64_t) * (P1 + 1)));
+    CKS(s.bp_hist.ensure(sizeof(int64_t) * (N1 + 1)));
+    int64_t ncontact = 0;
+    if (npair > 0) {
+        k_pair_inputs<<<grid(npair), 256, 0, st>>>(as<int2>(s.bp_pairs), npair, state, as<int32_t>(s.d_pmesh),
+                                                   as<int32_t>(s.pr_mesh), as<double>(s.pr_pose),
+                                                   as<uint32_t>(s.tr_key), as<int32_t>(s.tr_idx));
+        int pbits = 0;
+        while ((1ll << pbits) < np) pbits++;
+        CKS(s.bp_tmp.ensure(radix_scratch_bytes(npair)));
+        CKS(radix_sort_u32(as<uint32_t>(s.tr_key), as<int32_t>(s.tr_idx), as<uint32_t>(s.tr_key2),
+                           as<int32_t>(s.tr_idx2), npair, std::max(pbits, 1), s.bp_tmp.p, st));
+        ctx->launches += 1 + 3 * ((std::max(pbits, 1) + 7) / 8);
+        if (s.contact_cap < 4 * npair + 64) s.contact_cap = 4 * npair + 64;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            CKS(s.pr_geom.ensure(sizeof(double) * 20 * (size_t)s.contact_cap));
+            CKS(s.pr_info.ensure(sizeof(int32_t) * 4 * (size_t)s.contact_cap));
+            zdx_pair_opts op{ZDX_MODE_ZDEM, s.cfg.split_contacts ? 1 : 0, 0.0, 1.0, ZDX_MEM_DEVICE, ZDX_SCHED_BATCHED, 0, 0};
+            const int nm = (int)s.mesh_off.size() - 1;
+            zdx_mesh_set ms{nm, as<double>(s.d_mtris), as<int64_t>(s.d_moff), as<double>(s.d_mme), as<double>(s.d_mbd)};
+            zdx_pair_batch pb{npair, as<int32_t>(s.pr_mesh), as<double>(s.pr_pose)};
+            zdx_pair_result r{};
+            r.pair_ncontact = as<int32_t>(s.pr_ncontact);
+            r.pair_contact_off = as<int64_t>(s.pr_coff);
+            r.pair_stats = as<int32_t>(s.pr_stats);
+            r.contact_cap = s.contact_cap;
+            r.contact_geom = as<double>(s.pr_geom);
+            r.contact_info = as<int32_t>(s.pr_info);
+            int rc = zdx_pair_contacts(ctx, &op, &ms, &pb, &r);
+            if (rc == ZDX_ERR_CAPACITY && r.totals[0] > s.contact_cap && attempt == 0) {
+                s.contact_cap = r.totals[0] + 64;
+                continue;
+            }
+            if (rc != ZDX_OK) return rc;
+            ncontact = r.totals[0];
+            stats.segments = r.totals[1];
+            stats.tri_checks = r.totals[2];
+            stats.tri_ms = ctx->pair_ms[1];
+            stats.rebuild_ms = ctx->pair_ms[2];
+            break;
+        }
+        // per-pair stats (components, raw loops) summed on the host: small
+        std::vector<int32_t> ps(4 * (size_t)npair);
+        CKS(cudaMemcpyAsync(ps.data(), s.pr_stats.p, sizeof(int32_t) * 4 * npair, cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        for (int64_t p = 0; p < npair; ++p) {
+            stats.comps += ps[4 * p + 1];
+            stats.loops += ps[4 * p + 2];
+        }
+    } else {
+        CKS(cudaMemsetAsync(s.pr_coff.p, 0, sizeof(int64_t), st));
+    }
+    CKS(s.pr_contrib.ensure(sizeof(double) * 9 * (size_t)std::max<int64_t>(ncontact, 1)));
+    k_key_bounds<<<grid(np + 1), 256, 0, st>>>(as<uint32_t>(s.tr_key), npair, np, as<int64_t>(s.tr_start));
+    k_range_bounds<<<grid(np + 1), 256, 0, st>>>(as<int2>(s.bp_pairs), npair, np, as<int64_t>(s.bp_hist));
+    ctx->launches += 2;
+
+    // ---- 3. particle-particle forces
+    if (npair > 0) {
+        k_pp_force<<<grid(npair, 128), 128, 0, st>>>(as<int2>(s.bp_pairs), npair, as<int64_t>(s.pr_coff),
+                                                     as<double>(s.pr_geom), state, mat, s.cfg.dt,
+                                                     as<int64_t>(s.d_hist_key), as<double>(s.d_hist_ds), s.nhist,
+                                                     as<double>(s.pr_contrib), as<int32_t>(s.pr_active),
+                                                     as<double>(s.pr_ds));
+        ctx->launches += 1;
+    }
+
+    // ---- 4. walls
+    int max_wtri = 1;
+    for (int w = 0; w < s.nw; ++w) max_wtri = std::max<int>(max_wtri, (int)(s.wtri_off[w + 1] - s.wtri_off[w]));
+    int64_t ncand = 0;
+    CKS(s.w_scan.ensure(sizeof(int64_t) * (N1 + 1)));
+    if (s.nw > 0 && np > 0) {
+        CKS(s.w_active.ensure(sizeof(int32_t) * N1));
+        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+                                              as<int32_t>(s.w_active), nullptr, nullptr);
+        CKS(scan_counts_i32(as<int32_t>(s.w_active), np, as<int64_t>(s.w_scan), st));
+        CKS(cudaMemcpyAsync(&ncand, as<int64_t>(s.w_scan) + np, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        CKS(s.w_pairs.ensure(sizeof(int2) * std::max<int64_t>(ncand, 1)));
+        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw, nullptr,
+                                              as<int64_t>(s.w_scan), as<int2>(s.w_pairs));
+        ctx->launches += 3;
+    } else {
+        CKS(cudaMemsetAsync(s.w_scan.p, 0, sizeof(int64_t) * (N1 + 1), st));
+    }
+    const size_t C1 = (size_t)std::max<int64_t>(ncand, 1);
+    CKS(s.w_contrib.ensure(sizeof(double) * 6 * C1 * max_wtri));
+    CKS(s.w_valid.ensure(sizeof(int32_t) * C1 * max_wtri));
+    CKS(s.w_ds.ensure(sizeof(double) * 3 * C1));
+    DevBuf& w_act = s.bp_cnt;  // reused: wall candidate active flags
+    CKS(w_act.ensure(sizeof(int32_t) * std::max(C1, N1)));
+    if (ncand > 0) {
+        int maxpt = 0;
+        for (int i = 0; i < np; ++i)
+            maxpt = std::max<int>(maxpt, (int)(s.mesh_off[s.pmesh[i] + 1] - s.mesh_off[s.pmesh[i]]));
+        int64_t spts = 3 * (int64_t)maxpt + 8;
+        int nwarps = (int)std::min<int64_t>(ncand, (int64_t)ctx->num_sms * 4);
+        size_t per_warp = sizeof(double) * (3 * spts + 4 * (8 * spts + 16));
+        CKS(s.bp_tmp.ensure(std::max(s.bp_tmp.bytes, per_warp * nwarps)));
+        CKS(cudaMemsetAsync(s.w_valid.p, 0, sizeof(int32_t) * C1 * max_wtri, st));
+        WallArgs wa{state, mat, as<int32_t>(s.d_pmesh), as<double>(s.d_mtris), as<int64_t>(s.d_moff), as<double>(s.d_mrad),
+                    as<double>(s.d_wtris), as<double>(s.d_wnorm), as<int64_t>(s.d_wtri_off), as<double>(s.d_wmat),
+                    as<int2>(s.w_pairs), ncand, max_wtri, s.cfg.dt, as<int64_t>(s.d_whist_key), as<double>(s.d_whist_ds),
+                    s.nwhist, as<double>(s.w_contrib), as<int32_t>(s.w_valid), as<int32_t>(w_act),
+                    as<double>(s.w_ds), as<double>(s.bp_tmp), spts, nwarps};
+        k_walls<<<(nwarps + 3) / 4, 128, 0, st>>>(wa);
+        ctx->launches += 1;
+        CKS(s.pr_scan.ensure(sizeof(int64_t) * (std::max(P1, C1) + 1)));
+        unsigned long long* cntd = nullptr;
+        CKS(s.bp_end.ensure(sizeof(int) * T + 16));
+        cntd = reinterpret_cast<unsigned long long*>(s.bp_end.p);
+        CKS(cudaMemsetAsync(cntd, 0, sizeof(unsigned long long), st));
+        k_count_valid<<<grid(C1 * max_wtri), 256, 0, st>>>(as<int32_t>(s.w_valid), (int64_t)C1 * max_wtri, cntd);
+        unsigned long long wc = 0;
+        CKS(cudaMemcpyAsync(&wc, cntd, sizeof(wc), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        stats.wall_contacts = (int64_t)wc;
+        ctx->launches += 1;
+    }
+
+    // ---- 5+6. scatter, integrate
+    const double g3[3] = {s.cfg.gravity[0], s.cfg.gravity[1], s.cfg.gravity[2]};
+    DevBuf& d_g = s.bp_key2;
+    CKS(d_g.ensure(std::max(d_g.bytes, sizeof(g3))));
+    CKS(cudaMemcpyAsync(d_g.p, g3, sizeof(g3), cudaMemcpyHostToDevice, st));
+    if (np > 0) {
+        k_scatter_integrate<<<grid(np, 128), 128, 0, st>>>(
+            np, as<int2>(s.bp_pairs), as<int64_t>(s.bp_hist), as<int32_t>(s.tr_idx), as<int64_t>(s.tr_start),
+            as<int64_t>(s.pr_coff), as<double>(s.pr_contrib), as<int64_t>(s.w_scan), as<double>(s.w_contrib),
+            as<int32_t>(s.w_valid), max_wtri, state, mat, as<double>(d_g), s.cfg.dt, as<double>(s.d_force),
+            as<double>(s.d_torque), as<int32_t>(s.d_count));
+        ctx->launches += 1;
+    }
+
+    // ---- history prune: this step's active keys, in order
+    if (npair > 0) {
+        CKS(scan_counts_i32(as<int32_t>(s.pr_active), npair, as<int64_t>(s.pr_scan), st));
+        int64_t nn = 0;
+        CKS(cudaMemcpyAsync(&nn, as<int64_t>(s.pr_scan) + npair, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        CKS(s.d_hist_key2.ensure(sizeof(int64_t) * std::max<int64_t>(nn, 1)));
+        CKS(s.d_hist_ds2.ensure(sizeof(double) * 3 * std::max<int64_t>(nn, 1)));
+        k_hist_write<<<grid(npair), 256, 0, st>>>(as<int32_t>(s.pr_active), as<int64_t>(s.pr_scan), npair,
+                                                  as<int2>(s.bp_pairs), 32, as<double>(s.pr_ds),
+                                                  as<int64_t>(s.d_hist_key2), as<double>(s.d_hist_ds2));
+        std::swap(s.d_hist_key, s.d_hist_key2);
+        std::swap(s.d_hist_ds, s.d_hist_ds2);
+        s.nhist = nn;
+        ctx->launches += 2;
+    } else {
+        s.nhist = 0;
+    }
+    if (ncand > 0) {
+        CKS(scan_counts_i32(as<int32_t>(w_act), ncand, as<int64_t>(s.pr_scan), st));
+        int64_t nn = 0;
+        CKS(cudaMemcpyAsync(&nn, as<int64_t>(s.pr_scan) + ncand, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        CKS(s.d_whist_key2.ensure(sizeof(int64_t) * std::max<int64_t>(nn, 1)));
+        CKS(s.d_whist_ds2.ensure(sizeof(double) * 3 * std::max<int64_t>(nn, 1)));
+        k_hist_write<<<grid(ncand), 256, 0, st>>>(as<int32_t>(w_act), as<int64_t>(s.pr_scan), ncand,
+                                                  as<int2>(s.w_pairs), 16, as<double>(s.w_ds),
+                                                  as<int64_t>(s.d_whist_key2), as<double>(s.d_whist_ds2));
+        std::swap(s.d_whist_key, s.d_whist_key2);
+        std::swap(s.d_whist_ds, s.d_whist_ds2);
+        s.nwhist = nn;
+        ctx->launches += 2;
+    } else {
+        s.nwhist = 0;
+    }
+    CKS(cudaGetLastError());
+    CKS(cudaStreamSynchronize(st));
+    stats.contacts = ncontact + stats.wall_contacts;
+    stats.step_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_step0).count();
+    s.last = stats;
+    s.have_forces = true;
+    s.host_dirty = true;
+    s.step++;
+    return ZDX_OK;
+}
+
+}  // namespace zdx

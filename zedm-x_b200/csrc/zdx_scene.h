@@ -1,0 +1,123 @@
+// zdx_scene.h -- the DEM scene: config, host set-up, device state and the step.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "zdx_ctx.h"
+
+namespace zdx {
+
+// ParticleInit / WallInit / SimConfig of src/main.cpp:238-277, 1512-1529, with the same defaults.
+struct ParticleInit {
+    std::string stl;
+    double pos[3] = {0.0, 0.0, 0.0};
+    double vel[3] = {0.0, 0.0, 0.0};
+    double omega[3] = {0.0, 0.0, 0.0};
+    double quat[4] = {1.0, 0.0, 0.0, 0.0};
+    double scale = 0.0;
+    double density = 1.0;
+    double young = 1e7;
+    double poisson = 0.25;
+    double mu = 0.5;
+    double restitution = 0.5;
+};
+struct WallInit {
+    std::string stl;
+    double pos[3] = {0.0, 0.0, 0.0};
+    double quat[4] = {1.0, 0.0, 0.0, 0.0};
+    double scale = 1.0;
+    double mu = 0.5;
+    double restitution = 0.5;
+};
+struct SimConfig {
+    int n = 2;
+    int steps = 1;
+    double dt = 1e-4;
+    double spacing = 2.5;
+    double gravity[3] = {0.0, -9.81, 0.0};
+    bool split_contacts = true;
+    bool center_mesh = true;
+    bool contact_debug = false;
+    std::string stl;
+    std::string vtk_prefix = "particles";
+    int output_interval = 1;
+    std::string output_dir = "output";
+    double v0[3] = {0.0, 0.0, 0.0};
+    double v1[3] = {0.0, 0.0, 0.0};
+    std::vector<ParticleInit> particles;
+    std::vector<WallInit> walls;
+};
+
+// parse_config_file, src/main.cpp:1531-1689 (same grammar, defaults and acceptance rule).
+bool parse_config(const std::string& path, SimConfig& cfg, std::string& err);
+
+// Per-step statistics, as the step log of src/main.cpp:2489-2499 prints them.
+struct StepStats {
+    int64_t contacts = 0, tri_checks = 0, segments = 0, comps = 0, loops = 0;
+    int64_t pairs = 0, wall_contacts = 0;
+    double tri_ms = 0, rebuild_ms = 0, step_ms = 0, output_ms = 0;
+};
+
+struct Scene {
+    SimConfig cfg;
+    std::vector<ParticleInit> inits;
+    // meshes: particle meshes, then wall meshes; 9 doubles per triangle, build_mesh props (17)
+    std::vector<double> mesh_tris;
+    std::vector<int64_t> mesh_off{0};
+    std::vector<double> mesh_props;
+    // particles: state np x 16 (pos3 quat4 vel3 omega3 L3), mat np x 17 (mass inv_mass radius
+    // equiv_radius young poisson mu restitution Ibody_inv9), mesh index
+    int np = 0;
+    std::vector<double> state, mat;
+    std::vector<int32_t> pmesh;
+    // walls: mesh, pose (7), mu/restitution, world triangles (9) and unit normals (3) per triangle
+    int nw = 0;
+    std::vector<int32_t> wmesh;
+    std::vector<double> wpose, wmat;
+    std::vector<int64_t> wtri_off{0};
+    std::vector<double> wtris, wnormals;
+    int64_t step = 0;
+    StepStats last;
+    std::vector<double> force, torque;  // host copies after a step (np x 3)
+    std::vector<int32_t> contact_count;
+    bool host_dirty = true;             // host copies out of date
+    bool have_forces = false;
+
+    // device
+    DevBuf d_state, d_mat, d_pmesh, d_mtris, d_moff, d_mme, d_mbd, d_mrad;
+    DevBuf d_wtris, d_wnorm, d_wtri_off, d_wpose, d_wmat, d_wrad;
+    DevBuf d_force, d_torque, d_count;
+    DevBuf d_hist_key, d_hist_ds, d_whist_key, d_whist_ds;   // tangential history (sorted keys)
+    DevBuf d_hist_key2, d_hist_ds2, d_whist_key2, d_whist_ds2;
+    int64_t nhist = 0, nwhist = 0;
+    // broad phase and per-step work
+    DevBuf bp_cell, bp_key, bp_idx, bp_key2, bp_idx2, bp_start, bp_end, bp_cnt, bp_off, bp_pairs, bp_hist, bp_tmp;
+    DevBuf tr_key, tr_idx, tr_key2, tr_idx2, tr_start;
+    DevBuf pr_mesh, pr_pose, pr_ncontact, pr_coff, pr_stats, pr_geom, pr_info, pr_contrib, pr_active, pr_ds, pr_scan;
+    DevBuf w_contrib, w_valid, w_active, w_ds, w_scan, w_pairs;
+    int64_t pair_cap = 0, contact_cap = 0;
+
+    void release_device() {
+        for (DevBuf* b : {&d_state, &d_mat, &d_pmesh, &d_mtris, &d_moff, &d_mme, &d_mbd, &d_mrad, &d_wtris, &d_wnorm,
+                          &d_wtri_off, &d_wpose, &d_wmat, &d_wrad, &d_force, &d_torque, &d_count, &d_hist_key,
+                          &d_hist_ds, &d_whist_key, &d_whist_ds, &d_hist_key2, &d_hist_ds2, &d_whist_key2,
+                          &d_whist_ds2, &bp_cell, &bp_key, &bp_idx, &bp_key2, &bp_idx2, &bp_start, &bp_end, &bp_cnt,
+                          &bp_off, &bp_pairs, &bp_hist, &bp_tmp, &tr_key, &tr_idx, &tr_key2, &tr_idx2, &tr_start,
+                          &pr_mesh, &pr_pose, &pr_ncontact, &pr_coff, &pr_stats, &pr_geom, &pr_info, &pr_contrib,
+                          &pr_active, &pr_ds, &pr_scan, &w_contrib, &w_valid, &w_active, &w_ds, &w_scan, &w_pairs})
+            b->release();
+    }
+};
+
+int scene_from_config(zdx_ctx* ctx, const SimConfig& cfg, Scene& s, std::string& err);
+int scene_upload(zdx_ctx* ctx, Scene& s);
+int scene_step(zdx_ctx* ctx, Scene& s);
+int scene_download(zdx_ctx* ctx, Scene& s);
+// write_vtk_particles / write_particle_state_txt, src/main.cpp:1710-1870
+bool write_vtk_particles(const std::string& path, const Scene& s);
+bool write_state_txt(const std::string& path, const Scene& s);
+
+}  // namespace zdx

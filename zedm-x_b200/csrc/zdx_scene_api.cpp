@@ -1,0 +1,161 @@
+// zdx_scene_api.cpp -- C ABI of the DEM scene and the zdem_cpu-compatible program loop.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+
+#include "../../include/zdemx.h"
+#include "zdx_scene.h"
+
+using namespace zdx;
+
+void zdx_ctx::scene_release() {
+    if (scene) {
+        scene->release_device();
+        delete scene;
+        scene = nullptr;
+    }
+}
+
+static void zdx_ctx_scene_release(zdx_ctx* ctx) {
+    if (ctx) ctx->scene_release();
+}
+
+extern "C" int zdx_scene_load(zdx_ctx* ctx, const char* config_path) {
+    if (!ctx || !config_path) return ZDX_ERR_INVALID;
+    SimConfig cfg;
+    std::string err;
+    if (!parse_config(config_path, cfg, err)) return ctx_fail(ctx, ZDX_ERR_CONFIG, "%s", err.c_str());
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "cudaSetDevice failed");
+    Scene* s = new Scene();
+    int rc = scene_from_config(ctx, cfg, *s, err);
+    if (rc) {
+        delete s;
+        return ctx_fail(ctx, rc, "%s", err.c_str());
+    }
+    rc = scene_upload(ctx, *s);
+    if (rc) {
+        s->release_device();
+        delete s;
+        return rc;
+    }
+    zdx_ctx_scene_release(ctx);
+    ctx->scene = s;
+    return ZDX_OK;
+}
+
+extern "C" int zdx_scene_step(zdx_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "cudaSetDevice failed");
+    for (int k = 0; k < nsteps; ++k) {
+        int rc = scene_step(ctx, *ctx->scene);
+        if (rc) return rc;
+    }
+    return ZDX_OK;
+}
+
+extern "C" int zdx_scene_info(zdx_ctx* ctx, int64_t* info) {
+    if (!ctx || !info) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    const Scene& s = *ctx->scene;
+    int64_t v[12] = {s.np, s.nw, s.step, s.last.contacts, s.last.tri_checks, s.last.segments, s.last.comps,
+                     s.last.loops, s.last.pairs, s.last.wall_contacts, s.nhist, s.nwhist};
+    std::memcpy(info, v, sizeof(v));
+    return ZDX_OK;
+}
+
+extern "C" int zdx_scene_get_state(zdx_ctx* ctx, double* state16, double* force3, double* torque3, int32_t* count) {
+    if (!ctx) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    Scene& s = *ctx->scene;
+    if (s.host_dirty) {
+        int rc = scene_download(ctx, s);
+        if (rc) return rc;
+    }
+    if (state16) std::memcpy(state16, s.state.data(), sizeof(double) * s.state.size());
+    if (force3) std::memcpy(force3, s.force.data(), sizeof(double) * s.force.size());
+    if (torque3) std::memcpy(torque3, s.torque.data(), sizeof(double) * s.torque.size());
+    if (count) std::memcpy(count, s.contact_count.data(), sizeof(int32_t) * s.contact_count.size());
+    return ZDX_OK;
+}
+
+extern "C" int zdx_scene_set_state(zdx_ctx* ctx, const double* state16) {
+    if (!ctx || !state16) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    Scene& s = *ctx->scene;
+    std::memcpy(s.state.data(), state16, sizeof(double) * s.state.size());
+    if (cudaMemcpy(s.d_state.p, s.state.data(), sizeof(double) * s.state.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return ctx_fail(ctx, ZDX_ERR_CUDA, "state upload failed");
+    s.host_dirty = false;
+    return ZDX_OK;
+}
+
+static std::string out_name(const Scene& s, int64_t step, const char* ext) {
+    std::ostringstream oss;
+    oss << s.cfg.vtk_prefix << "_" << std::setw(6) << std::setfill('0') << step << ext;
+    return (std::filesystem::path(s.cfg.output_dir) / oss.str()).string();
+}
+
+extern "C" int zdx_scene_write_output(zdx_ctx* ctx, int64_t step) {
+    if (!ctx) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    Scene& s = *ctx->scene;
+    if (s.host_dirty) {
+        int rc = scene_download(ctx, s);
+        if (rc) return rc;
+    }
+    std::error_code ec;
+    std::filesystem::create_directories(s.cfg.output_dir, ec);
+    bool ok = write_vtk_particles(out_name(s, step, ".vtk"), s);
+    ok = write_state_txt(out_name(s, step, ".txt"), s) && ok;
+    return ok ? ZDX_OK : ctx_fail(ctx, ZDX_ERR_IO, "could not write outputs to %s", s.cfg.output_dir.c_str());
+}
+
+// The body of zdem_cpu's main after argument parsing (src/main.cpp:1879-2503): load, then per step the
+// device step, outputs every output_interval steps and the same log line.
+extern "C" int zdx_run_config(const char* config_path, int device) {
+    if (!config_path) return 1;
+    zdx_ctx* ctx = nullptr;
+    int rc = zdx_create(&ctx, device);
+    if (rc) {
+        std::cerr << "zdem_gpu: " << zdx_status_string(rc) << "\n";
+        return 1;
+    }
+    rc = zdx_scene_load(ctx, config_path);
+    if (rc) {
+        std::string msg = zdx_last_error(ctx);
+        if (!msg.empty()) std::cerr << msg << "\n";
+        zdx_destroy(ctx);
+        return 1;
+    }
+    Scene& s = *ctx->scene;
+    std::error_code ec;
+    std::filesystem::create_directories(s.cfg.output_dir, ec);
+    for (int step = 0; step < s.cfg.steps; ++step) {
+        auto t0 = std::chrono::steady_clock::now();
+        rc = scene_step(ctx, s);
+        if (rc) {
+            std::cerr << "zdem_gpu: step " << step << ": " << zdx_last_error(ctx) << "\n";
+            zdx_destroy(ctx);
+            return 1;
+        }
+        if (step % s.cfg.output_interval == 0) {
+            auto to = std::chrono::steady_clock::now();
+            zdx_scene_write_output(ctx, step);
+            double out_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - to).count();
+            double step_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            std::cout << "step=" << step << " contacts=" << s.last.contacts << " step_ms=" << (long long)step_ms
+                      << " tri_ms=" << (long long)s.last.tri_ms << " rebuild_ms=" << (long long)s.last.rebuild_ms
+                      << " output_ms=" << (long long)out_ms << " tri_checks=" << s.last.tri_checks
+                      << " segments=" << s.last.segments << " comps=" << s.last.comps << " loops=" << s.last.loops
+                      << "\n";
+        }
+    }
+    std::cout << "done\n";
+    zdx_destroy(ctx);
+    return 0;
+}

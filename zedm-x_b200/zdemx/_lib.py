@@ -85,6 +85,13 @@ def lib() -> C.CDLL:
     L.zdx_pair_contacts.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                     C.POINTER(PairResult)]
     L.zdx_pair_timings.argtypes = [C.c_void_p, _dp, _i64p]
+    L.zdx_scene_load.argtypes = [C.c_void_p, C.c_char_p]
+    L.zdx_scene_step.argtypes = [C.c_void_p, C.c_int]
+    L.zdx_scene_info.argtypes = [C.c_void_p, _i64p]
+    L.zdx_scene_get_state.argtypes = [C.c_void_p, _dp, _dp, _dp, _i32p]
+    L.zdx_scene_set_state.argtypes = [C.c_void_p, _dp]
+    L.zdx_scene_write_output.argtypes = [C.c_void_p, C.c_int64]
+    L.zdx_run_config.argtypes = [C.c_char_p, C.c_int]
     L.zdx_pair_contacts_noalloc.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                             C.POINTER(PairResult)]
     _lib = L

@@ -1,0 +1,55 @@
+"""The DEM scene of zdem_cpu on the GPU: load a config (same grammar), step, read the state back.
+
+    sc = Scene("config.txt")      # parse_config_file + particle/wall set-up (src/main.cpp:1531-2022)
+    sc.step(100)                   # 100 iterations of the step loop body (src/main.cpp:2034-2468)
+    st = sc.state()                # (np, 16): pos quat(w,x,y,z) vel omega L
+    sc.info()                      # the step log's counters for the last step
+    sc.write_output(step)          # the particle VTK and state txt files (src/main.cpp:1710-1870)
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+INFO_KEYS = ("particles", "walls", "steps", "contacts", "tri_checks", "segments", "comps", "loops", "pairs",
+             "wall_contacts", "history", "wall_history")
+
+
+class Scene:
+    def __init__(self, config_path: str, ctx: _lib.Context | None = None, device: int = 0):
+        self.ctx = ctx or _lib.Context(device)
+        _lib.check(_lib.lib().zdx_scene_load(self.ctx.handle, config_path.encode()), self.ctx.handle)
+        self.n = self.info()["particles"]
+
+    def step(self, n: int = 1):
+        _lib.check(_lib.lib().zdx_scene_step(self.ctx.handle, int(n)), self.ctx.handle)
+
+    def info(self) -> dict:
+        v = np.zeros(12, np.int64)
+        _lib.check(_lib.lib().zdx_scene_info(self.ctx.handle, v.ctypes.data_as(_lib._i64p)), self.ctx.handle)
+        return dict(zip(INFO_KEYS, (int(x) for x in v)))
+
+    def state(self):
+        st = np.zeros((self.n, 16))
+        f = np.zeros((self.n, 3))
+        t = np.zeros((self.n, 3))
+        c = np.zeros(self.n, np.int32)
+        _lib.check(_lib.lib().zdx_scene_get_state(self.ctx.handle, st.ctypes.data_as(_lib._dp), f.ctypes.data_as(_lib._dp),
+                                                  t.ctypes.data_as(_lib._dp), c.ctypes.data_as(_lib._i32p)),
+                   self.ctx.handle)
+        return st, f, t, c
+
+    def set_state(self, st):
+        st = np.ascontiguousarray(st, dtype=np.float64)
+        _lib.check(_lib.lib().zdx_scene_set_state(self.ctx.handle, st.ctypes.data_as(_lib._dp)), self.ctx.handle)
+
+    def write_output(self, step: int):
+        _lib.check(_lib.lib().zdx_scene_write_output(self.ctx.handle, int(step)), self.ctx.handle)
+
+
+def run_config(config_path: str, device: int = 0) -> int:
+    """zdem_cpu's whole run (outputs and log line included); returns the exit code."""
+    return _lib.lib().zdx_run_config(config_path.encode(), int(device))
