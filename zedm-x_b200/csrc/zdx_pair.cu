@@ -28,6 +28,10 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int K1_THREADS = 256;
 constexpr int K1_ITER = 8;
 constexpr int K1_QCAP = K1_THREADS * K1_ITER;
+constexpr int K1_HCAP = 2048;  // B survivors handled by the hierarchical test (shared memory)
+constexpr size_t K1_DSMEM = sizeof(float) * 6 * K1_HCAP + sizeof(uint32_t) * K1_HCAP + sizeof(int) * K1_HCAP +
+                            sizeof(float) * 6 * (K1_HCAP / 32) + sizeof(int2) * 64 * (K1_THREADS / 32);
+static_assert(sizeof(int2) * K1_QCAP <= (sizeof(uint32_t) + sizeof(int)) * K1_HCAP, "flat queue must fit the alias");
 constexpr int K2_WARPS = 4;
 
 int k1_blocks_per_sm() { return 2; }
@@ -146,13 +150,62 @@ __host__ __device__ inline size_t carve_k1(char* base, int cap, int cap_seg, K1S
 
 size_t tritest_slot_bytes(int cap_side, int cap_seg) { return carve_k1(nullptr, cap_side, cap_seg, nullptr); }
 
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+    v &= 1023u;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+// 30-bit Morton code of a point already scaled to [0, 1024) per axis (clamped).
+__device__ __forceinline__ uint32_t morton3(double x, double y, double z) {
+    auto q = [](double t) -> uint32_t { return t <= 0.0 ? 0u : (t >= 1023.0 ? 1023u : (uint32_t)t); };
+    return (expand10(q(x)) << 2) | (expand10(q(y)) << 1) | expand10(q(z));
+}
+__host__ __device__ inline int next_pow2(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// tri_tri_intersection_segment on one queued (A survivor, B survivor) entry; the segment and its
+// (ta, tb) key go to the CTA's segment list.
+__device__ __forceinline__ void eval_entry(const PairArgs& a, const K1Slot& S, const K1Side& SA, const K1Side& SB,
+                                           int cap, int2 e, int* nseg) {
+    V3 TA[3], TB[3];
+    for (int k = 0; k < 3; ++k) {
+        TA[k] = V3{SA.tri[(3 * k) * cap + e.x], SA.tri[(3 * k + 1) * cap + e.x], SA.tri[(3 * k + 2) * cap + e.x]};
+        TB[k] = V3{SB.tri[(3 * k) * cap + e.y], SB.tri[(3 * k + 1) * cap + e.y], SB.tri[(3 * k + 2) * cap + e.y]};
+    }
+    V3 na{SA.pl[e.x], SA.pl[cap + e.x], SA.pl[2 * cap + e.x]};
+    V3 nb{SB.pl[e.y], SB.pl[cap + e.y], SB.pl[2 * cap + e.y]};
+    V3 o0, o1;
+    if (tri_tri(TA, na, SA.pl[3 * cap + e.x], TB, nb, SB.pl[3 * cap + e.y], o0, o1)) {
+        int si = atomicAdd(nseg, 1);
+        if (si < a.cap_seg) {
+            st3(S.seg + 6 * si, o0);
+            st3(S.seg + 6 * si + 3, o1);
+            S.key[si] = ((uint64_t)(uint32_t)SA.id[e.x] << 32) | (uint64_t)(uint32_t)SB.id[e.y];
+        }
+    }
+}
+
 __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     __shared__ int sh_item;
     __shared__ int sh_n[2];
     __shared__ int sh_nq;
     __shared__ int sh_nseg;
     __shared__ unsigned long long sh_base;
-    __shared__ int2 sh_q[K1_QCAP];
+    extern __shared__ __align__(16) unsigned char k1_dsm[];
+    // dynamic shared memory: float boxes | keys | values (the flat path's queue aliases keys+values)
+    //                        | group boxes | per-warp overlap queues
+    float* sm_box = reinterpret_cast<float*>(k1_dsm);
+    uint32_t* sm_key = reinterpret_cast<uint32_t*>(sm_box + 6 * K1_HCAP);
+    int* sm_val = reinterpret_cast<int*>(sm_key + K1_HCAP);
+    int2* sh_q = reinterpret_cast<int2*>(sm_key);
+    float* sm_gbox = reinterpret_cast<float*>(sm_val + K1_HCAP);
+    int2* sm_wq = reinterpret_cast<int2*>(sm_gbox + 6 * (K1_HCAP / 32));
     const int tid = threadIdx.x;
     K1Slot S;
     carve_k1(a.k1_slots + (size_t)blockIdx.x * a.k1_slot_bytes, a.cap_side, a.cap_seg, &S);
@@ -229,58 +282,154 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         const int64_t total = (int64_t)nA * nB;
         const K1Side& SA = S.side[0];
         const K1Side& SB = S.side[1];
-        int ia = 0, ib = 0, dA = 0, dB = 0;
-        if (nB > 0) {
-            ia = tid / nB;
-            ib = tid % nB;
-            dA = K1_THREADS / nB;
-            dB = K1_THREADS % nB;
-        }
-        for (int64_t base = 0; base < total; base += K1_QCAP) {
-#pragma unroll 1
-            for (int it = 0; it < K1_ITER; ++it) {
-                int64_t kk = base + (int64_t)it * K1_THREADS + tid;
-                if (kk < total) {
-                    // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
-                    bool sep = SA.box[3 * cap + ia] < SB.box[0 * cap + ib] || SA.box[0 * cap + ia] > SB.box[3 * cap + ib] ||
-                               SA.box[4 * cap + ia] < SB.box[1 * cap + ib] || SA.box[1 * cap + ia] > SB.box[4 * cap + ib] ||
-                               SA.box[5 * cap + ia] < SB.box[2 * cap + ib] || SA.box[2 * cap + ia] > SB.box[5 * cap + ib];
-                    if (!sep) {
-                        int qi = atomicAdd(&sh_nq, 1);
-                        sh_q[qi] = make_int2(ia, ib);
-                    }
-                }
-                ib += dB;
-                ia += dA;
-                if (ib >= nB) {
-                    ib -= nB;
-                    ia++;
+        if (nA > 0 && nB > 0 && nB <= K1_HCAP) {
+            // ---- hierarchical test: B's survivors in Morton order, outward-rounded float AABBs and
+            // 32-triangle group boxes in shared memory; one warp per A triangle rejects whole groups
+            // first.  A float reject is exact (the float box contains the double one); every float
+            // overlap is re-tested with the reference's strict double compare.
+            const int N2 = next_pow2(nB);
+            const double Rb = R[1] + pad;
+            const V3 lo = tpos[1] - V3{Rb, Rb, Rb};
+            const double sc = 1024.0 / (2.0 * Rb);
+            for (int i = tid; i < N2; i += K1_THREADS) {
+                if (i < nB) {
+                    V3 c{(SB.tri[i] + SB.tri[3 * cap + i] + SB.tri[6 * cap + i]),
+                         (SB.tri[cap + i] + SB.tri[4 * cap + i] + SB.tri[7 * cap + i]),
+                         (SB.tri[2 * cap + i] + SB.tri[5 * cap + i] + SB.tri[8 * cap + i])};
+                    c = c * (1.0 / 3.0);
+                    sm_key[i] = morton3((c.x - lo.x) * sc, (c.y - lo.y) * sc, (c.z - lo.z) * sc);
+                    sm_val[i] = i;
+                } else {
+                    sm_key[i] = 0xffffffffu;
+                    sm_val[i] = -1;
                 }
             }
             __syncthreads();
-            const int nq = sh_nq;
-            for (int qi = tid; qi < nq; qi += K1_THREADS) {
-                int2 e = sh_q[qi];
-                V3 TA[3], TB[3];
-                for (int k = 0; k < 3; ++k) {
-                    TA[k] = V3{SA.tri[(3 * k) * cap + e.x], SA.tri[(3 * k + 1) * cap + e.x], SA.tri[(3 * k + 2) * cap + e.x]};
-                    TB[k] = V3{SB.tri[(3 * k) * cap + e.y], SB.tri[(3 * k + 1) * cap + e.y], SB.tri[(3 * k + 2) * cap + e.y]};
+            for (int kk2 = 2; kk2 <= N2; kk2 <<= 1)
+                for (int j = kk2 >> 1; j > 0; j >>= 1) {
+                    for (int i = tid; i < N2; i += K1_THREADS) {
+                        int ixj = i ^ j;
+                        if (ixj > i) {
+                            bool up = (i & kk2) == 0;
+                            uint32_t ki = sm_key[i], kj = sm_key[ixj];
+                            if ((ki > kj) == up) {
+                                sm_key[i] = kj;
+                                sm_key[ixj] = ki;
+                                int vi = sm_val[i];
+                                sm_val[i] = sm_val[ixj];
+                                sm_val[ixj] = vi;
+                            }
+                        }
+                    }
+                    __syncthreads();
                 }
-                V3 na{SA.pl[e.x], SA.pl[cap + e.x], SA.pl[2 * cap + e.x]};
-                V3 nb{SB.pl[e.y], SB.pl[cap + e.y], SB.pl[2 * cap + e.y]};
-                V3 o0, o1;
-                if (tri_tri(TA, na, SA.pl[3 * cap + e.x], TB, nb, SB.pl[3 * cap + e.y], o0, o1)) {
-                    int si = atomicAdd(&sh_nseg, 1);
-                    if (si < a.cap_seg) {
-                        st3(S.seg + 6 * si, o0);
-                        st3(S.seg + 6 * si + 3, o1);
-                        S.key[si] = ((uint64_t)(uint32_t)SA.id[e.x] << 32) | (uint64_t)(uint32_t)SB.id[e.y];
+            for (int m = tid; m < nB; m += K1_THREADS) {
+                int ib = sm_val[m];
+                for (int k = 0; k < 3; ++k) sm_box[k * K1_HCAP + m] = __double2float_rd(SB.box[k * cap + ib]);
+                for (int k = 3; k < 6; ++k) sm_box[k * K1_HCAP + m] = __double2float_ru(SB.box[k * cap + ib]);
+            }
+            __syncthreads();
+            const int ng = (nB + 31) >> 5;
+            const int lane = tid & 31, warp = tid >> 5;
+            for (int g = warp; g < ng; g += K1_THREADS / 32) {
+                int m = g * 32 + lane;
+                float v[6];
+                for (int k = 0; k < 3; ++k) v[k] = m < nB ? sm_box[k * K1_HCAP + m] : __int_as_float(0x7f800000);
+                for (int k = 3; k < 6; ++k) v[k] = m < nB ? sm_box[k * K1_HCAP + m] : -__int_as_float(0x7f800000);
+                for (int o = 16; o > 0; o >>= 1) {
+                    for (int k = 0; k < 3; ++k) v[k] = fminf(v[k], __shfl_xor_sync(FULL, v[k], o));
+                    for (int k = 3; k < 6; ++k) v[k] = fmaxf(v[k], __shfl_xor_sync(FULL, v[k], o));
+                }
+                if (lane < 6) sm_gbox[lane * (K1_HCAP / 32) + g] = v[lane];
+            }
+            __syncthreads();
+            int2* wq = sm_wq + warp * 64;
+            int wq_n = 0;
+            for (int ia = warp; ia < nA; ia += K1_THREADS / 32) {
+                double da[6];
+                for (int k = 0; k < 6; ++k) da[k] = SA.box[k * cap + ia];
+                float fa[6];
+                for (int k = 0; k < 3; ++k) fa[k] = __double2float_rd(da[k]);
+                for (int k = 3; k < 6; ++k) fa[k] = __double2float_ru(da[k]);
+                for (int gb = 0; gb < ng; gb += 32) {
+                    const int g = gb + lane;
+                    bool ov = false;
+                    if (g < ng) {
+                        const float* G = sm_gbox + g;
+                        const int gs = K1_HCAP / 32;
+                        ov = !(fa[3] < G[0] || fa[0] > G[3 * gs] || fa[4] < G[gs] || fa[1] > G[4 * gs] ||
+                               fa[5] < G[2 * gs] || fa[2] > G[5 * gs]);
+                    }
+                    unsigned gbal = __ballot_sync(FULL, ov);
+                    while (gbal) {
+                        const int gg = gb + __ffs(gbal) - 1;
+                        gbal &= gbal - 1u;
+                        const int m = gg * 32 + lane;
+                        bool hit = false;
+                        int ib = 0;
+                        if (m < nB) {
+                            const float* Bm = sm_box + m;
+                            bool fov = !(fa[3] < Bm[0] || fa[0] > Bm[3 * K1_HCAP] || fa[4] < Bm[K1_HCAP] ||
+                                         fa[1] > Bm[4 * K1_HCAP] || fa[5] < Bm[2 * K1_HCAP] || fa[2] > Bm[5 * K1_HCAP]);
+                            if (fov) {
+                                ib = sm_val[m];
+                                // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
+                                hit = !(da[3] < SB.box[ib] || da[0] > SB.box[3 * cap + ib] || da[4] < SB.box[cap + ib] ||
+                                        da[1] > SB.box[4 * cap + ib] || da[5] < SB.box[2 * cap + ib] ||
+                                        da[2] > SB.box[5 * cap + ib]);
+                            }
+                        }
+                        unsigned hb = __ballot_sync(FULL, hit);
+                        if (hit) wq[wq_n + __popc(hb & ((1u << lane) - 1u))] = make_int2(ia, ib);
+                        wq_n += __popc(hb);
+                        if (wq_n >= 32) {
+                            __syncwarp();
+                            for (int q = lane; q < wq_n; q += 32) eval_entry(a, S, SA, SB, cap, wq[q], &sh_nseg);
+                            __syncwarp();
+                            wq_n = 0;
+                        }
                     }
                 }
             }
+            __syncwarp();
+            for (int q = lane; q < wq_n; q += 32) eval_entry(a, S, SA, SB, cap, wq[q], &sh_nseg);
             __syncthreads();
-            if (tid == 0) sh_nq = 0;
-            __syncthreads();
+        } else if (nB > 0) {
+            int ia = 0, ib = 0, dA = 0, dB = 0;
+            if (nB > 0) {
+                ia = tid / nB;
+                ib = tid % nB;
+                dA = K1_THREADS / nB;
+                dB = K1_THREADS % nB;
+            }
+            for (int64_t base = 0; base < total; base += K1_QCAP) {
+    #pragma unroll 1
+                for (int it = 0; it < K1_ITER; ++it) {
+                    int64_t kk = base + (int64_t)it * K1_THREADS + tid;
+                    if (kk < total) {
+                        // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
+                        bool sep = SA.box[3 * cap + ia] < SB.box[0 * cap + ib] || SA.box[0 * cap + ia] > SB.box[3 * cap + ib] ||
+                                   SA.box[4 * cap + ia] < SB.box[1 * cap + ib] || SA.box[1 * cap + ia] > SB.box[4 * cap + ib] ||
+                                   SA.box[5 * cap + ia] < SB.box[2 * cap + ib] || SA.box[2 * cap + ia] > SB.box[5 * cap + ib];
+                        if (!sep) {
+                            int qi = atomicAdd(&sh_nq, 1);
+                            sh_q[qi] = make_int2(ia, ib);
+                        }
+                    }
+                    ib += dB;
+                    ia += dA;
+                    if (ib >= nB) {
+                        ib -= nB;
+                        ia++;
+                    }
+                }
+                __syncthreads();
+                const int nq = sh_nq;
+                for (int qi = tid; qi < nq; qi += K1_THREADS) eval_entry(a, S, SA, SB, cap, sh_q[qi], &sh_nseg);
+                __syncthreads();
+                if (tid == 0) sh_nq = 0;
+                __syncthreads();
+            }
         }
         int ns = sh_nseg;
         int status = 0;
@@ -318,7 +467,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
 
 void launch_segments(const PairArgs& a, int grid, cudaStream_t s) {
     if (grid <= 0) return;
-    k_segments<<<grid, K1_THREADS, 0, s>>>(a);
+    // per device and cheap: set it on every launch
+    cudaFuncSetAttribute(k_segments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+    k_segments<<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
 }
 
 // --------------------------------------------------------------------------------------------- stage 2
