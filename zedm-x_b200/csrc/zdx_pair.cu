@@ -661,21 +661,23 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                         bool el = false;
                         int best = 1 << 30;
                         if (j < n && j != i && !B.visited[j]) {
-                            // first visit of j in the reference's hash-grid walk: smallest
-                            // r*27 + neighbour-cell rank over the rep points (p0, p1, mid)
-                            for (int r = 0; r < 3; ++r)
-                                for (int rj = 0; rj < 3; ++rj) {
-                                    I3 cj = ld_cell(B.rcell + 9 * j + 3 * rj);
-                                    int dx = cj.x - ci[r].x, dy = cj.y - ci[r].y, dz = cj.z - ci[r].z;
-                                    if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
-                                    int k = r * 27 + (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
-                                    if (k < best) best = k;
-                                }
-                            if (best != (1 << 30)) {
-                                V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
-                                bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y ||
-                                            imx.z < jmn.z || imn.z > jmx.z);
-                                if (ov && seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2) el = true;
+                            // the padded-box overlap is necessary too; test it first (cheapest reject)
+                            V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
+                            bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y ||
+                                        imx.z < jmn.z || imn.z > jmx.z);
+                            if (ov) {
+                                // first visit of j in the reference's hash-grid walk: smallest
+                                // r*27 + neighbour-cell rank over the rep points (p0, p1, mid)
+                                for (int r = 0; r < 3; ++r)
+                                    for (int rj = 0; rj < 3; ++rj) {
+                                        I3 cj = ld_cell(B.rcell + 9 * j + 3 * rj);
+                                        int dx = cj.x - ci[r].x, dy = cj.y - ci[r].y, dz = cj.z - ci[r].z;
+                                        if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+                                        int k = r * 27 + (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+                                        if (k < best) best = k;
+                                    }
+                                if (best != (1 << 30) && seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2)
+                                    el = true;
                             }
                         }
                         unsigned bal = __ballot_sync(FULL, el);
