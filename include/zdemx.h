@@ -116,6 +116,20 @@ typedef struct zdx_pair_result {
 int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* meshes,
                       const zdx_pair_batch* pairs, zdx_pair_result* out);
 
+/* Reverse mode of zdx_pair_contacts, the hand-written adjoint of the contact geometry.  No counterpart in
+ * the reference (which has no derivatives); it differentiates the same computation (src/main.cpp:499-559
+ * and 680-1052).  grad_contact holds, for every contact of the forward call on the same inputs and in
+ * its order, dL/dSn(3) and dL/dGn(3).  Outputs: grad_tris (9 per triangle of the mesh set, mesh-local
+ * corners, summed over all pairs that use the mesh) and grad_pose (12 per pair: dL/dposA(3), dL/drotA(3),
+ * dL/dposB(3), dL/drotB(3), rotations as a world-frame rotation vector applied on top of the current
+ * orientation).  Everything after Sn and Gn (|Sn|, n, xc0, force laws) is closed-form and is
+ * differentiated by the caller (zdemx.autograd does it in torch).  The forward call is re-run with the
+ * adjoint tape on.  Topology changes are not differentiable: gradients are those of the current
+ * topology. */
+int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* meshes,
+                              const zdx_pair_batch* pairs, const double* grad_contact, int64_t n_contacts,
+                              double* grad_tris, double* grad_pose);
+
 /* Device times of the last pair call, in milliseconds (CUDA events on the context stream):
  * [0] inputs in + mesh bounds + work order, [1] the triangle-test kernel, [2] the rebuild kernel,
  * [3] gather + outputs out, [4] whole call.  *launches (may be NULL) receives the number of kernels

@@ -268,6 +268,12 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     CK(ctx->seg_arena.ensure(sizeof(double) * 6 * (size_t)seg_cap));
     a.seg = as<double>(ctx->seg_arena);
     a.seg_cap = seg_cap;
+    if (ctx->tape_on) {
+        CK(ctx->t_segtri.ensure(sizeof(int32_t) * 2 * (size_t)seg_cap));
+        CK(ctx->t_segcand.ensure(2 * (size_t)seg_cap));
+        a.seg_tri = as<int32_t>(ctx->t_segtri);
+        a.seg_cand = as<uint8_t>(ctx->t_segcand);
+    }
 
     // plain form: each pair runs its two stages in its own launches, one after the other
     if (plain) {
@@ -289,6 +295,18 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     a.contact_cap = ccap;
     a.pts_stage = as<double>(ctx->pstage);
     a.pts_cap = pcap;
+    int64_t* ctape_final = nullptr;
+    if (ctx->tape_on) {
+        const int64_t tcap = 48 * std::max<int64_t>(ccap, 1) + (1 << 16);
+        CK(ctx->t_arena.ensure(sizeof(int) * (size_t)tcap));
+        CK(ctx->t_cstage.ensure(sizeof(int64_t) * (size_t)std::max<int64_t>(ccap, 1)));
+        CK(ctx->t_cfinal.ensure(sizeof(int64_t) * (size_t)std::max<int64_t>(ccap, 1)));
+        a.tape_stage = as<int>(ctx->t_arena);
+        a.tape_cap = tcap;
+        a.tape_counter = cnt + 8;
+        a.ctape_stage = as<int64_t>(ctx->t_cstage);
+        ctape_final = as<int64_t>(ctx->t_cfinal);
+    }
 
     unsigned long long hc[8];
     if (plain) {
@@ -328,6 +346,12 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
             CK(ctx->seg_arena.ensure(sizeof(double) * 6 * (size_t)need));
             a.seg = as<double>(ctx->seg_arena);
             a.seg_cap = need;
+            if (ctx->tape_on) {
+                CK(ctx->t_segtri.ensure(sizeof(int32_t) * 2 * (size_t)need));
+                CK(ctx->t_segcand.ensure(2 * (size_t)need));
+                a.seg_tri = as<int32_t>(ctx->t_segtri);
+                a.seg_cand = as<uint8_t>(ctx->t_segcand);
+            }
             CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
             CK(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
         }
@@ -355,6 +379,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     out->totals[1] = (int64_t)hc[0];
     out->totals[2] = (int64_t)hc[3];
     out->totals[3] = (int64_t)hc[2];
+    if (err & ERR_TAPE) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "adjoint tape arena too small");
     if (err & (ERR_CONTACT_STAGE | ERR_POINT_STAGE))
         return ctx_fail(ctx, ZDX_ERR_CAPACITY, "need contact_cap >= %lld and loop_point_cap >= %lld",
                         (long long)hc[1], (long long)hc[2]);
@@ -393,7 +418,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         pstats = out->pair_stats;
     }
     CK(cudaEventRecord(ctx->ev[6], st));
-    launch_gather(a, coff, poff, cg, ci, pts, cpo, pstats, nullptr, st);
+    launch_gather(a, coff, poff, cg, ci, pts, cpo, pstats, ctape_final, st);
     ctx->launches += a.want_pts ? 4 : 2;
     CK(cudaGetLastError());
     if (host) {
@@ -429,3 +454,129 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     return ZDX_OK;
 }
 
+
+// Reverse mode of zdx_pair_contacts (see include/zdemx.h).  Runs the forward call again with the adjoint
+// tape on (same inputs -> the same contacts in the same order), then the adjoint kernel.
+extern "C" int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* ms,
+                                         const zdx_pair_batch* pb, const double* grad_contact, int64_t n_contacts,
+                                         double* grad_tris, double* grad_pose) {
+    if (!ctx || !opts || !ms || !pb || (n_contacts > 0 && !grad_contact) || !grad_tris || !grad_pose)
+        return ZDX_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const bool host = opts->mem == ZDX_MEM_HOST;
+    const int64_t NP = pb->n_pairs;
+    const size_t P1 = (size_t)std::max<int64_t>(NP, 1);
+    int64_t total_tris = 0;
+    if (ms->n_mesh > 0) {
+        if (host) total_tris = ms->tri_off[ms->n_mesh];
+        else CK(cudaMemcpy(&total_tris, ms->tri_off + ms->n_mesh, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    }
+    // forward with the tape, into the context's own device buffers
+    zdx_pair_opts fo = *opts;
+    fo.want_loop_points = 1;
+    fo.sched = ZDX_SCHED_BATCHED;
+    int64_t ccap = std::max<int64_t>(n_contacts, 1);
+    const int64_t pcap = 256 * ccap + 1024;
+    CK(ctx->a_nc.ensure(sizeof(int32_t) * P1));
+    CK(ctx->a_coff.ensure(sizeof(int64_t) * (P1 + 1)));
+    CK(ctx->a_stats.ensure(sizeof(int32_t) * 4 * P1));
+    CK(ctx->a_geom.ensure(sizeof(double) * 20 * ccap));
+    CK(ctx->a_info.ensure(sizeof(int32_t) * 4 * ccap));
+    CK(ctx->a_pts.ensure(sizeof(double) * 3 * pcap));
+    CK(ctx->a_cpo.ensure(sizeof(int64_t) * (ccap + 1)));
+    zdx_pair_result r{};
+    r.pair_ncontact = as<int32_t>(ctx->a_nc);
+    r.pair_contact_off = as<int64_t>(ctx->a_coff);
+    r.pair_stats = as<int32_t>(ctx->a_stats);
+    r.contact_cap = ccap;
+    r.contact_geom = as<double>(ctx->a_geom);
+    r.contact_info = as<int32_t>(ctx->a_info);
+    r.loop_point_cap = pcap;
+    r.loop_points = as<double>(ctx->a_pts);
+    r.contact_point_off = as<int64_t>(ctx->a_cpo);
+    // in host mode the inputs are staged by the forward call; results stay on the device
+    zdx_pair_opts fwd = fo;
+    int rc;
+    if (host) {
+        // stage the inputs here so that the forward call and the adjoint read the same device copies
+        int64_t NM = ms->n_mesh;
+        CK(ctx->in_tris.ensure(sizeof(double) * 9 * (size_t)std::max<int64_t>(total_tris, 1)));
+        CK(ctx->in_off.ensure(sizeof(int64_t) * (NM + 1)));
+        CK(ctx->in_me.ensure(sizeof(double) * std::max<int64_t>(NM, 1)));
+        CK(ctx->in_bd.ensure(sizeof(double) * std::max<int64_t>(NM, 1)));
+        CK(ctx->in_pm.ensure(sizeof(int32_t) * 2 * P1));
+        CK(ctx->in_pose.ensure(sizeof(double) * 14 * P1));
+        if (total_tris) CK(cudaMemcpyAsync(ctx->in_tris.p, ms->tris, sizeof(double) * 9 * total_tris, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->in_off.p, ms->tri_off, sizeof(int64_t) * (NM + 1), cudaMemcpyHostToDevice, st));
+        if (NM) {
+            CK(cudaMemcpyAsync(ctx->in_me.p, ms->mean_edge, sizeof(double) * NM, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(ctx->in_bd.p, ms->bbox_diag, sizeof(double) * NM, cudaMemcpyHostToDevice, st));
+        }
+        if (NP) {
+            CK(cudaMemcpyAsync(ctx->in_pm.p, pb->mesh, sizeof(int32_t) * 2 * NP, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(ctx->in_pose.p, pb->pose, sizeof(double) * 14 * NP, cudaMemcpyHostToDevice, st));
+        }
+        CK(cudaStreamSynchronize(st));
+    }
+    // device copies of the mesh set and pairs used by both passes (aliases in device mode)
+    zdx_mesh_set dms = *ms;
+    zdx_pair_batch dpb = *pb;
+    if (host) {
+        dms.tris = as<double>(ctx->in_tris);
+        dms.tri_off = as<int64_t>(ctx->in_off);
+        dms.mean_edge = as<double>(ctx->in_me);
+        dms.bbox_diag = as<double>(ctx->in_bd);
+        dpb.mesh = as<int32_t>(ctx->in_pm);
+        dpb.pose = as<double>(ctx->in_pose);
+    }
+    fwd.mem = ZDX_MEM_DEVICE;
+    ctx->tape_on = true;
+    rc = zdx_pair_contacts(ctx, &fwd, &dms, &dpb, &r);
+    ctx->tape_on = false;
+    if (rc) return rc;
+    if (r.totals[0] != n_contacts)
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "grad has %lld contacts, the forward pass gives %lld", (long long)n_contacts,
+                        (long long)r.totals[0]);
+    const double* gc = grad_contact;
+    double* gt = grad_tris;
+    double* gp = grad_pose;
+    if (host) {
+        CK(ctx->a_gc.ensure(sizeof(double) * 6 * (size_t)std::max<int64_t>(n_contacts, 1)));
+        CK(ctx->a_gt.ensure(sizeof(double) * 9 * (size_t)std::max<int64_t>(total_tris, 1)));
+        CK(ctx->a_gp.ensure(sizeof(double) * 12 * P1));
+        if (n_contacts) CK(cudaMemcpyAsync(ctx->a_gc.p, grad_contact, sizeof(double) * 6 * n_contacts, cudaMemcpyHostToDevice, st));
+        gc = as<double>(ctx->a_gc);
+        gt = as<double>(ctx->a_gt);
+        gp = as<double>(ctx->a_gp);
+    }
+    CK(cudaMemsetAsync(gt, 0, sizeof(double) * 9 * (size_t)std::max<int64_t>(total_tris, 1), st));
+    CK(cudaMemsetAsync(gp, 0, sizeof(double) * 12 * P1, st));
+    AdjointArgs aa{};
+    aa.tris = dms.tris;
+    aa.tri_off = dms.tri_off;
+    aa.pmesh = dpb.mesh;
+    aa.pose = dpb.pose;
+    aa.mode = opts->mode;
+    aa.n_contacts = n_contacts;
+    aa.cinfo = as<int32_t>(ctx->a_info);
+    aa.pts = as<double>(ctx->a_pts);
+    aa.cpt_off = as<int64_t>(ctx->a_cpo);
+    aa.ctape_off = as<int64_t>(ctx->t_cfinal);
+    aa.tape = as<int>(ctx->t_arena);
+    aa.pair_seg_off = as<int64_t>(ctx->pair_i64);
+    aa.seg_tri = as<int32_t>(ctx->t_segtri);
+    aa.seg_cand = as<uint8_t>(ctx->t_segcand);
+    aa.grad_contact = gc;
+    aa.grad_tris = gt;
+    aa.grad_pose = gp;
+    launch_adjoint(aa, st);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    if (host) {
+        if (total_tris) CK(cudaMemcpyAsync(grad_tris, gt, sizeof(double) * 9 * total_tris, cudaMemcpyDeviceToHost, st));
+        if (NP) CK(cudaMemcpyAsync(grad_pose, gp, sizeof(double) * 12 * NP, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    return ZDX_OK;
+}

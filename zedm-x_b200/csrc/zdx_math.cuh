@@ -117,12 +117,16 @@ ZDX_HD bool seg_plane(V3 p0, V3 p1, V3 n, double d, V3& out) {
 }
 
 // tri_tri_intersection_segment, src/main.cpp:579-631, including unique_points(., 1e-9) (:561-577).
-ZDX_HD bool tri_tri(const V3* A, V3 nA, double dA, const V3* B, V3 nB, double dB, V3& o0, V3& o1) {
+// src0/src1 (may be null) receive which edge-plane candidate each endpoint is: side*3 + i, i.e. edge
+// (i, i+1) of A cut by B's plane (side 0) or edge (i, i+1) of B cut by A's plane (side 1).
+ZDX_HD bool tri_tri_src(const V3* A, V3 nA, double dA, const V3* B, V3 nB, double dB, V3& o0, V3& o1, int* src0,
+                        int* src1) {
     V3 tau = cross(nA, nB);
     double lt = norm(tau);
     if (lt < 1e-20) return false;
     tau = tau / lt;
     V3 u[6];
+    int us[6];
     int nu = 0;
     const double tol2 = 1e-9 * 1e-9;
 #pragma unroll 1
@@ -143,7 +147,10 @@ ZDX_HD bool tri_tri(const V3* A, V3 nA, double dA, const V3* B, V3 nB, double dB
                         break;
                     }
                 }
-                if (keep) u[nu++] = p;
+                if (keep) {
+                    us[nu] = side * 3 + i;
+                    u[nu++] = p;
+                }
             }
         }
     }
@@ -168,10 +175,18 @@ ZDX_HD bool tri_tri(const V3* A, V3 nA, double dA, const V3* B, V3 nB, double dB
         V3 t = p0;
         p0 = p1;
         p1 = t;
+        int ti = i0;
+        i0 = i1;
+        i1 = ti;
     }
     o0 = p0;
     o1 = p1;
+    if (src0) *src0 = us[i0];
+    if (src1) *src1 = us[i1];
     return true;
+}
+ZDX_HD bool tri_tri(const V3* A, V3 nA, double dA, const V3* B, V3 nB, double dB, V3& o0, V3& o1) {
+    return tri_tri_src(A, nA, dA, B, nB, dB, o0, o1, nullptr, nullptr);
 }
 
 struct I3 {

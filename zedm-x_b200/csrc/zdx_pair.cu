@@ -122,6 +122,7 @@ struct K1Slot {
     K1Side side[2];
     double* seg;    // 6 x cap_seg
     uint64_t* key;  // cap_seg
+    uint8_t* cand;  // 2 x cap_seg: candidate index of each endpoint (adjoint tape)
 };
 
 __host__ __device__ inline size_t carve_k1(char* base, int cap, int cap_seg, K1Slot* s) {
@@ -141,9 +142,11 @@ __host__ __device__ inline size_t carve_k1(char* base, int cap, int cap_seg, K1S
     }
     double* seg = (double*)take(sizeof(double) * 6 * (size_t)cap_seg);
     uint64_t* key = (uint64_t*)take(sizeof(uint64_t) * (size_t)cap_seg);
+    uint8_t* cand = (uint8_t*)take(2 * (size_t)cap_seg);
     if (s) {
         s->seg = seg;
         s->key = key;
+        s->cand = cand;
     }
     return off;
 }
@@ -181,12 +184,15 @@ __device__ __forceinline__ void eval_entry(const PairArgs& a, const K1Slot& S, c
     V3 na{SA.pl[e.x], SA.pl[cap + e.x], SA.pl[2 * cap + e.x]};
     V3 nb{SB.pl[e.y], SB.pl[cap + e.y], SB.pl[2 * cap + e.y]};
     V3 o0, o1;
-    if (tri_tri(TA, na, SA.pl[3 * cap + e.x], TB, nb, SB.pl[3 * cap + e.y], o0, o1)) {
+    int c0 = 0, c1 = 0;
+    if (tri_tri_src(TA, na, SA.pl[3 * cap + e.x], TB, nb, SB.pl[3 * cap + e.y], o0, o1, &c0, &c1)) {
         int si = atomicAdd(nseg, 1);
         if (si < a.cap_seg) {
             st3(S.seg + 6 * si, o0);
             st3(S.seg + 6 * si + 3, o1);
             S.key[si] = ((uint64_t)(uint32_t)SA.id[e.x] << 32) | (uint64_t)(uint32_t)SB.id[e.y];
+            S.cand[2 * si] = (uint8_t)c0;
+            S.cand[2 * si + 1] = (uint8_t)c1;
         }
     }
 }
@@ -448,6 +454,13 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 for (int j = 0; j < ns; ++j) r += (S.key[j] < ki);
                 double* dst = a.seg + 6 * (sbase + (unsigned long long)r);
                 for (int k = 0; k < 6; ++k) dst[k] = S.seg[6 * i + k];
+                if (a.seg_tri) {
+                    const uint64_t o = sbase + (unsigned long long)r;
+                    a.seg_tri[2 * o] = (int32_t)(ki >> 32);
+                    a.seg_tri[2 * o + 1] = (int32_t)(ki & 0xffffffffu);
+                    a.seg_cand[2 * o] = S.cand[2 * i];
+                    a.seg_cand[2 * o + 1] = S.cand[2 * i + 1];
+                }
             }
         } else if (tid == 0) {
             atomicOr(a.err, ERR_SEG_ARENA);
@@ -513,6 +526,11 @@ struct PostBufs {
     double* cgeom;
     int* cinfo;
     double* cpts;
+    int* vstart;   // snapped vertex -> its endpoints (adjoint tape)
+    int* vmem;
+    int* ltape;    // this pair's tape records
+    int* ltoff;
+    int ltcap;
     int cap2;
     int capc;
 };
@@ -570,6 +588,12 @@ __host__ __device__ inline size_t carve_post(char* base, int n, PostBufs* b) {
     t.cgeom = (double*)take(sizeof(double) * 20 * capc);
     t.cinfo = (int*)take(sizeof(int) * 4 * capc);
     t.cpts = (double*)take(sizeof(double) * 3 * C2);
+    t.vstart = (int*)take(sizeof(int) * (2 * N + 2));
+    t.vmem = (int*)take(sizeof(int) * 2 * N);
+    const size_t LT = 2 * capc + 2 * C2 + 8 * N + 16;
+    t.ltape = (int*)take(sizeof(int) * LT);
+    t.ltoff = (int*)take(sizeof(int) * (capc + 1));
+    t.ltcap = (int)LT;
     t.cap2 = cap2;
     t.capc = (int)capc;
     if (b) *b = t;
@@ -620,7 +644,7 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
     const double tol2 = h * h;
     const double area_eps = me > 0.0 ? (me * me * 1e-4) : 1e-12;
 
-    int ncomp = 0, nloops = 0, nctc = 0, npts = 0;
+    int ncomp = 0, nloops = 0, nctc = 0, npts = 0, lt_n = 0;
     if (n > 0 && !(status & PAIR_SEG_OVERFLOW)) {
         // ---- components: label_segments_by_contact_greedy, src/main.cpp:804-898
         if (a.split) {
@@ -797,6 +821,17 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     } else {
                         st3(B.V + 3 * v, ld3(B.V + 3 * v) + pt);
                         B.cnt[v] += 1;
+                    }
+                }
+                if (a.tape_stage) {
+                    B.vstart[0] = 0;
+                    for (int v = 0; v < nv; ++v) {
+                        B.vstart[v + 1] = B.vstart[v] + B.cnt[v];
+                        B.afill[v] = 0;
+                    }
+                    for (int i = 0; i < np; ++i) {
+                        int v = B.rootv[B.root[i]];
+                        B.vmem[B.vstart[v] + B.afill[v]++] = i;
                     }
                 }
                 for (int s = 0; s < m; ++s) {
@@ -1042,24 +1077,60 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     if (a.want_pts) {
                         for (int q = 0; q < len && npts < B.cap2; ++q) st3(B.cpts + 3 * (npts++), ld3(B.V + 3 * lv[q]));
                     }
+                    if (a.tape_stage) {
+                        // [L, member offsets (L+1), members as 2*segment + end]
+                        int need = 2 + len;
+                        for (int q = 0; q < len; ++q) need += B.vstart[lv[q] + 1] - B.vstart[lv[q]];
+                        if (lt_n + need > B.ltcap) {
+                            status |= PAIR_TAPE_OVERFLOW;
+                        } else {
+                            B.ltoff[nctc] = lt_n;
+                            int* r = B.ltape + lt_n;
+                            r[0] = len;
+                            int mo = 0;
+                            for (int q = 0; q < len; ++q) {
+                                r[1 + q] = mo;
+                                const int v = lv[q];
+                                for (int x = B.vstart[v]; x < B.vstart[v + 1]; ++x) {
+                                    const int ep = B.vmem[x];
+                                    r[2 + len + mo++] = 2 * idx[ep >> 1] + (ep & 1);
+                                }
+                            }
+                            r[1 + len] = mo;
+                            lt_n += need;
+                        }
+                    }
                     nctc++;
                 }
             }
             nloops = __shfl_sync(FULL, nloops, 0);
             nctc = __shfl_sync(FULL, nctc, 0);
+            lt_n = __shfl_sync(FULL, lt_n, 0);
             npts = __shfl_sync(FULL, npts, 0);
             status = __shfl_sync(FULL, status, 0);
             __syncwarp();
         }
     }
     // ---- publish this pair's contacts
-    unsigned long long cbase = 0, pbase = 0;
+    unsigned long long cbase = 0, pbase = 0, tbase = 0;
     if (lane == 0) {
         cbase = atomicAdd(a.contact_counter, (unsigned long long)nctc);
         if (a.want_pts) pbase = atomicAdd(a.pts_counter, (unsigned long long)npts);
+        if (a.tape_stage) tbase = atomicAdd(a.tape_counter, (unsigned long long)lt_n);
     }
     cbase = __shfl_sync(FULL, cbase, 0);
     pbase = __shfl_sync(FULL, pbase, 0);
+    tbase = __shfl_sync(FULL, tbase, 0);
+    if (a.tape_stage) {
+        const bool tfit = tbase + (unsigned long long)lt_n <= (unsigned long long)a.tape_cap;
+        if (tfit) {
+            for (int i = lane; i < lt_n; i += 32) a.tape_stage[tbase + i] = B.ltape[i];
+            if (cbase + (unsigned long long)nctc <= (unsigned long long)a.contact_cap)
+                for (int i = lane; i < nctc; i += 32) a.ctape_stage[cbase + i] = (int64_t)tbase + B.ltoff[i];
+        } else if (lane == 0) {
+            atomicOr(a.err, ERR_TAPE);
+        }
+    }
     const bool cfit = cbase + (unsigned long long)nctc <= (unsigned long long)a.contact_cap;
     if (cfit) {
         for (int i = lane; i < 20 * nctc; i += 32) a.cgeom_stage[20 * cbase + i] = B.cgeom[i];
@@ -1143,7 +1214,7 @@ __global__ void k_scan_counts(const T* cnt, int64_t n, int64_t* off) {
 }
 
 __global__ void k_gather(PairArgs a, const int64_t* coff, const int64_t* poff, double* cgeom, int32_t* cinfo,
-                         double* pts, int64_t* cpt_off, int32_t* pair_stats) {
+                         double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* ctape_off) {
     const int lane = threadIdx.x & 31;
     const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (p >= a.n_pairs) return;
@@ -1151,6 +1222,8 @@ __global__ void k_gather(PairArgs a, const int64_t* coff, const int64_t* poff, d
     const int64_t src = a.pair_stage_off[p], dst = coff[p];
     for (int i = lane; i < 20 * nc; i += 32) cgeom[20 * dst + i] = a.cgeom_stage[20 * src + i];
     for (int i = lane; i < 4 * nc; i += 32) cinfo[4 * dst + i] = a.cinfo_stage[4 * src + i];
+    if (ctape_off)
+        for (int i = lane; i < nc; i += 32) ctape_off[dst + i] = a.ctape_stage[src + i];
     if (a.want_pts) {
         const int64_t np = a.pair_npts[p], ps = a.pair_pts_stage_off[p], pd = poff[p];
         for (int64_t i = lane; i < 3 * np; i += 32) pts[3 * pd + i] = a.pts_stage[3 * ps + i];
@@ -1175,13 +1248,12 @@ __global__ void k_finish_cpt(const int64_t* coff, const int64_t* poff, int64_t n
 }
 
 void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_pts_off, double* cgeom, int32_t* cinfo,
-                   double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* scan_tmp, cudaStream_t s) {
-    (void)scan_tmp;
+                   double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* ctape_off, cudaStream_t s) {
     if (a.n_pairs <= 0) return;
     k_scan_counts<int32_t><<<1, 1024, 0, s>>>(a.pair_ncontact, a.n_pairs, pair_contact_off);
     if (a.want_pts) k_scan_counts<int64_t><<<1, 1024, 0, s>>>(a.pair_npts, a.n_pairs, pair_pts_off);
     unsigned blocks = (unsigned)((a.n_pairs + 7) / 8);
-    k_gather<<<blocks, 256, 0, s>>>(a, pair_contact_off, pair_pts_off, cgeom, cinfo, pts, cpt_off, pair_stats);
+    k_gather<<<blocks, 256, 0, s>>>(a, pair_contact_off, pair_pts_off, cgeom, cinfo, pts, cpt_off, pair_stats, ctape_off);
     if (a.want_pts) k_finish_cpt<<<1, 1, 0, s>>>(pair_contact_off, pair_pts_off, a.n_pairs, cpt_off);
 }
 

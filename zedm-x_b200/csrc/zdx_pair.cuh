@@ -11,6 +11,7 @@ namespace zdx {
 enum : int {
     PAIR_SEG_OVERFLOW = 1,   // more segments than max_seg_per_pair
     PAIR_EDGE_OVERFLOW = 2,  // the T-junction split produced more edges than the rebuild slot holds
+    PAIR_TAPE_OVERFLOW = 4,  // the adjoint tape of the pair did not fit its slot
 };
 // Call-wide error bits (*err).
 enum : int {
@@ -18,6 +19,7 @@ enum : int {
     ERR_CONTACT_STAGE = 2,  // more contacts than contact_cap
     ERR_POINT_STAGE = 4,    // more loop points than loop_point_cap
     ERR_PAIR = 8,           // some pair has a non-zero status
+    ERR_TAPE = 16,          // the adjoint tape arena is too small
 };
 
 struct PairArgs {
@@ -57,6 +59,14 @@ struct PairArgs {
     int32_t* pair_status;
     int* max_nseg;
     unsigned long long* checks_total;
+    // adjoint tape (null unless recording): per segment of the arena its triangles (ta, tb) and the
+    // candidate index of each endpoint; per contact a record mapping loop vertices to endpoints
+    int32_t* seg_tri;
+    uint8_t* seg_cand;
+    int* tape_stage;
+    int64_t tape_cap;
+    unsigned long long* tape_counter;
+    int64_t* ctape_stage;
     // rebuild stage (k_rebuild)
     int* queue2;
     char* k2_slots;
@@ -90,8 +100,31 @@ void launch_cost_order(const PairArgs& a, int32_t* order, int* buckets, cudaStre
 void launch_segments(const PairArgs& a, int grid, cudaStream_t s);
 void launch_rebuild(const PairArgs& a, int warps, cudaStream_t s);
 void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_pts_off, double* cgeom,
-                   int32_t* cinfo, double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* scan_tmp,
+                   int32_t* cinfo, double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* ctape_off,
                    cudaStream_t s);
+
+// Adjoint of the contact geometry: per contact dL/dSn, dL/dGn -> dL/d(mesh-local corners) (accumulated
+// over pairs) and per pair dL/d(posA, rotA, posB, rotB) (rotations as world-frame rotation vectors).
+struct AdjointArgs {
+    const double* tris;
+    const int64_t* tri_off;
+    const int32_t* pmesh;
+    const double* pose;
+    int mode;
+    int64_t n_contacts;
+    const int32_t* cinfo;
+    const double* pts;
+    const int64_t* cpt_off;
+    const int64_t* ctape_off;
+    const int* tape;
+    const int64_t* pair_seg_off;
+    const int32_t* seg_tri;
+    const uint8_t* seg_cand;
+    const double* grad_contact;  // 6 per contact
+    double* grad_tris;           // 9 per triangle of the mesh set
+    double* grad_pose;           // 12 per pair
+};
+void launch_adjoint(const AdjointArgs& a, cudaStream_t s);
 int k1_blocks_per_sm();
 int k2_warps_per_block();
 

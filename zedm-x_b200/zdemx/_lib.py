@@ -92,6 +92,8 @@ def lib() -> C.CDLL:
     L.zdx_scene_set_state.argtypes = [C.c_void_p, _dp]
     L.zdx_scene_write_output.argtypes = [C.c_void_p, C.c_int64]
     L.zdx_run_config.argtypes = [C.c_char_p, C.c_int]
+    L.zdx_pair_contacts_adjoint.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
+                                            C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.zdx_pair_contacts_noalloc.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                             C.POINTER(PairResult)]
     _lib = L
@@ -248,3 +250,15 @@ def pair_contacts_noalloc(ctx: Context, meshes: dict, pairs: dict, out: dict, *,
     check(lib().zdx_pair_contacts_noalloc(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), C.byref(res)),
           ctx.handle)
     return list(res.totals)
+
+
+def pair_contacts_adjoint(ctx: Context, meshes: dict, pairs: dict, grad_contact, grad_tris, grad_pose, *,
+                          mode=MODE_ZDEM, split=True, tol=0.0, k=1.0, mem=MEM_DEVICE):
+    """zdx_pair_contacts_adjoint on caller buffers (torch tensors or numpy arrays, all on one side)."""
+    opts = PairOpts(mode, int(split), float(tol), float(k), mem, SCHED_BATCHED, 0, 0)
+    ms = MeshSet(int(meshes["tri_off"].shape[0] - 1), _ptr(meshes["tris"]), _ptr(meshes["tri_off"]),
+                 _ptr(meshes["mean_edge"]), _ptr(meshes["bbox_diag"]))
+    pb = PairBatch(int(pairs["mesh"].shape[0]), _ptr(pairs["mesh"]), _ptr(pairs["pose"]))
+    n = int(grad_contact.shape[0])
+    check(lib().zdx_pair_contacts_adjoint(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), _ptr(grad_contact), n,
+                                          _ptr(grad_tris), _ptr(grad_pose)), ctx.handle)
