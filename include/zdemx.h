@@ -156,9 +156,20 @@ int zdx_scene_get_state(zdx_ctx* ctx, double* state16, double* force3, double* t
 int zdx_scene_set_state(zdx_ctx* ctx, const double* state16);
 /* write_vtk_particles + write_particle_state_txt (src/main.cpp:1710-1870, 2470-2483) for `step`. */
 int zdx_scene_write_output(zdx_ctx* ctx, int64_t step);
+/* The same steps as zdx_scene_step, with every count kept on the device and the whole step captured
+ * once into a CUDA graph that is replayed (no counterpart in the reference).  Buffers have fixed
+ * capacities; a step that would exceed one leaves state and history untouched, and the call grows the
+ * capacities, captures again and repeats that step, so results are those of zdx_scene_step.  The
+ * last step's counters land in zdx_scene_info (no stage timings). */
+int zdx_scene_step_graph(zdx_ctx* ctx, int nsteps);
+/* Initial capacities of the graph step (0 keeps a default): candidate pairs, contacts, arena segments,
+ * segments of one pair.  Growth on overflow still applies; call before the first graph step. */
+int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t contacts, int64_t segments, int seg_per_pair);
 /* The whole zdem_cpu run after argument parsing (src/main.cpp:1879-2503) on CUDA device `device`:
- * returns the process exit code (0, or 1 on a bad config / STL, as the reference). */
+ * returns the process exit code (0, or 1 on a bad config / STL, as the reference).
+ * zdx_run_config_graph runs the steps between outputs with zdx_scene_step_graph. */
 int zdx_run_config(const char* config_path, int device);
+int zdx_run_config_graph(const char* config_path, int device);
 
 /* ---- pair contacts without device allocation ------------------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate GPU memory (a host program whose

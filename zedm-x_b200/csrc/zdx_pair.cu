@@ -20,6 +20,7 @@
 
 #include "zdx_math.cuh"
 #include "zdx_pair.cuh"
+#include "zdx_radix.cuh"
 #include "zdx_sortrep.cuh"
 
 namespace zdx {
@@ -74,9 +75,20 @@ void launch_mesh_prep(const PairArgs& a, int64_t total_tris, cudaStream_t s) {
 // ------------------------------------------------------------------------- cost order (work queue)
 // Pairs are bucketed by floor(log2(nA*nB)) and the buckets laid out most expensive first.  The order
 // only schedules work; results do not depend on it.
+__device__ __forceinline__ int64_t pairs_of(const PairArgs& a) {
+    if (!a.n_dev) return a.n_pairs;
+    const int64_t d = *a.n_dev;
+    return d < a.n_pairs ? d : a.n_pairs;
+}
+__device__ __forceinline__ int64_t item_end_of(const PairArgs& a) {
+    if (!a.n_dev) return a.item_end;
+    const int64_t d = a.item_begin + *a.n_dev;
+    return d < a.item_end ? d : a.item_end;
+}
+
 __global__ void k_cost_count(PairArgs a, int* buckets) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (p >= a.n_pairs) return;
+    if (p >= pairs_of(a)) return;
     int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
     unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
                            (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
@@ -94,7 +106,7 @@ __global__ void k_cost_scan(int* buckets) {
 }
 __global__ void k_cost_scatter(PairArgs a, int* buckets, int32_t* order) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (p >= a.n_pairs) return;
+    if (p >= pairs_of(a)) return;
     int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
     unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
                            (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
@@ -217,6 +229,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     carve_k1(a.k1_slots + (size_t)blockIdx.x * a.k1_slot_bytes, a.cap_side, a.cap_seg, &S);
     const int cap = a.cap_side;
     const bool py = a.mode == 1;
+    const int64_t iend = item_end_of(a);
 
     for (;;) {
         if (tid == 0) {
@@ -227,7 +240,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         }
         __syncthreads();
         const int64_t item = sh_item;
-        if (item >= a.item_end) break;
+        if (item >= iend) break;
         const int p = a.order[item];
         const double* ps = a.pose + 14 * (int64_t)p;
         V3 tpos[2] = {V3{ps[0], ps[1], ps[2]}, V3{ps[7], ps[8], ps[9]}};
@@ -462,8 +475,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     a.seg_cand[2 * o + 1] = S.cand[2 * i + 1];
                 }
             }
-        } else if (tid == 0) {
-            atomicOr(a.err, ERR_SEG_ARENA);
+        } else {
+            status |= PAIR_NO_ARENA;
+            if (tid == 0) atomicOr(a.err, ERR_SEG_ARENA);
         }
         if (tid == 0) {
             a.pair_seg_off[p] = (int64_t)sbase;
@@ -645,7 +659,7 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
     const double area_eps = me > 0.0 ? (me * me * 1e-4) : 1e-12;
 
     int ncomp = 0, nloops = 0, nctc = 0, npts = 0, lt_n = 0;
-    if (n > 0 && !(status & PAIR_SEG_OVERFLOW)) {
+    if (n > 0 && !(status & (PAIR_SEG_OVERFLOW | PAIR_NO_ARENA))) {
         // ---- components: label_segments_by_contact_greedy, src/main.cpp:804-898
         if (a.split) {
             for (int i = lane; i < n; i += 32) {
@@ -1161,11 +1175,12 @@ __global__ __launch_bounds__(K2_WARPS * 32) void k_rebuild(PairArgs a) {
     if (wslot >= a.k2_nslots) return;
     PostBufs B;
     carve_post(a.k2_slots + (size_t)wslot * a.k2_slot_bytes, a.k2_nmax, &B);
+    const int64_t iend = item_end_of(a);
     for (;;) {
         int item = 0;
         if (lane == 0) item = (int)(a.item_begin + atomicAdd(a.queue2, 1));
         item = __shfl_sync(FULL, item, 0);
-        if (item >= a.item_end) break;
+        if (item >= iend) break;
         rebuild_pair(a, a.order[item], B, lane);
     }
 }
@@ -1217,7 +1232,9 @@ __global__ void k_gather(PairArgs a, const int64_t* coff, const int64_t* poff, d
                          double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* ctape_off) {
     const int lane = threadIdx.x & 31;
     const int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (p >= a.n_pairs) return;
+    if (p >= pairs_of(a)) return;
+    // with a device-resident count nothing checked the staging on the host: an overflowed stage is not copied
+    if (a.n_dev && (*a.err & (ERR_CONTACT_STAGE | ERR_POINT_STAGE))) return;
     const int nc = a.pair_ncontact[p];
     const int64_t src = a.pair_stage_off[p], dst = coff[p];
     for (int i = lane; i < 20 * nc; i += 32) cgeom[20 * dst + i] = a.cgeom_stage[20 * src + i];
@@ -1255,6 +1272,14 @@ void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_p
     unsigned blocks = (unsigned)((a.n_pairs + 7) / 8);
     k_gather<<<blocks, 256, 0, s>>>(a, pair_contact_off, pair_pts_off, cgeom, cinfo, pts, cpt_off, pair_stats, ctape_off);
     if (a.want_pts) k_finish_cpt<<<1, 1, 0, s>>>(pair_contact_off, pair_pts_off, a.n_pairs, cpt_off);
+}
+
+void launch_gather_dev(const PairArgs& a, int64_t* pair_contact_off, double* cgeom, int32_t* cinfo,
+                       int32_t* pair_stats, void* scan_scratch, cudaStream_t s) {
+    if (a.n_pairs <= 0) return;
+    scan_offsets<int32_t>(a.pair_ncontact, a.n_pairs, a.n_dev, pair_contact_off, scan_scratch, s);
+    unsigned blocks = (unsigned)((a.n_pairs + 7) / 8);
+    k_gather<<<blocks, 256, 0, s>>>(a, pair_contact_off, nullptr, cgeom, cinfo, nullptr, nullptr, pair_stats, nullptr);
 }
 
 }  // namespace zdx

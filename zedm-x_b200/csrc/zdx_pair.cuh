@@ -12,6 +12,7 @@ enum : int {
     PAIR_SEG_OVERFLOW = 1,   // more segments than max_seg_per_pair
     PAIR_EDGE_OVERFLOW = 2,  // the T-junction split produced more edges than the rebuild slot holds
     PAIR_TAPE_OVERFLOW = 4,  // the adjoint tape of the pair did not fit its slot
+    PAIR_NO_ARENA = 8,       // the pair's segments did not fit the call's segment arena (not rebuilt)
 };
 // Call-wide error bits (*err).
 enum : int {
@@ -35,6 +36,9 @@ struct PairArgs {
     int* mesh_valid;                  // triangles with a plane (|e1 x e2| >= 1e-30) per mesh
     // pairs
     int64_t n_pairs;
+    // null, or the device-resident pair count: n_pairs and item_end are then capacities that size the
+    // launches and the kernels work on min(*n_dev, capacity) pairs (a step captured in a CUDA graph)
+    const int64_t* n_dev;
     const int32_t* pmesh;
     const double* pose;
     const int32_t* order;  // work item -> pair, most expensive first
@@ -102,6 +106,10 @@ void launch_rebuild(const PairArgs& a, int warps, cudaStream_t s);
 void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_pts_off, double* cgeom,
                    int32_t* cinfo, double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* ctape_off,
                    cudaStream_t s);
+// Contacts-only gather for a device-resident pair count (a.n_dev): multi-block scan of the per-pair
+// contact counts (scratch: scan_scratch_bytes(a.n_pairs)), then the copy into CSR order.
+void launch_gather_dev(const PairArgs& a, int64_t* pair_contact_off, double* cgeom, int32_t* cinfo,
+                       int32_t* pair_stats, void* scan_scratch, cudaStream_t s);
 
 // Adjoint of the contact geometry: per contact dL/dSn, dL/dGn -> dL/d(mesh-local corners) (accumulated
 // over pairs) and per pair dL/d(posA, rotA, posB, rotB) (rotations as world-frame rotation vectors).

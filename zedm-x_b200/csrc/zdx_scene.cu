@@ -23,6 +23,7 @@
 
 #include "../../include/zdemx.h"
 #include "zdx_math.cuh"
+#include "zdx_pair.cuh"
 #include "zdx_radix.cuh"
 #include "zdx_scene.h"
 
@@ -38,6 +39,13 @@ __device__ __forceinline__ void S3(double* p, V3 v) {
     p[0] = v.x;
     p[1] = v.y;
     p[2] = v.z;
+}
+
+// min(n, *n_dev) when a device-resident count is given (a step captured in a CUDA graph)
+__device__ __forceinline__ int64_t dev_count(int64_t n, const int64_t* n_dev) {
+    if (!n_dev) return n;
+    const int64_t d = *n_dev;
+    return d < n ? d : n;
 }
 
 __device__ __forceinline__ uint32_t cell_hash(int x, int y, int z, uint32_t mask) {
@@ -68,9 +76,10 @@ __global__ void k_bp_bounds(const uint32_t* key, int np, int* start, int* end) {
 template <bool WRITE>
 __global__ void k_bp_pairs(const double* state, const double* mat, int np, const int4* cell, const int32_t* sidx,
                            const int* start, const int* end, uint32_t mask, int32_t* cnt, const int64_t* off,
-                           int2* pairs) {
+                           int2* pairs, int64_t cap) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
+    if (WRITE && off[i + 1] > cap) return;  // over capacity: the caller sees the total and grows
     const double* si = state + 16 * (int64_t)i;
     const V3 pi{si[0], si[1], si[2]};
     const double ri = mat[17 * (int64_t)i + 2];
@@ -112,10 +121,10 @@ __global__ void k_bp_pairs(const double* state, const double* mat, int np, const
     }
 }
 
-__global__ void k_pair_inputs(const int2* pairs, int64_t npair, const double* state, const int32_t* pmesh,
-                              int32_t* pr_mesh, double* pr_pose, uint32_t* tkey, int32_t* tval) {
+__global__ void k_pair_inputs(const int2* pairs, int64_t npair, const int64_t* n_dev, const double* state,
+                              const int32_t* pmesh, int32_t* pr_mesh, double* pr_pose, uint32_t* tkey, int32_t* tval) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (p >= npair) return;
+    if (p >= dev_count(npair, n_dev)) return;
     int2 ij = pairs[p];
     const double* a = state + 16 * (int64_t)ij.x;
     const double* b = state + 16 * (int64_t)ij.y;
@@ -142,11 +151,14 @@ __device__ int64_t find_key(const int64_t* keys, int64_t n, int64_t k) {
 
 // ---------------------------------------------------------------- particle-particle force law
 // src/main.cpp:2220-2278 (normal damping is commented out in the reference for this law).
-__global__ void k_pp_force(const int2* pairs, int64_t npair, const int64_t* coff, const double* geom, const double* state,
-                           const double* mat, double dt, const int64_t* hkey, const double* hds, int64_t nh,
-                           double* contrib, int32_t* active, double* ds_out) {
+__global__ void k_pp_force(const int2* pairs, int64_t npair, const int64_t* n_dev, const int64_t* coff, const double* geom,
+                           const double* state, const double* mat, double dt, const int64_t* hkey, const double* hds,
+                           int64_t nh, const int64_t* nh_dev, double* contrib, int32_t* active, double* ds_out,
+                           const int* stop) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (p >= npair) return;
+    if (p >= dev_count(npair, n_dev)) return;
+    if (stop && *stop) return;
+    if (nh_dev) nh = *nh_dev;
     const int64_t c0 = coff[p], c1 = coff[p + 1];
     if (c0 == c1) {
         active[p] = 0;
@@ -208,9 +220,10 @@ __global__ void k_pp_force(const int2* pairs, int64_t npair, const int64_t* coff
 
 // ---------------------------------------------------------------- walls
 __global__ void k_wall_cand(const double* state, const double* mat, int np, const double* wpose, const double* wrad,
-                            int nw, int32_t* cnt, const int64_t* off, int2* cand) {
+                            int nw, int32_t* cnt, const int64_t* off, int2* cand, int64_t cap) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
+    if (off && off[i + 1] > cap) return;
     const double* s = state + 16 * (int64_t)i;
     int n = 0;
     for (int w = 0; w < nw; ++w) {
@@ -262,6 +275,9 @@ struct WallArgs {
     double* scratch;  // per warp: section points (3 doubles each), polygons
     int64_t scratch_pts;
     int nwarps;
+    const int64_t* ncand_dev;  // null, or device-resident candidate / history counts
+    const int64_t* nh_dev;
+    const int* stop;           // null, or a flag that makes the step skip (capacity overflow)
 };
 
 // compute_wall_contact (src/main.cpp:1205-1258) for one wall triangle, by one warp: lanes collect the
@@ -379,8 +395,11 @@ __global__ void k_walls(WallArgs a) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (warp >= a.nwarps) return;
+    if (a.stop && *a.stop) return;
     double* pts = a.scratch + warp * (3 * a.scratch_pts + 4 * (8 * a.scratch_pts + 16));
-    for (int64_t k = warp; k < a.ncand; k += a.nwarps) {
+    const int64_t ncand = dev_count(a.ncand, a.ncand_dev);
+    const int64_t nh = a.nh_dev ? *a.nh_dev : a.nh;
+    for (int64_t k = warp; k < ncand; k += a.nwarps) {
         const int2 iw = a.cand[k];
         const int i = iw.x, w = iw.y;
         const double* sp = a.state + 16 * (int64_t)i;
@@ -391,7 +410,7 @@ __global__ void k_walls(WallArgs a) {
         double tol = a.mprops[2 * pm] > 0.0 ? (a.mprops[2 * pm] * 0.1) : (a.mprops[2 * pm + 1] * 1e-2);
         if (tol <= 0.0) tol = 1e-6;
         const int64_t key = ((int64_t)i << 16) | (int64_t)w;
-        int64_t h = find_key(a.hkey, a.nh, key);
+        int64_t h = find_key(a.hkey, nh, key);
         V3 ds = h >= 0 ? L3(a.hds + 3 * h) : V3{0.0, 0.0, 0.0};
         const Q4 qn = qnormalize(Q4{sp[3], sp[4], sp[5], sp[6]});
         const V3 xp = L3(sp);
@@ -467,9 +486,10 @@ __global__ void k_scatter_integrate(int np, const int2* pairs, const int64_t* ps
                                     const int64_t* tstart, const int64_t* coff, const double* pcontrib,
                                     const int64_t* wstart, const double* wcontrib, const int32_t* wvalid, int max_wtri,
                                     double* state, const double* mat, const double* g3, double dt, double* force,
-                                    double* torque, int32_t* count) {
+                                    double* torque, int32_t* count, const int* stop) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np) return;
+    if (stop && *stop) return;  // a capacity overflow earlier in this step: leave the state as it was
     V3 F{0.0, 0.0, 0.0}, T{0.0, 0.0, 0.0};
     int cnt = 0;
     // pairs (i, p), i < p, in increasing i: p receives +f and cross(rB, f)
@@ -548,10 +568,11 @@ __global__ void k_scatter_integrate(int np, const int2* pairs, const int64_t* ps
     S3(s + 13, L);
 }
 
-__global__ void k_range_bounds(const int2* pairs, int64_t npair, int np, int64_t* pstart) {
+__global__ void k_range_bounds(const int2* pairs, int64_t npair, const int64_t* n_dev, int np, int64_t* pstart) {
     // pstart[i] = first pair with first index >= i (pairs sorted by i)
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > np) return;
+    npair = dev_count(npair, n_dev);
     int64_t lo = 0, hi = npair;
     while (lo < hi) {
         int64_t mid = (lo + hi) >> 1;
@@ -561,9 +582,10 @@ __global__ void k_range_bounds(const int2* pairs, int64_t npair, int np, int64_t
     pstart[i] = lo;
 }
 
-__global__ void k_key_bounds(const uint32_t* keys, int64_t n, int np, int64_t* start) {
+__global__ void k_key_bounds(const uint32_t* keys, int64_t n, const int64_t* n_dev, int np, int64_t* start) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > np) return;
+    n = dev_count(n, n_dev);
     int64_t lo = 0, hi = n;
     while (lo < hi) {
         int64_t mid = (lo + hi) >> 1;
@@ -574,10 +596,12 @@ __global__ void k_key_bounds(const uint32_t* keys, int64_t n, int np, int64_t* s
 }
 
 // history compaction: keep active entries in order
-__global__ void k_hist_write(const int32_t* active, const int64_t* pos, int64_t n, const int2* items, int shift,
-                             const double* ds, int64_t* key_out, double* ds_out) {
+__global__ void k_hist_write(const int32_t* active, const int64_t* pos, int64_t n, const int64_t* n_dev,
+                             const int2* items, int shift, const double* ds, int64_t* key_out, double* ds_out,
+                             const int* stop) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (k >= n || !active[k]) return;
+    if (k >= dev_count(n, n_dev) || !active[k]) return;
+    if (stop && *stop) return;
     int64_t o = pos[k];
     int2 it = items[k];
     key_out[o] = shift == 32 ? (((int64_t)it.x << 32) | (int64_t)(uint32_t)it.y) : (((int64_t)it.x << 16) | (int64_t)it.y);
@@ -586,8 +610,9 @@ __global__ void k_hist_write(const int32_t* active, const int64_t* pos, int64_t 
     ds_out[3 * o + 2] = ds[3 * k + 2];
 }
 
-__global__ void k_count_valid(const int32_t* v, int64_t n, unsigned long long* out) {
+__global__ void k_count_valid(const int32_t* v, int64_t n, const int64_t* rows_dev, int per_row, unsigned long long* out) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (rows_dev) n = dev_count(n / per_row, rows_dev) * per_row;  // n = capacity rows x per_row
     int c = (k < n && v[k]) ? 1 : 0;
     c = __reduce_add_sync(FULLM, c);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
@@ -669,6 +694,10 @@ int scene_download(zdx_ctx* ctx, Scene& s) {
 }
 
 int scene_step(zdx_ctx* ctx, Scene& s) {
+    if (s.gs.active) {
+        int rc = scene_graph_leave(ctx, s);
+        if (rc) return rc;
+    }
     cudaStream_t st = ctx->stream;
     const int np = s.np;
     StepStats stats;
@@ -706,9 +735,9 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(s.bp_key), np, as<int>(s.bp_start), as<int>(s.bp_end));
         k_bp_pairs<false><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
                                                     as<int>(s.bp_start), as<int>(s.bp_end), T - 1, as<int32_t>(s.bp_cnt),
-                                                    nullptr, nullptr);
+                                                    nullptr, nullptr, INT64_MAX);
         CKS(scan_counts_i32(as<int32_t>(s.bp_cnt), np, as<int64_t>(s.bp_off), st));
-        ctx->launches += 5 + 3 * ((bits + 7) / 8);
+        ctx->launches += 5 + 5 * ((bits + 7) / 8);  // a radix pass: histogram, 3 scan kernels, scatter
     }
     int64_t npair = 0;
     if (np > 0) {
@@ -720,7 +749,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
     if (np > 0) {
         k_bp_pairs<true><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
                                                    as<int>(s.bp_start), as<int>(s.bp_end), T - 1, nullptr,
-                                                   as<int64_t>(s.bp_off), as<int2>(s.bp_pairs));
+                                                   as<int64_t>(s.bp_off), as<int2>(s.bp_pairs), INT64_MAX);
         ctx->launches += 1;
     }
     stats.pairs = npair;
@@ -742,7 +771,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
     CKS(s.bp_hist.ensure(sizeof(int64_t) * (N1 + 1)));
     int64_t ncontact = 0;
     if (npair > 0) {
-        k_pair_inputs<<<grid(npair), 256, 0, st>>>(as<int2>(s.bp_pairs), npair, state, as<int32_t>(s.d_pmesh),
+        k_pair_inputs<<<grid(npair), 256, 0, st>>>(as<int2>(s.bp_pairs), npair, nullptr, state, as<int32_t>(s.d_pmesh),
                                                    as<int32_t>(s.pr_mesh), as<double>(s.pr_pose),
                                                    as<uint32_t>(s.tr_key), as<int32_t>(s.tr_idx));
         int pbits = 0;
@@ -750,7 +779,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         CKS(s.bp_tmp.ensure(radix_scratch_bytes(npair)));
         CKS(radix_sort_u32(as<uint32_t>(s.tr_key), as<int32_t>(s.tr_idx), as<uint32_t>(s.tr_key2),
                            as<int32_t>(s.tr_idx2), npair, std::max(pbits, 1), s.bp_tmp.p, st));
-        ctx->launches += 1 + 3 * ((std::max(pbits, 1) + 7) / 8);
+        ctx->launches += 1 + 5 * ((std::max(pbits, 1) + 7) / 8);
         if (s.contact_cap < 4 * npair + 64) s.contact_cap = 4 * npair + 64;
         for (int attempt = 0; attempt < 2; ++attempt) {
             CKS(s.pr_geom.ensure(sizeof(double) * 20 * (size_t)s.contact_cap));
@@ -791,17 +820,17 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         CKS(cudaMemsetAsync(s.pr_coff.p, 0, sizeof(int64_t), st));
     }
     CKS(s.pr_contrib.ensure(sizeof(double) * 9 * (size_t)std::max<int64_t>(ncontact, 1)));
-    k_key_bounds<<<grid(np + 1), 256, 0, st>>>(as<uint32_t>(s.tr_key), npair, np, as<int64_t>(s.tr_start));
-    k_range_bounds<<<grid(np + 1), 256, 0, st>>>(as<int2>(s.bp_pairs), npair, np, as<int64_t>(s.bp_hist));
+    k_key_bounds<<<grid(np + 1), 256, 0, st>>>(as<uint32_t>(s.tr_key), npair, nullptr, np, as<int64_t>(s.tr_start));
+    k_range_bounds<<<grid(np + 1), 256, 0, st>>>(as<int2>(s.bp_pairs), npair, nullptr, np, as<int64_t>(s.bp_hist));
     ctx->launches += 2;
 
     // ---- 3. particle-particle forces
     if (npair > 0) {
-        k_pp_force<<<grid(npair, 128), 128, 0, st>>>(as<int2>(s.bp_pairs), npair, as<int64_t>(s.pr_coff),
+        k_pp_force<<<grid(npair, 128), 128, 0, st>>>(as<int2>(s.bp_pairs), npair, nullptr, as<int64_t>(s.pr_coff),
                                                      as<double>(s.pr_geom), state, mat, s.cfg.dt,
                                                      as<int64_t>(s.d_hist_key), as<double>(s.d_hist_ds), s.nhist,
-                                                     as<double>(s.pr_contrib), as<int32_t>(s.pr_active),
-                                                     as<double>(s.pr_ds));
+                                                     nullptr, as<double>(s.pr_contrib), as<int32_t>(s.pr_active),
+                                                     as<double>(s.pr_ds), nullptr);
         ctx->launches += 1;
     }
 
@@ -813,13 +842,13 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
     if (s.nw > 0 && np > 0) {
         CKS(s.w_active.ensure(sizeof(int32_t) * N1));
         k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
-                                              as<int32_t>(s.w_active), nullptr, nullptr);
+                                              as<int32_t>(s.w_active), nullptr, nullptr, INT64_MAX);
         CKS(scan_counts_i32(as<int32_t>(s.w_active), np, as<int64_t>(s.w_scan), st));
         CKS(cudaMemcpyAsync(&ncand, as<int64_t>(s.w_scan) + np, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         CKS(cudaStreamSynchronize(st));
         CKS(s.w_pairs.ensure(sizeof(int2) * std::max<int64_t>(ncand, 1)));
         k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw, nullptr,
-                                              as<int64_t>(s.w_scan), as<int2>(s.w_pairs));
+                                              as<int64_t>(s.w_scan), as<int2>(s.w_pairs), INT64_MAX);
         ctx->launches += 3;
     } else {
         CKS(cudaMemsetAsync(s.w_scan.p, 0, sizeof(int64_t) * (N1 + 1), st));
@@ -843,7 +872,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
                     as<double>(s.d_wtris), as<double>(s.d_wnorm), as<int64_t>(s.d_wtri_off), as<double>(s.d_wmat),
                     as<int2>(s.w_pairs), ncand, max_wtri, s.cfg.dt, as<int64_t>(s.d_whist_key), as<double>(s.d_whist_ds),
                     s.nwhist, as<double>(s.w_contrib), as<int32_t>(s.w_valid), as<int32_t>(w_act),
-                    as<double>(s.w_ds), as<double>(s.bp_tmp), spts, nwarps};
+                    as<double>(s.w_ds), as<double>(s.bp_tmp), spts, nwarps, nullptr, nullptr, nullptr};
         k_walls<<<(nwarps + 3) / 4, 128, 0, st>>>(wa);
         ctx->launches += 1;
         CKS(s.pr_scan.ensure(sizeof(int64_t) * (std::max(P1, C1) + 1)));
@@ -851,7 +880,8 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         CKS(s.bp_end.ensure(sizeof(int) * T + 16));
         cntd = reinterpret_cast<unsigned long long*>(s.bp_end.p);
         CKS(cudaMemsetAsync(cntd, 0, sizeof(unsigned long long), st));
-        k_count_valid<<<grid(C1 * max_wtri), 256, 0, st>>>(as<int32_t>(s.w_valid), (int64_t)C1 * max_wtri, cntd);
+        k_count_valid<<<grid(C1 * max_wtri), 256, 0, st>>>(as<int32_t>(s.w_valid), (int64_t)C1 * max_wtri, nullptr, max_wtri,
+                                                           cntd);
         unsigned long long wc = 0;
         CKS(cudaMemcpyAsync(&wc, cntd, sizeof(wc), cudaMemcpyDeviceToHost, st));
         CKS(cudaStreamSynchronize(st));
@@ -869,7 +899,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
             np, as<int2>(s.bp_pairs), as<int64_t>(s.bp_hist), as<int32_t>(s.tr_idx), as<int64_t>(s.tr_start),
             as<int64_t>(s.pr_coff), as<double>(s.pr_contrib), as<int64_t>(s.w_scan), as<double>(s.w_contrib),
             as<int32_t>(s.w_valid), max_wtri, state, mat, as<double>(d_g), s.cfg.dt, as<double>(s.d_force),
-            as<double>(s.d_torque), as<int32_t>(s.d_count));
+            as<double>(s.d_torque), as<int32_t>(s.d_count), nullptr);
         ctx->launches += 1;
     }
 
@@ -881,9 +911,9 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         CKS(cudaStreamSynchronize(st));
         CKS(s.d_hist_key2.ensure(sizeof(int64_t) * std::max<int64_t>(nn, 1)));
         CKS(s.d_hist_ds2.ensure(sizeof(double) * 3 * std::max<int64_t>(nn, 1)));
-        k_hist_write<<<grid(npair), 256, 0, st>>>(as<int32_t>(s.pr_active), as<int64_t>(s.pr_scan), npair,
+        k_hist_write<<<grid(npair), 256, 0, st>>>(as<int32_t>(s.pr_active), as<int64_t>(s.pr_scan), npair, nullptr,
                                                   as<int2>(s.bp_pairs), 32, as<double>(s.pr_ds),
-                                                  as<int64_t>(s.d_hist_key2), as<double>(s.d_hist_ds2));
+                                                  as<int64_t>(s.d_hist_key2), as<double>(s.d_hist_ds2), nullptr);
         std::swap(s.d_hist_key, s.d_hist_key2);
         std::swap(s.d_hist_ds, s.d_hist_ds2);
         s.nhist = nn;
@@ -898,9 +928,9 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         CKS(cudaStreamSynchronize(st));
         CKS(s.d_whist_key2.ensure(sizeof(int64_t) * std::max<int64_t>(nn, 1)));
         CKS(s.d_whist_ds2.ensure(sizeof(double) * 3 * std::max<int64_t>(nn, 1)));
-        k_hist_write<<<grid(ncand), 256, 0, st>>>(as<int32_t>(w_act), as<int64_t>(s.pr_scan), ncand,
+        k_hist_write<<<grid(ncand), 256, 0, st>>>(as<int32_t>(w_act), as<int64_t>(s.pr_scan), ncand, nullptr,
                                                   as<int2>(s.w_pairs), 16, as<double>(s.w_ds),
-                                                  as<int64_t>(s.d_whist_key2), as<double>(s.d_whist_ds2));
+                                                  as<int64_t>(s.d_whist_key2), as<double>(s.d_whist_ds2), nullptr);
         std::swap(s.d_whist_key, s.d_whist_key2);
         std::swap(s.d_whist_ds, s.d_whist_ds2);
         s.nwhist = nn;
@@ -916,6 +946,507 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
     s.have_forces = true;
     s.host_dirty = true;
     s.step++;
+    return ZDX_OK;
+}
+
+
+// ================================================================= the step as one CUDA graph
+namespace {
+
+__global__ void k_g_begin(GraphCounts* g) {
+    g->flags = 0;
+    g->contacts = g->wall_contacts = g->tri_checks = g->segments = g->comps = g->loops = 0;
+}
+
+// n_out = total if it fits the capacity, else 0 (and a flag): nothing downstream reads a partial list.
+__global__ void k_g_take(const int64_t* total, int64_t cap, int64_t* n_out, int64_t* need, int* flags, int bit) {
+    const int64_t t = *total;
+    *need = t;
+    if (t > cap) {
+        *n_out = 0;
+        atomicOr(flags, bit);
+    } else {
+        *n_out = t;
+    }
+}
+
+__global__ void k_g_pair_done(const unsigned long long* cnt, GraphCounts* g) {
+    for (int i = 0; i < 8; ++i) g->pair_counters[i] = cnt[i];
+    const int err = reinterpret_cast<const int*>(cnt + 7)[0];
+    int f = 0;
+    if (err & ERR_SEG_ARENA) f |= GRAPH_OVF_SEGS;
+    if (err & ERR_CONTACT_STAGE) f |= GRAPH_OVF_CONTACTS;
+    if (err & ERR_PAIR) f |= GRAPH_OVF_PAIR;
+    if (f) atomicOr(&g->flags, f);
+    g->segments = cnt[0];
+    g->contacts = cnt[1];
+    g->tri_checks = cnt[3];
+}
+
+__global__ void k_g_pair_stats(const int32_t* pstats, const GraphCounts* gc, GraphCounts* g) {
+    const int64_t n = gc->npair;
+    unsigned long long c = 0, l = 0;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        c += (unsigned long long)pstats[4 * p + 1];
+        l += (unsigned long long)pstats[4 * p + 2];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_down_sync(FULLM, c, o);
+        l += __shfl_down_sync(FULLM, l, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (c || l)) {
+        atomicAdd(&g->comps, c);
+        atomicAdd(&g->loops, l);
+    }
+}
+
+// The step completed: the compacted histories become the current ones.
+__global__ void k_g_commit(GraphCounts* g, const int64_t* hscan, const int64_t* whscan, int64_t* hkey, double* hds,
+                           const int64_t* hkey2, const double* hds2, int64_t* whkey, double* whds,
+                           const int64_t* whkey2, const double* whds2) {
+    if (g->flags) return;
+    const int64_t nn = hscan[g->npair], wn = whscan[g->ncand];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nn; k += stride) {
+        hkey[k] = hkey2[k];
+        hds[3 * k] = hds2[3 * k];
+        hds[3 * k + 1] = hds2[3 * k + 1];
+        hds[3 * k + 2] = hds2[3 * k + 2];
+    }
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < wn; k += stride) {
+        whkey[k] = whkey2[k];
+        whds[3 * k] = whds2[3 * k];
+        whds[3 * k + 1] = whds2[3 * k + 1];
+        whds[3 * k + 2] = whds2[3 * k + 2];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        g->nhist = nn;
+        g->nwhist = wn;
+        g->steps_done += 1;
+    }
+}
+
+}  // namespace
+
+// Buffers at the current capacities (pointers the captured graph holds).
+static int graph_alloc(zdx_ctx* ctx, Scene& s) {
+    GraphStep& G = s.gs;
+    const int np = s.np;
+    const size_t N1 = (size_t)std::max(np, 1);
+    const size_t P1 = (size_t)std::max<int64_t>(G.pcap, 1);
+    const size_t C1 = (size_t)std::max<int64_t>(G.ccap, 1);
+    const size_t W1 = (size_t)std::max<int64_t>(G.wcap, 1);
+    const int nm = (int)s.mesh_off.size() - 1;
+    int max_ntri = 1;
+    for (int m = 0; m < nm; ++m) max_ntri = std::max<int>(max_ntri, (int)(s.mesh_off[m + 1] - s.mesh_off[m]));
+    CKS(G.g.ensure(sizeof(GraphCounts)));
+    CKS(G.grav.ensure(sizeof(double) * 3));
+    CKS(G.bp_cell.ensure(sizeof(int4) * N1));
+    CKS(G.bp_key.ensure(sizeof(uint32_t) * N1));
+    CKS(G.bp_idx.ensure(sizeof(int32_t) * N1));
+    CKS(G.bp_key2.ensure(sizeof(uint32_t) * N1));
+    CKS(G.bp_idx2.ensure(sizeof(int32_t) * N1));
+    CKS(G.bp_start.ensure(sizeof(int) * G.T));
+    CKS(G.bp_end.ensure(sizeof(int) * G.T));
+    CKS(G.bp_cnt.ensure(sizeof(int32_t) * N1));
+    CKS(G.bp_off.ensure(sizeof(int64_t) * (N1 + 1)));
+    CKS(G.bp_pairs.ensure(sizeof(int2) * P1));
+    CKS(G.bp_pstart.ensure(sizeof(int64_t) * (N1 + 1)));
+    CKS(G.rs_tmp.ensure(std::max(radix_scratch_bytes((int64_t)N1), radix_scratch_bytes((int64_t)P1))));
+    CKS(G.scan_tmp.ensure(scan_scratch_bytes((int64_t)std::max({N1, P1, W1}) + 1)));
+    CKS(G.tr_key.ensure(sizeof(uint32_t) * P1));
+    CKS(G.tr_idx.ensure(sizeof(int32_t) * P1));
+    CKS(G.tr_key2.ensure(sizeof(uint32_t) * P1));
+    CKS(G.tr_idx2.ensure(sizeof(int32_t) * P1));
+    CKS(G.tr_start.ensure(sizeof(int64_t) * (N1 + 1)));
+    CKS(G.pr_mesh.ensure(sizeof(int32_t) * 2 * P1));
+    CKS(G.pr_pose.ensure(sizeof(double) * 14 * P1));
+    CKS(G.pr_coff.ensure(sizeof(int64_t) * (P1 + 1)));
+    CKS(G.pr_stats.ensure(sizeof(int32_t) * 4 * P1));
+    CKS(G.pr_geom.ensure(sizeof(double) * 20 * C1));
+    CKS(G.pr_info.ensure(sizeof(int32_t) * 4 * C1));
+    CKS(G.pr_contrib.ensure(sizeof(double) * 9 * C1));
+    CKS(G.pr_active.ensure(sizeof(int32_t) * P1));
+    CKS(G.pr_ds.ensure(sizeof(double) * 3 * P1));
+    CKS(G.pr_hscan.ensure(sizeof(int64_t) * (P1 + 1)));
+    CKS(G.w_active.ensure(sizeof(int32_t) * N1));
+    CKS(G.w_scan.ensure(sizeof(int64_t) * (N1 + 1)));
+    CKS(G.w_pairs.ensure(sizeof(int2) * W1));
+    CKS(G.w_contrib.ensure(sizeof(double) * 6 * W1 * G.max_wtri));
+    CKS(G.w_valid.ensure(sizeof(int32_t) * W1 * G.max_wtri));
+    CKS(G.w_act.ensure(sizeof(int32_t) * W1));
+    CKS(G.w_ds.ensure(sizeof(double) * 3 * W1));
+    CKS(G.w_hscan.ensure(sizeof(int64_t) * (W1 + 1)));
+    CKS(G.w_scratch.ensure(sizeof(double) * (3 * G.spts + 4 * (8 * G.spts + 16)) * (size_t)std::max(G.wall_warps, 1)));
+    // histories: at most one entry per pair / candidate of a step
+    CKS(G.hkey.ensure(sizeof(int64_t) * P1));
+    CKS(G.hds.ensure(sizeof(double) * 3 * P1));
+    CKS(G.hkey2.ensure(sizeof(int64_t) * P1));
+    CKS(G.hds2.ensure(sizeof(double) * 3 * P1));
+    CKS(G.whkey.ensure(sizeof(int64_t) * W1));
+    CKS(G.whds.ensure(sizeof(double) * 3 * W1));
+    CKS(G.whkey2.ensure(sizeof(int64_t) * W1));
+    CKS(G.whds2.ensure(sizeof(double) * 3 * W1));
+    // pair kernels
+    const int64_t total_tris = s.mesh_off.back();
+    CKS(G.tri_sph.ensure(sizeof(double4) * (size_t)std::max<int64_t>(total_tris, 1)));
+    CKS(G.mesh_R.ensure(sizeof(unsigned long long) * std::max(nm, 1)));
+    CKS(G.mesh_valid.ensure(sizeof(int) * std::max(nm, 1)));
+    CKS(G.order.ensure(sizeof(int32_t) * P1));
+    CKS(G.buckets.ensure(sizeof(int) * 128));
+    CKS(G.pair_i64.ensure(sizeof(int64_t) * 5 * P1));
+    CKS(G.pair_i32.ensure(sizeof(int32_t) * 6 * P1));
+    CKS(G.counters.ensure(sizeof(unsigned long long) * 16));
+    G.k1_grid = (int)std::min<int64_t>(P1, (int64_t)ctx->num_sms * k1_blocks_per_sm());
+    CKS(G.k1_slots.ensure(tritest_slot_bytes(max_ntri, G.cap_seg) * (size_t)G.k1_grid));
+    CKS(G.seg_arena.ensure(sizeof(double) * 6 * (size_t)std::max<int64_t>(G.segcap, 1)));
+    const size_t slot = rebuild_slot_bytes(G.cap_seg);
+    int64_t warps = std::min<int64_t>((int64_t)P1, (int64_t)ctx->num_sms * 32);
+    warps = std::min<int64_t>(warps, std::max<int64_t>(1, (int64_t)(((size_t)2 << 30) / slot)));
+    warps = (warps + k2_warps_per_block() - 1) / k2_warps_per_block() * k2_warps_per_block();
+    G.k2_warps = (int)warps;
+    CKS(G.k2_slots.ensure(slot * (size_t)warps));
+    CKS(G.cstage.ensure(sizeof(double) * 20 * C1));
+    CKS(G.cistage.ensure(sizeof(int32_t) * 5 * C1));
+    // activity flags are read (by the history scans) even in a step that stops early
+    CKS(cudaMemsetAsync(G.pr_active.p, 0, sizeof(int32_t) * P1, ctx->stream));
+    CKS(cudaMemsetAsync(G.w_act.p, 0, sizeof(int32_t) * W1, ctx->stream));
+    return ZDX_OK;
+}
+
+// Launches one step on the context stream (captured into the graph).  Every count is read on the device.
+static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
+    GraphStep& G = s.gs;
+    cudaStream_t st = ctx->stream;
+    const int np = s.np;
+    double* state = as<double>(s.d_state);
+    const double* mat = as<double>(s.d_mat);
+    GraphCounts* g = as<GraphCounts>(G.g);
+    int* flags = &g->flags;
+    k_g_begin<<<1, 1, 0, st>>>(g);
+
+    // ---- 1. broad phase
+    k_bp_cells<<<grid(np), 256, 0, st>>>(state, np, 1.0 / G.h, G.T - 1, as<int4>(G.bp_cell), as<uint32_t>(G.bp_key),
+                                         as<int32_t>(G.bp_idx));
+    CKS(radix_sort_u32(as<uint32_t>(G.bp_key), as<int32_t>(G.bp_idx), as<uint32_t>(G.bp_key2), as<int32_t>(G.bp_idx2), np,
+                       G.bits, G.rs_tmp.p, st));
+    CKS(cudaMemsetAsync(G.bp_start.p, 0, sizeof(int) * G.T, st));
+    CKS(cudaMemsetAsync(G.bp_end.p, 0, sizeof(int) * G.T, st));
+    k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(G.bp_key), np, as<int>(G.bp_start), as<int>(G.bp_end));
+    k_bp_pairs<false><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
+                                                as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1, as<int32_t>(G.bp_cnt),
+                                                nullptr, nullptr, INT64_MAX);
+    CKS(scan_offsets<int32_t>(as<int32_t>(G.bp_cnt), np, nullptr, as<int64_t>(G.bp_off), G.scan_tmp.p, st));
+    k_bp_pairs<true><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
+                                               as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1, nullptr,
+                                               as<int64_t>(G.bp_off), as<int2>(G.bp_pairs), G.pcap);
+    k_g_take<<<1, 1, 0, st>>>(as<int64_t>(G.bp_off) + np, G.pcap, &g->npair, &g->need_pairs, flags, GRAPH_OVF_PAIRS);
+    const int64_t* npair = &g->npair;
+
+    // ---- 2. pair contacts
+    k_pair_inputs<<<grid(G.pcap), 256, 0, st>>>(as<int2>(G.bp_pairs), G.pcap, npair, state, as<int32_t>(s.d_pmesh),
+                                                as<int32_t>(G.pr_mesh), as<double>(G.pr_pose), as<uint32_t>(G.tr_key),
+                                                as<int32_t>(G.tr_idx));
+    CKS(radix_sort_u32(as<uint32_t>(G.tr_key), as<int32_t>(G.tr_idx), as<uint32_t>(G.tr_key2), as<int32_t>(G.tr_idx2),
+                       G.pcap, G.pbits, G.rs_tmp.p, st, npair));
+    {
+        PairArgs a{};
+        const int nm = (int)s.mesh_off.size() - 1;
+        a.n_mesh = nm;
+        a.tris = as<double>(s.d_mtris);
+        a.tri_off = as<int64_t>(s.d_moff);
+        a.mean_edge = as<double>(s.d_mme);
+        a.bbox_diag = as<double>(s.d_mbd);
+        a.tri_sph = as<double4>(G.tri_sph);
+        a.mesh_R_bits = as<unsigned long long>(G.mesh_R);
+        a.mesh_valid = as<int>(G.mesh_valid);
+        a.n_pairs = G.pcap;
+        a.n_dev = npair;
+        a.pmesh = as<int32_t>(G.pr_mesh);
+        a.pose = as<double>(G.pr_pose);
+        a.mode = ZDX_MODE_ZDEM;
+        a.split = s.cfg.split_contacts ? 1 : 0;
+        a.tol_in = 0.0;
+        a.k = 1.0;
+        a.want_pts = 0;
+        int max_ntri = 1;
+        for (int m = 0; m < nm; ++m) max_ntri = std::max<int>(max_ntri, (int)(s.mesh_off[m + 1] - s.mesh_off[m]));
+        a.cap_side = max_ntri;
+        a.cap_seg = G.cap_seg;
+        const size_t P1 = (size_t)std::max<int64_t>(G.pcap, 1);
+        int64_t* pi64 = as<int64_t>(G.pair_i64);
+        int32_t* pi32 = as<int32_t>(G.pair_i32);
+        a.pair_seg_off = pi64;
+        a.pair_checks = pi64 + P1;
+        a.pair_stage_off = pi64 + 2 * P1;
+        a.pair_pts_stage_off = pi64 + 3 * P1;
+        a.pair_npts = pi64 + 4 * P1;
+        a.pair_nseg = pi32;
+        a.pair_status = pi32 + P1;
+        a.pair_ncontact = pi32 + 2 * P1;
+        a.pair_ncomp = pi32 + 3 * P1;
+        a.pair_nloop = pi32 + 4 * P1;
+        unsigned long long* cnt = as<unsigned long long>(G.counters);
+        a.seg_counter = cnt + 0;
+        a.contact_counter = cnt + 1;
+        a.pts_counter = cnt + 2;
+        a.checks_total = cnt + 3;
+        a.queue1 = reinterpret_cast<int*>(cnt + 4);
+        a.queue2 = reinterpret_cast<int*>(cnt + 5);
+        a.max_nseg = reinterpret_cast<int*>(cnt + 6);
+        a.err = reinterpret_cast<int*>(cnt + 7);
+        CKS(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
+        CKS(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
+        CKS(cudaMemsetAsync(G.mesh_R.p, 0, sizeof(unsigned long long) * std::max(nm, 1), st));
+        CKS(cudaMemsetAsync(G.mesh_valid.p, 0, sizeof(int) * std::max(nm, 1), st));
+        launch_mesh_prep(a, s.mesh_off.back(), st);
+        launch_cost_order(a, as<int32_t>(G.order), as<int>(G.buckets), st);
+        a.order = as<int32_t>(G.order);
+        a.item_begin = 0;
+        a.item_end = G.pcap;
+        a.k1_slot_bytes = tritest_slot_bytes(a.cap_side, a.cap_seg);
+        a.k1_slots = as<char>(G.k1_slots);
+        a.seg = as<double>(G.seg_arena);
+        a.seg_cap = G.segcap;
+        launch_segments(a, G.k1_grid, st);
+        a.k2_nmax = G.cap_seg;
+        a.k2_slot_bytes = rebuild_slot_bytes(G.cap_seg);
+        a.k2_nslots = G.k2_warps;
+        a.k2_slots = as<char>(G.k2_slots);
+        a.cgeom_stage = as<double>(G.cstage);
+        a.cinfo_stage = as<int32_t>(G.cistage);
+        a.clen_stage = as<int32_t>(G.cistage) + 4 * std::max<int64_t>(G.ccap, 1);
+        a.contact_cap = G.ccap;
+        a.pts_stage = nullptr;
+        a.pts_cap = 0;
+        launch_rebuild(a, G.k2_warps, st);
+        launch_gather_dev(a, as<int64_t>(G.pr_coff), as<double>(G.pr_geom), as<int32_t>(G.pr_info),
+                          as<int32_t>(G.pr_stats), G.scan_tmp.p, st);
+        k_g_pair_done<<<1, 1, 0, st>>>(cnt, g);
+        k_g_pair_stats<<<std::max(1, ctx->num_sms), 256, 0, st>>>(as<int32_t>(G.pr_stats), g, g);
+    }
+    k_key_bounds<<<grid(np + 1), 256, 0, st>>>(as<uint32_t>(G.tr_key), G.pcap, npair, np, as<int64_t>(G.tr_start));
+    k_range_bounds<<<grid(np + 1), 256, 0, st>>>(as<int2>(G.bp_pairs), G.pcap, npair, np, as<int64_t>(G.bp_pstart));
+
+    // ---- 3. particle-particle forces
+    k_pp_force<<<grid(G.pcap, 128), 128, 0, st>>>(as<int2>(G.bp_pairs), G.pcap, npair, as<int64_t>(G.pr_coff),
+                                                  as<double>(G.pr_geom), state, mat, s.cfg.dt, as<int64_t>(G.hkey),
+                                                  as<double>(G.hds), 0, &g->nhist, as<double>(G.pr_contrib),
+                                                  as<int32_t>(G.pr_active), as<double>(G.pr_ds), flags);
+
+    // ---- 4. walls
+    const int64_t* ncand = &g->ncand;
+    if (s.nw > 0) {
+        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+                                              as<int32_t>(G.w_active), nullptr, nullptr, INT64_MAX);
+        CKS(scan_offsets<int32_t>(as<int32_t>(G.w_active), np, nullptr, as<int64_t>(G.w_scan), G.scan_tmp.p, st));
+        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw, nullptr,
+                                              as<int64_t>(G.w_scan), as<int2>(G.w_pairs), G.wcap);
+        k_g_take<<<1, 1, 0, st>>>(as<int64_t>(G.w_scan) + np, G.wcap, &g->ncand, &g->need_cand, flags, GRAPH_OVF_CAND);
+        CKS(cudaMemsetAsync(G.w_valid.p, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(G.wcap, 1) * G.max_wtri, st));
+        WallArgs wa{state, mat, as<int32_t>(s.d_pmesh), as<double>(s.d_mtris), as<int64_t>(s.d_moff), as<double>(s.d_mrad),
+                    as<double>(s.d_wtris), as<double>(s.d_wnorm), as<int64_t>(s.d_wtri_off), as<double>(s.d_wmat),
+                    as<int2>(G.w_pairs), G.wcap, G.max_wtri, s.cfg.dt, as<int64_t>(G.whkey), as<double>(G.whds), 0,
+                    as<double>(G.w_contrib), as<int32_t>(G.w_valid), as<int32_t>(G.w_act), as<double>(G.w_ds),
+                    as<double>(G.w_scratch), G.spts, G.wall_warps, ncand, &g->nwhist, flags};
+        k_walls<<<(G.wall_warps + 3) / 4, 128, 0, st>>>(wa);
+        k_count_valid<<<grid((int64_t)std::max<int64_t>(G.wcap, 1) * G.max_wtri), 256, 0, st>>>(
+            as<int32_t>(G.w_valid), (int64_t)std::max<int64_t>(G.wcap, 1) * G.max_wtri, ncand, G.max_wtri,
+            &g->wall_contacts);
+    } else {
+        CKS(cudaMemsetAsync(G.w_scan.p, 0, sizeof(int64_t) * (size_t)(np + 1), st));
+    }
+
+    // ---- 5+6. scatter, integrate (skipped when a capacity overflowed in this step)
+    k_scatter_integrate<<<grid(np, 128), 128, 0, st>>>(
+        np, as<int2>(G.bp_pairs), as<int64_t>(G.bp_pstart), as<int32_t>(G.tr_idx), as<int64_t>(G.tr_start),
+        as<int64_t>(G.pr_coff), as<double>(G.pr_contrib), as<int64_t>(G.w_scan), as<double>(G.w_contrib),
+        as<int32_t>(G.w_valid), G.max_wtri, state, mat, as<double>(G.grav), s.cfg.dt, as<double>(s.d_force),
+        as<double>(s.d_torque), as<int32_t>(s.d_count), flags);
+
+    // ---- history: this step's active keys, in order
+    CKS(scan_offsets<int32_t>(as<int32_t>(G.pr_active), G.pcap, npair, as<int64_t>(G.pr_hscan), G.scan_tmp.p, st));
+    k_hist_write<<<grid(G.pcap), 256, 0, st>>>(as<int32_t>(G.pr_active), as<int64_t>(G.pr_hscan), G.pcap, npair,
+                                               as<int2>(G.bp_pairs), 32, as<double>(G.pr_ds), as<int64_t>(G.hkey2),
+                                               as<double>(G.hds2), flags);
+    if (s.nw > 0) {
+        CKS(scan_offsets<int32_t>(as<int32_t>(G.w_act), G.wcap, ncand, as<int64_t>(G.w_hscan), G.scan_tmp.p, st));
+        k_hist_write<<<grid(G.wcap), 256, 0, st>>>(as<int32_t>(G.w_act), as<int64_t>(G.w_hscan), G.wcap, ncand,
+                                                   as<int2>(G.w_pairs), 16, as<double>(G.w_ds), as<int64_t>(G.whkey2),
+                                                   as<double>(G.whds2), flags);
+    } else {
+        CKS(cudaMemsetAsync(G.w_hscan.p, 0, sizeof(int64_t), st));
+    }
+    k_g_commit<<<std::max(1, ctx->num_sms), 256, 0, st>>>(g, as<int64_t>(G.pr_hscan), as<int64_t>(G.w_hscan),
+                                                           as<int64_t>(G.hkey), as<double>(G.hds), as<int64_t>(G.hkey2),
+                                                           as<double>(G.hds2), as<int64_t>(G.whkey), as<double>(G.whds),
+                                                           as<int64_t>(G.whkey2), as<double>(G.whds2));
+    CKS(cudaGetLastError());
+    return ZDX_OK;
+}
+
+static int graph_capture(zdx_ctx* ctx, Scene& s) {
+    GraphStep& G = s.gs;
+    G.drop_graph();
+    int rc = graph_alloc(ctx, s);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    CKS(cudaStreamSynchronize(st));
+    cudaGraph_t graph = nullptr;
+    CKS(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    rc = graph_launch_step(ctx, s);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    size_t nn = 0;
+    cudaGraphGetNodes(graph, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) cudaGraphGetNodes(graph, nodes.data(), &nn);
+    G.kernels_per_step = 0;
+    for (size_t i = 0; i < nn; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) G.kernels_per_step++;
+    }
+    e = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    return ZDX_OK;
+}
+
+// First use: fixed sizes, capacities, the history moved in from the Scene's buffers.
+static int graph_enter(zdx_ctx* ctx, Scene& s) {
+    GraphStep& G = s.gs;
+    cudaStream_t st = ctx->stream;
+    const int np = s.np;
+    if (!G.host) CKS(cudaMallocHost(&G.host, sizeof(GraphCounts)));
+    G.drop_graph();  // buffers may move below
+    double rmax = 0.0;
+    for (int i = 0; i < np; ++i) rmax = std::max(rmax, s.mat[17 * (size_t)i + 2]);
+    G.h = 2.0 * rmax * (1.0 + 1e-9);
+    if (!(G.h > 0.0)) G.h = 1.0;
+    G.T = 1;
+    while (G.T < (uint32_t)std::max(2 * np, 2)) G.T <<= 1;
+    G.bits = 0;
+    while ((1u << G.bits) < G.T) G.bits++;
+    G.pbits = 0;
+    while ((1ll << G.pbits) < np) G.pbits++;
+    G.pbits = std::max(G.pbits, 1);
+    G.max_wtri = 1;
+    for (int w = 0; w < s.nw; ++w) G.max_wtri = std::max<int>(G.max_wtri, (int)(s.wtri_off[w + 1] - s.wtri_off[w]));
+    int maxpt = 0;
+    for (int i = 0; i < np; ++i) maxpt = std::max<int>(maxpt, (int)(s.mesh_off[s.pmesh[i] + 1] - s.mesh_off[s.pmesh[i]]));
+    G.spts = 3 * (int64_t)maxpt + 8;
+    G.wall_warps = ctx->num_sms * 4;
+    // capacities: grown later from what a step asks for
+    const int64_t hist_need = std::max<int64_t>(s.nhist, 1), whist_need = std::max<int64_t>(s.nwhist, 1);
+    if (G.pcap == 0) G.pcap = std::max<int64_t>(8 * (int64_t)np + 1024, hist_need);
+    if (G.wcap == 0) G.wcap = std::max<int64_t>((int64_t)np * std::max(s.nw, 1), whist_need);
+    if (G.ccap == 0) G.ccap = G.pcap + 1024;
+    if (G.segcap == 0) G.segcap = 16 * G.pcap + (1 << 20);
+    if (G.cap_seg == 0) G.cap_seg = 1024;
+    int rc = graph_alloc(ctx, s);
+    if (rc) return rc;
+    GraphCounts z{};
+    z.nhist = s.nhist;
+    z.nwhist = s.nwhist;
+    CKS(cudaMemcpyAsync(G.g.p, &z, sizeof(z), cudaMemcpyHostToDevice, st));
+    const double g3[3] = {s.cfg.gravity[0], s.cfg.gravity[1], s.cfg.gravity[2]};
+    CKS(cudaMemcpyAsync(G.grav.p, g3, sizeof(g3), cudaMemcpyHostToDevice, st));
+    if (s.nhist) {
+        CKS(cudaMemcpyAsync(G.hkey.p, s.d_hist_key.p, sizeof(int64_t) * s.nhist, cudaMemcpyDeviceToDevice, st));
+        CKS(cudaMemcpyAsync(G.hds.p, s.d_hist_ds.p, sizeof(double) * 3 * s.nhist, cudaMemcpyDeviceToDevice, st));
+    }
+    if (s.nwhist) {
+        CKS(cudaMemcpyAsync(G.whkey.p, s.d_whist_key.p, sizeof(int64_t) * s.nwhist, cudaMemcpyDeviceToDevice, st));
+        CKS(cudaMemcpyAsync(G.whds.p, s.d_whist_ds.p, sizeof(double) * 3 * s.nwhist, cudaMemcpyDeviceToDevice, st));
+    }
+    CKS(cudaStreamSynchronize(st));
+    G.active = true;
+    return ZDX_OK;
+}
+
+int scene_graph_leave(zdx_ctx* ctx, Scene& s) {
+    GraphStep& G = s.gs;
+    if (!G.active) return ZDX_OK;
+    cudaStream_t st = ctx->stream;
+    CKS(cudaMemcpyAsync(G.host, G.g.p, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st));
+    CKS(cudaStreamSynchronize(st));
+    const int64_t nh = G.host->nhist, nw = G.host->nwhist;
+    CKS(s.d_hist_key.ensure(sizeof(int64_t) * std::max<int64_t>(nh, 1)));
+    CKS(s.d_hist_ds.ensure(sizeof(double) * 3 * std::max<int64_t>(nh, 1)));
+    CKS(s.d_whist_key.ensure(sizeof(int64_t) * std::max<int64_t>(nw, 1)));
+    CKS(s.d_whist_ds.ensure(sizeof(double) * 3 * std::max<int64_t>(nw, 1)));
+    if (nh) {
+        CKS(cudaMemcpyAsync(s.d_hist_key.p, G.hkey.p, sizeof(int64_t) * nh, cudaMemcpyDeviceToDevice, st));
+        CKS(cudaMemcpyAsync(s.d_hist_ds.p, G.hds.p, sizeof(double) * 3 * nh, cudaMemcpyDeviceToDevice, st));
+    }
+    if (nw) {
+        CKS(cudaMemcpyAsync(s.d_whist_key.p, G.whkey.p, sizeof(int64_t) * nw, cudaMemcpyDeviceToDevice, st));
+        CKS(cudaMemcpyAsync(s.d_whist_ds.p, G.whds.p, sizeof(double) * 3 * nw, cudaMemcpyDeviceToDevice, st));
+    }
+    CKS(cudaStreamSynchronize(st));
+    s.nhist = nh;
+    s.nwhist = nw;
+    G.active = false;
+    return ZDX_OK;
+}
+
+int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps) {
+    GraphStep& G = s.gs;
+    cudaStream_t st = ctx->stream;
+    if (nsteps <= 0) return ZDX_OK;
+    if (!G.active) {
+        int rc = graph_enter(ctx, s);
+        if (rc) return rc;
+    }
+    if (!G.exec) {
+        int rc = graph_capture(ctx, s);
+        if (rc) return rc;
+    }
+    // launch in chunks; after each chunk read the counters and grow + capture again on an overflow
+    int remaining = nsteps, regrow = 0;
+    while (remaining > 0) {
+        CKS(cudaMemcpyAsync(G.host, G.g.p, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        const int64_t before = G.host->steps_done;
+        const int chunk = std::min(remaining, 64);
+        for (int k = 0; k < chunk; ++k) CKS(cudaGraphLaunch(G.exec, st));
+        ctx->launches += (long long)chunk * G.kernels_per_step;
+        CKS(cudaMemcpyAsync(G.host, G.g.p, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        const GraphCounts& h = *G.host;
+        const int done = (int)(h.steps_done - before);
+        remaining -= done;
+        s.step += done;
+        if (h.flags == 0) continue;
+        if (++regrow > 32) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "graph step: capacities keep overflowing (flags %d)", h.flags);
+        if (h.flags & GRAPH_OVF_PAIRS) G.pcap = h.need_pairs + h.need_pairs / 4 + 1024;
+        if (h.flags & GRAPH_OVF_CAND) G.wcap = h.need_cand + h.need_cand / 4 + 1024;
+        if (h.flags & GRAPH_OVF_SEGS) G.segcap = (int64_t)h.pair_counters[0] + (int64_t)h.pair_counters[0] / 4 + 4096;
+        if (h.flags & GRAPH_OVF_CONTACTS) G.ccap = (int64_t)h.pair_counters[1] + (int64_t)h.pair_counters[1] / 4 + 1024;
+        if (h.flags & GRAPH_OVF_PAIR) G.cap_seg *= 4;
+        G.ccap = std::max(G.ccap, G.pcap / 4);
+        // the history buffers may be reallocated: park it in the Scene's buffers, then come back
+        int rc = scene_graph_leave(ctx, s);
+        if (!rc) rc = graph_enter(ctx, s);
+        if (!rc) rc = graph_capture(ctx, s);
+        if (rc) return rc;
+    }
+    const GraphCounts& h = *G.host;
+    StepStats stats;
+    stats.pairs = h.npair;
+    stats.segments = (int64_t)h.segments;
+    stats.tri_checks = (int64_t)h.tri_checks;
+    stats.comps = (int64_t)h.comps;
+    stats.loops = (int64_t)h.loops;
+    stats.wall_contacts = (int64_t)h.wall_contacts;
+    stats.contacts = (int64_t)h.contacts + stats.wall_contacts;
+    s.last = stats;
+    s.have_forces = true;
+    s.host_dirty = true;
     return ZDX_OK;
 }
 

@@ -61,6 +61,69 @@ struct StepStats {
     double tri_ms = 0, rebuild_ms = 0, step_ms = 0, output_ms = 0;
 };
 
+// Device-resident counters of the graph step (one per scene), mirrored to pinned host memory after a
+// batch of steps.
+struct GraphCounts {
+    int64_t npair, ncand, nhist, nwhist;  // this step's pairs / wall candidates, history sizes
+    int64_t steps_done;                   // steps that ran to the end (state advanced)
+    int64_t need_pairs, need_cand;        // totals the last step asked for
+    int32_t flags, pad;                   // GRAPH_OVF_* bits of the last step (0: it completed)
+    unsigned long long contacts, wall_contacts, tri_checks, segments, comps, loops;
+    unsigned long long pair_counters[8];  // the pair kernels' counters (segments, contacts, ..., max nseg, err)
+};
+enum : int {
+    GRAPH_OVF_PAIRS = 1,     // broad-phase pairs above the pair capacity
+    GRAPH_OVF_CAND = 2,      // wall candidates above their capacity
+    GRAPH_OVF_SEGS = 4,      // segment arena
+    GRAPH_OVF_CONTACTS = 8,  // contact staging
+    GRAPH_OVF_PAIR = 16,     // a pair above the per-pair segment or edge capacity
+};
+
+// The step with every count on the device and every buffer at a fixed capacity, captured once into a
+// CUDA graph and replayed.  A step that would overflow a capacity leaves the state and history
+// untouched and raises a flag; the host then grows the capacities, captures again and repeats it.
+struct GraphStep {
+    bool active = false;       // the history lives in these buffers (not in the Scene's)
+    cudaGraphExec_t exec = nullptr;
+    int64_t pcap = 0, ccap = 0, wcap = 0, segcap = 0;
+    int cap_seg = 0, k2_warps = 0, k1_grid = 0, wall_warps = 0, max_wtri = 1, kernels_per_step = 0;
+    int64_t spts = 0;
+    uint32_t T = 1;
+    int bits = 0, pbits = 1;
+    double h = 1.0;
+    GraphCounts* host = nullptr;  // pinned
+    DevBuf g, grav;
+    DevBuf bp_cell, bp_key, bp_idx, bp_key2, bp_idx2, bp_start, bp_end, bp_cnt, bp_off, bp_pairs, bp_pstart;
+    DevBuf rs_tmp, scan_tmp;
+    DevBuf tr_key, tr_idx, tr_key2, tr_idx2, tr_start;
+    DevBuf pr_mesh, pr_pose, pr_coff, pr_stats, pr_geom, pr_info, pr_contrib, pr_active, pr_ds, pr_hscan;
+    DevBuf w_active, w_scan, w_pairs, w_contrib, w_valid, w_act, w_ds, w_hscan, w_scratch;
+    DevBuf hkey, hds, hkey2, hds2, whkey, whds, whkey2, whds2;
+    // pair kernels' workspaces
+    DevBuf tri_sph, mesh_R, mesh_valid, order, buckets, pair_i64, pair_i32, counters, k1_slots, seg_arena, k2_slots,
+        cstage, cistage;
+
+    std::vector<DevBuf*> bufs() {
+        return {&g, &grav, &bp_cell, &bp_key, &bp_idx, &bp_key2, &bp_idx2, &bp_start, &bp_end, &bp_cnt, &bp_off,
+                &bp_pairs, &bp_pstart, &rs_tmp, &scan_tmp, &tr_key, &tr_idx, &tr_key2, &tr_idx2, &tr_start, &pr_mesh,
+                &pr_pose, &pr_coff, &pr_stats, &pr_geom, &pr_info, &pr_contrib, &pr_active, &pr_ds, &pr_hscan,
+                &w_active, &w_scan, &w_pairs, &w_contrib, &w_valid, &w_act, &w_ds, &w_hscan, &w_scratch, &hkey, &hds,
+                &hkey2, &hds2, &whkey, &whds, &whkey2, &whds2, &tri_sph, &mesh_R, &mesh_valid, &order, &buckets,
+                &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &cstage, &cistage};
+    }
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    void release() {
+        drop_graph();
+        for (DevBuf* b : bufs()) b->release();
+        if (host) cudaFreeHost(host);
+        host = nullptr;
+        active = false;
+    }
+};
+
 struct Scene {
     SimConfig cfg;
     std::vector<ParticleInit> inits;
@@ -99,8 +162,10 @@ struct Scene {
     DevBuf pr_mesh, pr_pose, pr_ncontact, pr_coff, pr_stats, pr_geom, pr_info, pr_contrib, pr_active, pr_ds, pr_scan;
     DevBuf w_contrib, w_valid, w_active, w_ds, w_scan, w_pairs;
     int64_t pair_cap = 0, contact_cap = 0;
+    GraphStep gs;
 
     void release_device() {
+        gs.release();
         for (DevBuf* b : {&d_state, &d_mat, &d_pmesh, &d_mtris, &d_moff, &d_mme, &d_mbd, &d_mrad, &d_wtris, &d_wnorm,
                           &d_wtri_off, &d_wpose, &d_wmat, &d_wrad, &d_force, &d_torque, &d_count, &d_hist_key,
                           &d_hist_ds, &d_whist_key, &d_whist_ds, &d_hist_key2, &d_hist_ds2, &d_whist_key2,
@@ -115,6 +180,11 @@ struct Scene {
 int scene_from_config(zdx_ctx* ctx, const SimConfig& cfg, Scene& s, std::string& err);
 int scene_upload(zdx_ctx* ctx, Scene& s);
 int scene_step(zdx_ctx* ctx, Scene& s);
+// nsteps steps through the captured graph; statistics of the last step land in s.last (no timings).
+int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps);
+// Moves the tangential history from the graph step's buffers back to the Scene's (before a plain step
+// or a state download that needs it).
+int scene_graph_leave(zdx_ctx* ctx, Scene& s);
 int scene_download(zdx_ctx* ctx, Scene& s);
 // write_vtk_particles / write_particle_state_txt, src/main.cpp:1710-1870
 bool write_vtk_particles(const std::string& path, const Scene& s);

@@ -58,12 +58,34 @@ extern "C" int zdx_scene_step(zdx_ctx* ctx, int nsteps) {
     return ZDX_OK;
 }
 
+extern "C" int zdx_scene_step_graph(zdx_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "cudaSetDevice failed");
+    return scene_step_graph(ctx, *ctx->scene, nsteps);
+}
+
+extern "C" int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t contacts, int64_t segments,
+                                       int seg_per_pair) {
+    if (!ctx || pairs < 0 || contacts < 0 || segments < 0 || seg_per_pair < 0) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    GraphStep& G = ctx->scene->gs;
+    if (G.active) return ctx_fail(ctx, ZDX_ERR_STATE, "graph step already running; reserve before the first one");
+    G.pcap = pairs;
+    G.ccap = contacts;
+    G.segcap = segments;
+    G.cap_seg = seg_per_pair;
+    return ZDX_OK;
+}
+
 extern "C" int zdx_scene_info(zdx_ctx* ctx, int64_t* info) {
     if (!ctx || !info) return ZDX_ERR_INVALID;
     if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
     const Scene& s = *ctx->scene;
+    const bool g = s.gs.active && s.gs.host;  // the graph step keeps the history sizes on the device
     int64_t v[12] = {s.np, s.nw, s.step, s.last.contacts, s.last.tri_checks, s.last.segments, s.last.comps,
-                     s.last.loops, s.last.pairs, s.last.wall_contacts, s.nhist, s.nwhist};
+                     s.last.loops, s.last.pairs, s.last.wall_contacts, g ? s.gs.host->nhist : s.nhist,
+                     g ? s.gs.host->nwhist : s.nwhist};
     std::memcpy(info, v, sizeof(v));
     return ZDX_OK;
 }
@@ -117,7 +139,7 @@ extern "C" int zdx_scene_write_output(zdx_ctx* ctx, int64_t step) {
 
 // The body of zdem_cpu's main after argument parsing (src/main.cpp:1879-2503): load, then per step the
 // device step, outputs every output_interval steps and the same log line.
-extern "C" int zdx_run_config(const char* config_path, int device) {
+static int run_config(const char* config_path, int device, bool graph) {
     if (!config_path) return 1;
     zdx_ctx* ctx = nullptr;
     int rc = zdx_create(&ctx, device);
@@ -137,7 +159,17 @@ extern "C" int zdx_run_config(const char* config_path, int device) {
     std::filesystem::create_directories(s.cfg.output_dir, ec);
     for (int step = 0; step < s.cfg.steps; ++step) {
         auto t0 = std::chrono::steady_clock::now();
-        rc = scene_step(ctx, s);
+        int batch = 1;
+        if (graph) {
+            // up to and including the next output step, in one graph batch
+            const int every = std::max(s.cfg.output_interval, 1);
+            const int next = std::min(((step + every - 1) / every) * every, s.cfg.steps - 1);
+            batch = next - step + 1;
+            rc = scene_step_graph(ctx, s, batch);
+            step = next;
+        } else {
+            rc = scene_step(ctx, s);
+        }
         if (rc) {
             std::cerr << "zdem_gpu: step " << step << ": " << zdx_last_error(ctx) << "\n";
             zdx_destroy(ctx);
@@ -147,7 +179,7 @@ extern "C" int zdx_run_config(const char* config_path, int device) {
             auto to = std::chrono::steady_clock::now();
             zdx_scene_write_output(ctx, step);
             double out_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - to).count();
-            double step_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            double step_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / batch;
             std::cout << "step=" << step << " contacts=" << s.last.contacts << " step_ms=" << (long long)step_ms
                       << " tri_ms=" << (long long)s.last.tri_ms << " rebuild_ms=" << (long long)s.last.rebuild_ms
                       << " output_ms=" << (long long)out_ms << " tri_checks=" << s.last.tri_checks
@@ -159,3 +191,6 @@ extern "C" int zdx_run_config(const char* config_path, int device) {
     zdx_destroy(ctx);
     return 0;
 }
+
+extern "C" int zdx_run_config(const char* config_path, int device) { return run_config(config_path, device, false); }
+extern "C" int zdx_run_config_graph(const char* config_path, int device) { return run_config(config_path, device, true); }

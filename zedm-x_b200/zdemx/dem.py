@@ -2,6 +2,7 @@
 
     sc = Scene("config.txt")      # parse_config_file + particle/wall set-up (src/main.cpp:1531-2022)
     sc.step(100)                   # 100 iterations of the step loop body (src/main.cpp:2034-2468)
+    sc.step_graph(100)             # the same steps, replayed from one captured CUDA graph
     st = sc.state()                # (np, 16): pos quat(w,x,y,z) vel omega L
     sc.info()                      # the step log's counters for the last step
     sc.write_output(step)          # the particle VTK and state txt files (src/main.cpp:1710-1870)
@@ -27,6 +28,15 @@ class Scene:
     def step(self, n: int = 1):
         _lib.check(_lib.lib().zdx_scene_step(self.ctx.handle, int(n)), self.ctx.handle)
 
+    def step_graph(self, n: int = 1):
+        """n steps through the captured CUDA graph (device-resident counts, same results as step)."""
+        _lib.check(_lib.lib().zdx_scene_step_graph(self.ctx.handle, int(n)), self.ctx.handle)
+
+    def graph_reserve(self, pairs: int = 0, contacts: int = 0, segments: int = 0, seg_per_pair: int = 0):
+        """Initial capacities of the graph step (0 = default); it grows them on overflow."""
+        _lib.check(_lib.lib().zdx_scene_graph_reserve(self.ctx.handle, int(pairs), int(contacts), int(segments),
+                                                      int(seg_per_pair)), self.ctx.handle)
+
     def info(self) -> dict:
         v = np.zeros(12, np.int64)
         _lib.check(_lib.lib().zdx_scene_info(self.ctx.handle, v.ctypes.data_as(_lib._i64p)), self.ctx.handle)
@@ -50,6 +60,8 @@ class Scene:
         _lib.check(_lib.lib().zdx_scene_write_output(self.ctx.handle, int(step)), self.ctx.handle)
 
 
-def run_config(config_path: str, device: int = 0) -> int:
+def run_config(config_path: str, device: int = 0, graph: bool = False) -> int:
     """zdem_cpu's whole run (outputs and log line included); returns the exit code."""
+    if graph:
+        return _lib.lib().zdx_run_config_graph(config_path.encode(), int(device))
     return _lib.lib().zdx_run_config(config_path.encode(), int(device))
