@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--plain-pairs", type=int, default=2048, help="pairs timed in the plain per-pair form")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--workload", choices=["sweep", "pour", "two", "adjoint"], default="sweep",
+                    help="sweep: the batched pair sweep (default); pour: 100k-particle DEM step in one CUDA graph; "
+                         "two: the two-particle DEM run; adjoint: contact geometry + its adjoint")
+    ap.add_argument("--particles", type=int, default=100_000, help="pour: particle count")
+    ap.add_argument("--preroll", type=int, default=1500, help="pour: untimed steps before warm-up (collisions start)")
     return ap.parse_args()
 
 
@@ -192,6 +197,12 @@ def emit(d):
 
 def main():
     args = parse()
+    if args.workload == "pour":
+        return run_pour(args)
+    if args.workload == "two":
+        return run_two(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -382,6 +393,470 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
 
+# ---------------------------------------------------------------------------------- DEM legs
+def _ref_exe():
+    return os.path.join(ROOT, "oracle", "_ref", "zdem_cpu")
+
+
+def _ref_step_ms(cfg_path, steps, timeout=3600):
+    """zdem_cpu (the reference program, oracle/_ref) on a copy of the config with `steps` steps and an
+    output every step: per step its own std::chrono step time minus its output time (step_ms - output_ms of
+    its log line).  Each output path is made a directory, so the reference's writers fail to open it and
+    return at once (src/main.cpp:1716-1719, 1846-1849): a 100k-particle VTK is gigabytes of text."""
+    import re
+    import tempfile
+
+    text = open(cfg_path).read()
+    out = tempfile.mkdtemp(prefix="zdx_ref_")
+    prefix = re.search(r"(?m)^vtk_prefix = (.*)$", text).group(1).strip()
+    text = re.sub(r"(?m)^steps = .*$", f"steps = {steps}", text)
+    text = re.sub(r"(?m)^output_interval = .*$", "output_interval = 1", text)
+    text = re.sub(r"(?m)^output_dir = .*$", f"output_dir = {out}", text)
+    for k in range(steps):
+        for ext in (".vtk", ".txt"):
+            os.makedirs(os.path.join(out, f"{prefix}_{k:06d}{ext}"))
+    c = os.path.join(out, "ref.cfg")
+    open(c, "w").write(text)
+    p = subprocess.run([_ref_exe(), "--config", c], capture_output=True, text=True, timeout=timeout)
+    if p.returncode != 0:
+        raise RuntimeError(p.stderr[-500:])
+    ms = [float(a) - float(b) for a, b in re.findall(r"step_ms=([0-9.]+).*?output_ms=([0-9.]+)", p.stdout)]
+    return ms, p.stdout
+
+
+def _ref_run_wall(cfg_path, steps, dt=None, every=None, hiprec=False, timeout=3600):
+    """The reference program on a copy of the config: wall seconds of the whole run and its output dir."""
+    import re
+    import tempfile
+
+    text = open(cfg_path).read()
+    out = tempfile.mkdtemp(prefix="zdx_ref_")
+    text = re.sub(r"(?m)^steps = .*$", f"steps = {steps}", text)
+    if dt is not None:
+        text = re.sub(r"(?m)^dt = .*$", f"dt = {dt!r}", text)
+    text = re.sub(r"(?m)^output_interval = .*$", f"output_interval = {every or (1 << 30)}", text)
+    text = re.sub(r"(?m)^output_dir = .*$", f"output_dir = {out}", text)
+    c = os.path.join(out, "ref.cfg")
+    open(c, "w").write(text)
+    if hiprec:
+        from oracle import LIB_REF_HIPREC
+
+        code = ("import sys; sys.path.insert(0, %r); from oracle import Reference; import ctypes; "
+                "r = Reference(%r); rc = r.main(['--config', %r]); ctypes.CDLL(None).fflush(None); sys.exit(rc)") % (
+            os.path.join(ROOT, "oracle"), LIB_REF_HIPREC, c)
+        cmd = [sys.executable, "-c", code]
+    else:
+        cmd = [_ref_exe(), "--config", c]
+    t0 = time.perf_counter()
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    wall = time.perf_counter() - t0
+    if p.returncode != 0:
+        raise RuntimeError(p.stderr[-500:])
+    return wall, out
+
+
+def _state_txt(path):
+    rows, cur = [], {}
+    for line in open(path):
+        line = line.strip()
+        if line == "particle":
+            cur = {}
+        elif line == "end_particle":
+            rows.append(np.r_[cur["pos"], cur["quat"], cur["vel"], cur["omega"]])
+        elif "=" in line:
+            k, v = [x.strip() for x in line.split("=", 1)]
+            if k in ("pos", "quat", "vel", "omega"):
+                cur[k] = np.array([float(x) for x in v.split()])
+    return np.asarray(rows)
+
+
+def _mean_particle_tris(cfg_path):
+    """Mean triangle count over the particles of a config (binary STL headers)."""
+    import re
+    from collections import Counter
+
+    paths = Counter(re.findall(r"(?ms)^particle\nstl = (.*?)$", open(cfg_path).read()))
+    total = 0
+    for p, c in paths.items():
+        with open(p, "rb") as f:
+            f.seek(80)
+            total += c * int(np.frombuffer(f.read(4), "<u4")[0])
+    return total / max(sum(paths.values()), 1)
+
+
+def _lib_stream(ctx):
+    import torch
+
+    return torch.cuda.ExternalStream(ctx.stream_ptr())
+
+
+def _timed_steps(sc, stream, flush, n, graph):
+    """Device time of n single steps (CUDA events on the library stream, L2 flushed before each)."""
+    import torch
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    for k in range(n):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[k][0].record(stream)
+        (sc.step_graph if graph else sc.step)(1)
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def run_pour(args):
+    """A 100,000-particle pour (five templates, closed box, gravity), the whole step as one CUDA graph."""
+    import tempfile
+
+    import torch
+
+    from zdemx import _lib
+    from zdemx.dem import Scene
+    from zdemx.workloads import pour_scene
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    d = tempfile.mkdtemp(prefix="zdx_pour_")
+    cfg_path = pour_scene(d, n=args.particles, seed=args.seed)
+    desc = (f"pour: {args.particles} particles (3 ellipsoid hulls of 64 points + icospheres s=2,3; circumradius 1 mm), "
+            "jittered lattice in a closed 12-triangle box (60 x 60 mm floor), g=-9.81 z, dt=2e-6, "
+            "velocities N(0, 0.05 m/s), zdem force law, split_contacts=1, FP64")
+    if args.impl == "reference":
+        if not os.path.exists(_ref_exe()):
+            emit({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"})
+            return
+        ms, _ = _ref_step_ms(cfg_path, max(1, min(args.steps, 2)))
+        T = sum(ms) / 1e3
+        value = len(ms) / T
+        emit({"impl": "reference", "metric": "DEM steps/s", "value": value, "unit": "steps/s", "n_gpus": 1,
+              "steps": len(ms), "warmup": 0, "ms_per_step": 1e3 * T / len(ms), "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pour scene)",
+              "config": {"workload": desc},
+              "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
+                               "sample": f"the first {len(ms)} steps of zdem_cpu on the same config (its step_ms)"},
+              "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctx = _lib.Context(0)
+    t0 = time.perf_counter()
+    sc = Scene(cfg_path, ctx)
+    load_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sc.step_graph(args.preroll)
+    preroll_s = time.perf_counter() - t0
+    sc.step_graph(max(args.warmup, 3))
+    stream = _lib_stream(ctx)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    launches0 = ctx.timings()["launches"]
+    infos = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                ev[k][0].record(stream)
+            sc.step_graph(1)
+            with torch.cuda.stream(stream):
+                ev[k][1].record(stream)
+            infos.append(sc.info())
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    launches = ctx.timings()["launches"] - launches0
+    T = sum(step_ms) / 1e3
+    value = args.steps / T
+    # the same steps without the graph (one launch per kernel, the host reads the counts)
+    plain_ms = _timed_steps(sc, stream, flush, 3, graph=False)
+    # e2e: the graph step plus the whole state brought back to the host every step
+    e2e = []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        sc.step_graph(1)
+        sc.state()
+        e2e.append(time.perf_counter() - t1)
+    np_ = sc.n
+    d2h = np_ * (16 * 8 + 3 * 8 * 2 + 4)
+    peak, peak_kind = measured_peaks()
+    # algorithmic bytes of a step: particle state read + written, material read, and every candidate pair's
+    # two FP64 triangle soups (72 B per triangle) read once
+    pairs = int(np.mean([i["pairs"] for i in infos]))
+    mean_tris = _mean_particle_tris(cfg_path)
+    abytes = np_ * (2 * 128 + 136) + pairs * 72.0 * 2 * mean_tris
+    achieved = abytes / (T / args.steps) / 1e9
+    try:
+        if args.cpu_seconds <= 0:
+            raise RuntimeError("skipped (--cpu-seconds 0)")
+        ms_ref, _ = _ref_step_ms(cfg_path, 1)
+        cpu = {"value": 1e3 / ms_ref[0], "unit": "steps/s", "cores": 1, "kind": "reference",
+               "sample": f"step 0 of zdem_cpu on the same config ({ms_ref[0] / 1e3:.1f} s, its step_ms - output_ms)"}
+    except Exception as e:
+        cpu = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
+    last = infos[-1]
+    emit({"metric": "DEM steps/s", "value": value, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+          "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * T / args.steps, "higher_is_better": True,
+          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pour scene)",
+          "config": {"workload": desc, "particles": np_, "preroll_steps": args.preroll, "mean_tris": mean_tris,
+                     "l2": "flushed (256 MB write) before every timed step", "graph": "whole step, one CUDA graph",
+                     "pairs_per_step": pairs, "contacts_last_step": last["contacts"],
+                     "wall_contacts_last_step": last["wall_contacts"], "segments_last_step": last["segments"],
+                     "load_s": load_s, "preroll_s": preroll_s},
+          "e2e": {"value": args.steps / sum(e2e), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
+          "gpu_launches": int(launches),
+          "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "traffic": None, "kernel": "whole step (graph)", "peak_kind": f"{peak_kind} hbm_gbs",
+                       "algorithmic_bytes_per_launch": abytes},
+          "plain_step_ms": plain_ms, "cpu_baseline": cpu, "clocks": clk.summary()})
+
+
+def run_two(args):
+    """Two 320-triangle noised icospheres colliding (2000 steps, dt 1e-6), and the same pair held in
+    contact (dt 1e-15): steps/s of the whole DEM step, graph and plain, and the trajectory against the
+    reference program."""
+    import tempfile
+
+    import torch
+
+    from zdemx import _lib
+    from zdemx.dem import Scene
+    from zdemx.workloads import two_particle_scene
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    d = tempfile.mkdtemp(prefix="zdx_two_")
+    steps_run = 2000
+    cfg_path = two_particle_scene(d, seed=args.seed, steps=steps_run)
+    desc = ("two particles: 320-triangle noised icospheres (r 1 mm, +-15%), 1.9 mm apart, +-0.05 m/s, dt=1e-6, "
+            "2000 steps, split_contacts=1, zdem force law, FP64")
+    if args.impl == "reference":
+        if not os.path.exists(_ref_exe()):
+            emit({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"})
+            return
+        wall, _ = _ref_run_wall(cfg_path, steps_run)
+        value = steps_run / wall
+        emit({"impl": "reference", "metric": "DEM steps/s", "value": value, "unit": "steps/s", "n_gpus": 1,
+              "steps": steps_run, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+              "config": {"workload": desc},
+              "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
+                               "sample": f"the whole {steps_run}-step zdem_cpu run (wall clock)"},
+              "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctx = _lib.Context(0)
+    stream = _lib_stream(ctx)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    sc = Scene(cfg_path, ctx)
+    launches0 = ctx.timings()["launches"]
+    with ClockSampler(0) as clk:
+        g_ms = _timed_steps(sc, stream, flush, steps_run, graph=True)
+    launches = ctx.timings()["launches"] - launches0
+    final = sc.state()[0][:, :13]
+    sp = Scene(cfg_path, ctx)
+    p_ms = _timed_steps(sp, stream, flush, steps_run, graph=False)
+    same = bool(np.array_equal(sp.state()[0], sc.state()[0]))
+    se = Scene(cfg_path, ctx)
+    e2e = []
+    for k in range(steps_run):
+        t1 = time.perf_counter()
+        se.step_graph(1)
+        se.state()
+        e2e.append(time.perf_counter() - t1)
+    try:
+        _, out = _ref_run_wall(cfg_path, steps_run, every=steps_run - 1, hiprec=True)
+        ref = _state_txt(os.path.join(out, f"p_{steps_run - 1:06d}.txt"))
+        traj = {}
+        for name, cols in (("pos", slice(0, 3)), ("quat", slice(3, 7)), ("vel", slice(7, 10)), ("omega", slice(10, 13))):
+            scale = max(np.max(np.abs(ref[:, cols])), 1e-300)
+            traj[name] = float(np.max(np.abs(final[:, cols] - ref[:, cols])) / scale)
+    except Exception as e:
+        traj = {"unavailable": str(e)[:200]}
+    # sustained contact: the same pair with dt = 1e-15 (it stays in contact every step)
+    sus_path = os.path.join(d, "sustained.txt")
+    open(sus_path, "w").write(open(cfg_path).read().replace("dt = 1e-06", "dt = 1e-15"))
+    ss = Scene(sus_path, ctx)
+    ss.step_graph(10)
+    s_ms = _timed_steps(ss, stream, flush, 500, graph=True)
+    sus_contacts = ss.info()["contacts"]
+    cpu = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": "unavailable"}
+    sus_ref = None
+    try:
+        wall, _ = _ref_run_wall(cfg_path, steps_run)
+        cpu = {"value": steps_run / wall, "unit": "steps/s", "cores": 1, "kind": "reference",
+               "sample": f"the whole {steps_run}-step zdem_cpu run (wall clock, 1 thread)"}
+        wall_s, _ = _ref_run_wall(sus_path, 500)
+        sus_ref = 500 / wall_s
+    except Exception as e:
+        cpu["sample"] = f"unavailable: {e}"
+    T = sum(g_ms) / 1e3
+    emit({"metric": "DEM steps/s", "value": steps_run / T, "unit": "steps/s", "n_gpus": 1, "steps": steps_run,
+          "warmup": 0, "ms_per_step": 1e3 * T / steps_run, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+          "config": {"workload": desc, "l2": "flushed (256 MB write) before every timed step",
+                     "graph": "whole step, one CUDA graph"},
+          "e2e": {"value": steps_run / sum(e2e), "unit": "steps/s", "h2d_bytes_per_step": 0,
+                  "d2h_bytes_per_step": 2 * (16 * 8 + 6 * 8 + 4)},
+          "gpu_launches": int(launches),
+          "plain": {"value": steps_run / (sum(p_ms) / 1e3), "unit": "steps/s", "bit_identical_to_graph": same},
+          "trajectory_rel_err_vs_reference": traj,
+          "sustained_contact": {"value": 500 / (sum(s_ms) / 1e3), "unit": "pair-contacts/s", "dt": 1e-15,
+                                "contacts_per_step": sus_contacts, "reference_value": sus_ref},
+          "cpu_baseline": cpu, "clocks": clk.summary()})
+
+
+def run_adjoint(args):
+    """16,384 pairs of 320-triangle noised icospheres at depth U(0.01, 0.08) r: the forward call plus the
+    hand-written adjoint (dL/d corners and poses from dL/dSn, dL/dGn), and a batched central-difference
+    check of the pose gradients (h = 1e-7 r) with pairs whose stencil changes the loop topology flagged."""
+    import torch
+
+    from zdemx import _lib, synth
+    from zdemx.contact import MeshLibrary
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    if args.impl == "reference":
+        emit({"impl": "reference", "unavailable": "the reference has no derivatives (no adjoint to time)"})
+        return
+    npairs = 16384
+    rng = np.random.default_rng(args.seed)
+    lib = MeshLibrary.build(list(synth.noised_icospheres(2, 256, 1e-3, 0.15, rng)))
+    pm = rng.integers(0, 256, size=(npairs, 2)).astype(np.int32)
+    pp = synth.pair_poses(rng, npairs, 1e-3, 0.01, 0.08)
+    pp[:, 3:7] = synth.random_unit_quat(rng, npairs)
+    desc = ("adjoint: 16384 pairs of 320-triangle noised icospheres (256-mesh library, r 1 mm, +-15%), depth "
+            "U(0.01,0.08) r; forward + reverse of Sn, Gn w.r.t. corners and poses; FP64")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctx = _lib.Context(0)
+    stream = _lib_stream(ctx)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    meshes = {"tris": T(lib.tris), "tri_off": T(lib.tri_off), "mean_edge": T(lib.mean_edge), "bbox_diag": T(lib.bbox_diag)}
+    pairs = {"mesh": T(pm), "pose": T(pp)}
+    cap = 8 * npairs
+    out = {"ncontact": torch.zeros(npairs, dtype=torch.int32, device=dev),
+           "contact_off": torch.zeros(npairs + 1, dtype=torch.int64, device=dev),
+           "stats": torch.zeros(npairs, 4, dtype=torch.int32, device=dev),
+           "geom": torch.zeros(cap, 20, dtype=torch.float64, device=dev),
+           "info": torch.zeros(cap, 4, dtype=torch.int32, device=dev)}
+    tot = _lib.pair_contacts_device(ctx, meshes, pairs, out, k=1e7)
+    nc = int(tot[0])
+    wrng = np.random.default_rng(7)
+    w = np.concatenate([wrng.normal(size=(nc, 3)) / 1e-6, wrng.normal(size=(nc, 3)) / 1e-9], 1)
+    gc = T(w)
+    gt = torch.zeros_like(meshes["tris"])
+    gp = torch.zeros(npairs, 12, dtype=torch.float64, device=dev)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        _lib.pair_contacts_device(ctx, meshes, pairs, out, k=1e7)
+        _lib.pair_contacts_adjoint(ctx, meshes, pairs, gc, gt, gp)
+    fwd, adj = [], []
+    launches0 = ctx.timings()["launches"]
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            torch.cuda.synchronize()
+            _lib.pair_contacts_device(ctx, meshes, pairs, out, k=1e7)
+            fwd.append(ctx.timings()["total"])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0.record(stream)
+            _lib.pair_contacts_adjoint(ctx, meshes, pairs, gc, gt, gp)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            torch.cuda.synchronize()
+            adj.append(e0.elapsed_time(e1))
+    launches = ctx.timings()["launches"] - launches0
+    step_s = (sum(fwd) + sum(adj)) / 1e3 / args.steps
+    # batched central differences of the per-pair objective w.r.t. the 12 pose coordinates
+    gpose = gp.cpu().numpy()
+    base = _lib.pair_contacts_raw(ctx, lib.tris, lib.tri_off, lib.mean_edge, lib.bbox_diag, pm, pp)
+    coff = base["contact_off"]
+    incontact = np.diff(coff) > 0
+
+    def per_pair(r):
+        """Per pair sum of w . (Sn, Gn), contacts matched to the base call's by position within the pair
+        (pairs whose contact count changed are flagged by topo())."""
+        cr = r["contact_off"]
+        cnt = np.diff(cr)
+        pid = np.repeat(np.arange(npairs), cnt)
+        same = cnt == np.diff(coff)
+        loc = np.arange(len(pid)) - cr[pid]
+        bidx = np.where(same[pid], coff[pid] + loc, 0)
+        g = r["geom"]
+        v = np.einsum("ij,ij->i", w[bidx, 0:3], g[:, 0:3]) + np.einsum("ij,ij->i", w[bidx, 3:6], g[:, 3:6])
+        v = np.where(same[pid], v, 0.0)
+        return np.bincount(pid, weights=v, minlength=npairs)
+
+    def topo(r):
+        return np.concatenate([r["stats"], np.diff(r["contact_off"])[:, None]], 1)
+
+    def qmul(a, b):
+        aw, ax, ay, az = a
+        bw, bx, by, bz = b.T
+        return np.stack([aw * bw - ax * bx - ay * by - az * bz, aw * bx + ax * bw + ay * bz - az * by,
+                         aw * by - ax * bz + ay * bw + az * bx, aw * bz + ax * by - ay * bx + az * bw], 1)
+
+    t_base = topo(base)
+    flagged = np.zeros(npairs, bool)
+    fds = []
+    for h in (1e-7 * 1e-3, 0.25e-7 * 1e-3):
+        fd = np.zeros((npairs, 12))
+        fds.append(fd)
+        for b in range(2):
+            for k in range(3):
+                for kind in ("pos", "rot"):
+                    vals = []
+                    for sgn in (1, -1):
+                        q = pp.copy()
+                        if kind == "pos":
+                            q[:, 7 * b + k] += sgn * h
+                        else:
+                            th = sgn * h / 1e-3
+                            qe = np.zeros(4)
+                            qe[0] = np.cos(abs(th) / 2)
+                            qe[1 + k] = np.sin(th / 2)
+                            q[:, 7 * b + 3: 7 * b + 7] = qmul(qe, q[:, 7 * b + 3: 7 * b + 7])
+                        r = _lib.pair_contacts_raw(ctx, lib.tris, lib.tri_off, lib.mean_edge, lib.bbox_diag, pm, q)
+                        flagged |= ~np.all(topo(r) == t_base, axis=1)
+                        vals.append(per_pair(r))
+                    col = 6 * b + (k if kind == "pos" else 3 + k)
+                    fd[:, col] = (vals[0] - vals[1]) / (2 * h) * (1.0 if kind == "pos" else 1e-3)
+    fd = fds[0]
+    # a stencil that straddles a kink of the piecewise-smooth map (a clamp, a dedup or snap decision that
+    # flips without changing any count) shows as disagreement between the two step sizes
+    nonsmooth = np.zeros(npairs, bool)
+    rel = np.zeros(npairs)
+    for cols in ([0, 1, 2, 6, 7, 8], [3, 4, 5, 9, 10, 11]):  # translations, rotation vectors: each to its own scale
+        sc2 = np.maximum(np.max(np.abs(fds[1][:, cols]), 1), 1e-300)
+        nonsmooth |= np.max(np.abs(fds[0][:, cols] - fds[1][:, cols]), 1) / sc2 > 1e-4
+        scale = np.maximum(np.max(np.abs(fd[:, cols]), 1), 1e-300)
+        rel = np.maximum(rel, np.max(np.abs(gpose[:, cols] - fd[:, cols]), 1) / scale)
+    ok = (~flagged) & (~nonsmooth) & incontact
+    rel_ok = rel[ok]
+    emit({"metric": "gradient pairs/s", "value": npairs / step_s, "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
+          "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * step_s, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded noised icospheres)",
+          "config": {"workload": desc, "contacts": nc, "l2": "flushed (256 MB write) before the forward and the adjoint"},
+          "stages_ms": {"forward": statistics.mean(fwd), "adjoint_call (forward with tape + reverse)": statistics.mean(adj)},
+          "gpu_launches": int(launches),
+          "fd_check": {"pairs_in_contact": int(incontact.sum()), "pairs_checked": int(ok.sum()),
+                       "pairs_flagged_topology_change": int(np.sum(flagged & incontact)),
+                       "pairs_flagged_nonsmooth_stencil": int(np.sum(nonsmooth & ~flagged & incontact)),
+                       "max_rel_err": float(rel_ok.max()) if len(rel_ok) else None,
+                       "median_rel_err": float(np.median(rel_ok)) if len(rel_ok) else None,
+                       "frac_within_1e-6": float(np.mean(rel_ok <= 1e-6)) if len(rel_ok) else None,
+                       "h": "1e-7 r (and 2.5e-8 r for the smoothness flag)"},
+          "clocks": clk.summary()})
+
 
 if __name__ == "__main__":
     main()
+

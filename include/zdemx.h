@@ -136,6 +136,9 @@ int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx
  * this context has launched so far.  No reference counterpart (the reference times with std::chrono
  * around its stages, src/main.cpp:2061-2304). */
 int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launches);
+/* The context's CUDA stream (a cudaStream_t), on which every call of the context runs: for callers that
+ * order their own work after it or time it with their own events.  No reference counterpart. */
+int zdx_get_stream(const zdx_ctx* ctx, void** stream);
 
 /* ---- the DEM scene (the zdem_cpu step loop) ------------------------------------------------------
  * zdx_scene_load replaces parse_config_file (src/main.cpp:1531-1689), load_mesh_for and the particle

@@ -121,6 +121,12 @@ extern "C" int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launch
     return ZDX_OK;
 }
 
+extern "C" int zdx_get_stream(const zdx_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return ZDX_ERR_INVALID;
+    *stream = (void*)ctx->stream;
+    return ZDX_OK;
+}
+
 namespace {
 
 template <class T>
@@ -206,6 +212,9 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     CK(ctx->mesh_valid.ensure(sizeof(int) * std::max(NM, 1)));
     CK(cudaMemsetAsync(ctx->mesh_R.p, 0, sizeof(unsigned long long) * std::max(NM, 1), st));
     CK(cudaMemsetAsync(ctx->mesh_valid.p, 0, sizeof(int) * std::max(NM, 1), st));
+    CK(ctx->mesh_infl.ensure(sizeof(unsigned long long) * std::max(NM, 1)));
+    CK(cudaMemsetAsync(ctx->mesh_infl.p, 0, sizeof(unsigned long long) * std::max(NM, 1), st));
+    a.mesh_infl_bits = as<unsigned long long>(ctx->mesh_infl);
     a.tri_sph = as<double4>(ctx->tri_sph);
     a.mesh_R_bits = as<unsigned long long>(ctx->mesh_R);
     a.mesh_valid = as<int>(ctx->mesh_valid);
@@ -297,7 +306,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     a.pts_cap = pcap;
     int64_t* ctape_final = nullptr;
     if (ctx->tape_on) {
-        const int64_t tcap = 48 * std::max<int64_t>(ccap, 1) + (1 << 16);
+        const int64_t tcap = std::max<int64_t>(48 * std::max<int64_t>(ccap, 1) + (1 << 16), ctx->tape_hint);
         CK(ctx->t_arena.ensure(sizeof(int) * (size_t)tcap));
         CK(ctx->t_cstage.ensure(sizeof(int64_t) * (size_t)std::max<int64_t>(ccap, 1)));
         CK(ctx->t_cfinal.ensure(sizeof(int64_t) * (size_t)std::max<int64_t>(ccap, 1)));
@@ -308,7 +317,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         ctape_final = as<int64_t>(ctx->t_cfinal);
     }
 
-    unsigned long long hc[8];
+    unsigned long long hc[9];
     if (plain) {
         ctx->launches += 1 + 2 * NP;
         for (int64_t p = 0; p < NP; ++p) {
@@ -375,6 +384,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         CK(cudaStreamSynchronize(st));
     }
     const int err = ((int*)&hc[7])[0];
+    ctx->tape_need = (int64_t)hc[8];
     out->totals[0] = (int64_t)hc[1];
     out->totals[1] = (int64_t)hc[0];
     out->totals[2] = (int64_t)hc[3];
@@ -477,13 +487,12 @@ extern "C" int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts
     fo.want_loop_points = 1;
     fo.sched = ZDX_SCHED_BATCHED;
     int64_t ccap = std::max<int64_t>(n_contacts, 1);
-    const int64_t pcap = 256 * ccap + 1024;
+    int64_t pcap = 64 * ccap + 1024;
     CK(ctx->a_nc.ensure(sizeof(int32_t) * P1));
     CK(ctx->a_coff.ensure(sizeof(int64_t) * (P1 + 1)));
     CK(ctx->a_stats.ensure(sizeof(int32_t) * 4 * P1));
     CK(ctx->a_geom.ensure(sizeof(double) * 20 * ccap));
     CK(ctx->a_info.ensure(sizeof(int32_t) * 4 * ccap));
-    CK(ctx->a_pts.ensure(sizeof(double) * 3 * pcap));
     CK(ctx->a_cpo.ensure(sizeof(int64_t) * (ccap + 1)));
     zdx_pair_result r{};
     r.pair_ncontact = as<int32_t>(ctx->a_nc);
@@ -492,8 +501,6 @@ extern "C" int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts
     r.contact_cap = ccap;
     r.contact_geom = as<double>(ctx->a_geom);
     r.contact_info = as<int32_t>(ctx->a_info);
-    r.loop_point_cap = pcap;
-    r.loop_points = as<double>(ctx->a_pts);
     r.contact_point_off = as<int64_t>(ctx->a_cpo);
     // in host mode the inputs are staged by the forward call; results stay on the device
     zdx_pair_opts fwd = fo;
@@ -531,9 +538,26 @@ extern "C" int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts
         dpb.pose = as<double>(ctx->in_pose);
     }
     fwd.mem = ZDX_MEM_DEVICE;
-    ctx->tape_on = true;
-    rc = zdx_pair_contacts(ctx, &fwd, &dms, &dpb, &r);
-    ctx->tape_on = false;
+    // the tape and loop-point sizes are known only after a pass: grow to what it reports and run again
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        CK(ctx->a_pts.ensure(sizeof(double) * 3 * pcap));
+        r.loop_point_cap = pcap;
+        r.loop_points = as<double>(ctx->a_pts);
+        ctx->tape_on = true;
+        rc = zdx_pair_contacts(ctx, &fwd, &dms, &dpb, &r);
+        ctx->tape_on = false;
+        if (rc != ZDX_ERR_CAPACITY || attempt == 2 || r.totals[0] > ccap) break;
+        bool grew = false;
+        if (r.totals[3] > pcap) {
+            pcap = r.totals[3] + 1024;
+            grew = true;
+        }
+        if (ctx->tape_need > std::max<int64_t>(48 * ccap + (1 << 16), ctx->tape_hint)) {
+            ctx->tape_hint = ctx->tape_need + (1 << 16);
+            grew = true;
+        }
+        if (!grew) break;
+    }
     if (rc) return rc;
     if (r.totals[0] != n_contacts)
         return ctx_fail(ctx, ZDX_ERR_INVALID, "grad has %lld contacts, the forward pass gives %lld", (long long)n_contacts,

@@ -64,6 +64,18 @@ __global__ void k_mesh_prep(PairArgs a, int64_t total) {
     double R = (norm(c) + r) * (1.0 + 1e-12);
     atomicMax(a.mesh_R_bits + lo, (unsigned long long)__double_as_longlong(R));
     if (!(norm(cross(p1 - p0, p2 - p0)) < 1e-30)) atomicAdd(a.mesh_valid + lo, 1);
+    if (a.mesh_infl_bits && !(norm(cross(p1 - p0, p2 - p0)) < 1e-30)) {
+        // point_in_tri accepts c_k = |e_k| x (in-plane distance to edge line k) >= -1e-10: each edge line
+        // moves out by 1e-10 / |e_k| and a vertex by at most 2 max_k(1e-10 / |e_k|) / sin(its angle)
+        const V3 e0 = p1 - p0, e1 = p2 - p1, e2 = p0 - p2;
+        const double l0 = norm(e0), l1 = norm(e1), l2 = norm(e2);
+        const double cr = norm(cross(e0, e2));
+        const double smin_ang = smin3(cr / (l0 * l2), cr / (l0 * l1), cr / (l1 * l2));
+        const double dmax = 1e-10 / smin3(l0, l1, l2);
+        double infl = 2.0 * dmax / smin_ang;
+        if (!(infl < 1e300)) infl = 1e300;
+        atomicMax(a.mesh_infl_bits + lo, (unsigned long long)__double_as_longlong(infl * (1.0 + 1e-6)));
+    }
 }
 
 void launch_mesh_prep(const PairArgs& a, int64_t total_tris, cudaStream_t s) {
@@ -210,6 +222,9 @@ __device__ __forceinline__ void eval_entry(const PairArgs& a, const K1Slot& S, c
 }
 
 __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
+    __shared__ double sh_red[2][K1_THREADS / 32];
+    __shared__ double sh_slab[3];  // hi(A.d), lo(B.d), slack of the certificate (the slab cull uses them)
+    __shared__ int sh_sep;
     __shared__ int sh_item;
     __shared__ int sh_n[2];
     __shared__ int sh_nq;
@@ -255,13 +270,95 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         auto inf = [](V3 v) { return smax3(fabs(v.x), fabs(v.y), fabs(v.z)); };
         const double pad = 1e-9 * (inf(tpos[0]) + inf(tpos[1]) + R[0] + R[1]);
 
+        // Separation certificate along the line of centres d: every point of A lies below the largest
+        // corner projection max_v (v.d) of A's triangles, every point of B above B's smallest one.  A
+        // segment endpoint is on an edge of one body (seg_plane clamps t to [0, 1], src/main.cpp:545-559)
+        // and inside a triangle of the other up to point_in_tri's tolerance (src/main.cpp:529-543), i.e.
+        // within that mesh's inflation distance of it.  A gap wider than the larger inflation (plus
+        // rounding) means no triangle pair can yield a segment: the pair has none, as the full test finds.
+        bool slab = false;
+        V3 dslab{0.0, 0.0, 0.0};
+        if (a.mesh_infl_bits) {
+            const V3 dv = tpos[1] - tpos[0];
+            const double dl = norm(dv);
+            const double infl = smax(__longlong_as_double((long long)a.mesh_infl_bits[mesh[0]]),
+                                     __longlong_as_double((long long)a.mesh_infl_bits[mesh[1]]));
+            if (dl > 0.0 && infl < 1e300) {
+                const V3 d = dv / dl;
+                for (int s2 = 0; s2 < 2; ++s2) {
+                    const Q4 qc{qn[s2].w, -qn[s2].x, -qn[s2].y, -qn[s2].z};
+                    const V3 dloc = py ? qrotate_py_n(qc, d) : qrotate_n(qc, d);
+                    double e = s2 == 0 ? -__builtin_huge_val() : __builtin_huge_val();
+                    const double* tv = a.tris + 9 * off[s2];
+                    for (int q = tid; q < 3 * nt[s2]; q += K1_THREADS) {
+                        const double v = tv[3 * q] * dloc.x + tv[3 * q + 1] * dloc.y + tv[3 * q + 2] * dloc.z;
+                        e = s2 == 0 ? fmax(e, v) : fmin(e, v);
+                    }
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const double y = __shfl_xor_sync(FULL, e, o);
+                        e = s2 == 0 ? fmax(e, y) : fmin(e, y);
+                    }
+                    if ((tid & 31) == 0) sh_red[s2][tid >> 5] = e;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    double hi = -__builtin_huge_val(), lo = __builtin_huge_val();
+                    for (int w = 0; w < K1_THREADS / 32; ++w) {
+                        hi = fmax(hi, sh_red[0][w]);
+                        lo = fmin(lo, sh_red[1][w]);
+                    }
+                    const double hiA = dot(tpos[0], d) + hi, loB = dot(tpos[1], d) + lo;
+                    const double slack = infl * (1.0 + 1e-6) + 4.0 * pad;
+                    sh_sep = (hiA + slack < loB) ? 1 : 0;
+                    sh_slab[0] = hiA;
+                    sh_slab[1] = loB;
+                    sh_slab[2] = slack;
+                }
+                __syncthreads();
+                if (sh_sep) {
+                    if (tid == 0) {
+                        a.pair_seg_off[p] = 0;
+                        a.pair_nseg[p] = 0;
+                        a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
+                        a.pair_status[p] = 0;
+                        atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
+                    }
+                    __syncthreads();
+                    continue;
+                }
+                slab = true;
+                dslab = d;
+            }
+        }
+
         // Cull each side against the other body's bounding cube; keep the exact world triangles,
         // planes and AABBs of the survivors (src/main.cpp:2064-2116).
+        //
+        // With the certificate's projections, also drop every triangle that lies wholly outside the slab
+        // where the two bodies overlap along d: an A triangle whose corners all project below
+        // lo(B.d) - slack, a B triangle whose corners all project above hi(A.d) + slack.  By the
+        // certificate's argument neither can take part in a segment.
         for (int s = 0; s < 2; ++s) {
             const V3 other = tpos[1 - s];
             const double lim = R[1 - s] + pad;
             K1Side& D = S.side[s];
+            V3 dl{0.0, 0.0, 0.0};
+            double bound = 0.0;
+            if (slab) {
+                const Q4 qc{qn[s].w, -qn[s].x, -qn[s].y, -qn[s].z};
+                dl = py ? qrotate_py_n(qc, dslab) : qrotate_n(qc, dslab);
+                // in the mesh frame: A keeps corners reaching lo(B.d) - slack, B corners below hi(A.d) + slack
+                bound = s == 0 ? sh_slab[1] - sh_slab[2] - dot(tpos[0], dslab)
+                               : sh_slab[0] + sh_slab[2] - dot(tpos[1], dslab);
+            }
             for (int t = tid; t < nt[s]; t += K1_THREADS) {
+                if (slab) {
+                    const double* lv = a.tris + 9 * (off[s] + t);
+                    const double p0 = lv[0] * dl.x + lv[1] * dl.y + lv[2] * dl.z;
+                    const double p1 = lv[3] * dl.x + lv[4] * dl.y + lv[5] * dl.z;
+                    const double p2 = lv[6] * dl.x + lv[7] * dl.y + lv[8] * dl.z;
+                    if (s == 0 ? (smax3(p0, p1, p2) < bound) : (smin3(p0, p1, p2) > bound)) continue;
+                }
                 double4 sp = a.tri_sph[off[s] + t];
                 V3 c = V3{sp.x, sp.y, sp.z};
                 V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];

@@ -34,6 +34,10 @@ struct PairArgs {
     double4* tri_sph;
     unsigned long long* mesh_R_bits;  // max over triangles of |c| + r, as the bits of a positive double
     int* mesh_valid;                  // triangles with a plane (|e1 x e2| >= 1e-30) per mesh
+    // per mesh, how far outside a triangle point_in_tri's tolerance can accept a point (bits of a
+    // non-negative double, max over the triangles with a plane; k_mesh_prep); null disables the
+    // separation certificate and slab cull of k_segments
+    unsigned long long* mesh_infl_bits;
     // pairs
     int64_t n_pairs;
     // null, or the device-resident pair count: n_pairs and item_end are then capacities that size the

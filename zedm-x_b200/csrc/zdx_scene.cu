@@ -416,62 +416,74 @@ __global__ void k_walls(WallArgs a) {
         const V3 xp = L3(sp);
         int touched = 0;
         const int64_t t0 = a.wtri_off[w], t1 = a.wtri_off[w + 1];
-        for (int64_t t = t0; t < t1; ++t) {
-            const int slot = (int)(t - t0);
-            if (lane == 0) a.valid[k * a.max_wtri + slot] = 0;
-            const double* wt = a.wtris + 9 * t;
-            V3 w0 = L3(wt), w1 = L3(wt + 3), w2 = L3(wt + 6);
-            V3 wmn{smin3(w0.x, w1.x, w2.x), smin3(w0.y, w1.y, w2.y), smin3(w0.z, w1.z, w2.z)};
-            V3 wmx{smax3(w0.x, w1.x, w2.x), smax3(w0.y, w1.y, w2.y), smax3(w0.z, w1.z, w2.z)};
-            const double r = mp[2];
-            V3 pmn = xp - V3{r, r, r}, pmx = xp + V3{r, r, r};
-            if (pmx.x < wmn.x || pmn.x > wmx.x || pmx.y < wmn.y || pmn.y > wmx.y || pmx.z < wmn.z || pmn.z > wmx.z)
-                continue;
-            const V3 n = L3(a.wnorm + 3 * t);
-            double area = 0.0;
-            V3 cpt{0.0, 0.0, 0.0};
-            bool ok = wall_contact_warp(a, lane, qn, xp, ptris, pnt, wt, n, tol, pts, area, cpt);
-            ok = __shfl_sync(FULLM, ok ? 1 : 0, 0) != 0;
-            if (ok && lane == 0) {
-                V3 cn = n;
-                V3 to_p = xp - cpt;
-                if (dot(cn, to_p) < 0.0) cn = cn * -1.0;
-                V3 rP = cpt - xp;
-                V3 vrel = L3(sp + 7) + cross(L3(sp + 10), rP);
-                double vn = dot(vrel, cn);
-                double Rp = smax(mp[3], 1e-12), Ep = smax(mp[4], 1e-12), nup = mp[5];
-                double kn = (Ep / Rp) * area;
-                double kt = (Ep / (2.0 * (1.0 + nup) * Rp)) * area;
-                double m_eff = mp[0];
-                double e = mp[7];
-                e = smin(0.9999, smax(1e-6, e));
-                double loge = log(e);
-                double cnd = 2.0 * loge * sqrt(kn * m_eff) / sqrt(loge * loge + PI_D * PI_D);
-                double ctd = 2.0 * loge * sqrt(kt * m_eff) / sqrt(loge * loge + PI_D * PI_D);
-                cnd = fabs(cnd);
-                ctd = fabs(ctd);
-                double deltaV = pow(area, 1.5);
-                double fn = kn * cbrt(deltaV) + -cnd * vn;
-                if (fn < 0.0) fn = 0.0;
-                V3 fn_vec = cn * fn;
-                V3 vt = vrel - cn * vn;
-                ds = ds + vt * a.dt;
-                ds = ds - cn * dot(ds, cn);
-                V3 ft = ds * (-kt) + vt * (-ctd);
-                double mu = smin(mp[6], a.wmat[2 * w]);
-                double ftn = norm(ft), ftmax = mu * fn;
-                if (ftn > ftmax && ftn > 1e-14) {
-                    ft = ft * (ftmax / ftn);
-                    if (kt > 1e-12) ds = ft * (-1.0 / kt);
-                }
-                V3 f = fn_vec + ft;
-                double* o = a.contrib + 6 * (k * a.max_wtri + slot);
-                S3(o, f);
-                S3(o + 3, cross(rP, f));
-                a.valid[k * a.max_wtri + slot] = 1;
-                touched = 1;
+        const double r = mp[2];
+        const V3 pmn = xp - V3{r, r, r}, pmx = xp + V3{r, r, r};
+        // the lanes test 32 wall triangles' AABBs at a time (src/main.cpp:2330-2345); the warp then
+        // visits the overlapping ones in triangle order
+        for (int64_t tb = t0; tb < t1; tb += 32) {
+            bool hit = false;
+            if (tb + lane < t1) {
+                a.valid[k * a.max_wtri + (int)(tb + lane - t0)] = 0;
+                const double* wt = a.wtris + 9 * (tb + lane);
+                const V3 w0 = L3(wt), w1 = L3(wt + 3), w2 = L3(wt + 6);
+                const V3 wmn{smin3(w0.x, w1.x, w2.x), smin3(w0.y, w1.y, w2.y), smin3(w0.z, w1.z, w2.z)};
+                const V3 wmx{smax3(w0.x, w1.x, w2.x), smax3(w0.y, w1.y, w2.y), smax3(w0.z, w1.z, w2.z)};
+                hit = !(pmx.x < wmn.x || pmn.x > wmx.x || pmx.y < wmn.y || pmn.y > wmx.y || pmx.z < wmn.z ||
+                        pmn.z > wmx.z);
             }
-            __syncwarp();
+            unsigned hits = __ballot_sync(FULLM, hit);
+            __syncwarp();  // the zeroed flags are visible before lane 0 sets any
+            while (hits) {
+                const int64_t t = tb + (__ffs(hits) - 1);
+                hits &= hits - 1u;
+                const int slot = (int)(t - t0);
+                const double* wt = a.wtris + 9 * t;
+                const V3 n = L3(a.wnorm + 3 * t);
+                double area = 0.0;
+                V3 cpt{0.0, 0.0, 0.0};
+                bool ok = wall_contact_warp(a, lane, qn, xp, ptris, pnt, wt, n, tol, pts, area, cpt);
+                ok = __shfl_sync(FULLM, ok ? 1 : 0, 0) != 0;
+                if (ok && lane == 0) {
+                    V3 cn = n;
+                    V3 to_p = xp - cpt;
+                    if (dot(cn, to_p) < 0.0) cn = cn * -1.0;
+                    V3 rP = cpt - xp;
+                    V3 vrel = L3(sp + 7) + cross(L3(sp + 10), rP);
+                    double vn = dot(vrel, cn);
+                    double Rp = smax(mp[3], 1e-12), Ep = smax(mp[4], 1e-12), nup = mp[5];
+                    double kn = (Ep / Rp) * area;
+                    double kt = (Ep / (2.0 * (1.0 + nup) * Rp)) * area;
+                    double m_eff = mp[0];
+                    double e = mp[7];
+                    e = smin(0.9999, smax(1e-6, e));
+                    double loge = log(e);
+                    double cnd = 2.0 * loge * sqrt(kn * m_eff) / sqrt(loge * loge + PI_D * PI_D);
+                    double ctd = 2.0 * loge * sqrt(kt * m_eff) / sqrt(loge * loge + PI_D * PI_D);
+                    cnd = fabs(cnd);
+                    ctd = fabs(ctd);
+                    double deltaV = pow(area, 1.5);
+                    double fn = kn * cbrt(deltaV) + -cnd * vn;
+                    if (fn < 0.0) fn = 0.0;
+                    V3 fn_vec = cn * fn;
+                    V3 vt = vrel - cn * vn;
+                    ds = ds + vt * a.dt;
+                    ds = ds - cn * dot(ds, cn);
+                    V3 ft = ds * (-kt) + vt * (-ctd);
+                    double mu = smin(mp[6], a.wmat[2 * w]);
+                    double ftn = norm(ft), ftmax = mu * fn;
+                    if (ftn > ftmax && ftn > 1e-14) {
+                        ft = ft * (ftmax / ftn);
+                        if (kt > 1e-12) ds = ft * (-1.0 / kt);
+                    }
+                    V3 f = fn_vec + ft;
+                    double* o = a.contrib + 6 * (k * a.max_wtri + slot);
+                    S3(o, f);
+                    S3(o + 3, cross(rP, f));
+                    a.valid[k * a.max_wtri + slot] = 1;
+                    touched = 1;
+                }
+                __syncwarp();
+            }
         }
         if (lane == 0) {
             a.active[k] = touched;
@@ -1092,6 +1104,7 @@ static int graph_alloc(zdx_ctx* ctx, Scene& s) {
     CKS(G.tri_sph.ensure(sizeof(double4) * (size_t)std::max<int64_t>(total_tris, 1)));
     CKS(G.mesh_R.ensure(sizeof(unsigned long long) * std::max(nm, 1)));
     CKS(G.mesh_valid.ensure(sizeof(int) * std::max(nm, 1)));
+    CKS(G.mesh_infl.ensure(sizeof(unsigned long long) * std::max(nm, 1)));
     CKS(G.order.ensure(sizeof(int32_t) * P1));
     CKS(G.buckets.ensure(sizeof(int) * 128));
     CKS(G.pair_i64.ensure(sizeof(int64_t) * 5 * P1));
@@ -1199,6 +1212,8 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
         CKS(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
         CKS(cudaMemsetAsync(G.mesh_R.p, 0, sizeof(unsigned long long) * std::max(nm, 1), st));
         CKS(cudaMemsetAsync(G.mesh_valid.p, 0, sizeof(int) * std::max(nm, 1), st));
+        CKS(cudaMemsetAsync(G.mesh_infl.p, 0, sizeof(unsigned long long) * std::max(nm, 1), st));
+        a.mesh_infl_bits = as<unsigned long long>(G.mesh_infl);
         launch_mesh_prep(a, s.mesh_off.back(), st);
         launch_cost_order(a, as<int32_t>(G.order), as<int>(G.buckets), st);
         a.order = as<int32_t>(G.order);

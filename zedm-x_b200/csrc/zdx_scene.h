@@ -100,7 +100,7 @@ struct GraphStep {
     DevBuf w_active, w_scan, w_pairs, w_contrib, w_valid, w_act, w_ds, w_hscan, w_scratch;
     DevBuf hkey, hds, hkey2, hds2, whkey, whds, whkey2, whds2;
     // pair kernels' workspaces
-    DevBuf tri_sph, mesh_R, mesh_valid, order, buckets, pair_i64, pair_i32, counters, k1_slots, seg_arena, k2_slots,
+    DevBuf tri_sph, mesh_R, mesh_valid, mesh_infl, order, buckets, pair_i64, pair_i32, counters, k1_slots, seg_arena, k2_slots,
         cstage, cistage;
 
     std::vector<DevBuf*> bufs() {
@@ -108,7 +108,7 @@ struct GraphStep {
                 &bp_pairs, &bp_pstart, &rs_tmp, &scan_tmp, &tr_key, &tr_idx, &tr_key2, &tr_idx2, &tr_start, &pr_mesh,
                 &pr_pose, &pr_coff, &pr_stats, &pr_geom, &pr_info, &pr_contrib, &pr_active, &pr_ds, &pr_hscan,
                 &w_active, &w_scan, &w_pairs, &w_contrib, &w_valid, &w_act, &w_ds, &w_hscan, &w_scratch, &hkey, &hds,
-                &hkey2, &hds2, &whkey, &whds, &whkey2, &whds2, &tri_sph, &mesh_R, &mesh_valid, &order, &buckets,
+                &hkey2, &hds2, &whkey, &whds, &whkey2, &whds2, &tri_sph, &mesh_R, &mesh_valid, &mesh_infl, &order, &buckets,
                 &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &cstage, &cistage};
     }
     void drop_graph() {

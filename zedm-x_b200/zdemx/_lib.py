@@ -85,6 +85,7 @@ def lib() -> C.CDLL:
     L.zdx_pair_contacts.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                     C.POINTER(PairResult)]
     L.zdx_pair_timings.argtypes = [C.c_void_p, _dp, _i64p]
+    L.zdx_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.zdx_scene_load.argtypes = [C.c_void_p, C.c_char_p]
     L.zdx_scene_step.argtypes = [C.c_void_p, C.c_int]
     L.zdx_scene_info.argtypes = [C.c_void_p, _i64p]
@@ -166,6 +167,12 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def stream_ptr(self) -> int:
+        """The context's cudaStream_t as an integer (torch.cuda.ExternalStream(ptr) orders / times on it)."""
+        v = C.c_void_p()
+        check(lib().zdx_get_stream(self.handle, C.byref(v)), self.handle)
+        return int(v.value or 0)
 
     def timings(self):
         t = np.zeros(5)

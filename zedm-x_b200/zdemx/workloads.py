@@ -1,0 +1,120 @@
+"""Seeded synthetic scenes of the zdem_cpu config grammar (src/main.cpp:1531-1689), written to disk.
+
+pour_scene: 100,000 particles from five templates (three convex hulls of 64 points on a 1 : 0.8 : 0.6
+ellipsoid, noised icospheres of subdivision 2 and 3; circumradius 1 mm) on a jittered lattice inside a
+closed 12-triangle box, gravity -z, with small random velocities so that collisions start within a few
+hundred steps.  100,000 particles of circumradius 1 mm cannot sit inside a 60 x 60 x 120 mm box without
+overlapping (the densest packing of their circumspheres holds about 76,000), so the box keeps the
+60 x 60 mm floor and is as tall as the lattice needs.
+
+two_particle_scene: two 320-triangle noised icospheres colliding head-on.
+"""
+from __future__ import annotations
+
+import os
+import struct
+
+import numpy as np
+
+from . import synth
+
+MATERIAL = {"density": 2500, "young": 1e7, "poisson": 0.25, "mu": 0.5, "restitution": 0.5}
+
+
+def write_binary_stl(path: str, tris) -> None:
+    """Binary STL (float32 corners), the format load_stl reads (src/main.cpp:308-371)."""
+    tris = np.asarray(tris, np.float64).reshape(-1, 3, 3)
+    n = np.cross(tris[:, 1] - tris[:, 0], tris[:, 2] - tris[:, 0])
+    ln = np.linalg.norm(n, axis=1, keepdims=True)
+    n = np.where(ln > 0, n / np.where(ln > 0, ln, 1.0), n)
+    rec = np.zeros(len(tris), dtype=[("n", "<f4", 3), ("v", "<f4", 9), ("a", "<u2")])
+    rec["n"] = n
+    rec["v"] = tris.reshape(-1, 9)
+    with open(path, "wb") as f:
+        f.write(b"zdemx synthetic mesh".ljust(80, b"\0"))
+        f.write(struct.pack("<I", len(tris)))
+        f.write(rec.tobytes())
+
+
+def box_tris(sx: float, sy: float, sz: float) -> np.ndarray:
+    """Closed axis-aligned box centred at the origin, 12 triangles wound outward."""
+    hx, hy, hz = sx / 2, sy / 2, sz / 2
+    v = np.array([[-hx, -hy, -hz], [hx, -hy, -hz], [hx, hy, -hz], [-hx, hy, -hz],
+                  [-hx, -hy, hz], [hx, -hy, hz], [hx, hy, hz], [-hx, hy, hz]])
+    f = [(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4), (2, 3, 7), (2, 7, 6), (0, 4, 7), (0, 7, 3),
+         (1, 2, 6), (1, 6, 5)]
+    return v[np.array(f)]
+
+
+def _fmt(v) -> str:
+    return " ".join(repr(float(x)) for x in np.atleast_1d(v))
+
+
+def pour_templates(rng: np.random.Generator, circumradius: float = 1e-3) -> list[np.ndarray]:
+    """The five particle templates: three ellipsoid hulls, icospheres of subdivision 2 and 3."""
+    noise = 0.15
+    out = [synth.ellipsoid_hull(64, (1.0, 0.8, 0.6), circumradius, rng) for _ in range(3)]
+    out.append(synth.noised_icosphere(2, circumradius / (1 + noise), noise, rng))
+    out.append(synth.noised_icosphere(3, circumradius / (1 + noise), noise, rng))
+    return out
+
+
+def pour_scene(dirpath: str, n: int = 100_000, seed: int = 0, steps: int = 10_000, dt: float = 2e-6,
+               spacing: float = 2.02e-3, floor: float = 60e-3, vel_sigma: float = 0.05,
+               output_interval: int = 1 << 30) -> str:
+    """Writes the templates, the box and the config under dirpath; returns the config path."""
+    rng = np.random.default_rng(seed)
+    os.makedirs(dirpath, exist_ok=True)
+    names = []
+    for k, t in enumerate(pour_templates(rng)):
+        p = os.path.join(dirpath, f"template{k}.stl")
+        write_binary_stl(p, t)
+        names.append(p)
+    per_row = int(floor // spacing)
+    per_layer = per_row * per_row
+    layers = (n + per_layer - 1) // per_layer
+    height = layers * spacing + 2 * spacing
+    box = os.path.join(dirpath, "box.stl")
+    write_binary_stl(box, box_tris(floor, floor, height))
+    k = np.arange(n)
+    ix, iy, iz = k % per_row, (k // per_row) % per_row, k // per_layer
+    x0 = -0.5 * (per_row - 1) * spacing
+    pos = np.stack([x0 + ix * spacing, x0 + iy * spacing, spacing * 0.55 + iz * spacing], 1)
+    pos += rng.uniform(-5e-6, 5e-6, size=pos.shape)
+    vel = rng.normal(0.0, vel_sigma, size=(n, 3))
+    quat = synth.random_unit_quat(rng, n)
+    tmpl = rng.integers(0, len(names), size=n)
+    lines = [f"steps = {steps}", f"dt = {dt!r}", "gravity = 0 0 -9.81", "split_contacts = 1",
+             f"output_interval = {output_interval}", f"output_dir = {os.path.join(dirpath, 'out')}",
+             "vtk_prefix = pour", "wall", f"stl = {box}", f"pos = 0 0 {height / 2!r}", "quat = 1 0 0 0", "scale = 1",
+             "mu = 0.5", "restitution = 0.5", "end_wall"]
+    mat = [f"{key} = {val}" for key, val in MATERIAL.items()]
+    for i in range(n):
+        lines += ["particle", f"stl = {names[tmpl[i]]}", f"pos = {_fmt(pos[i])}", f"vel = {_fmt(vel[i])}",
+                  f"quat = {_fmt(quat[i])}", "omega = 0 0 0", "scale = 1"] + mat + ["end_particle"]
+    cfg = os.path.join(dirpath, "pour.txt")
+    with open(cfg, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return cfg
+
+
+def two_particle_scene(dirpath: str, seed: int = 1, steps: int = 2000, dt: float = 1e-6,
+                       output_interval: int = 1 << 30) -> str:
+    """Two 320-triangle noised icospheres (radius 1 mm), 1.9 mm apart, approaching at 0.05 m/s each."""
+    rng = np.random.default_rng(seed)
+    os.makedirs(dirpath, exist_ok=True)
+    paths = []
+    for k in range(2):
+        p = os.path.join(dirpath, f"m{k}.stl")
+        write_binary_stl(p, synth.noised_icosphere(2, 1e-3, 0.15, rng))
+        paths.append(p)
+    lines = [f"steps = {steps}", f"dt = {dt!r}", "gravity = 0 0 0", "split_contacts = 1",
+             f"output_interval = {output_interval}", f"output_dir = {os.path.join(dirpath, 'out')}", "vtk_prefix = p"]
+    mat = [f"{key} = {val}" for key, val in MATERIAL.items()]
+    for p, x, v in ((paths[0], "0 0 0", "0.05 0 0"), (paths[1], "0.0019 0 0", "-0.05 0 0")):
+        lines += ["particle", f"stl = {p}", f"pos = {x}", f"vel = {v}", "quat = 1 0 0 0", "omega = 0 0 0",
+                  "scale = 1"] + mat + ["end_particle"]
+    cfg = os.path.join(dirpath, "two.txt")
+    with open(cfg, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return cfg
