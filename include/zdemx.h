@@ -153,6 +153,26 @@ int zdx_scene_step(zdx_ctx* ctx, int nsteps);
  * components, loops (the step log's fields, src/main.cpp:2489-2499), candidate pairs, wall contacts,
  * pair history entries, wall history entries. */
 int zdx_scene_info(zdx_ctx* ctx, int64_t* info);
+/* Copies of the scene's set-up arrays, for callers that rebuild or differentiate the step themselves
+ * (no reference counterpart; the values are those of the particle and wall set-up, src/main.cpp:1883-2022).
+ * *count receives the element count; out may be NULL to ask for it. */
+enum {
+    ZDX_SCENE_MAT = 0,          /* np x 17 doubles: mass, 1/mass, radius, equivalent radius, young, poisson, mu,
+                                   restitution, inverse body inertia (3x3, row-major) */
+    ZDX_SCENE_PMESH = 1,        /* np int32: mesh of each particle */
+    ZDX_SCENE_MESH_TRIS = 2,    /* T x 9 doubles: the meshes as build_mesh leaves them (centred, scaled) */
+    ZDX_SCENE_MESH_OFF = 3,     /* M+1 int64 */
+    ZDX_SCENE_MESH_PROPS = 4,   /* M x 17 doubles: build_mesh properties (5 = mean edge, 6 = bbox diagonal) */
+    ZDX_SCENE_WALL_TRIS = 5,    /* Tw x 9 doubles: wall triangles in world coordinates */
+    ZDX_SCENE_WALL_NORMALS = 6, /* Tw x 3 doubles: their unit normals */
+    ZDX_SCENE_WALL_OFF = 7,     /* nw+1 int64 */
+    ZDX_SCENE_WALL_MAT = 8,     /* nw x 2 doubles: mu, restitution */
+    ZDX_SCENE_WALL_POSE = 9,    /* nw x 7 doubles: position, quaternion */
+    ZDX_SCENE_WALL_MESH = 10,   /* nw int32: mesh of each wall */
+    ZDX_SCENE_PARAMS = 11       /* 7 doubles: dt, gravity (3), split_contacts, force_law (0 zdem, 1 feng_min),
+                                   feng_k */
+};
+int zdx_scene_array(zdx_ctx* ctx, int which, void* out, int64_t* count);
 /* Host copies (any pointer may be NULL): state np x 16 = pos(3) quat(w,x,y,z) vel(3) omega(3) L(3);
  * force/torque np x 3 and contact_count np as used by the last step's integration. */
 int zdx_scene_get_state(zdx_ctx* ctx, double* state16, double* force3, double* torque3, int32_t* contact_count);

@@ -1,0 +1,122 @@
+"""Differentiable rollouts (zdemx.rollout): the torch step against the CUDA scene step, reverse-mode
+gradients of a final-position loss against central differences, checkpointed against unsegmented."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(tmp_path, n_side=3, seed=5):
+    from zdemx.dem import Scene
+    from zdemx.workloads import calibration_scene
+
+    cfg = calibration_scene(str(tmp_path / "cal"), n_side=n_side, seed=seed, steps=100, spacing=1.8e-3)
+    return Scene(cfg)
+
+
+def test_torch_step_follows_the_cuda_step(tmp_path):
+    """Same counters every step; state within summation-order rounding (forces summed in another order)."""
+    import torch
+
+    from zdemx.rollout import DiffScene
+
+    sc = _scene(tmp_path)
+    ds = DiffScene(sc)
+    st = torch.from_numpy(sc.state()[0]).cuda()
+    hk, hd, wk, wd = ds.initial_history()
+    k = torch.tensor(ds.feng_k, dtype=torch.float64, device="cuda")
+    e = torch.tensor(float(ds.mat[0, 7]), dtype=torch.float64, device="cuda")
+    seen = 0
+    with torch.no_grad():
+        for s in range(40):
+            sc.step(1)
+            st, hk, hd, wk, wd, stats = ds.step(st, hk, hd, wk, wd, k, e)
+            info = sc.info()
+            assert info["pairs"] == stats["pairs"], f"step {s}: pairs"
+            assert info["contacts"] == stats.get("contacts", 0) + stats["wall_contacts"], f"step {s}: contacts"
+            assert info["wall_contacts"] == stats["wall_contacts"], f"step {s}: wall contacts"
+            assert info["history"] == hk.numel() and info["wall_history"] == wk.numel()
+            seen += info["contacts"]
+    ref = sc.state()[0]
+    got = st.cpu().numpy()
+    for cols, tol in ((slice(0, 3), 1e-12), (slice(7, 10), 1e-7), (slice(3, 7), 1e-12)):
+        scale = max(np.max(np.abs(ref[:, cols])), 1e-300)
+        err = np.max(np.abs(got[:, cols] - ref[:, cols])) / scale
+        assert err <= tol, f"cols {cols}: rel err {err}"
+    assert seen > 0
+
+
+def _loss_fn(ds, state0, v_init, target, steps):
+    import torch
+
+    def loss(k, e, v0, checkpoint_every=None):
+        st = torch.cat([state0[:, 0:7], v0, state0[:, 10:16]], 1)
+        xT, _ = ds.rollout(st, k, e, steps, checkpoint_every=checkpoint_every)
+        return ((xT[:, 0:3] - target) ** 2).sum()
+
+    return loss
+
+
+def test_rollout_gradients_match_central_differences(tmp_path):
+    import torch
+
+    from zdemx.rollout import DiffScene
+
+    sc = _scene(tmp_path)
+    ds = DiffScene(sc)
+    state0 = torch.from_numpy(sc.state()[0]).cuda()
+    steps = 30
+    with torch.no_grad():
+        tgt, _ = ds.rollout(state0, torch.tensor(1.3e7, dtype=torch.float64, device="cuda"),
+                            torch.tensor(0.35, dtype=torch.float64, device="cuda"), steps)
+    target = tgt[:, 0:3].clone()
+    loss = _loss_fn(ds, state0, None, target, steps)
+    k = torch.tensor(1e7, dtype=torch.float64, device="cuda", requires_grad=True)
+    e = torch.tensor(0.5, dtype=torch.float64, device="cuda", requires_grad=True)
+    v0 = state0[:, 7:10].clone().requires_grad_(True)
+    L = loss(k, e, v0)
+    L.backward()
+    assert k.grad is not None and e.grad is not None, "no particle-particle contact in the rollout"
+    gk, ge, gv = k.grad.item(), e.grad.item(), v0.grad.cpu().numpy()
+    with torch.no_grad():
+        def fd(fn, h):
+            return (fn(h) - fn(-h)) / (2 * h)
+
+        fk = fd(lambda h: loss(k + h, e, v0).item(), 1e7 * 1e-6)
+        fe = fd(lambda h: loss(k, e + h, v0).item(), 1e-6)
+        idx = [(0, 0), (13, 2), (26, 1)]
+        fv = []
+        for i, c in idx:
+            def f(h, i=i, c=c):
+                vv = v0.clone()
+                vv[i, c] += h
+                return loss(k, e, vv).item()
+            fv.append(fd(f, 1e-7))
+    assert abs(gk - fk) <= 1e-4 * abs(fk) + 1e-30, (gk, fk)
+    assert abs(ge - fe) <= 1e-4 * abs(fe) + 1e-30, (ge, fe)
+    for (i, c), f in zip(idx, fv):
+        assert abs(gv[i, c] - f) <= 1e-4 * max(abs(f), np.max(np.abs(gv)) * 1e-3), (i, c, gv[i, c], f)
+
+
+def test_checkpointed_rollout_gives_the_same_gradients(tmp_path):
+    import torch
+
+    from zdemx.rollout import DiffScene
+
+    sc = _scene(tmp_path, seed=6)
+    ds = DiffScene(sc)
+    state0 = torch.from_numpy(sc.state()[0]).cuda()
+    target = state0[:, 0:3] + 1e-5
+    loss = _loss_fn(ds, state0, None, target, 24)
+    out = []
+    for ck in (None, 8):
+        k = torch.tensor(1e7, dtype=torch.float64, device="cuda", requires_grad=True)
+        e = torch.tensor(0.5, dtype=torch.float64, device="cuda", requires_grad=True)
+        v0 = state0[:, 7:10].clone().requires_grad_(True)
+        L = loss(k, e, v0, checkpoint_every=ck)
+        L.backward()
+        out.append((L.item(), k.grad.item(), e.grad.item(), v0.grad.cpu().numpy()))
+    (l0, k0, e0, v0a), (l1, k1, e1, v1a) = out
+    assert l0 == l1
+    np.testing.assert_allclose([k1, e1], [k0, e0], rtol=1e-10)
+    np.testing.assert_allclose(v1a, v0a, rtol=1e-10, atol=1e-10 * np.max(np.abs(v0a)))

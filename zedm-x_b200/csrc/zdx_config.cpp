@@ -209,6 +209,17 @@ bool parse_config(const std::string& path, SimConfig& cfg, std::string& err) {
             iss >> cfg.v0[0] >> cfg.v0[1] >> cfg.v0[2];
         } else if (key == "v1") {
             iss >> cfg.v1[0] >> cfg.v1[1] >> cfg.v1[2];
+        } else if (key == "force_law") {
+            std::string law;
+            iss >> law;
+            if (law == "zdem") cfg.force_law = 0;
+            else if (law == "feng_min") cfg.force_law = 1;
+            else {
+                err = "Unknown force_law: " + law + " (zdem or feng_min)";
+                return false;
+            }
+        } else if (key == "feng_k") {
+            iss >> cfg.feng_k;
         }
         // unknown keys are ignored, as in the reference
     }

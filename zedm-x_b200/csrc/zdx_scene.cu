@@ -154,7 +154,7 @@ __device__ int64_t find_key(const int64_t* keys, int64_t n, int64_t k) {
 __global__ void k_pp_force(const int2* pairs, int64_t npair, const int64_t* n_dev, const int64_t* coff, const double* geom,
                            const double* state, const double* mat, double dt, const int64_t* hkey, const double* hds,
                            int64_t nh, const int64_t* nh_dev, double* contrib, int32_t* active, double* ds_out,
-                           const int* stop) {
+                           const int* stop, int law, double feng_k) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= dev_count(npair, n_dev)) return;
     if (stop && *stop) return;
@@ -193,8 +193,13 @@ __global__ void k_pp_force(const int2* pairs, int64_t npair, const int64_t* n_de
         double loge = log(e);
         double ct = 2.0 * loge * sqrt(kt * m_eff) / sqrt(loge * loge + PI_D * PI_D);
         ct = fabs(ct);
-        double deltaV = pow(A_n, 1.5);
-        double fn = kn * cbrt(deltaV);
+        double fn;
+        if (law == 1) {
+            fn = 0.5 * feng_k * A_n;  // feng_min, polyline.py:677
+        } else {
+            double deltaV = pow(A_n, 1.5);
+            fn = kn * cbrt(deltaV);
+        }
         if (fn < 0.0) fn = 0.0;
         V3 fn_vec = nA * fn;
         V3 vt = vrel - nA * vn;
@@ -842,7 +847,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
                                                      as<double>(s.pr_geom), state, mat, s.cfg.dt,
                                                      as<int64_t>(s.d_hist_key), as<double>(s.d_hist_ds), s.nhist,
                                                      nullptr, as<double>(s.pr_contrib), as<int32_t>(s.pr_active),
-                                                     as<double>(s.pr_ds), nullptr);
+                                                     as<double>(s.pr_ds), nullptr, s.cfg.force_law, s.cfg.feng_k);
         ctx->launches += 1;
     }
 
@@ -1247,7 +1252,8 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
     k_pp_force<<<grid(G.pcap, 128), 128, 0, st>>>(as<int2>(G.bp_pairs), G.pcap, npair, as<int64_t>(G.pr_coff),
                                                   as<double>(G.pr_geom), state, mat, s.cfg.dt, as<int64_t>(G.hkey),
                                                   as<double>(G.hds), 0, &g->nhist, as<double>(G.pr_contrib),
-                                                  as<int32_t>(G.pr_active), as<double>(G.pr_ds), flags);
+                                                  as<int32_t>(G.pr_active), as<double>(G.pr_ds), flags,
+                                                  s.cfg.force_law, s.cfg.feng_k);
 
     // ---- 4. walls
     const int64_t* ncand = &g->ncand;

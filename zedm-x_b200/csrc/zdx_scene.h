@@ -49,6 +49,11 @@ struct SimConfig {
     double v1[3] = {0.0, 0.0, 0.0};
     std::vector<ParticleInit> particles;
     std::vector<WallInit> walls;
+    // addition (the reference ignores these keys): the particle-particle normal law.  0 = zdem
+    // (Fn = (E1/R1 + E2/R2) A^1.5, src/main.cpp:2237-2247), 1 = feng_min (Fn = k/2 |Sn|, polyline.py:677)
+    // with the zdem tangential, damping and Coulomb terms
+    int force_law = 0;
+    double feng_k = 1e7;
 };
 
 // parse_config_file, src/main.cpp:1531-1689 (same grammar, defaults and acceptance rule).

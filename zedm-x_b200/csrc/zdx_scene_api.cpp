@@ -78,6 +78,38 @@ extern "C" int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t cont
     return ZDX_OK;
 }
 
+extern "C" int zdx_scene_array(zdx_ctx* ctx, int which, void* out, int64_t* count) {
+    if (!ctx || !count) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    const Scene& s = *ctx->scene;
+    const void* src = nullptr;
+    size_t n = 0, esz = sizeof(double);
+    switch (which) {
+        case ZDX_SCENE_MAT: src = s.mat.data(); n = s.mat.size(); break;
+        case ZDX_SCENE_PMESH: src = s.pmesh.data(); n = s.pmesh.size(); esz = sizeof(int32_t); break;
+        case ZDX_SCENE_MESH_TRIS: src = s.mesh_tris.data(); n = s.mesh_tris.size(); break;
+        case ZDX_SCENE_MESH_OFF: src = s.mesh_off.data(); n = s.mesh_off.size(); esz = sizeof(int64_t); break;
+        case ZDX_SCENE_MESH_PROPS: src = s.mesh_props.data(); n = s.mesh_props.size(); break;
+        case ZDX_SCENE_WALL_TRIS: src = s.wtris.data(); n = s.wtris.size(); break;
+        case ZDX_SCENE_WALL_NORMALS: src = s.wnormals.data(); n = s.wnormals.size(); break;
+        case ZDX_SCENE_WALL_OFF: src = s.wtri_off.data(); n = s.wtri_off.size(); esz = sizeof(int64_t); break;
+        case ZDX_SCENE_WALL_MAT: src = s.wmat.data(); n = s.wmat.size(); break;
+        case ZDX_SCENE_WALL_POSE: src = s.wpose.data(); n = s.wpose.size(); break;
+        case ZDX_SCENE_WALL_MESH: src = s.wmesh.data(); n = s.wmesh.size(); esz = sizeof(int32_t); break;
+        case ZDX_SCENE_PARAMS: {
+            const double v[7] = {s.cfg.dt, s.cfg.gravity[0], s.cfg.gravity[1], s.cfg.gravity[2],
+                                 s.cfg.split_contacts ? 1.0 : 0.0, (double)s.cfg.force_law, s.cfg.feng_k};
+            *count = 7;
+            if (out) std::memcpy(out, v, sizeof(v));
+            return ZDX_OK;
+        }
+        default: return ctx_fail(ctx, ZDX_ERR_INVALID, "unknown scene array %d", which);
+    }
+    *count = (int64_t)n;
+    if (out && n) std::memcpy(out, src, n * esz);
+    return ZDX_OK;
+}
+
 extern "C" int zdx_scene_info(zdx_ctx* ctx, int64_t* info) {
     if (!ctx || !info) return ZDX_ERR_INVALID;
     if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");

@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
     L.zdx_scene_load.argtypes = [C.c_void_p, C.c_char_p]
     L.zdx_scene_step.argtypes = [C.c_void_p, C.c_int]
     L.zdx_scene_info.argtypes = [C.c_void_p, _i64p]
+    L.zdx_scene_array.argtypes = [C.c_void_p, C.c_int, C.c_void_p, _i64p]
     L.zdx_scene_get_state.argtypes = [C.c_void_p, _dp, _dp, _dp, _i32p]
     L.zdx_scene_set_state.argtypes = [C.c_void_p, _dp]
     L.zdx_scene_write_output.argtypes = [C.c_void_p, C.c_int64]

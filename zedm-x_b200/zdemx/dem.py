@@ -37,6 +37,23 @@ class Scene:
         _lib.check(_lib.lib().zdx_scene_graph_reserve(self.ctx.handle, int(pairs), int(contacts), int(segments),
                                                       int(seg_per_pair)), self.ctx.handle)
 
+    ARRAYS = {"mat": (0, np.float64, 17), "pmesh": (1, np.int32, 1), "mesh_tris": (2, np.float64, 9),
+              "mesh_off": (3, np.int64, 1), "mesh_props": (4, np.float64, 17), "wall_tris": (5, np.float64, 9),
+              "wall_normals": (6, np.float64, 3), "wall_off": (7, np.int64, 1), "wall_mat": (8, np.float64, 2),
+              "wall_pose": (9, np.float64, 7), "wall_mesh": (10, np.int32, 1), "params": (11, np.float64, 1)}
+
+    def array(self, name: str) -> np.ndarray:
+        """A set-up array of the scene (zdx_scene_array): mat, pmesh, mesh_tris, mesh_off, mesh_props,
+        wall_tris, wall_normals, wall_off, wall_mat, wall_pose, wall_mesh, params (dt, gravity, split,
+        force_law, feng_k)."""
+        which, dt, width = self.ARRAYS[name]
+        n = C.c_int64(0)
+        _lib.check(_lib.lib().zdx_scene_array(self.ctx.handle, which, None, C.byref(n)), self.ctx.handle)
+        out = np.zeros(max(n.value, 1), dt)
+        _lib.check(_lib.lib().zdx_scene_array(self.ctx.handle, which, out.ctypes.data, C.byref(n)), self.ctx.handle)
+        out = out[: n.value]
+        return out.reshape(-1, width) if width > 1 else out
+
     def info(self) -> dict:
         v = np.zeros(12, np.int64)
         _lib.check(_lib.lib().zdx_scene_info(self.ctx.handle, v.ctypes.data_as(_lib._i64p)), self.ctx.handle)

@@ -8,6 +8,9 @@ overlapping (the densest packing of their circumspheres holds about 76,000), so 
 60 x 60 mm floor and is as tall as the lattice needs.
 
 two_particle_scene: two 320-triangle noised icospheres colliding head-on.
+
+calibration_scene: a lattice of 320-triangle noised icospheres resting on a 2-triangle plane, the
+feng_min law (a calibration target for k and the restitution).
 """
 from __future__ import annotations
 
@@ -115,6 +118,46 @@ def two_particle_scene(dirpath: str, seed: int = 1, steps: int = 2000, dt: float
         lines += ["particle", f"stl = {p}", f"pos = {x}", f"vel = {v}", "quat = 1 0 0 0", "omega = 0 0 0",
                   "scale = 1"] + mat + ["end_particle"]
     cfg = os.path.join(dirpath, "two.txt")
+    with open(cfg, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return cfg
+
+
+def plane_tris(half: float) -> np.ndarray:
+    """Two triangles spanning [-half, half]^2 at z = 0, normal +z; their shared edge is the diagonal y = x."""
+    h = half
+    return np.array([[[-h, -h, 0.0], [h, -h, 0.0], [h, h, 0.0]], [[-h, -h, 0.0], [h, h, 0.0], [-h, h, 0.0]]])
+
+
+def calibration_scene(dirpath: str, n_side: int = 10, seed: int = 5, steps: int = 2000, dt: float = 2e-6,
+                      k: float = 1e7, restitution: float = 0.5, spacing: float = 1.85e-3, vel_sigma: float = 0.02,
+                      output_interval: int = 1 << 30) -> str:
+    """n_side^3 noised icospheres (320 triangles, circumradius 1 mm) in a lattice resting on a 2-triangle
+    plane, the feng_min law with stiffness k; the lattice sits inside one of the plane's triangles (well
+    away from the shared diagonal).  Returns the config path."""
+    rng = np.random.default_rng(seed)
+    os.makedirs(dirpath, exist_ok=True)
+    mesh = os.path.join(dirpath, "ico320.stl")
+    write_binary_stl(mesh, synth.noised_icosphere(2, 1e-3 / 1.15, 0.15, rng))
+    plane = os.path.join(dirpath, "plane.stl")
+    write_binary_stl(plane, plane_tris(0.1))
+    n = n_side ** 3
+    k_ = np.arange(n)
+    ix, iy, iz = k_ % n_side, (k_ // n_side) % n_side, k_ // (n_side * n_side)
+    pos = np.stack([10e-3 + ix * spacing, -10e-3 - iy * spacing, 0.95e-3 + iz * spacing], 1)
+    pos += rng.uniform(-2e-6, 2e-6, size=pos.shape)
+    vel = rng.normal(0.0, vel_sigma, size=(n, 3))
+    quat = synth.random_unit_quat(rng, n)
+    lines = [f"steps = {steps}", f"dt = {dt!r}", "gravity = 0 0 -9.81", "split_contacts = 1",
+             "force_law = feng_min", f"feng_k = {k!r}", f"output_interval = {output_interval}",
+             f"output_dir = {os.path.join(dirpath, 'out')}", "vtk_prefix = cal", "wall", f"stl = {plane}",
+             "pos = 0 0 0", "quat = 1 0 0 0", "scale = 1", "mu = 0.5", "restitution = 0.5", "end_wall"]
+    mat = [f"density = {MATERIAL['density']}", f"young = {MATERIAL['young']}", f"poisson = {MATERIAL['poisson']}",
+           f"mu = {MATERIAL['mu']}", f"restitution = {restitution!r}"]
+    for i in range(n):
+        lines += ["particle", f"stl = {mesh}", f"pos = {_fmt(pos[i])}", f"vel = {_fmt(vel[i])}",
+                  f"quat = {_fmt(quat[i])}", "omega = 0 0 0", "scale = 1"] + mat + ["end_particle"]
+    cfg = os.path.join(dirpath, "calibration.txt")
     with open(cfg, "w") as f:
         f.write("\n".join(lines) + "\n")
     return cfg
