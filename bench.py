@@ -51,11 +51,14 @@ def parse():
     ap.add_argument("--plain-pairs", type=int, default=2048, help="pairs timed in the plain per-pair form")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--workload", choices=["sweep", "pour", "two", "adjoint"], default="sweep",
+    ap.add_argument("--workload", choices=["sweep", "pour", "two", "adjoint", "rollout"], default="sweep",
                     help="sweep: the batched pair sweep (default); pour: 100k-particle DEM step in one CUDA graph; "
-                         "two: the two-particle DEM run; adjoint: contact geometry + its adjoint")
+                         "two: the two-particle DEM run; adjoint: contact geometry + its adjoint; "
+                         "rollout: gradients of a 2000-step, 1000-particle rollout, checkpointed vs stored")
     ap.add_argument("--particles", type=int, default=100_000, help="pour: particle count")
     ap.add_argument("--preroll", type=int, default=1500, help="pour: untimed steps before warm-up (collisions start)")
+    ap.add_argument("--rollout-steps", type=int, default=2000, help="rollout: steps of the rollout")
+    ap.add_argument("--rollout-side", type=int, default=10, help="rollout: particles per lattice side")
     return ap.parse_args()
 
 
@@ -203,6 +206,8 @@ def main():
         return run_two(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "rollout":
+        return run_rollout(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -855,6 +860,111 @@ def run_adjoint(args):
                        "frac_within_1e-6": float(np.mean(rel_ok <= 1e-6)) if len(rel_ok) else None,
                        "h": "1e-7 r (and 2.5e-8 r for the smoothness flag)"},
           "clocks": clk.summary()})
+
+
+def run_rollout(args):
+    """Calibration rollout: n^3 320-triangle icospheres on a 2-triangle plane, the feng_min law, 2000
+    steps of dt 2e-6; loss = sum of squared final-position errors against a target made with k = 1.3e7,
+    e = 0.35; gradients w.r.t. k, e and the initial velocities v0, with the rollout checkpointed every
+    100 steps and with every step's intermediates stored."""
+    import tempfile
+
+    import torch
+
+    from zdemx import _lib
+    from zdemx.dem import Scene
+    from zdemx.rollout import DiffScene
+    from zdemx.workloads import calibration_scene
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    d = tempfile.mkdtemp(prefix="zdx_cal_")
+    steps = args.rollout_steps
+    cfg_path = calibration_scene(d, n_side=args.rollout_side, seed=args.seed, steps=steps)
+    n = args.rollout_side ** 3
+    desc = (f"calibration rollout: {n} noised icospheres (320 triangles, circumradius 1 mm) on a 2-triangle plane, "
+            f"feng_min law, {steps} steps of dt 2e-6; loss = sum |x_T - x_T(k=1.3e7, e=0.35)|^2; "
+            "gradients w.r.t. k, e, v0 (reverse mode through the CUDA contact adjoint), FP64")
+    if args.impl == "reference":
+        emit({"impl": "reference", "unavailable": "the reference has no derivatives (no gradient rollout to time)"})
+        return
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctx = _lib.Context(0)
+    sc = Scene(cfg_path, ctx)
+    ds = DiffScene(sc)
+    state0 = torch.from_numpy(sc.state()[0]).to(dev)
+    f64 = lambda v: torch.tensor(v, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.no_grad():
+        tgt, _ = ds.rollout(state0, f64(1.3e7), f64(0.35), steps)
+    torch.cuda.synchronize()
+    fwd_torch_s = time.perf_counter() - t0
+    target = tgt[:, 0:3].clone()
+    del tgt
+
+    def grad_run(ck):
+        k = f64(1e7).requires_grad_(True)
+        e = f64(0.5).requires_grad_(True)
+        v0 = state0[:, 7:10].clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        base = torch.cuda.memory_allocated()
+        t1 = time.perf_counter()
+        st = torch.cat([state0[:, 0:7], v0, state0[:, 10:16]], 1)
+        xT, last = ds.rollout(st, k, e, steps, checkpoint_every=ck)
+        loss = ((xT[:, 0:3] - target) ** 2).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        dt_s = time.perf_counter() - t1
+        peak = torch.cuda.max_memory_allocated() - base
+        free, total = torch.cuda.mem_get_info()
+        print(f"rollout ck={ck}: {dt_s:.1f} s, torch peak {peak / 1e9:.2f} GB, reserved "
+              f"{torch.cuda.memory_reserved() / 1e9:.2f} GB, device free {free / 1e9:.1f} of {total / 1e9:.1f} GB",
+              file=sys.stderr, flush=True)
+        return {"seconds": dt_s, "peak_torch_bytes": int(peak), "loss": loss.item(), "dL_dk": k.grad.item(),
+                "dL_de": e.grad.item(), "dL_dv0_norm": float(v0.grad.norm().item()), "last_step": last}
+
+    ck = grad_run(100)
+    try:
+        full = grad_run(None)
+        same = abs(full["dL_dk"] - ck["dL_dk"]) <= 1e-9 * abs(ck["dL_dk"])
+        full["matches_checkpointed"] = bool(same)
+    except torch.cuda.OutOfMemoryError as exc:
+        full = {"unavailable": f"out of memory: {str(exc)[:120]}"}
+    torch.cuda.empty_cache()
+    free, total = torch.cuda.mem_get_info()
+    print(f"before the graph forward: device free {free / 1e9:.1f} of {total / 1e9:.1f} GB", file=sys.stderr, flush=True)
+    # the same forward on the CUDA graph step (no gradients)
+    try:
+        sg = Scene(cfg_path, ctx)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        sg.step_graph(steps)
+        torch.cuda.synchronize()
+        graph_s = time.perf_counter() - t1
+        moved = float(np.max(np.abs(sg.state()[0][:, 0:3] - state0[:, 0:3].cpu().numpy())))
+    except _lib.ZdxError as exc:
+        graph_s, moved = None, f"unavailable: {exc}"
+    cpu = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": "skipped (--cpu-seconds 0)"}
+    if args.cpu_seconds > 0 and os.path.exists(_ref_exe()):
+        try:
+            ms, _ = _ref_step_ms(cfg_path, 3)
+            cpu = {"value": 1e3 / np.mean(ms), "unit": "steps/s", "cores": 1, "kind": "reference",
+                   "sample": "3 forward steps of zdem_cpu on the same scene (its zdem law; it has no feng_min and no "
+                             "gradients)"}
+        except Exception as exc:
+            cpu["sample"] = f"unavailable: {exc}"
+    value = steps / ck["seconds"]
+    emit({"metric": "gradient rollout steps/s", "value": value, "unit": "steps/s", "n_gpus": 1, "steps": steps,
+          "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+          "dtype": "f64", "data": "synthetic (seeded calibration scene)",
+          "config": {"workload": desc, "particles": n, "checkpoint_every": 100},
+          "checkpointed": ck, "stored": full,
+          "forward_only": {"torch_step_s": fwd_torch_s, "cuda_graph_step_s": graph_s,
+                           "max_displacement_m": moved},
+          "cpu_baseline": cpu})
 
 
 if __name__ == "__main__":

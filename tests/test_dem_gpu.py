@@ -140,3 +140,33 @@ def test_cli_outputs_match_reference_program(tmp_path):
     bad.write_text("steps = 3\n")
     assert subprocess.run([os.path.join(root, "zedm-x_b200", "bin", "zdem_gpu"), "--config", str(bad)],
                           capture_output=True).returncode == 1
+
+
+def test_lattice_of_216_particles_on_a_plane(tmp_path):
+    """More particles than one block of the broad-phase kernels: every candidate pair of the reference's
+    O(N^2) loop is found (the step log's tri_checks counts their triangle tests)."""
+    from zdemx.workloads import calibration_scene
+
+    cfg = calibration_scene(str(tmp_path / "lat"), n_side=6, seed=9, steps=6, spacing=1.85e-3)
+    text = "\n".join(ln for ln in open(cfg).read().splitlines()
+                     if not ln.startswith(("force_law", "feng_k", "output_interval", "output_dir")))
+    glob = {"output_interval": 2, "output_dir": str(tmp_path / "ref")}
+    text = "\n".join(f"{k} = {v}" for k, v in glob.items()) + "\n" + text
+    path = str(tmp_path / "lattice.txt")
+    open(path, "w").write(text + "\n")
+    from zdemx.dem import Scene
+
+    log = parse_log(run_reference(path))
+    sc = Scene(path)
+    done = 0
+    for s in range(0, 6, 2):
+        sc.step(s + 1 - done)
+        done = s + 1
+        info = sc.info()
+        got = (info["contacts"], info["tri_checks"], info["segments"], info["comps"], info["loops"])
+        assert got == log[s], f"step {s}: gpu {got} reference {log[s]}"
+        assert info["pairs"] > 256
+    ref = parse_state_txt(out_file(str(tmp_path / "ref"), "cal", 4, ".txt"))
+    st = sc.state()[0]
+    scale = np.max(np.abs(ref[:, 0:3]))
+    assert np.max(np.abs(st[:, 0:3] - ref[:, 0:3])) / scale <= 1e-9

@@ -750,7 +750,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         CKS(cudaMemsetAsync(s.bp_start.p, 0, sizeof(int) * T, st));
         CKS(cudaMemsetAsync(s.bp_end.p, 0, sizeof(int) * T, st));
         k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(s.bp_key), np, as<int>(s.bp_start), as<int>(s.bp_end));
-        k_bp_pairs<false><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
+        k_bp_pairs<false><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
                                                     as<int>(s.bp_start), as<int>(s.bp_end), T - 1, as<int32_t>(s.bp_cnt),
                                                     nullptr, nullptr, INT64_MAX);
         CKS(scan_counts_i32(as<int32_t>(s.bp_cnt), np, as<int64_t>(s.bp_off), st));
@@ -764,7 +764,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
     const size_t P1 = (size_t)std::max<int64_t>(npair, 1);
     CKS(s.bp_pairs.ensure(sizeof(int2) * P1));
     if (np > 0) {
-        k_bp_pairs<true><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
+        k_bp_pairs<true><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(s.bp_cell), as<int32_t>(s.bp_idx),
                                                    as<int>(s.bp_start), as<int>(s.bp_end), T - 1, nullptr,
                                                    as<int64_t>(s.bp_off), as<int2>(s.bp_pairs), INT64_MAX);
         ctx->launches += 1;
@@ -1151,11 +1151,11 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
     CKS(cudaMemsetAsync(G.bp_start.p, 0, sizeof(int) * G.T, st));
     CKS(cudaMemsetAsync(G.bp_end.p, 0, sizeof(int) * G.T, st));
     k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(G.bp_key), np, as<int>(G.bp_start), as<int>(G.bp_end));
-    k_bp_pairs<false><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
+    k_bp_pairs<false><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
                                                 as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1, as<int32_t>(G.bp_cnt),
                                                 nullptr, nullptr, INT64_MAX);
     CKS(scan_offsets<int32_t>(as<int32_t>(G.bp_cnt), np, nullptr, as<int64_t>(G.bp_off), G.scan_tmp.p, st));
-    k_bp_pairs<true><<<grid(np), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
+    k_bp_pairs<true><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
                                                as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1, nullptr,
                                                as<int64_t>(G.bp_off), as<int2>(G.bp_pairs), G.pcap);
     k_g_take<<<1, 1, 0, st>>>(as<int64_t>(G.bp_off) + np, G.pcap, &g->npair, &g->need_pairs, flags, GRAPH_OVF_PAIRS);
