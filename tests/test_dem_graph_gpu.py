@@ -103,3 +103,17 @@ def test_zdem_gpu_graph_flag_writes_the_same_files(tmp_path):
         a = parse_state_txt(out_file(str(tmp_path / "plain"), "p", step, ".txt"))
         b = parse_state_txt(out_file(str(tmp_path / "graph"), "p", step, ".txt"))
         assert np.array_equal(a, b)
+
+
+def test_graph_step_matches_plain_step_with_many_particles(tmp_path):
+    """216 particles: more than one block of every per-particle kernel, on both step forms."""
+    from zdemx.dem import Scene
+    from zdemx.workloads import calibration_scene
+
+    cfg = calibration_scene(str(tmp_path / "lat"), n_side=6, seed=9, steps=40, spacing=1.85e-3)
+    plain, graph = Scene(cfg), Scene(cfg)
+    for chunk in (1, 9, 30):
+        plain.step(chunk)
+        graph.step_graph(chunk)
+        _same(plain, graph, f"after {plain.info()['steps']} steps")
+    assert plain.info()["pairs"] > 256
