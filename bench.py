@@ -71,7 +71,9 @@ def workload(args, rank):
     for s in (1, 2, 3, 4):
         raw.extend(list(synth.noised_icospheres(s, args.lib_per_level, 1e-3, 0.15, rng)))
     lib = MeshLibrary.build(raw)
-    prng = np.random.default_rng(args.seed + 1 + rank)
+    from zdemx.replicas import rank_seed
+
+    prng = np.random.default_rng(rank_seed(args.seed, rank))
     lv = prng.integers(0, 4, size=(args.pairs, 2))
     idx = prng.integers(0, args.lib_per_level, size=(args.pairs, 2))
     pm = (lv * args.lib_per_level + idx).astype(np.int32)
@@ -306,9 +308,9 @@ def main():
     launches = ctx.timings()["launches"] - launches0
     T = sum(step_ms) / 1e3
     if world > 1:
-        tt = torch.tensor([T], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        T = float(tt.item())
+        from zdemx.replicas import max_over_ranks
+
+        T = max_over_ranks(T, dev)
         dist.barrier()
     value = world * args.pairs * args.steps / T
 
@@ -337,9 +339,9 @@ def main():
         e2e_t.append(time.perf_counter() - t0)
     TE = sum(e2e_t)
     if world > 1:
-        tt = torch.tensor([TE], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        TE = float(tt.item())
+        from zdemx.replicas import max_over_ranks
+
+        TE = max_over_ranks(TE, dev)
     e2e_value = world * args.pairs * args.steps / TE
     h2d = sum(int(v.numel() * v.element_size()) for v in h.values())
     nct = int(tot_e[0])

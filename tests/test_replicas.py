@@ -1,0 +1,60 @@
+"""Host logic of the multi-GPU sweep on two gloo ranks (CPU): the slowest rank's time and the counts
+reach every rank, each rank draws a different batch, and the strong-scaling split covers every pair
+once with balanced triangle-test work."""
+import os
+
+import numpy as np
+import pytest
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    from zdemx.replicas import gather_counts, max_over_ranks, rank_seed
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        t = max_over_ranks(1.5 + rank)
+        counts = gather_counts(10 * (rank + 1))
+        q.put((rank, t, counts, rank_seed(7, rank)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks():
+    import socket
+
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(2))
+    assert [r[1] for r in res] == [2.5, 2.5]
+    assert all(r[2] == [10, 20] for r in res)
+    assert res[0][3] != res[1][3]
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_cost_balanced_ranges(world):
+    from zdemx.replicas import cost_balanced_ranges, pair_costs
+
+    rng = np.random.default_rng(world)
+    tri_off = np.r_[0, np.cumsum(20 * 4 ** rng.integers(1, 5, size=40))]
+    pm = rng.integers(0, 40, size=(5000, 2))
+    costs = pair_costs(tri_off, pm)
+    order = np.argsort(-costs, kind="stable")          # the cost order of the work queue
+    ranges = cost_balanced_ranges(costs[order], world)
+    assert len(ranges) == world and ranges[0][0] == 0 and ranges[-1][1] == len(pm)
+    assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
+    loads = [costs[order][a:b].sum() for a, b in ranges]
+    assert max(loads) - min(loads) <= 2 * costs.max() + 1

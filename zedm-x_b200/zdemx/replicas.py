@@ -1,0 +1,66 @@
+"""Host logic of running the pair sweep on several GPUs, one process per GPU.
+
+Pairs are independent, so ranks never exchange data on the path: each rank either runs its own batch
+(weak scaling, what bench.py measures) or takes a contiguous range of one cost-ordered batch with an
+equal share of the triangle-test work (strong scaling).  The only collectives are host-side: the
+slowest rank's time, and one gather of the per-rank results.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def pair_costs(tri_off, pair_mesh) -> np.ndarray:
+    """nA * nB per pair: the triangle-pair count the reference's loop tests (src/main.cpp:2123-2145)."""
+    n = np.diff(np.asarray(tri_off, np.int64))
+    pm = np.asarray(pair_mesh).reshape(-1, 2)
+    return n[pm[:, 0]] * n[pm[:, 1]]
+
+
+def cost_balanced_ranges(costs, world: int) -> list[tuple[int, int]]:
+    """Split pairs 0..n-1, in the order given, into `world` contiguous ranges of nearly equal total cost
+    (each boundary at the first pair whose cumulative cost reaches r/world of the total)."""
+    c = np.asarray(costs, np.float64)
+    n = len(c)
+    if world <= 1 or n == 0:
+        return [(0, n)] + [(n, n)] * max(world - 1, 0)
+    cum = np.cumsum(c)
+    total = cum[-1]
+    cuts = [0]
+    for r in range(1, world):
+        cuts.append(int(np.searchsorted(cum, total * r / world, side="left")) + 1 if total > 0 else n * r // world)
+    cuts = [min(max(x, 0), n) for x in cuts] + [n]
+    for i in range(1, len(cuts)):
+        cuts[i] = max(cuts[i], cuts[i - 1])
+    return [(cuts[r], cuts[r + 1]) for r in range(world)]
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Seed of a rank's own batch in the weak-scaling run (every rank a different batch)."""
+    return int(base) + 1 + int(rank)
+
+
+def max_over_ranks(value: float, device=None) -> float:
+    """The largest value over the ranks of the default process group (the time of the slowest rank);
+    the value itself when no group is initialised."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gather_counts(count: int, device=None) -> list[int]:
+    """Every rank's count (for example its contacts), on every rank."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return [int(count)]
+    t = torch.tensor([int(count)], dtype=torch.int64, device=device)
+    out = [torch.zeros_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(out, t)
+    return [int(x.item()) for x in out]
