@@ -179,6 +179,19 @@ int zdx_scene_get_state(zdx_ctx* ctx, double* state16, double* force3, double* t
 int zdx_scene_set_state(zdx_ctx* ctx, const double* state16);
 /* write_vtk_particles + write_particle_state_txt (src/main.cpp:1710-1870, 2470-2483) for `step`. */
 int zdx_scene_write_output(zdx_ctx* ctx, int64_t step);
+/* Steps in which no pair passes the broad-phase sphere test and no particle a wall's have no contact:
+ * for scenes of up to 1024 particles a run of them goes through one single-block kernel that repeats the
+ * test and the integration until a step has a candidate (the results are those of the full step).  On by
+ * default; enable = 0 sends every step through the full step. */
+int zdx_scene_set_free_flight(zdx_ctx* ctx, int enable);
+/* The same two files, written while the caller goes on stepping (no counterpart in the reference, whose
+ * outputs stop the run): the call snapshots the current particle arrays on the device, in stream order,
+ * and returns; a copy stream and a writer thread produce the files.  At most two outputs are in flight;
+ * a third call waits for the oldest.  The files are byte-identical to zdx_scene_write_output's. */
+int zdx_scene_write_output_async(zdx_ctx* ctx, int64_t step);
+/* Waits until every output queued by zdx_scene_write_output_async is on disk; ZDX_ERR_IO if any could
+ * not be written since the last wait.  Loading another scene or destroying the context also waits. */
+int zdx_scene_output_wait(zdx_ctx* ctx);
 /* The same steps as zdx_scene_step, with every count kept on the device and the whole step captured
  * once into a CUDA graph that is replayed (no counterpart in the reference).  Buffers have fixed
  * capacities; a step that would exceed one leaves state and history untouched, and the call grows the

@@ -13,9 +13,11 @@
 #include <iomanip>
 #include <iostream>
 #include <sstream>
+#include <thread>
 #include <unordered_map>
 
 #include "../../include/zdemx.h"
+#include "zdx_format.h"
 #include "zdx_host.h"
 #include "zdx_math.cuh"
 #include "zdx_scene.h"
@@ -388,102 +390,181 @@ int scene_from_config(zdx_ctx* ctx, const SimConfig& cfg, Scene& s, std::string&
     return ZDX_OK;
 }
 
-bool write_vtk_particles(const std::string& path, const Scene& s) {
-    std::ofstream out(path);
-    if (!out) {
+namespace {
+struct FileCloser {
+    std::FILE* f;
+    ~FileCloser() {
+        if (f) std::fclose(f);
+    }
+};
+}  // namespace
+
+int output_threads() {
+    unsigned h = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(h > 1 ? h - 1 : 1u, 16u));
+}
+
+ParticleFrame host_frame(const Scene& s) {
+    return ParticleFrame{s.np, s.state.data(), s.force.data(), s.torque.data(), s.contact_count.data()};
+}
+
+// write_vtk_particles (src/main.cpp:1710-1840): the same sections, lines and number formats.
+bool write_vtk_particles(const std::string& path, const Scene& s, const ParticleFrame& fr, int threads) {
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) {
         std::cerr << "Failed to write VTK: " << path << "\n";
         return false;
     }
-    out << "# vtk DataFile Version 3.0\n";
-    out << "zdem particles\n";
-    out << "ASCII\n";
-    out << "DATASET POLYDATA\n";
-    std::size_t total_tris = 0;
+    FileCloser closer{f};
+    const int np = fr.np;
     auto ntri = [&](int i) { return static_cast<std::size_t>(s.mesh_off[s.pmesh[i] + 1] - s.mesh_off[s.pmesh[i]]); };
-    for (int i = 0; i < s.np; ++i) total_tris += ntri(i);
-    out << "POINTS " << total_tris * 3 << " float\n";
-    for (int i = 0; i < s.np; ++i) {
-        const double* st = &s.state[16 * (size_t)i];
-        Q4 qn = qnormalize(Q4{st[3], st[4], st[5], st[6]});
-        V3 pos{st[0], st[1], st[2]};
-        const double* mt = &s.mesh_tris[9 * (size_t)s.mesh_off[s.pmesh[i]]];
-        for (std::size_t k = 0; k < ntri(i); ++k)
-            for (int c = 0; c < 3; ++c) {
-                V3 v = qrotate_n(qn, V3{mt[9 * k + 3 * c], mt[9 * k + 3 * c + 1], mt[9 * k + 3 * c + 2]}) + pos;
-                out << static_cast<float>(v.x) << " " << static_cast<float>(v.y) << " " << static_cast<float>(v.z) << "\n";
-            }
-    }
-    out << "POLYGONS " << total_tris << " " << total_tris * 4 << "\n";
-    for (std::size_t i = 0; i < total_tris; ++i) {
-        std::size_t b = i * 3;
-        out << "3 " << b << " " << b + 1 << " " << b + 2 << "\n";
-    }
-    out << "CELL_DATA " << total_tris << "\n";
-    out << "SCALARS id int 1\n";
-    out << "LOOKUP_TABLE default\n";
-    for (int i = 0; i < s.np; ++i)
-        for (std::size_t t = 0; t < ntri(i); ++t) out << i << "\n";
-    out << "SCALARS mass float 1\n";
-    out << "LOOKUP_TABLE default\n";
-    for (int i = 0; i < s.np; ++i)
-        for (std::size_t t = 0; t < ntri(i); ++t) out << static_cast<float>(s.mat[17 * (size_t)i]) << "\n";
-    out << "SCALARS radius float 1\n";
-    out << "LOOKUP_TABLE default\n";
-    for (int i = 0; i < s.np; ++i)
-        for (std::size_t t = 0; t < ntri(i); ++t) out << static_cast<float>(s.mat[17 * (size_t)i + 2]) << "\n";
-    out << "SCALARS contact_count int 1\n";
-    out << "LOOKUP_TABLE default\n";
-    for (int i = 0; i < s.np; ++i)
-        for (std::size_t t = 0; t < ntri(i); ++t) out << s.contact_count[i] << "\n";
-    auto vec = [&](const char* name, const double* base, std::size_t stride) {
-        out << "VECTORS " << name << " float\n";
-        for (int i = 0; i < s.np; ++i) {
-            const double* v = base + stride * (size_t)i;
-            for (std::size_t t = 0; t < ntri(i); ++t)
-                out << static_cast<float>(v[0]) << " " << static_cast<float>(v[1]) << " " << static_cast<float>(v[2]) << "\n";
+    std::size_t total_tris = 0;
+    for (int i = 0; i < np; ++i) total_tris += ntri(i);
+    TextBuf h;
+    h.lit("# vtk DataFile Version 3.0\nzdem particles\nASCII\nDATASET POLYDATA\nPOINTS ");
+    h.integer(total_tris * 3);
+    h.lit(" float\n");
+    bool ok = std::fwrite(h.s.data(), 1, h.s.size(), f) == h.s.size();
+    ok = write_sliced(f, np, threads, [&](int64_t b, int64_t e, TextBuf& o) {
+        for (int64_t i = b; i < e; ++i) {
+            const double* st = fr.state + 16 * i;
+            Q4 qn = qnormalize(Q4{st[3], st[4], st[5], st[6]});
+            V3 pos{st[0], st[1], st[2]};
+            const double* mt = &s.mesh_tris[9 * (size_t)s.mesh_off[s.pmesh[i]]];
+            for (std::size_t k = 0; k < ntri((int)i); ++k)
+                for (int c = 0; c < 3; ++c) {
+                    V3 v = qrotate_n(qn, V3{mt[9 * k + 3 * c], mt[9 * k + 3 * c + 1], mt[9 * k + 3 * c + 2]}) + pos;
+                    o.f6(v.x);
+                    o.ch(' ');
+                    o.f6(v.y);
+                    o.ch(' ');
+                    o.f6(v.z);
+                    o.ch('\n');
+                }
         }
+    }) && ok;
+    h.s.clear();
+    h.lit("POLYGONS ");
+    h.integer(total_tris);
+    h.ch(' ');
+    h.integer(total_tris * 4);
+    h.ch('\n');
+    ok = std::fwrite(h.s.data(), 1, h.s.size(), f) == h.s.size() && ok;
+    ok = write_sliced(f, (int64_t)total_tris, threads, [&](int64_t b, int64_t e, TextBuf& o) {
+        for (int64_t i = b; i < e; ++i) {
+            const std::size_t v = (std::size_t)i * 3;
+            o.lit("3 ");
+            o.integer(v);
+            o.ch(' ');
+            o.integer(v + 1);
+            o.ch(' ');
+            o.integer(v + 2);
+            o.ch('\n');
+        }
+    }) && ok;
+    h.s.clear();
+    h.lit("CELL_DATA ");
+    h.integer(total_tris);
+    h.lit("\n");
+    // one value per triangle of each particle
+    auto per_tri = [&](const char* head, auto&& put) {
+        h.lit(head);
+        ok = std::fwrite(h.s.data(), 1, h.s.size(), f) == h.s.size() && ok;
+        h.s.clear();
+        ok = write_sliced(f, np, threads, [&](int64_t b, int64_t e, TextBuf& o) {
+            for (int64_t i = b; i < e; ++i)
+                for (std::size_t t = 0, n = ntri((int)i); t < n; ++t) put((int)i, o);
+        }) && ok;
     };
-    vec("velocity", s.state.data() + 7, 16);
-    vec("omega", s.state.data() + 10, 16);
-    vec("force", s.force.data(), 3);
-    vec("torque", s.torque.data(), 3);
-    out << "FIELD FieldData 1\n";
-    out << "orientation 4 " << total_tris << " float\n";
-    for (int i = 0; i < s.np; ++i) {
-        const double* st = &s.state[16 * (size_t)i];
-        for (std::size_t t = 0; t < ntri(i); ++t)
-            out << static_cast<float>(st[3]) << " " << static_cast<float>(st[4]) << " " << static_cast<float>(st[5]) << " "
-                << static_cast<float>(st[6]) << "\n";
-    }
-    return true;
+    per_tri("SCALARS id int 1\nLOOKUP_TABLE default\n", [&](int i, TextBuf& o) {
+        o.integer(i);
+        o.ch('\n');
+    });
+    per_tri("SCALARS mass float 1\nLOOKUP_TABLE default\n", [&](int i, TextBuf& o) {
+        o.f6(s.mat[17 * (size_t)i]);
+        o.ch('\n');
+    });
+    per_tri("SCALARS radius float 1\nLOOKUP_TABLE default\n", [&](int i, TextBuf& o) {
+        o.f6(s.mat[17 * (size_t)i + 2]);
+        o.ch('\n');
+    });
+    per_tri("SCALARS contact_count int 1\nLOOKUP_TABLE default\n", [&](int i, TextBuf& o) {
+        o.integer(fr.count[i]);
+        o.ch('\n');
+    });
+    auto vec = [&](const char* head, const double* base, std::size_t stride) {
+        per_tri(head, [&, base, stride](int i, TextBuf& o) {
+            const double* v = base + stride * (size_t)i;
+            o.f6(v[0]);
+            o.ch(' ');
+            o.f6(v[1]);
+            o.ch(' ');
+            o.f6(v[2]);
+            o.ch('\n');
+        });
+    };
+    vec("VECTORS velocity float\n", fr.state + 7, 16);
+    vec("VECTORS omega float\n", fr.state + 10, 16);
+    vec("VECTORS force float\n", fr.force, 3);
+    vec("VECTORS torque float\n", fr.torque, 3);
+    h.lit("FIELD FieldData 1\norientation 4 ");
+    h.integer(total_tris);
+    h.lit(" float\n");
+    per_tri("", [&](int i, TextBuf& o) {
+        const double* st = fr.state + 16 * (size_t)i;
+        o.f6(st[3]);
+        o.ch(' ');
+        o.f6(st[4]);
+        o.ch(' ');
+        o.f6(st[5]);
+        o.ch(' ');
+        o.f6(st[6]);
+        o.ch('\n');
+    });
+    return ok;
 }
 
-bool write_state_txt(const std::string& path, const Scene& s) {
-    std::ofstream out(path);
-    if (!out) {
+// write_particle_state_txt (src/main.cpp:1842-1870): fixed, 9 decimals.
+bool write_state_txt(const std::string& path, const Scene& s, const ParticleFrame& fr, int threads) {
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) {
         std::cerr << "Failed to write particle state: " << path << "\n";
         return false;
     }
-    out.setf(std::ios::fixed);
-    out << std::setprecision(9);
-    for (int i = 0; i < s.np; ++i) {
-        const double* st = &s.state[16 * (size_t)i];
-        const ParticleInit& init = s.inits[i];
-        out << "particle\n";
-        out << "stl = " << init.stl << "\n";
-        out << "pos = " << st[0] << " " << st[1] << " " << st[2] << "\n";
-        out << "vel = " << st[7] << " " << st[8] << " " << st[9] << "\n";
-        out << "quat = " << st[3] << " " << st[4] << " " << st[5] << " " << st[6] << "\n";
-        out << "omega = " << st[10] << " " << st[11] << " " << st[12] << "\n";
-        out << "scale = " << init.scale << "\n";
-        out << "density = " << init.density << "\n";
-        out << "young = " << init.young << "\n";
-        out << "poisson = " << init.poisson << "\n";
-        out << "mu = " << init.mu << "\n";
-        out << "restitution = " << init.restitution << "\n";
-        out << "end_particle\n\n";
-    }
-    return true;
+    FileCloser closer{f};
+    return write_sliced(f, fr.np, threads, [&](int64_t b, int64_t e, TextBuf& o) {
+        auto line3 = [&o](const char* key, const double* v, int n) {
+            o.lit(key);
+            for (int k = 0; k < n; ++k) {
+                if (k) o.ch(' ');
+                o.fixed9(v[k]);
+            }
+            o.ch('\n');
+        };
+        auto line1 = [&o](const char* key, double v) {
+            o.lit(key);
+            o.fixed9(v);
+            o.ch('\n');
+        };
+        for (int64_t i = b; i < e; ++i) {
+            const double* st = fr.state + 16 * i;
+            const ParticleInit& init = s.inits[i];
+            o.lit("particle\nstl = ");
+            o.lit(init.stl.c_str());
+            o.ch('\n');
+            line3("pos = ", st, 3);
+            line3("vel = ", st + 7, 3);
+            line3("quat = ", st + 3, 4);
+            line3("omega = ", st + 10, 3);
+            line1("scale = ", init.scale);
+            line1("density = ", init.density);
+            line1("young = ", init.young);
+            line1("poisson = ", init.poisson);
+            line1("mu = ", init.mu);
+            line1("restitution = ", init.restitution);
+            o.lit("end_particle\n\n");
+        }
+    });
 }
 
 }  // namespace zdx

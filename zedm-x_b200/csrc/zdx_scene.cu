@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <iostream>
 #include <string>
 #include <vector>
 
@@ -283,6 +284,7 @@ struct WallArgs {
     const int64_t* ncand_dev;  // null, or device-resident candidate / history counts
     const int64_t* nh_dev;
     const int* stop;           // null, or a flag that makes the step skip (capacity overflow)
+    double* dbg;               // null, or ncand x max_wtri x 7 (area, contact point, normal) for contact_debug
 };
 
 // compute_wall_contact (src/main.cpp:1205-1258) for one wall triangle, by one warp: lanes collect the
@@ -485,6 +487,12 @@ __global__ void k_walls(WallArgs a) {
                     S3(o, f);
                     S3(o + 3, cross(rP, f));
                     a.valid[k * a.max_wtri + slot] = 1;
+                    if (a.dbg) {
+                        double* d = a.dbg + 7 * (k * a.max_wtri + slot);
+                        d[0] = area;
+                        S3(d + 1, cpt);
+                        S3(d + 4, cn);
+                    }
                     touched = 1;
                 }
                 __syncwarp();
@@ -499,6 +507,50 @@ __global__ void k_walls(WallArgs a) {
 }
 
 // ---------------------------------------------------------------- scatter + integrate
+// integrate_particle, src/main.cpp:1494-1510, on one state row s (16) with material row m (17).
+__device__ __forceinline__ void integrate_state(double* s, const double* m, V3 F, V3 T, const double* g3, double dt) {
+    V3 acc = F * m[1] + L3(g3);
+    V3 vel = L3(s + 7) + acc * dt;
+    V3 pos = L3(s) + vel * dt;
+    Q4 q{s[3], s[4], s[5], s[6]};
+    Q4 qn = qnormalize(q);
+    double w = qn.w, x = qn.x, y = qn.y, z = qn.z;
+    double R[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
+                   2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
+                   2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)};
+    const double* Ib = m + 8;
+    double RI[9], Iinv[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double acc2 = 0.0;
+            for (int k = 0; k < 3; ++k) acc2 += R[3 * r + k] * Ib[3 * k + c];
+            RI[3 * r + c] = acc2;
+        }
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double acc2 = 0.0;
+            for (int k = 0; k < 3; ++k) acc2 += RI[3 * r + k] * R[3 * c + k];
+            Iinv[3 * r + c] = acc2;
+        }
+    V3 L = L3(s + 13) + T * dt;
+    V3 om{Iinv[0] * L.x + Iinv[1] * L.y + Iinv[2] * L.z, Iinv[3] * L.x + Iinv[4] * L.y + Iinv[5] * L.z,
+          Iinv[6] * L.x + Iinv[7] * L.y + Iinv[8] * L.z};
+    Q4 qd = qmul(Q4{0.0, om.x, om.y, om.z}, q);
+    q.w += 0.5 * qd.w * dt;
+    q.x += 0.5 * qd.x * dt;
+    q.y += 0.5 * qd.y * dt;
+    q.z += 0.5 * qd.z * dt;
+    q = qnormalize(q);
+    S3(s, pos);
+    s[3] = q.w;
+    s[4] = q.x;
+    s[5] = q.y;
+    s[6] = q.z;
+    S3(s + 7, vel);
+    S3(s + 10, om);
+    S3(s + 13, L);
+}
+
 __global__ void k_scatter_integrate(int np, const int2* pairs, const int64_t* pstart, const int32_t* tidx,
                                     const int64_t* tstart, const int64_t* coff, const double* pcontrib,
                                     const int64_t* wstart, const double* wcontrib, const int32_t* wvalid, int max_wtri,
@@ -540,49 +592,93 @@ __global__ void k_scatter_integrate(int np, const int2* pairs, const int64_t* ps
     S3(force + 3 * p, F);
     S3(torque + 3 * p, T);
     count[p] = cnt;
-    // integrate_particle, src/main.cpp:1494-1510
-    double* s = state + 16 * (int64_t)p;
-    const double* m = mat + 17 * (int64_t)p;
-    V3 acc = F * m[1] + L3(g3);
-    V3 vel = L3(s + 7) + acc * dt;
-    V3 pos = L3(s) + vel * dt;
-    Q4 q{s[3], s[4], s[5], s[6]};
-    Q4 qn = qnormalize(q);
-    double w = qn.w, x = qn.x, y = qn.y, z = qn.z;
-    double R[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
-                   2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
-                   2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)};
-    const double* Ib = m + 8;
-    double RI[9], Iinv[9];
-    for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) {
-            double acc2 = 0.0;
-            for (int k = 0; k < 3; ++k) acc2 += R[3 * r + k] * Ib[3 * k + c];
-            RI[3 * r + c] = acc2;
+    integrate_state(state + 16 * (int64_t)p, mat + 17 * (int64_t)p, F, T, g3, dt);
+}
+
+// ---------------------------------------------------------------- free flight
+// Steps of a small scene in which no pair passes the broad-phase sphere test (src/main.cpp:2050-2058, as
+// in k_bp_pairs) and no particle's box overlaps the box of a triangle of a wall whose sphere test it
+// passes (src/main.cpp:2312-2345, as in k_wall_cand and k_walls).  With no candidate there is no contact:
+// every force, torque and contact count is zero, both tangential histories are pruned to nothing
+// (src/main.cpp:2452-2468), and the step is the integration alone (integrate_state, the arithmetic of
+// k_scatter_integrate with zero sums).  One block runs up to max_steps such steps and stops before the
+// first step that has a candidate; the full step takes that one.  The launch has one thread per particle.
+__global__ void __launch_bounds__(FF_THREADS) k_free_flight(double* state, const double* mat, int np,
+                                                            const double* wpose, const double* wrad, int nw,
+                                                            const double* wtris, const int64_t* wtri_off,
+                                                            const double* g3, double dt, int max_steps, double* force,
+                                                            double* torque, int32_t* count, int64_t* done_out,
+                                                            GraphCounts* g) {
+    // thread i keeps particle i's state row in registers; positions and radii are shared for the tests
+    __shared__ double sp[3 * FF_MAX_NP];
+    __shared__ double sr[FF_MAX_NP];
+    __shared__ int hit;
+    const int i = threadIdx.x;
+    const bool own = i < np;
+    const double* m = mat + 17 * (int64_t)i;
+    double st[16];
+    if (own) {
+        for (int c = 0; c < 16; ++c) st[c] = state[16 * (int64_t)i + c];
+        sp[3 * i] = st[0];
+        sp[3 * i + 1] = st[1];
+        sp[3 * i + 2] = st[2];
+        sr[i] = m[2];
+    }
+    int k = 0;
+    for (; k < max_steps; ++k) {
+        if (i == 0) hit = 0;
+        __syncthreads();
+        if (own) {
+            const V3 pi{sp[3 * i], sp[3 * i + 1], sp[3 * i + 2]};
+            const double ri = sr[i];
+            bool any = false;
+            for (int j = i + 1; j < np && !any; ++j) {
+                V3 d = V3{sp[3 * j], sp[3 * j + 1], sp[3 * j + 2]} - pi;
+                double dist2 = dot(d, d);
+                double rsum = ri + sr[j];
+                any = !(dist2 > rsum * rsum);
+            }
+            for (int w = 0; w < nw && !any; ++w) {
+                V3 d = pi - L3(wpose + 7 * w);
+                double dist2 = dot(d, d);
+                double rsum = ri + wrad[w];
+                if (dist2 > rsum * rsum) continue;
+                const V3 pmn = pi - V3{ri, ri, ri}, pmx = pi + V3{ri, ri, ri};
+                for (int64_t t = wtri_off[w]; t < wtri_off[w + 1] && !any; ++t) {
+                    const double* wt = wtris + 9 * t;
+                    const V3 w0 = L3(wt), w1 = L3(wt + 3), w2 = L3(wt + 6);
+                    const V3 wmn{smin3(w0.x, w1.x, w2.x), smin3(w0.y, w1.y, w2.y), smin3(w0.z, w1.z, w2.z)};
+                    const V3 wmx{smax3(w0.x, w1.x, w2.x), smax3(w0.y, w1.y, w2.y), smax3(w0.z, w1.z, w2.z)};
+                    any = !(pmx.x < wmn.x || pmn.x > wmx.x || pmx.y < wmn.y || pmn.y > wmx.y || pmx.z < wmn.z ||
+                            pmn.z > wmx.z);
+                }
+            }
+            if (any) hit = 1;
         }
-    for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) {
-            double acc2 = 0.0;
-            for (int k = 0; k < 3; ++k) acc2 += RI[3 * r + k] * R[3 * c + k];
-            Iinv[3 * r + c] = acc2;
+        __syncthreads();
+        if (hit) break;  // block-uniform: read after the barrier, reset only after the next one
+        if (own) {
+            integrate_state(st, m, V3{0.0, 0.0, 0.0}, V3{0.0, 0.0, 0.0}, g3, dt);
+            sp[3 * i] = st[0];
+            sp[3 * i + 1] = st[1];
+            sp[3 * i + 2] = st[2];
         }
-    V3 L = L3(s + 13) + T * dt;
-    V3 om{Iinv[0] * L.x + Iinv[1] * L.y + Iinv[2] * L.z, Iinv[3] * L.x + Iinv[4] * L.y + Iinv[5] * L.z,
-          Iinv[6] * L.x + Iinv[7] * L.y + Iinv[8] * L.z};
-    Q4 qd = qmul(Q4{0.0, om.x, om.y, om.z}, q);
-    q.w += 0.5 * qd.w * dt;
-    q.x += 0.5 * qd.x * dt;
-    q.y += 0.5 * qd.y * dt;
-    q.z += 0.5 * qd.z * dt;
-    q = qnormalize(q);
-    S3(s, pos);
-    s[3] = q.w;
-    s[4] = q.x;
-    s[5] = q.y;
-    s[6] = q.z;
-    S3(s + 7, vel);
-    S3(s + 10, om);
-    S3(s + 13, L);
+    }
+    if (k > 0 && own) {
+        for (int c = 0; c < 16; ++c) state[16 * (int64_t)i + c] = st[c];
+        S3(force + 3 * (int64_t)i, V3{0.0, 0.0, 0.0});
+        S3(torque + 3 * (int64_t)i, V3{0.0, 0.0, 0.0});
+        count[i] = 0;
+    }
+    if (k > 0 && g && i == 0) {
+        g->steps_done += k;
+        g->npair = 0;
+        g->ncand = 0;
+        g->nhist = 0;
+        g->nwhist = 0;
+        g->contacts = g->wall_contacts = g->tri_checks = g->segments = g->comps = g->loops = 0;
+    }
+    if (done_out && i == 0) *done_out = k;
 }
 
 __global__ void k_range_bounds(const int2* pairs, int64_t npair, const int64_t* n_dev, int np, int64_t* pstart) {
@@ -708,6 +804,84 @@ int scene_download(zdx_ctx* ctx, Scene& s) {
     CKS(cudaStreamSynchronize(st));
     s.host_dirty = false;
     return ZDX_OK;
+}
+
+// contact_debug prints (src/main.cpp:2288-2299, 2436-2444), made before integration moves the particles:
+// the step's first particle-particle contact, then wall contacts in (particle, wall, triangle) order
+// while the running contact count, particle-particle ones included, stays below 3.
+static cudaError_t print_contact_debug(zdx_ctx* ctx, Scene& s, int64_t ncontact, int64_t ncand, int max_wtri) {
+    cudaStream_t st = ctx->stream;
+    auto put = [](const double* v) {
+        std::cout << v[0] << "," << v[1] << "," << v[2];
+    };
+    if (ncontact > 0) {
+        int32_t info[4];
+        double g[20], f[3];
+        int2 ij;
+        cudaError_t e = cudaMemcpyAsync(info, s.pr_info.p, sizeof(info), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(g, s.pr_geom.p, sizeof(g), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(f, s.pr_contrib.p, sizeof(f), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&ij, as<int2>(s.bp_pairs) + info[0], sizeof(ij), cudaMemcpyDeviceToHost, st);
+        double xa[16], xb[16];
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(xa, as<double>(s.d_state) + 16 * (int64_t)ij.x, sizeof(xa), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(xb, as<double>(s.d_state) + 16 * (int64_t)ij.y, sizeof(xb), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        const V3 xc0{g[6], g[7], g[8]}, F{f[0], f[1], f[2]};
+        const V3 rA = xc0 - V3{xa[0], xa[1], xa[2]}, rB = xc0 - V3{xb[0], xb[1], xb[2]};
+        const V3 tauA = cross(rA, F), tauB = cross(rB, F * -1.0);
+        const double ra[3] = {rA.x, rA.y, rA.z}, rb[3] = {rB.x, rB.y, rB.z};
+        const double ta[3] = {tauA.x, tauA.y, tauA.z}, tb[3] = {tauB.x, tauB.y, tauB.z};
+        std::cout << "  contact_debug: i=" << ij.x << " j=" << ij.y << " xc0=";
+        put(g + 6);
+        std::cout << " n=";
+        put(g + 9);
+        std::cout << " F=";
+        put(f);
+        std::cout << " rA=";
+        put(ra);
+        std::cout << " tauA=";
+        put(ta);
+        std::cout << " rB=";
+        put(rb);
+        std::cout << " tauB=";
+        put(tb);
+        std::cout << "\n";
+    }
+    int64_t running = ncontact;
+    if (ncand > 0 && running < 2) {
+        const size_t nslot = (size_t)ncand * max_wtri;
+        std::vector<int32_t> valid(nslot);
+        std::vector<int2> cand(ncand);
+        cudaError_t e = cudaMemcpyAsync(valid.data(), s.w_valid.p, sizeof(int32_t) * nslot, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(cand.data(), s.w_pairs.p, sizeof(int2) * ncand, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        for (size_t q = 0; q < nslot && running < 2; ++q) {
+            if (!valid[q]) continue;
+            running++;
+            double d[7], f[3];
+            e = cudaMemcpyAsync(d, as<double>(s.w_dbg) + 7 * q, sizeof(d), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(f, as<double>(s.w_contrib) + 6 * q, sizeof(f), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return e;
+            const int2 iw = cand[q / max_wtri];
+            std::cout << "  wall_contact: particle=" << iw.x << " wall=" << iw.y << " tri=" << (q % max_wtri)
+                      << " area=" << d[0] << " xc=";
+            put(d + 1);
+            std::cout << " n=";
+            put(d + 4);
+            std::cout << " F=";
+            put(f);
+            std::cout << "\n";
+        }
+    }
+    return cudaSuccess;
 }
 
 int scene_step(zdx_ctx* ctx, Scene& s) {
@@ -889,7 +1063,11 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
                     as<double>(s.d_wtris), as<double>(s.d_wnorm), as<int64_t>(s.d_wtri_off), as<double>(s.d_wmat),
                     as<int2>(s.w_pairs), ncand, max_wtri, s.cfg.dt, as<int64_t>(s.d_whist_key), as<double>(s.d_whist_ds),
                     s.nwhist, as<double>(s.w_contrib), as<int32_t>(s.w_valid), as<int32_t>(w_act),
-                    as<double>(s.w_ds), as<double>(s.bp_tmp), spts, nwarps, nullptr, nullptr, nullptr};
+                    as<double>(s.w_ds), as<double>(s.bp_tmp), spts, nwarps, nullptr, nullptr, nullptr, nullptr};
+        if (s.cfg.contact_debug) {
+            CKS(s.w_dbg.ensure(sizeof(double) * 7 * C1 * max_wtri));
+            wa.dbg = as<double>(s.w_dbg);
+        }
         k_walls<<<(nwarps + 3) / 4, 128, 0, st>>>(wa);
         ctx->launches += 1;
         CKS(s.pr_scan.ensure(sizeof(int64_t) * (std::max(P1, C1) + 1)));
@@ -905,6 +1083,8 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         stats.wall_contacts = (int64_t)wc;
         ctx->launches += 1;
     }
+
+    if (s.cfg.contact_debug) CKS(print_contact_debug(ctx, s, ncontact, ncand, max_wtri));
 
     // ---- 5+6. scatter, integrate
     const double g3[3] = {s.cfg.gravity[0], s.cfg.gravity[1], s.cfg.gravity[2]};
@@ -966,6 +1146,68 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
     return ZDX_OK;
 }
 
+
+static int ff_threads(int np) { return std::max(32, ((np + 31) / 32) * 32); }  // np <= FF_MAX_NP
+static bool free_flight_ok(const Scene& s) { return s.free_flight && s.np > 0 && s.np <= FF_MAX_NP; }
+
+// Plain-mode free flight: up to max_steps steps through k_free_flight; *done = the steps taken.
+static int scene_free_flight(zdx_ctx* ctx, Scene& s, int max_steps, int* done) {
+    *done = 0;
+    if (!free_flight_ok(s) || max_steps <= 0) return ZDX_OK;
+    if (s.gs.active) {
+        int rc = scene_graph_leave(ctx, s);
+        if (rc) return rc;
+    }
+    cudaStream_t st = ctx->stream;
+    CKS(s.d_ff.ensure(64));
+    double* dg = as<double>(s.d_ff);
+    int64_t* dd = reinterpret_cast<int64_t*>(dg + 4);
+    const double g3[3] = {s.cfg.gravity[0], s.cfg.gravity[1], s.cfg.gravity[2]};
+    CKS(cudaMemcpyAsync(dg, g3, sizeof(g3), cudaMemcpyHostToDevice, st));
+    int64_t total = 0;
+    while (total < max_steps) {
+        const int chunk = (int)std::min<int64_t>(max_steps - total, FF_CHUNK);
+        k_free_flight<<<1, ff_threads(s.np), 0, st>>>(as<double>(s.d_state), as<double>(s.d_mat), s.np,
+                                                      as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+                                                      as<double>(s.d_wtris), as<int64_t>(s.d_wtri_off), dg, s.cfg.dt,
+                                                      chunk, as<double>(s.d_force), as<double>(s.d_torque),
+                                                      as<int32_t>(s.d_count), dd, nullptr);
+        ctx->launches += 1;
+        int64_t k = 0;
+        CKS(cudaMemcpyAsync(&k, dd, sizeof(k), cudaMemcpyDeviceToHost, st));
+        CKS(cudaStreamSynchronize(st));
+        total += k;
+        if (k < chunk) break;
+    }
+    if (total > 0) {
+        s.nhist = 0;
+        s.nwhist = 0;
+        s.last = StepStats{};
+        s.have_forces = true;
+        s.host_dirty = true;
+        s.step += total;
+    }
+    *done = (int)total;
+    return ZDX_OK;
+}
+
+int scene_run(zdx_ctx* ctx, Scene& s, int nsteps) {
+    int k = 0;
+    while (k < nsteps) {
+        // free flight is tried while the last step had no pair and no wall contact
+        if (s.last.pairs == 0 && s.last.wall_contacts == 0) {
+            int done = 0;
+            int rc = scene_free_flight(ctx, s, nsteps - k, &done);
+            if (rc) return rc;
+            k += done;
+            if (k >= nsteps) break;
+        }
+        int rc = scene_step(ctx, s);
+        if (rc) return rc;
+        k++;
+    }
+    return ZDX_OK;
+}
 
 // ================================================================= the step as one CUDA graph
 namespace {
@@ -1269,7 +1511,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
                     as<double>(s.d_wtris), as<double>(s.d_wnorm), as<int64_t>(s.d_wtri_off), as<double>(s.d_wmat),
                     as<int2>(G.w_pairs), G.wcap, G.max_wtri, s.cfg.dt, as<int64_t>(G.whkey), as<double>(G.whds), 0,
                     as<double>(G.w_contrib), as<int32_t>(G.w_valid), as<int32_t>(G.w_act), as<double>(G.w_ds),
-                    as<double>(G.w_scratch), G.spts, G.wall_warps, ncand, &g->nwhist, flags};
+                    as<double>(G.w_scratch), G.spts, G.wall_warps, ncand, &g->nwhist, flags, nullptr};
         k_walls<<<(G.wall_warps + 3) / 4, 128, 0, st>>>(wa);
         k_count_valid<<<grid((int64_t)std::max<int64_t>(G.wcap, 1) * G.max_wtri), 256, 0, st>>>(
             as<int32_t>(G.w_valid), (int64_t)std::max<int64_t>(G.wcap, 1) * G.max_wtri, ncand, G.max_wtri,
@@ -1427,13 +1669,41 @@ int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps) {
         int rc = graph_capture(ctx, s);
         if (rc) return rc;
     }
-    // launch in chunks; after each chunk read the counters and grow + capture again on an overflow
+    // launch in chunks; after each chunk read the counters and grow + capture again on an overflow.
+    // A small scene runs its candidate-free stretches through k_free_flight, and the graph chunks
+    // after one start at a single step and double while every step keeps a candidate.
     int remaining = nsteps, regrow = 0;
+    const bool ff_ok = free_flight_ok(s);
+    bool try_ff = ff_ok;
+    int chunk_cap = ff_ok ? 1 : 64;
     while (remaining > 0) {
+        if (try_ff) {
+            CKS(cudaMemcpyAsync(G.host, G.g.p, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st));
+            CKS(cudaStreamSynchronize(st));
+            const int64_t ff0 = G.host->steps_done;
+            const int chunk = std::min(remaining, FF_CHUNK);
+            k_free_flight<<<1, ff_threads(s.np), 0, st>>>(as<double>(s.d_state), as<double>(s.d_mat), s.np,
+                                                          as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+                                                          as<double>(s.d_wtris), as<int64_t>(s.d_wtri_off),
+                                                          as<double>(G.grav), s.cfg.dt, chunk, as<double>(s.d_force),
+                                                          as<double>(s.d_torque), as<int32_t>(s.d_count), nullptr,
+                                                          as<GraphCounts>(G.g));
+            ctx->launches += 1;
+            CKS(cudaMemcpyAsync(G.host, G.g.p, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st));
+            CKS(cudaStreamSynchronize(st));
+            const int done = (int)(G.host->steps_done - ff0);
+            remaining -= done;
+            s.step += done;
+            // after free flight the contact stretch may be short; a test that found a candidate at once
+            // lets the chunks grow
+            chunk_cap = done > 0 ? 1 : std::min(8, 2 * chunk_cap);
+            if (done == chunk) continue;  // FF_CHUNK steps in free flight: keep going
+            if (remaining == 0) break;
+        }
         CKS(cudaMemcpyAsync(G.host, G.g.p, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st));
         CKS(cudaStreamSynchronize(st));
         const int64_t before = G.host->steps_done;
-        const int chunk = std::min(remaining, 64);
+        const int chunk = std::min(remaining, chunk_cap);
         for (int k = 0; k < chunk; ++k) CKS(cudaGraphLaunch(G.exec, st));
         ctx->launches += (long long)chunk * G.kernels_per_step;
         CKS(cudaMemcpyAsync(G.host, G.g.p, sizeof(GraphCounts), cudaMemcpyDeviceToHost, st));
@@ -1442,7 +1712,13 @@ int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps) {
         const int done = (int)(h.steps_done - before);
         remaining -= done;
         s.step += done;
-        if (h.flags == 0) continue;
+        if (h.flags == 0) {
+            // the last step had no pair and no wall contact: the next ones may be free flight.  A small
+            // scene's chunks stay short, so few full steps run past the end of a contact.
+            try_ff = ff_ok && h.npair == 0 && h.wall_contacts == 0;
+            if (!try_ff) chunk_cap = std::min(ff_ok ? 8 : 64, 2 * chunk_cap);
+            continue;
+        }
         if (++regrow > 32) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "graph step: capacities keep overflowing (flags %d)", h.flags);
         if (h.flags & GRAPH_OVF_PAIRS) G.pcap = h.need_pairs + h.need_pairs / 4 + 1024;
         if (h.flags & GRAPH_OVF_CAND) G.wcap = h.need_cand + h.need_cand / 4 + 1024;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -65,6 +66,11 @@ struct StepStats {
     int64_t pairs = 0, wall_contacts = 0;
     double tri_ms = 0, rebuild_ms = 0, step_ms = 0, output_ms = 0;
 };
+
+// Free-flight steps (k_free_flight): one block, scenes of up to FF_MAX_NP particles.
+constexpr int FF_THREADS = 1024;
+constexpr int FF_MAX_NP = 1024;  // one thread per particle
+constexpr int FF_CHUNK = 1 << 16;  // steps per launch at most
 
 // Device-resident counters of the graph step (one per scene), mirrored to pinned host memory after a
 // batch of steps.
@@ -129,6 +135,8 @@ struct GraphStep {
     }
 };
 
+struct OutputPipeline;  // zdx_output.cpp
+
 struct Scene {
     SimConfig cfg;
     std::vector<ParticleInit> inits;
@@ -166,10 +174,15 @@ struct Scene {
     DevBuf tr_key, tr_idx, tr_key2, tr_idx2, tr_start;
     DevBuf pr_mesh, pr_pose, pr_ncontact, pr_coff, pr_stats, pr_geom, pr_info, pr_contrib, pr_active, pr_ds, pr_scan;
     DevBuf w_contrib, w_valid, w_active, w_ds, w_scan, w_pairs;
+    DevBuf w_dbg;  // contact_debug only: area, contact point, normal per wall slot
+    DevBuf d_ff;   // free flight: gravity (3 doubles), steps done (int64)
+    bool free_flight = true;  // candidate-free steps through k_free_flight (zdx_scene_set_free_flight)
     int64_t pair_cap = 0, contact_cap = 0;
     GraphStep gs;
+    std::shared_ptr<OutputPipeline> out;  // asynchronous outputs, created by the first one
 
     void release_device() {
+        out.reset();  // drains the queued outputs first
         gs.release();
         for (DevBuf* b : {&d_state, &d_mat, &d_pmesh, &d_mtris, &d_moff, &d_mme, &d_mbd, &d_mrad, &d_wtris, &d_wnorm,
                           &d_wtri_off, &d_wpose, &d_wmat, &d_wrad, &d_force, &d_torque, &d_count, &d_hist_key,
@@ -177,7 +190,7 @@ struct Scene {
                           &d_whist_ds2, &bp_cell, &bp_key, &bp_idx, &bp_key2, &bp_idx2, &bp_start, &bp_end, &bp_cnt,
                           &bp_off, &bp_pairs, &bp_hist, &bp_tmp, &tr_key, &tr_idx, &tr_key2, &tr_idx2, &tr_start,
                           &pr_mesh, &pr_pose, &pr_ncontact, &pr_coff, &pr_stats, &pr_geom, &pr_info, &pr_contrib,
-                          &pr_active, &pr_ds, &pr_scan, &w_contrib, &w_valid, &w_active, &w_ds, &w_scan, &w_pairs})
+                          &pr_active, &pr_ds, &pr_scan, &w_contrib, &w_valid, &w_active, &w_ds, &w_scan, &w_pairs, &w_dbg, &d_ff})
             b->release();
     }
 };
@@ -185,14 +198,33 @@ struct Scene {
 int scene_from_config(zdx_ctx* ctx, const SimConfig& cfg, Scene& s, std::string& err);
 int scene_upload(zdx_ctx* ctx, Scene& s);
 int scene_step(zdx_ctx* ctx, Scene& s);
+// nsteps plain steps; runs of steps without any broad-phase or wall candidate go through k_free_flight.
+int scene_run(zdx_ctx* ctx, Scene& s, int nsteps);
 // nsteps steps through the captured graph; statistics of the last step land in s.last (no timings).
 int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps);
 // Moves the tangential history from the graph step's buffers back to the Scene's (before a plain step
 // or a state download that needs it).
 int scene_graph_leave(zdx_ctx* ctx, Scene& s);
 int scene_download(zdx_ctx* ctx, Scene& s);
-// write_vtk_particles / write_particle_state_txt, src/main.cpp:1710-1870
-bool write_vtk_particles(const std::string& path, const Scene& s);
-bool write_state_txt(const std::string& path, const Scene& s);
+// One output frame: per-particle state (np x 16), force and torque (np x 3), contact count (np).
+struct ParticleFrame {
+    int np;
+    const double* state;
+    const double* force;
+    const double* torque;
+    const int32_t* count;
+};
+ParticleFrame host_frame(const Scene& s);  // the Scene's host copies
+int output_threads();                      // formatting threads for one file
+// write_vtk_particles / write_particle_state_txt, src/main.cpp:1710-1870; the meshes, materials and
+// particle inits come from the Scene, the moving parts from the frame.
+bool write_vtk_particles(const std::string& path, const Scene& s, const ParticleFrame& fr, int threads);
+bool write_state_txt(const std::string& path, const Scene& s, const ParticleFrame& fr, int threads);
+// <output_dir>/<vtk_prefix>_<step, 6 digits><ext> (src/main.cpp:2471-2473)
+std::string output_name(const Scene& s, int64_t step, const char* ext);
+// Queues the output of `step` (zdx_output.cpp): a device snapshot now, the files on a writer thread.
+int output_submit(zdx_ctx* ctx, Scene& s, int64_t step);
+// Waits for the queued outputs; ZDX_ERR_IO if any could not be written.
+int output_wait(zdx_ctx* ctx, Scene& s);
 
 }  // namespace zdx

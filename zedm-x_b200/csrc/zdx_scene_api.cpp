@@ -51,11 +51,7 @@ extern "C" int zdx_scene_step(zdx_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0) return ZDX_ERR_INVALID;
     if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "cudaSetDevice failed");
-    for (int k = 0; k < nsteps; ++k) {
-        int rc = scene_step(ctx, *ctx->scene);
-        if (rc) return rc;
-    }
-    return ZDX_OK;
+    return scene_run(ctx, *ctx->scene, nsteps);
 }
 
 extern "C" int zdx_scene_step_graph(zdx_ctx* ctx, int nsteps) {
@@ -142,16 +138,13 @@ extern "C" int zdx_scene_set_state(zdx_ctx* ctx, const double* state16) {
     if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
     Scene& s = *ctx->scene;
     std::memcpy(s.state.data(), state16, sizeof(double) * s.state.size());
-    if (cudaMemcpy(s.d_state.p, s.state.data(), sizeof(double) * s.state.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    // on the context's stream, behind any step or output snapshot still queued there
+    if (cudaMemcpyAsync(s.d_state.p, s.state.data(), sizeof(double) * s.state.size(), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return ctx_fail(ctx, ZDX_ERR_CUDA, "state upload failed");
     s.host_dirty = false;
     return ZDX_OK;
-}
-
-static std::string out_name(const Scene& s, int64_t step, const char* ext) {
-    std::ostringstream oss;
-    oss << s.cfg.vtk_prefix << "_" << std::setw(6) << std::setfill('0') << step << ext;
-    return (std::filesystem::path(s.cfg.output_dir) / oss.str()).string();
 }
 
 extern "C" int zdx_scene_write_output(zdx_ctx* ctx, int64_t step) {
@@ -164,9 +157,31 @@ extern "C" int zdx_scene_write_output(zdx_ctx* ctx, int64_t step) {
     }
     std::error_code ec;
     std::filesystem::create_directories(s.cfg.output_dir, ec);
-    bool ok = write_vtk_particles(out_name(s, step, ".vtk"), s);
-    ok = write_state_txt(out_name(s, step, ".txt"), s) && ok;
+    const ParticleFrame fr = host_frame(s);
+    const int t = output_threads();
+    bool ok = write_vtk_particles(output_name(s, step, ".vtk"), s, fr, t);
+    ok = write_state_txt(output_name(s, step, ".txt"), s, fr, t) && ok;
     return ok ? ZDX_OK : ctx_fail(ctx, ZDX_ERR_IO, "could not write outputs to %s", s.cfg.output_dir.c_str());
+}
+
+extern "C" int zdx_scene_set_free_flight(zdx_ctx* ctx, int enable) {
+    if (!ctx) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    ctx->scene->free_flight = enable != 0;
+    return ZDX_OK;
+}
+
+extern "C" int zdx_scene_write_output_async(zdx_ctx* ctx, int64_t step) {
+    if (!ctx) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "cudaSetDevice failed");
+    return output_submit(ctx, *ctx->scene, step);
+}
+
+extern "C" int zdx_scene_output_wait(zdx_ctx* ctx) {
+    if (!ctx) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ZDX_OK;
+    return output_wait(ctx, *ctx->scene);
 }
 
 // The body of zdem_cpu's main after argument parsing (src/main.cpp:1879-2503): load, then per step the
@@ -191,17 +206,17 @@ static int run_config(const char* config_path, int device, bool graph) {
     std::filesystem::create_directories(s.cfg.output_dir, ec);
     for (int step = 0; step < s.cfg.steps; ++step) {
         auto t0 = std::chrono::steady_clock::now();
-        int batch = 1;
-        if (graph) {
-            // up to and including the next output step, in one graph batch
-            const int every = std::max(s.cfg.output_interval, 1);
-            const int next = std::min(((step + every - 1) / every) * every, s.cfg.steps - 1);
-            batch = next - step + 1;
-            rc = scene_step_graph(ctx, s, batch);
-            step = next;
+        // up to and including the next output step, in one batch (the log line and the outputs are those
+        // of that step)
+        const int every = std::max(s.cfg.output_interval, 1);
+        const int next = std::min(((step + every - 1) / every) * every, s.cfg.steps - 1);
+        const int batch = next - step + 1;
+        if (graph && !s.cfg.contact_debug) {
+            rc = scene_step_graph(ctx, s, batch);  // contact_debug prints per step: it keeps the plain step
         } else {
-            rc = scene_step(ctx, s);
+            rc = scene_run(ctx, s, batch);
         }
+        step = next;
         if (rc) {
             std::cerr << "zdem_gpu: step " << step << ": " << zdx_last_error(ctx) << "\n";
             zdx_destroy(ctx);
@@ -209,7 +224,12 @@ static int run_config(const char* config_path, int device, bool graph) {
         }
         if (step % s.cfg.output_interval == 0) {
             auto to = std::chrono::steady_clock::now();
-            zdx_scene_write_output(ctx, step);
+            rc = output_submit(ctx, s, step);  // the files are written while the next steps run
+            if (rc) {
+                std::cerr << "zdem_gpu: output " << step << ": " << zdx_last_error(ctx) << "\n";
+                zdx_destroy(ctx);
+                return 1;
+            }
             double out_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - to).count();
             double step_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / batch;
             std::cout << "step=" << step << " contacts=" << s.last.contacts << " step_ms=" << (long long)step_ms
@@ -219,6 +239,7 @@ static int run_config(const char* config_path, int device, bool graph) {
                       << "\n";
         }
     }
+    output_wait(ctx, s);  // a file that could not be written was reported, and the run goes on, as in the reference
     std::cout << "done\n";
     zdx_destroy(ctx);
     return 0;

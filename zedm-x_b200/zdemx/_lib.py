@@ -93,6 +93,9 @@ def lib() -> C.CDLL:
     L.zdx_scene_get_state.argtypes = [C.c_void_p, _dp, _dp, _dp, _i32p]
     L.zdx_scene_set_state.argtypes = [C.c_void_p, _dp]
     L.zdx_scene_write_output.argtypes = [C.c_void_p, C.c_int64]
+    L.zdx_scene_write_output_async.argtypes = [C.c_void_p, C.c_int64]
+    L.zdx_scene_output_wait.argtypes = [C.c_void_p]
+    L.zdx_scene_set_free_flight.argtypes = [C.c_void_p, C.c_int]
     L.zdx_run_config.argtypes = [C.c_char_p, C.c_int]
     L.zdx_run_config_graph.argtypes = [C.c_char_p, C.c_int]
     L.zdx_scene_step_graph.argtypes = [C.c_void_p, C.c_int]

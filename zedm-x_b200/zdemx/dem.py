@@ -73,8 +73,20 @@ class Scene:
         st = np.ascontiguousarray(st, dtype=np.float64)
         _lib.check(_lib.lib().zdx_scene_set_state(self.ctx.handle, st.ctypes.data_as(_lib._dp)), self.ctx.handle)
 
-    def write_output(self, step: int):
-        _lib.check(_lib.lib().zdx_scene_write_output(self.ctx.handle, int(step)), self.ctx.handle)
+    def write_output(self, step: int, wait: bool = True):
+        """The particle VTK and state txt files of `step`.  wait=False snapshots the particles on the device
+        and writes the files on a background thread while stepping goes on; output_wait() joins them."""
+        if wait:
+            _lib.check(_lib.lib().zdx_scene_write_output(self.ctx.handle, int(step)), self.ctx.handle)
+        else:
+            _lib.check(_lib.lib().zdx_scene_write_output_async(self.ctx.handle, int(step)), self.ctx.handle)
+
+    def set_free_flight(self, enable: bool):
+        """Candidate-free steps of a small scene through the single-block kernel (default on)."""
+        _lib.check(_lib.lib().zdx_scene_set_free_flight(self.ctx.handle, int(bool(enable))), self.ctx.handle)
+
+    def output_wait(self):
+        _lib.check(_lib.lib().zdx_scene_output_wait(self.ctx.handle), self.ctx.handle)
 
 
 def run_config(config_path: str, device: int = 0, graph: bool = False) -> int:
