@@ -161,3 +161,35 @@ def test_polyline_mode_matches_oracle_and_python_reference(ctx, oracle):
         for c, cc in enumerate(man["contacts"]):
             got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"], cc["Fn"], cc["F_A"]]
             assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)
+
+
+@pytest.mark.parametrize("split,mode", [(True, 0), (False, 0), (False, 1)])
+def test_large_pairs(ctx, oracle, split, mode):
+    """Pairs of 1,280- and 5,120-triangle meshes (160 to 560 segments and up to 17 contacts a pair: long
+    component searches, large snap classes, many T-junction candidates) against the oracle, bit for bit;
+    polyline mode (mode 1) too."""
+    from zdemx import contact, synth
+
+    rng = np.random.default_rng(77 + 2 * split + mode)
+    meshes = [synth.noised_icosphere(s, 1e-3, 0.15, rng) for s in (3, 4, 4)]
+    lib = _library(meshes)
+    npairs = 12
+    pm = np.array([[1 + (p % 2), 1 + ((p // 2) % 2)] if p % 3 else [0, 2] for p in range(npairs)], np.int32)
+    pp = synth.pair_poses(rng, npairs, 1e-3, 0.02, 0.12)
+    if mode == 1:
+        tol = 2e-5
+        res = contact.pair_contacts_batch(ctx, lib, pm, pp, want_points=True, split=split, k=1e7, mode=1, tol=tol)
+    else:
+        tol = 0.0
+        res = _run(ctx, lib, pm, pp, split=split, k=1e7)
+    big = 0
+    for p in range(npairs):
+        a, b = pm[p]
+        r = oracle.pair(lib.mesh(a), lib.mean_edge[a], lib.bbox_diag[a], lib.mesh(b), pp[p, :7], pp[p, 7:],
+                        split=split, mode=mode, tol=tol)
+        e = expected_contacts(r, polyline=mode == 1)
+        bad = compare_gpu_to_expected(gpu_pair_slice(res, p), e, r)
+        assert bad == [], f"pair {p}: {bad}"
+        assert res["stats"][p, 0] == r["nseg"]
+        big += r["nseg"] > 200
+    assert big >= 4
