@@ -152,6 +152,33 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def profiled_issue():
+    """Warp instructions per pair of the two pair kernels (profiles/issue.json, from one ncu capture)."""
+    p = os.path.join(ROOT, "profiles", "issue.json")
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return None
+
+
+def issue_roofline(reb_s, seg_s, pairs, clocks):
+    """Issue-rate roofline of the two pair kernels: profiled warp instructions per pair x pairs over the
+    live kernel time, against 4 warp instructions per cycle per SM at the median SM clock of the run."""
+    iss = profiled_issue()
+    if not iss:
+        return None
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+    peak = 4.0 * sms * mhz * 1e6
+    out = {"unit": "warp-inst/s", "peak": peak, "peak_kind": f"4 per cycle per SM x {sms} SMs x {mhz:.0f} MHz"}
+    for name, t in (("k_rebuild", reb_s), ("k_segments", seg_s)):
+        inst = float(iss[name]["warp_inst_per_pair"]) * pairs
+        out[name] = {"bound": "issue", "achieved": inst / t, "frac": inst / t / peak, "warp_inst_per_launch": inst}
+    return out
+
+
 def profiled_traffic():
     """DRAM bytes per pair of the pair kernels from the committed ncu summaries, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
@@ -396,6 +423,7 @@ def main():
                                   "frac": achieved / peak, "traffic": traffic, "kernel": "k_segments",
                                   "algorithmic_bytes_per_launch": abytes, "kernel_ms": 1e3 * seg_s,
                                   "note": "FP64 compare/ALU issue and scratch latency bound; see profiles/"},
+          "roofline_issue": issue_roofline(reb_s, seg_s, args.pairs, clk.summary()),
           "stages_ms": {"triangle_tests": statistics.mean(seg_ms), "rebuild": statistics.mean(reb_ms),
                         "whole_call": statistics.mean(step_ms)},
           "plain": {"value": plain_value, "unit": UNIT, "pairs": plain_n, "batched_same_pairs": plain_n / (batched_sub_ms / 1e3),
