@@ -95,8 +95,10 @@ def test_stl_loader_matches_reference(tmp_path, ref):
         a = ref.load_stl(p)
         b = _lib.stl_load(p)
         assert a.shape == b.shape and np.array_equal(a, b)
-    ref_geo = "/root/reference/geometry"
-    if os.path.isdir(ref_geo):
+    # the reference's own fixture STLs, where the tree the oracle was built from is present
+    root_file = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "REF_ROOT")
+    ref_geo = os.path.join(open(root_file).read().strip(), "geometry") if os.path.exists(root_file) else ""
+    if ref_geo and os.path.isdir(ref_geo):
         for f in sorted(os.listdir(ref_geo)):
             if f.endswith(".stl"):
                 a = ref.load_stl(os.path.join(ref_geo, f))
