@@ -10,14 +10,19 @@ import pytest
 def _worker(rank, world, port, q):
     import torch.distributed as dist
 
-    from zdemx.replicas import gather_counts, max_over_ranks, rank_seed
+    import torch
+
+    from zdemx.replicas import gather_counts, gather_rows, max_over_ranks, rank_seed
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         t = max_over_ranks(1.5 + rank)
         counts = gather_counts(10 * (rank + 1))
-        q.put((rank, t, counts, rank_seed(7, rank)))
+        # row blocks of different lengths
+        rows = torch.arange(3 * (2 - rank) * 4, dtype=torch.float64).reshape(-1, 4) + 100 * rank
+        got = [g.tolist() for g in gather_rows(rows)]
+        q.put((rank, t, counts, rank_seed(7, rank), got))
     finally:
         dist.destroy_process_group()
 
@@ -42,6 +47,8 @@ def test_two_gloo_ranks():
     assert [r[1] for r in res] == [2.5, 2.5]
     assert all(r[2] == [10, 20] for r in res)
     assert res[0][3] != res[1][3]
+    want = [np.arange(24.0).reshape(6, 4).tolist(), (np.arange(12.0).reshape(3, 4) + 100).tolist()]
+    assert all(r[4] == want for r in res)
 
 
 @pytest.mark.parametrize("world", [1, 2, 3, 8])
@@ -57,4 +64,20 @@ def test_cost_balanced_ranges(world):
     assert len(ranges) == world and ranges[0][0] == 0 and ranges[-1][1] == len(pm)
     assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
     loads = [costs[order][a:b].sum() for a, b in ranges]
+    assert max(loads) - min(loads) <= 2 * costs.max() + 1
+
+
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_strong_shards_cover_every_pair_once(world):
+    from zdemx.replicas import pair_costs, strong_shards
+
+    rng = np.random.default_rng(10 + world)
+    tri_off = np.r_[0, np.cumsum(20 * 4 ** rng.integers(1, 5, size=64))]
+    pm = rng.integers(0, 64, size=(3000, 2))
+    shards = strong_shards(tri_off, pm, world)
+    assert len(shards) == world
+    allp = np.sort(np.concatenate(shards))
+    assert np.array_equal(allp, np.arange(len(pm)))
+    costs = pair_costs(tri_off, pm)
+    loads = [costs[s].sum() for s in shards]
     assert max(loads) - min(loads) <= 2 * costs.max() + 1

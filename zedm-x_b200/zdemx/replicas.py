@@ -64,3 +64,28 @@ def gather_counts(count: int, device=None) -> list[int]:
     out = [torch.zeros_like(t) for _ in range(dist.get_world_size())]
     dist.all_gather(out, t)
     return [int(x.item()) for x in out]
+
+
+def strong_shards(tri_off, pair_mesh, world: int) -> list[np.ndarray]:
+    """Pair indices of each rank for one batch spread over `world` ranks: the pairs in the work queue's
+    cost order (nA * nB, descending, ties by index), cut into contiguous ranges of equal cost."""
+    costs = pair_costs(tri_off, pair_mesh)
+    order = np.argsort(-costs, kind="stable")
+    return [order[a:b] for a, b in cost_balanced_ranges(costs[order], world)]
+
+
+def gather_rows(t, device=None) -> list:
+    """Every rank's row block (a tensor of any length along dim 0, same trailing shape and dtype), on
+    every rank: one gather of the lengths, then one of the blocks padded to the longest."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return [t]
+    n = gather_counts(int(t.shape[0]), device)
+    m = max(max(n), 1)
+    pad = torch.zeros((m,) + tuple(t.shape[1:]), dtype=t.dtype, device=t.device)
+    pad[: t.shape[0]] = t
+    out = [torch.empty_like(pad) for _ in n]
+    dist.all_gather(out, pad)
+    return [o[:k] for o, k in zip(out, n)]
