@@ -202,7 +202,37 @@ __global__ void __launch_bounds__(ST) k_scan_apply(const T* cnt, int64_t ncap, c
         run += (int64_t)c[k];
     }
 }
+
+// the whole scan in one block when it fits one tile (small scenes: one launch instead of three)
+template <class T>
+__global__ void __launch_bounds__(ST) k_scan_one(const T* cnt, int64_t ncap, const int64_t* n_dev, int64_t* off) {
+    __shared__ int64_t ws[32];
+    const int64_t n = count_of(ncap, n_dev);
+    const int64_t base = (int64_t)threadIdx.x * SI;
+    T c[SI];
+    int64_t v = 0;
+    for (int k = 0; k < SI; ++k) {
+        c[k] = base + k < n ? cnt[base + k] : T(0);
+        v += (int64_t)c[k];
+    }
+    int64_t total;
+    int64_t run = block_excl_scan<T>(v, ws, total);
+    for (int k = 0; k < SI; ++k) {
+        if (base + k < n) off[base + k] = run;
+        run += (int64_t)c[k];
+    }
+    if (threadIdx.x == 0) off[n] = total;
+}
 }  // namespace
+
+int scan_kernels(int64_t ncap) { return ncap <= STILE ? 1 : 3; }
+
+int radix_kernels(int64_t n, int key_bits) {
+    if (n <= 0) return 0;
+    const int64_t nb = (n + TILE - 1) / TILE;
+    const int passes = std::max(1, (key_bits + 7) / 8);
+    return passes * (2 + scan_kernels(256 * nb));
+}
 
 size_t scan_scratch_bytes(int64_t ncap) {
     const int64_t nb = (ncap + STILE - 1) / STILE;
@@ -212,6 +242,10 @@ size_t scan_scratch_bytes(int64_t ncap) {
 template <class T>
 cudaError_t scan_offsets(const T* cnt, int64_t ncap, const int64_t* n_dev, int64_t* off, void* scratch, cudaStream_t s) {
     const int nb = (int)std::max<int64_t>(1, (ncap + STILE - 1) / STILE);
+    if (nb == 1) {
+        k_scan_one<T><<<1, ST, 0, s>>>(cnt, ncap, n_dev, off);
+        return cudaGetLastError();
+    }
     int64_t* ts = static_cast<int64_t*>(scratch);
     k_scan_tiles<T><<<nb, ST, 0, s>>>(cnt, ncap, n_dev, ts);
     k_scan_tile_sums<<<1, 1024, 0, s>>>(ts, nb, n_dev, ncap, off);

@@ -25,6 +25,9 @@ cudaError_t radix_sort_u32(uint32_t* keys, int32_t* vals, uint32_t* kt, int32_t*
 // Exclusive scan of counts into offsets, any size: off[0..n) and off[n] = total, n = ncap or, with
 // n_dev, min(*n_dev, ncap) read on the device.  scratch: scan_scratch_bytes(ncap).
 size_t scan_scratch_bytes(int64_t ncap);
+// kernels one scan_offsets / radix_sort_u32 call launches (for the launch counters)
+int scan_kernels(int64_t ncap);
+int radix_kernels(int64_t n, int key_bits);
 template <class T>
 cudaError_t scan_offsets(const T* cnt, int64_t ncap, const int64_t* n_dev, int64_t* off, void* scratch, cudaStream_t s);
 

@@ -928,7 +928,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
                                                     as<int>(s.bp_start), as<int>(s.bp_end), T - 1, as<int32_t>(s.bp_cnt),
                                                     nullptr, nullptr, INT64_MAX);
         CKS(scan_counts_i32(as<int32_t>(s.bp_cnt), np, as<int64_t>(s.bp_off), st));
-        ctx->launches += 5 + 5 * ((bits + 7) / 8);  // a radix pass: histogram, 3 scan kernels, scatter
+        ctx->launches += 5 + radix_kernels(np, bits);  // a radix pass: histogram, 1 or 3 scan kernels, scatter
     }
     int64_t npair = 0;
     if (np > 0) {
@@ -970,7 +970,7 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
         CKS(s.bp_tmp.ensure(radix_scratch_bytes(npair)));
         CKS(radix_sort_u32(as<uint32_t>(s.tr_key), as<int32_t>(s.tr_idx), as<uint32_t>(s.tr_key2),
                            as<int32_t>(s.tr_idx2), npair, std::max(pbits, 1), s.bp_tmp.p, st));
-        ctx->launches += 1 + 5 * ((std::max(pbits, 1) + 7) / 8);
+        ctx->launches += 1 + radix_kernels(npair, std::max(pbits, 1));
         if (s.contact_cap < 4 * npair + 64) s.contact_cap = 4 * npair + 64;
         for (int attempt = 0; attempt < 2; ++attempt) {
             CKS(s.pr_geom.ensure(sizeof(double) * 20 * (size_t)s.contact_cap));
