@@ -681,6 +681,99 @@ __global__ void __launch_bounds__(FF_THREADS) k_free_flight(double* state, const
     if (done_out && i == 0) *done_out = k;
 }
 
+// Candidates of a scene of up to FF_MAX_NP particles in one block, thread i = particle i: the pairs
+// (i, j > i) of k_bp_pairs and the (particle, wall) candidates of k_wall_cand, with the same tests, in the
+// same order (i, then j or w ascending), and their offsets (np + 1 each).  A list over its capacity is
+// not written; its total is, and the caller grows.  (One launch in place of the cell binning, its radix
+// sort, the two pair passes, the wall passes and their scans.)
+__device__ __forceinline__ int64_t block_excl_scan_small(int v, int64_t* ws, int64_t& total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int64_t x = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const int64_t y = __shfl_up_sync(FULLM, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t t = lane < nw ? ws[lane] : 0;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int64_t y = __shfl_up_sync(FULLM, t, d);
+            if (lane >= d) t += y;
+        }
+        ws[lane] = t;
+    }
+    __syncthreads();
+    const int64_t incl = x + (w > 0 ? ws[w - 1] : 0);
+    total = ws[nw - 1];
+    __syncthreads();
+    return incl - v;
+}
+
+__global__ void __launch_bounds__(FF_THREADS) k_cand_small(const double* state, const double* mat, int np,
+                                                           const double* wpose, const double* wrad, int nw,
+                                                           int64_t* poff, int2* pairs, int64_t pcap, int64_t* woff,
+                                                           int2* wcand, int64_t wcap) {
+    __shared__ int64_t ws[32];
+    const int i = threadIdx.x;
+    const bool own = i < np;
+    V3 pi{0.0, 0.0, 0.0};
+    double ri = 0.0;
+    int npi = 0, nwi = 0;
+    if (own) {
+        const double* si = state + 16 * (int64_t)i;
+        pi = V3{si[0], si[1], si[2]};
+        ri = mat[17 * (int64_t)i + 2];
+        for (int j = i + 1; j < np; ++j) {
+            const double* sj = state + 16 * (int64_t)j;
+            V3 d = V3{sj[0], sj[1], sj[2]} - pi;
+            double dist2 = dot(d, d);
+            double rsum = ri + mat[17 * (int64_t)j + 2];
+            if (dist2 > rsum * rsum) continue;
+            npi++;
+        }
+        for (int w = 0; w < nw; ++w) {
+            V3 d = pi - L3(wpose + 7 * w);
+            double dist2 = dot(d, d);
+            double rsum = ri + wrad[w];
+            if (dist2 > rsum * rsum) continue;
+            nwi++;
+        }
+    }
+    int64_t ptot, wtot;
+    const int64_t po = block_excl_scan_small(npi, ws, ptot);
+    const int64_t wo = block_excl_scan_small(nwi, ws, wtot);
+    if (own) {
+        poff[i] = po;
+        if (woff) woff[i] = wo;
+    }
+    if (i == 0) {
+        poff[np] = ptot;
+        if (woff) woff[np] = wtot;
+    }
+    if (own && ptot <= pcap) {
+        int64_t o = po;
+        for (int j = i + 1; j < np; ++j) {
+            const double* sj = state + 16 * (int64_t)j;
+            V3 d = V3{sj[0], sj[1], sj[2]} - pi;
+            double dist2 = dot(d, d);
+            double rsum = ri + mat[17 * (int64_t)j + 2];
+            if (dist2 > rsum * rsum) continue;
+            pairs[o++] = make_int2(i, j);
+        }
+    }
+    if (own && woff && wtot <= wcap) {
+        int64_t o = wo;
+        for (int w = 0; w < nw; ++w) {
+            V3 d = pi - L3(wpose + 7 * w);
+            double dist2 = dot(d, d);
+            double rsum = ri + wrad[w];
+            if (dist2 > rsum * rsum) continue;
+            wcand[o++] = make_int2(i, w);
+        }
+    }
+}
+
 __global__ void k_range_bounds(const int2* pairs, int64_t npair, const int64_t* n_dev, int np, int64_t* pstart) {
     // pstart[i] = first pair with first index >= i (pairs sorted by i)
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1385,21 +1478,28 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
     int* flags = &g->flags;
     k_g_begin<<<1, 1, 0, st>>>(g);
 
-    // ---- 1. broad phase
-    k_bp_cells<<<grid(np), 256, 0, st>>>(state, np, 1.0 / G.h, G.T - 1, as<int4>(G.bp_cell), as<uint32_t>(G.bp_key),
-                                         as<int32_t>(G.bp_idx));
-    CKS(radix_sort_u32(as<uint32_t>(G.bp_key), as<int32_t>(G.bp_idx), as<uint32_t>(G.bp_key2), as<int32_t>(G.bp_idx2), np,
-                       G.bits, G.rs_tmp.p, st));
-    CKS(cudaMemsetAsync(G.bp_start.p, 0, sizeof(int) * G.T, st));
-    CKS(cudaMemsetAsync(G.bp_end.p, 0, sizeof(int) * G.T, st));
-    k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(G.bp_key), np, as<int>(G.bp_start), as<int>(G.bp_end));
-    k_bp_pairs<false><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
-                                                as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1, as<int32_t>(G.bp_cnt),
-                                                nullptr, nullptr, INT64_MAX);
-    CKS(scan_offsets<int32_t>(as<int32_t>(G.bp_cnt), np, nullptr, as<int64_t>(G.bp_off), G.scan_tmp.p, st));
-    k_bp_pairs<true><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
-                                               as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1, nullptr,
-                                               as<int64_t>(G.bp_off), as<int2>(G.bp_pairs), G.pcap);
+    // ---- 1. broad phase (a small scene: with the wall candidates, in one block)
+    const bool small = np <= FF_MAX_NP;
+    if (small) {
+        k_cand_small<<<1, ff_threads(np), 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+                                                   as<int64_t>(G.bp_off), as<int2>(G.bp_pairs), G.pcap,
+                                                   s.nw > 0 ? as<int64_t>(G.w_scan) : nullptr, as<int2>(G.w_pairs), G.wcap);
+    } else {
+        k_bp_cells<<<grid(np), 256, 0, st>>>(state, np, 1.0 / G.h, G.T - 1, as<int4>(G.bp_cell), as<uint32_t>(G.bp_key),
+                                             as<int32_t>(G.bp_idx));
+        CKS(radix_sort_u32(as<uint32_t>(G.bp_key), as<int32_t>(G.bp_idx), as<uint32_t>(G.bp_key2),
+                           as<int32_t>(G.bp_idx2), np, G.bits, G.rs_tmp.p, st));
+        CKS(cudaMemsetAsync(G.bp_start.p, 0, sizeof(int) * G.T, st));
+        CKS(cudaMemsetAsync(G.bp_end.p, 0, sizeof(int) * G.T, st));
+        k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(G.bp_key), np, as<int>(G.bp_start), as<int>(G.bp_end));
+        k_bp_pairs<false><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
+                                                    as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1,
+                                                    as<int32_t>(G.bp_cnt), nullptr, nullptr, INT64_MAX);
+        CKS(scan_offsets<int32_t>(as<int32_t>(G.bp_cnt), np, nullptr, as<int64_t>(G.bp_off), G.scan_tmp.p, st));
+        k_bp_pairs<true><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(G.bp_cell), as<int32_t>(G.bp_idx),
+                                                   as<int>(G.bp_start), as<int>(G.bp_end), G.T - 1, nullptr,
+                                                   as<int64_t>(G.bp_off), as<int2>(G.bp_pairs), G.pcap);
+    }
     k_g_take<<<1, 1, 0, st>>>(as<int64_t>(G.bp_off) + np, G.pcap, &g->npair, &g->need_pairs, flags, GRAPH_OVF_PAIRS);
     const int64_t* npair = &g->npair;
 
@@ -1500,11 +1600,13 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
     // ---- 4. walls
     const int64_t* ncand = &g->ncand;
     if (s.nw > 0) {
-        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
-                                              as<int32_t>(G.w_active), nullptr, nullptr, INT64_MAX);
-        CKS(scan_offsets<int32_t>(as<int32_t>(G.w_active), np, nullptr, as<int64_t>(G.w_scan), G.scan_tmp.p, st));
-        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw, nullptr,
-                                              as<int64_t>(G.w_scan), as<int2>(G.w_pairs), G.wcap);
+        if (!small) {
+            k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+                                                  as<int32_t>(G.w_active), nullptr, nullptr, INT64_MAX);
+            CKS(scan_offsets<int32_t>(as<int32_t>(G.w_active), np, nullptr, as<int64_t>(G.w_scan), G.scan_tmp.p, st));
+            k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+                                                  nullptr, as<int64_t>(G.w_scan), as<int2>(G.w_pairs), G.wcap);
+        }
         k_g_take<<<1, 1, 0, st>>>(as<int64_t>(G.w_scan) + np, G.wcap, &g->ncand, &g->need_cand, flags, GRAPH_OVF_CAND);
         CKS(cudaMemsetAsync(G.w_valid.p, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(G.wcap, 1) * G.max_wtri, st));
         WallArgs wa{state, mat, as<int32_t>(s.d_pmesh), as<double>(s.d_mtris), as<int64_t>(s.d_moff), as<double>(s.d_mrad),
