@@ -965,6 +965,29 @@ def run_adjoint(args):
             adj.append(e0.elapsed_time(e1))
     launches = ctx.timings()["launches"] - launches0
     step_s = (sum(fwd) + sum(adj)) / 1e3 / args.steps
+    # the plain form (one launch per pair per stage) against the batched one on the same subset of pairs
+    ns = min(args.plain_pairs, npairs)
+    sub_p = {"mesh": pairs["mesh"][:ns].contiguous(), "pose": pairs["pose"][:ns].contiguous()}
+    sub_o = {kk: (v[:ns].contiguous() if kk in ("ncontact", "stats") else v) for kk, v in out.items()}
+    sub_o["contact_off"] = out["contact_off"][: ns + 1].contiguous()
+    forms = {}
+    for name, sched in (("batched", _lib.SCHED_BATCHED), ("plain", _lib.SCHED_PLAIN)):
+        tt = []
+        for rep in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tsub = _lib.pair_contacts_device(ctx, meshes, sub_p, sub_o, k=1e7, sched=sched)
+            gsub = torch.zeros(int(tsub[0]), 6, dtype=torch.float64, device=dev)
+            gsub[:] = gc[: int(tsub[0])] if int(tsub[0]) <= gc.shape[0] else 0.0
+            gps = torch.zeros(ns, 12, dtype=torch.float64, device=dev)
+            _lib.pair_contacts_adjoint(ctx, meshes, sub_p, gsub, gt, gps, sched=sched)
+            torch.cuda.synchronize()
+            tt.append(time.perf_counter() - t0)
+        forms[name] = (min(tt[1:]), gps.clone())
+    plain_form = {"pairs": ns, "batched_pairs_per_s": ns / forms["batched"][0], "plain_pairs_per_s": ns / forms["plain"][0],
+                  "speedup_batched_vs_plain": forms["plain"][0] / forms["batched"][0],
+                  "grad_pose_max_abs_diff": float((forms["plain"][1] - forms["batched"][1]).abs().max()),
+                  "note": "forward with tape + reverse, wall clock around each call (host syncs included)"}
     # batched central differences of the per-pair objective w.r.t. the 12 pose coordinates
     gpose = gp.cpu().numpy()
     base = _lib.pair_contacts_raw(ctx, lib.tris, lib.tri_off, lib.mean_edge, lib.bbox_diag, pm, pp)
@@ -1036,6 +1059,7 @@ def run_adjoint(args):
           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded noised icospheres)",
           "config": {"workload": desc, "contacts": nc, "l2": "flushed (256 MB write) before the forward and the adjoint"},
           "stages_ms": {"forward": statistics.mean(fwd), "adjoint_call (forward with tape + reverse)": statistics.mean(adj)},
+          "plain": plain_form,
           "gpu_launches": int(launches),
           "fd_check": {"pairs_in_contact": int(incontact.sum()), "pairs_checked": int(ok.sum()),
                        "pairs_flagged_topology_change": int(np.sum(flagged & incontact)),

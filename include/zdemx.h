@@ -124,8 +124,8 @@ int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_se
  * dL/dposB(3), dL/drotB(3), rotations as a world-frame rotation vector applied on top of the current
  * orientation).  Everything after Sn and Gn (|Sn|, n, xc0, force laws) is closed-form and is
  * differentiated by the caller (zdemx.autograd does it in torch).  The forward call is re-run with the
- * adjoint tape on.  Topology changes are not differentiable: gradients are those of the current
- * topology. */
+ * adjoint tape on, in opts->sched (ZDX_SCHED_PLAIN: one launch per pair per stage, the baseline form).
+ * Topology changes are not differentiable: gradients are those of the current topology. */
 int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* meshes,
                               const zdx_pair_batch* pairs, const double* grad_contact, int64_t n_contacts,
                               double* grad_tris, double* grad_pose);

@@ -5,7 +5,8 @@
   sampled mesh-local triangle corners: relative error <= 1e-6 of the gradient group's scale.  A
   coordinate whose +h or -h evaluation changes the topology (segment, component, loop or contact counts,
   loop vertex counts) is skipped, since the function is only piecewise smooth there.
-* Host-memory and device-memory adjoint calls agree to rounding (the scatter is atomic).
+* Host-memory and device-memory adjoint calls, and the batched and plain forms, agree to rounding (the
+  scatter is atomic).
 * The physical identity d(overlap volume)/d(translation of B) = -Sn for convex bodies: the overlap volume
   of two convex hulls comes from scipy's half-space intersection, independent of the library.
 """
@@ -194,6 +195,11 @@ def test_adjoint_host_and_device_agree(ctx):
     # a wrong contact count is an error, not a silent mismatch
     with pytest.raises(_lib.ZdxError):
         _lib.pair_contacts_adjoint(ctx, meshes, pairs, gc[:-1].copy(), gt_h, gp_h, mem=_lib.MEM_HOST)
+    # the plain form (one launch per pair per stage) gives the same gradients
+    gt_p, gp_p = np.zeros_like(lib.tris), np.zeros((8, 12))
+    _lib.pair_contacts_adjoint(ctx, meshes, pairs, gc, gt_p, gp_p, mem=_lib.MEM_HOST, sched=_lib.SCHED_PLAIN)
+    np.testing.assert_allclose(gt_p, gt_h, rtol=1e-12, atol=1e-12 * np.max(np.abs(gt_h)))
+    np.testing.assert_allclose(gp_p, gp_h, rtol=1e-12, atol=1e-12 * np.max(np.abs(gp_h)))
 
 
 def test_autograd_pose_quaternion_and_k(ctx):

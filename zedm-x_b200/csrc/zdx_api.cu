@@ -484,8 +484,7 @@ extern "C" int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts
     }
     // forward with the tape, into the context's own device buffers
     zdx_pair_opts fo = *opts;
-    fo.want_loop_points = 1;
-    fo.sched = ZDX_SCHED_BATCHED;
+    fo.want_loop_points = 1;  // the schedule is the caller's: the plain form is the comparison baseline
     int64_t ccap = std::max<int64_t>(n_contacts, 1);
     int64_t pcap = 64 * ccap + 1024;
     CK(ctx->a_nc.ensure(sizeof(int32_t) * P1));

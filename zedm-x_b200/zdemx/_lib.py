@@ -267,9 +267,9 @@ def pair_contacts_noalloc(ctx: Context, meshes: dict, pairs: dict, out: dict, *,
 
 
 def pair_contacts_adjoint(ctx: Context, meshes: dict, pairs: dict, grad_contact, grad_tris, grad_pose, *,
-                          mode=MODE_ZDEM, split=True, tol=0.0, k=1.0, mem=MEM_DEVICE):
+                          mode=MODE_ZDEM, split=True, tol=0.0, k=1.0, mem=MEM_DEVICE, sched=SCHED_BATCHED):
     """zdx_pair_contacts_adjoint on caller buffers (torch tensors or numpy arrays, all on one side)."""
-    opts = PairOpts(mode, int(split), float(tol), float(k), mem, SCHED_BATCHED, 0, 0)
+    opts = PairOpts(mode, int(split), float(tol), float(k), mem, sched, 0, 0)
     ms = MeshSet(int(meshes["tri_off"].shape[0] - 1), _ptr(meshes["tris"]), _ptr(meshes["tri_off"]),
                  _ptr(meshes["mean_edge"]), _ptr(meshes["bbox_diag"]))
     pb = PairBatch(int(pairs["mesh"].shape[0]), _ptr(pairs["mesh"]), _ptr(pairs["pose"]))
