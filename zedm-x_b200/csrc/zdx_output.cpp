@@ -114,11 +114,12 @@ struct OutputPipeline {
             const int nw = std::max(1, std::min(4, cores / 2));
             nslot = std::min(NSLOT, 2 * nw);
             slice_threads = std::max(1, cores / nw);
-            if (cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking) != cudaSuccess)
+            // (a failed start leaves what it made for the next call, or the destructor, to use or free)
+            if (!copy && cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking) != cudaSuccess)
                 return ctx_fail(ctx, ZDX_ERR_CUDA, "output stream creation failed");
             for (auto& sl : slot)
-                if (cudaEventCreateWithFlags(&sl.snapped, cudaEventDisableTiming) != cudaSuccess ||
-                    cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming) != cudaSuccess)
+                if ((!sl.snapped && cudaEventCreateWithFlags(&sl.snapped, cudaEventDisableTiming) != cudaSuccess) ||
+                    (!sl.copied && cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming) != cudaSuccess))
                     return ctx_fail(ctx, ZDX_ERR_CUDA, "output event creation failed");
             for (int w = 0; w < nw; ++w) writers.emplace_back([this] { run(); });
         }
