@@ -177,7 +177,8 @@ int zdx_scene_array(zdx_ctx* ctx, int which, void* out, int64_t* count);
  * force/torque np x 3 and contact_count np as used by the last step's integration. */
 int zdx_scene_get_state(zdx_ctx* ctx, double* state16, double* force3, double* torque3, int32_t* contact_count);
 int zdx_scene_set_state(zdx_ctx* ctx, const double* state16);
-/* write_vtk_particles + write_particle_state_txt (src/main.cpp:1710-1870, 2470-2483) for `step`. */
+/* write_vtk_particles + write_particle_state_txt (src/main.cpp:1710-1870, 2470-2483) for `step`, after
+ * any outputs queued by zdx_scene_write_output_async are on disk. */
 int zdx_scene_write_output(zdx_ctx* ctx, int64_t step);
 /* Steps in which no pair passes the broad-phase sphere test and no particle a wall's have no contact:
  * for scenes of up to 1024 particles a run of them goes through one single-block kernel that repeats the

@@ -151,6 +151,9 @@ extern "C" int zdx_scene_write_output(zdx_ctx* ctx, int64_t step) {
     if (!ctx) return ZDX_ERR_INVALID;
     if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
     Scene& s = *ctx->scene;
+    // queued outputs first: one of them may be writing the same files
+    int rc0 = output_wait(ctx, s);
+    if (rc0) return rc0;
     if (s.host_dirty) {
         int rc = scene_download(ctx, s);
         if (rc) return rc;
