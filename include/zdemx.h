@@ -148,6 +148,11 @@ int zdx_get_stream(const zdx_ctx* ctx, void** stream);
  * contacts, P-P force law with tangential history, walls, deterministic force/torque scatter,
  * integrate_particle, history prune. */
 int zdx_scene_load(zdx_ctx* ctx, const char* config_path);
+/* Reads a zdem_cpu config and sets up what it describes (STLs, meshes, particle mass and inertia,
+ * walls) on the host, with no GPU: ZDX_OK, or the status zdx_scene_load would return.  msg receives the
+ * message zdem_cpu prints for the failure (empty where it prints none); counts4, when non-null and the
+ * config is accepted: particles, walls, meshes, steps. */
+int zdx_config_check(const char* config_path, char* msg, size_t msg_cap, int64_t* counts4);
 int zdx_scene_step(zdx_ctx* ctx, int nsteps);
 /* info[12]: particles, walls, steps done, and for the last step: contacts, tri_checks, segments,
  * components, loops (the step log's fields, src/main.cpp:2489-2499), candidate pairs, wall contacts,

@@ -230,7 +230,7 @@ bool parse_config(const std::string& path, SimConfig& cfg, std::string& err) {
     if (cfg.output_interval < 1) cfg.output_interval = 1;
     if (!cfg.stl.empty()) return true;
     if (cfg.particles.empty()) {
-        err = "config has neither particle blocks nor a global stl";
+        err.clear();  // zdem_cpu fails here without a message (src/main.cpp:1685-1688)
         return false;
     }
     return true;

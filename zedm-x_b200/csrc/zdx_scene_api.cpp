@@ -28,7 +28,8 @@ extern "C" int zdx_scene_load(zdx_ctx* ctx, const char* config_path) {
     if (!ctx || !config_path) return ZDX_ERR_INVALID;
     SimConfig cfg;
     std::string err;
-    if (!parse_config(config_path, cfg, err)) return ctx_fail(ctx, ZDX_ERR_CONFIG, "%s", err.c_str());
+    if (!parse_config(config_path, cfg, err))
+        return ctx_fail(ctx, ZDX_ERR_CONFIG, "%s", err.empty() ? "config has neither particle blocks nor a global stl" : err.c_str());
     if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx_fail(ctx, ZDX_ERR_CUDA, "cudaSetDevice failed");
     Scene* s = new Scene();
     int rc = scene_from_config(ctx, cfg, *s, err);
@@ -45,6 +46,29 @@ extern "C" int zdx_scene_load(zdx_ctx* ctx, const char* config_path) {
     zdx_ctx_scene_release(ctx);
     ctx->scene = s;
     return ZDX_OK;
+}
+
+extern "C" int zdx_config_check(const char* config_path, char* msg, size_t msg_cap, int64_t* counts4) {
+    if (!config_path) return ZDX_ERR_INVALID;
+    SimConfig cfg;
+    std::string err;
+    int rc = ZDX_OK;
+    Scene s;
+    if (!parse_config(config_path, cfg, err)) {
+        rc = ZDX_ERR_CONFIG;
+    } else {
+        rc = scene_from_config(nullptr, cfg, s, err);
+    }
+    if (msg && msg_cap) {
+        std::snprintf(msg, msg_cap, "%s", err.c_str());
+    }
+    if (counts4 && rc == ZDX_OK) {
+        counts4[0] = s.np;
+        counts4[1] = s.nw;
+        counts4[2] = (int64_t)s.mesh_off.size() - 1;
+        counts4[3] = cfg.steps;
+    }
+    return rc;
 }
 
 extern "C" int zdx_scene_step(zdx_ctx* ctx, int nsteps) {
@@ -191,6 +215,15 @@ extern "C" int zdx_scene_output_wait(zdx_ctx* ctx) {
 // device step, outputs every output_interval steps and the same log line.
 static int run_config(const char* config_path, int device, bool graph) {
     if (!config_path) return 1;
+    {
+        // the config is read before anything else, with zdem_cpu's messages (src/main.cpp:1879-1881)
+        SimConfig cfg;
+        std::string err;
+        if (!parse_config(config_path, cfg, err)) {
+            if (!err.empty()) std::cerr << err << "\n";
+            return 1;
+        }
+    }
     zdx_ctx* ctx = nullptr;
     int rc = zdx_create(&ctx, device);
     if (rc) {

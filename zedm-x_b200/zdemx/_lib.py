@@ -87,6 +87,7 @@ def lib() -> C.CDLL:
     L.zdx_pair_timings.argtypes = [C.c_void_p, _dp, _i64p]
     L.zdx_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.zdx_scene_load.argtypes = [C.c_void_p, C.c_char_p]
+    L.zdx_config_check.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, _i64p]
     L.zdx_scene_step.argtypes = [C.c_void_p, C.c_int]
     L.zdx_scene_info.argtypes = [C.c_void_p, _i64p]
     L.zdx_scene_array.argtypes = [C.c_void_p, C.c_int, C.c_void_p, _i64p]
@@ -125,6 +126,15 @@ def check(status: int, ctx=None):
             if detail:
                 msg = f"{msg}: {detail}"
         raise ZdxError(status, msg)
+
+
+def config_check(path: str):
+    """zdx_config_check: (status, the message zdem_cpu would print, (particles, walls, meshes, steps)
+    or None).  Host only, no GPU."""
+    msg = C.create_string_buffer(4096)
+    counts = np.zeros(4, np.int64)
+    rc = lib().zdx_config_check(path.encode(), msg, 4096, counts.ctypes.data_as(_i64p))
+    return rc, msg.value.decode(), (tuple(int(x) for x in counts) if rc == 0 else None)
 
 
 def stl_load(path: str) -> np.ndarray:
