@@ -965,8 +965,46 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
             __syncwarp();
 
             // ---- split_t_junctions, src/main.cpp:900-961
+            // Lanes over edges first flag the edges that some vertex splits (the same test as below);
+            // runs of unsplit edges then go to E2 a warp at a time, and each split edge goes through the
+            // warp's scan of the vertices and lane 0's ordering, in edge order as before.
             int ne2 = 0;
-            for (int e = 0; e < ne; ++e) {
+            int* split_flag = B.deg;  // free until the loops below
+            for (int e = lane; e < ne; e += 32) {
+                const int ea = B.E[2 * e], eb = B.E[2 * e + 1];
+                const V3 pa = ld3(B.V + 3 * ea), pb = ld3(B.V + 3 * eb);
+                const V3 mn{smin(pa.x, pb.x) - h, smin(pa.y, pb.y) - h, smin(pa.z, pb.z) - h};
+                const V3 mx{smax(pa.x, pb.x) + h, smax(pa.y, pb.y) + h, smax(pa.z, pb.z) + h};
+                const I3 cmin = cell_of(mn, h), cmax = cell_of(mx, h);
+                int hit = 0;
+                for (int v = 0; v < nv && !hit; ++v) {
+                    if (v == ea || v == eb) continue;
+                    const I3 cv = ld_cell(B.vcell + 3 * v);
+                    if (cv.x < cmin.x || cv.x > cmax.x || cv.y < cmin.y || cv.y > cmax.y || cv.z < cmin.z || cv.z > cmax.z)
+                        continue;
+                    double t = 0.0;
+                    const double d2 = pt_seg_d2t(ld3(B.V + 3 * v), pa, pb, t);
+                    hit = (d2 <= tol2 && t > 1e-6 && t < 1.0 - 1e-6) ? 1 : 0;
+                }
+                split_flag[e] = hit;
+            }
+            __syncwarp();
+            for (int e = 0; e < ne;) {
+                const unsigned fl = __ballot_sync(FULL, e + lane < ne && split_flag[e + lane] != 0);
+                const int lim = min(32, ne - e);
+                const int run = fl ? min(__ffs(fl) - 1, lim) : lim;
+                if (run > 0) {
+                    const int room = max(0, min(run, B.cap2 - ne2));
+                    if (lane < room) {
+                        B.E2[2 * (ne2 + lane)] = B.E[2 * (e + lane)];
+                        B.E2[2 * (ne2 + lane) + 1] = B.E[2 * (e + lane) + 1];
+                    }
+                    if (room < run) status |= PAIR_EDGE_OVERFLOW;
+                    ne2 += room;
+                    e += run;
+                    __syncwarp();
+                    continue;
+                }
                 const int ea = B.E[2 * e], eb = B.E[2 * e + 1];
                 const V3 pa = ld3(B.V + 3 * ea), pb = ld3(B.V + 3 * eb);
                 const V3 mn{smin(pa.x, pb.x) - h, smin(pa.y, pb.y) - h, smin(pa.z, pb.z) - h};
@@ -1044,6 +1082,9 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     }
                 }
                 __syncwarp();
+                ne2 = __shfl_sync(FULL, ne2, 0);
+                status = __shfl_sync(FULL, status, 0);
+                e++;
             }
             ne2 = __shfl_sync(FULL, ne2, 0);
             status = __shfl_sync(FULL, status, 0);
