@@ -11,6 +11,12 @@ the tests that use them never touch the reference.
 * mesh_ref.npz       build_mesh (src/main.cpp:445-497) on a few meshes.
 * sort_ref.npz       std::sort permutations under the reference's three comparators.
 * polyline_ref.npz   polyline.py's own pipeline (polyline.py:743-822) on a few pairs.
+* vtk_ref.npz        the text polyline.py's two VTK writers (polyline.py:544-649) give for seeded loops,
+                     contact points and triangle soups: near-duplicate points inside and outside the
+                     1e-9 merge, loops too short to draw, None contact points, and contact lists
+                     shorter than the loop list.
+
+`python tests/golden/make_golden.py vtk` regenerates only the named fixtures.
 """
 from __future__ import annotations
 
@@ -156,12 +162,84 @@ def make_polyline():
     np.savez_compressed(os.path.join(HERE, "polyline_ref.npz"), **d)
 
 
+def _vtk_cases(rng):
+    """Seeded inputs of the VTK writers: (loops, contact points or None, contact ids) per case."""
+    cases = []
+    for ci in range(6):
+        nloop = int(rng.integers(0, 5))
+        loops = []
+        for _ in range(nloop):
+            m = int(rng.integers(1, 7))  # a loop of one point is skipped by the writer
+            base = rng.normal(size=(m, 3)) * 10.0 ** rng.integers(-4, 1)
+            if m > 2 and rng.random() < 0.5:
+                base[m - 1] = base[0] + rng.choice([3e-10, 3e-9]) * rng.normal(size=3)  # merge or not
+            loops.append(base)
+        if loops and rng.random() < 0.7:  # a loop sharing points with the previous one
+            prev = loops[-1]
+            loops.append(prev[::-1] + 1e-10 * rng.normal(size=prev.shape))
+        nl = len(loops)
+        ncp = nl if ci % 3 != 2 else max(0, nl - 1)
+        cps = []
+        for k in range(ncp):
+            if rng.random() < 0.25:
+                cps.append(None)
+            elif rng.random() < 0.3 and loops:
+                cps.append(loops[k % nl][0] + 2e-10)  # lands on a loop point
+            else:
+                cps.append(rng.normal(size=3))
+        cids = [int(x) for x in rng.integers(-1, 50, size=nl + int(ci == 4))]
+        cases.append((loops, cps, cids))
+    return cases
+
+
+def make_vtk():
+    sys.path.insert(0, REF_PY)
+    import tempfile
+
+    import polyline as P  # the reference module, imported read-only
+
+    rng = np.random.default_rng(7)
+    d = {}
+    cases = _vtk_cases(rng)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "x.vtk")
+        for ci, (loops, cps, cids) in enumerate(cases):
+            P.write_vtk_polydata_polylines(path, loops, cps, cids)
+            d[f"l{ci}_loop_len"] = np.array([len(x) for x in loops], np.int64)
+            d[f"l{ci}_loop_pts"] = np.concatenate(loops) if loops else np.zeros((0, 3))
+            d[f"l{ci}_cp_none"] = np.array([c is None for c in cps], bool)
+            d[f"l{ci}_cp"] = np.array([np.zeros(3) if c is None else c for c in cps], float).reshape(-1, 3)
+            d[f"l{ci}_cids"] = np.array(cids, np.int64)
+            d[f"l{ci}_text"] = np.array(open(path, encoding="utf-8").read())
+        for ti in range(3):
+            n = int(rng.integers(1, 40))
+            verts = rng.normal(size=(max(3, n // 2), 3))
+            tris = verts[rng.integers(0, len(verts), size=(n, 3))]
+            tris[::3] += 4e-10 * rng.normal(size=tris[::3].shape)  # inside the merge
+            tris[1::5] += 5e-9  # outside it
+            P.write_vtk_polydata_tris(path, tris, comment=f"mesh {ti}")
+            d[f"t{ti}_tris"] = tris
+            d[f"t{ti}_text"] = np.array(open(path, encoding="utf-8").read())
+    d["nloopcase"] = np.array(len(cases))
+    d["ntricase"] = np.array(3)
+    np.savez_compressed(os.path.join(HERE, "vtk_ref.npz"), **d)
+
+
 if __name__ == "__main__":
-    R = Reference()
-    make_pairs(R)
-    make_mesh(R)
-    make_sort(R)
-    make_polyline()
+    only = set(sys.argv[1:])
+    want = lambda name: not only or name in only
+    if want("pairs") or want("mesh") or want("sort"):
+        R = Reference()
+        if want("pairs"):
+            make_pairs(R)
+        if want("mesh"):
+            make_mesh(R)
+        if want("sort"):
+            make_sort(R)
+    if want("polyline"):
+        make_polyline()
+    if want("vtk"):
+        make_vtk()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
