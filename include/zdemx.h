@@ -111,6 +111,14 @@ typedef struct zdx_pair_result {
     int64_t* contact_point_off;/* contact_cap + 1                                                   */
     int64_t totals[4];         /* out: contacts, segments, triangle AABB checks (the step log's
                                   tri_checks, src/main.cpp:2129), loop points                        */
+    int64_t comp_stats_cap;    /* components recorded per pair (0: none)                            */
+    int32_t* comp_stats;       /* optional, n_pairs x comp_stats_cap x 3: per component in order, its
+                                  segments, snapped vertices and edges after the T-junction split
+                                  (with its accepted loops, the contacts whose contact_info component
+                                  is the same, these are the counts polyline.py main prints per
+                                  component, polyline.py:809); entries past the cap or past the
+                                  pair's component count are 0.  zdx_pair_contacts only; NULL to
+                                  skip                                                             */
 } zdx_pair_result;
 
 int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* meshes,

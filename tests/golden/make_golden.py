@@ -16,6 +16,10 @@ the tests that use them never touch the reference.
                      1e-9 merge, loops too short to draw, None contact points, and contact lists
                      shorter than the loop list.
 
+* cli_ref.npz        polyline.py's command line (polyline.py:707-834) on seeded binary STL pairs:
+                     its argv, stdout and the three VTK files it writes (no split, split into two
+                     components, no intersection, segments whose loops all snap away).
+
 `python tests/golden/make_golden.py vtk` regenerates only the named fixtures.
 """
 from __future__ import annotations
@@ -225,6 +229,69 @@ def make_vtk():
     np.savez_compressed(os.path.join(HERE, "vtk_ref.npz"), **d)
 
 
+CLI_CASES = [
+    # (name, mesh A spec, mesh B spec, extra argv); a spec is a list of (subdivision, centre) blobs
+    ("plain", [(2, (0, 0, 0))], [(2, (0, 0, 0))], ["--tB", "1.9e-3", "1e-4", "0", "--qB", "0.9", "0.1", "0.3", "0.2",
+                                                  "--k", "1e7"]),
+    ("split", [(2, (0, 0, 0))], [(1, (0, 1.7e-3, 0)), (1, (0, -1.7e-3, 0))],
+     ["--tA", "1e-4", "0", "0", "--qA", "1", "0.05", "0", "0", "--split-contacts", "--tol", "1e-5"]),
+    ("apart", [(1, (0, 0, 0))], [(1, (0, 0, 0))], ["--tB", "5e-3", "0", "0"]),
+    ("snapped_away", [(1, (0, 0, 0))], [(1, (0, 0, 0))], ["--tB", "1.8e-3", "0", "0", "--tol", "1e-2"]),
+]
+
+
+def cli_mesh(spec, rng):
+    """Triangles of a union of noised icospheres of radius 1 mm, rounded to float32 as in a binary STL."""
+    parts = [synth.noised_icosphere(sub, 1e-3, 0.1, rng) + np.asarray(c, float) for sub, c in spec]
+    return np.concatenate(parts).astype(np.float32).astype(np.float64)
+
+
+def make_cli():
+    sys.path.insert(0, REF_PY)
+    sys.path.insert(0, os.path.dirname(HERE))
+    import contextlib
+    import io
+    import tempfile
+
+    import polyline as P  # the reference module, imported read-only
+    from _dem_helpers import write_binary_stl
+
+    rng = np.random.default_rng(11)
+    d = {}
+    cwd = os.getcwd()
+    for ci, (name, sa, sb, extra) in enumerate(CLI_CASES):
+        A, B = cli_mesh(sa, rng), cli_mesh(sb, rng)
+        with tempfile.TemporaryDirectory() as tmp:
+            os.chdir(tmp)
+            try:
+                write_binary_stl("A.stl", A)
+                write_binary_stl("B.stl", B)
+                argv = ["A.stl", "B.stl"] + extra
+                old = sys.argv
+                sys.argv = ["polyline.py"] + argv
+                buf = io.StringIO()
+                try:
+                    with contextlib.redirect_stdout(buf):
+                        P.main()
+                finally:
+                    sys.argv = old
+                files = {}
+                for f in ("A_transformed.vtk", "B_transformed.vtk", "routeB_intersection.vtk"):
+                    files[f] = open(f, encoding="utf-8").read() if os.path.exists(f) else ""
+            finally:
+                os.chdir(cwd)
+        d[f"c{ci}_name"] = np.array(name)
+        d[f"c{ci}_A"] = A
+        d[f"c{ci}_B"] = B
+        d[f"c{ci}_argv"] = np.array(" ".join(argv))
+        d[f"c{ci}_stdout"] = np.array(buf.getvalue())
+        d[f"c{ci}_vtkA"] = np.array(files["A_transformed.vtk"])
+        d[f"c{ci}_vtkB"] = np.array(files["B_transformed.vtk"])
+        d[f"c{ci}_loops"] = np.array(files["routeB_intersection.vtk"])
+    d["ncase"] = np.array(len(CLI_CASES))
+    np.savez_compressed(os.path.join(HERE, "cli_ref.npz"), **d)
+
+
 if __name__ == "__main__":
     only = set(sys.argv[1:])
     want = lambda name: not only or name in only
@@ -240,6 +307,8 @@ if __name__ == "__main__":
         make_polyline()
     if want("vtk"):
         make_vtk()
+    if want("cli"):
+        make_cli()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

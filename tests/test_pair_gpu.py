@@ -193,3 +193,35 @@ def test_large_pairs(ctx, oracle, split, mode):
         assert res["stats"][p, 0] == r["nseg"]
         big += r["nseg"] > 200
     assert big >= 4
+
+
+@pytest.mark.parametrize("split,mode,sched", [(True, 0, 0), (True, 1, 0), (False, 1, 1)])
+def test_component_counts_match_oracle(ctx, oracle, split, mode, sched):
+    """The optional per-component counts (segments, snapped vertices, edges after the T-junction split)
+    against the oracle's components, batched and plain; components past the cap stay 0."""
+    from zdemx import _lib, synth
+
+    rng = np.random.default_rng(5 + 2 * split + mode)
+    meshes = [synth.noised_icosphere(s, 1e-3, 0.15, rng) for s in (1, 2, 2, 3)]
+    lib = _library(meshes)
+    npairs = 40
+    pm = rng.integers(0, lib.n_mesh, size=(npairs, 2)).astype(np.int32)
+    pp = synth.pair_poses(rng, npairs, 1e-3, 0.0, 0.15)
+    tol = 2e-5 if mode == 1 else 0.0
+    cap = 3
+    res = _lib.pair_contacts_raw(ctx, lib.tris, lib.tri_off, lib.mean_edge, lib.bbox_diag, pm, pp, mode=mode,
+                                 split=split, tol=tol, k=1e7, sched=sched, comp_cap=cap)
+    cs = res["comp_stats"]
+    assert cs.shape == (npairs, cap, 3)
+    multi = 0
+    for p in range(npairs):
+        a, b = pm[p]
+        r = oracle.pair(lib.mesh(a), lib.mean_edge[a], lib.bbox_diag[a], lib.mesh(b), pp[p, :7], pp[p, 7:],
+                        split=split, mode=mode, tol=tol)
+        want = np.zeros((cap, 3), np.int32)
+        for c in range(min(r["ncomp"], cap)):
+            want[c] = [r["comp_off"][c + 1] - r["comp_off"][c], r["v_off"][c + 1] - r["v_off"][c],
+                       r["e2_off"][c + 1] - r["e2_off"][c]]
+        assert np.array_equal(cs[p], want), (p, cs[p], want)
+        multi += r["ncomp"] > 1
+    assert multi >= (3 if split else 0)

@@ -1,0 +1,115 @@
+"""The polyline mirror's command line against polyline.py's own (polyline.py:707-834), on the seeded STL
+pairs of tests/golden/cli_ref.npz (its argv, stdout and the three VTK files it wrote):
+
+* CPU: the transformed-mesh VTK files byte for byte (host code only), and main's printing and file
+  logic, with the pair call replaced by the counts polyline.py printed, byte for byte on the cases
+  without contacts (no segments; segments whose loops all snap away).
+* GPU: the whole command line.  Lines and files are identical except for FP64 numbers, which polyline.py
+  computes with numpy (its own rounding) and which agree within 1e-9 relative."""
+import contextlib
+import io
+import os
+import re
+
+import numpy as np
+import pytest
+
+from _dem_helpers import write_binary_stl
+from conftest import GOLDEN
+
+NUM = re.compile(r"-?\d+(?:\.\d*)?(?:[eE][-+]?\d+)?")
+
+
+def _cases():
+    z = np.load(os.path.join(GOLDEN, "cli_ref.npz"))
+    out = []
+    for ci in range(int(z["ncase"])):
+        out.append({k: z[f"c{ci}_{k}"] for k in ("name", "A", "B", "argv", "stdout", "vtkA", "vtkB", "loops")})
+        for k in ("name", "argv", "stdout", "vtkA", "vtkB", "loops"):
+            out[-1][k] = str(out[-1][k])
+    return out
+
+
+def _run_main(case, tmp):
+    from zdemx import polyline
+
+    write_binary_stl(os.path.join(tmp, "A.stl"), case["A"])
+    write_binary_stl(os.path.join(tmp, "B.stl"), case["B"])
+    cwd = os.getcwd()
+    os.chdir(tmp)
+    buf = io.StringIO()
+    try:
+        with contextlib.redirect_stdout(buf):
+            polyline.main(case["argv"].split())
+    finally:
+        os.chdir(cwd)
+
+    def read(f):
+        p = os.path.join(tmp, f)
+        return open(p, encoding="utf-8").read() if os.path.exists(p) else ""
+
+    return buf.getvalue(), read("A_transformed.vtk"), read("B_transformed.vtk"), read("routeB_intersection.vtk")
+
+
+def _same_up_to_rounding(got, want, what):
+    """Identical text once every number is masked; the numbers within 1e-9 relative."""
+    assert NUM.sub("#", got) == NUM.sub("#", want), what
+    a = np.array([float(x) for x in NUM.findall(got)])
+    b = np.array([float(x) for x in NUM.findall(want)])
+    assert len(a) == len(b), what
+    bad = np.abs(a - b) > 1e-9 * np.maximum(np.abs(a), np.abs(b)) + 1e-15
+    assert not bad.any(), (what, a[bad][:5], b[bad][:5])
+
+
+def test_transformed_meshes_match_reference(tmp_path):
+    from zdemx import polyline
+
+    for case in _cases():
+        write_binary_stl(str(tmp_path / "A.stl"), case["A"])
+        write_binary_stl(str(tmp_path / "B.stl"), case["B"])
+        args = polyline.parse_args(case["argv"].split())
+        for f, pose, comment, want in ((args.stlA, (args.tA, args.qA), "Mesh A (transformed)", case["vtkA"]),
+                                       (args.stlB, (args.tB, args.qB), "Mesh B (transformed)", case["vtkB"])):
+            tris0 = polyline.load_stl(str(tmp_path / f))
+            tris = polyline.transform_points(tris0.reshape(-1, 3), *pose).reshape(-1, 3, 3)
+            out = str(tmp_path / "m.vtk")
+            polyline.write_vtk_polydata_tris(out, tris, comment=comment)
+            assert open(out, encoding="utf-8").read() == want, (case["name"], f)
+
+
+def test_main_without_contacts_matches_reference(tmp_path, monkeypatch):
+    """main's own logic around the pair call: the messages, the component lines and the (empty) loops
+    file, with the pair call giving the counts polyline.py printed."""
+    from zdemx import polyline
+
+    checked = 0
+    for case in _cases():
+        if "[Contact" in case["stdout"]:
+            continue
+        m = re.search(r"Raw intersection segments: (\d+)", case["stdout"])
+        nseg = int(m.group(1)) if m else 0
+        comps = [tuple(int(x) for x in c) for c in
+                 re.findall(r"rawSeg=(\d+) snappedV=(\d+) edges=(\d+) loops=(\d+)", case["stdout"])]
+
+        def fake(*a, comp_cap=0, _n=nseg, _c=comps):
+            return {"idA": 0, "idB": 1, "contacts": []}, [], [], [], _n, len(_c), _c
+
+        monkeypatch.setattr(polyline, "_pair_call", fake)
+        d = tmp_path / case["name"]
+        d.mkdir()
+        stdout, va, vb, loops = _run_main(case, str(d))
+        assert stdout == case["stdout"], case["name"]
+        assert (va, vb, loops) == (case["vtkA"], case["vtkB"], case["loops"]), case["name"]
+        checked += 1
+    assert checked == 2
+
+
+@pytest.mark.gpu
+def test_main_matches_reference(tmp_path):
+    for case in _cases():
+        d = tmp_path / case["name"]
+        d.mkdir()
+        stdout, va, vb, loops = _run_main(case, str(d))
+        assert (va, vb) == (case["vtkA"], case["vtkB"]), case["name"]
+        _same_up_to_rounding(stdout, case["stdout"], (case["name"], "stdout"))
+        _same_up_to_rounding(loops, case["loops"], (case["name"], "loops vtk"))

@@ -251,6 +251,19 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     a.err = reinterpret_cast<int*>(cnt + 7);
     CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
     CK(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
+    // optional per-component counts, written by the rebuild stage
+    const int64_t comp_cap = out->comp_stats ? std::max<int64_t>(out->comp_stats_cap, 0) : 0;
+    const size_t comp_bytes = sizeof(int32_t) * 3 * (size_t)comp_cap * (size_t)NP;
+    if (comp_bytes) {
+        if (host) {
+            CK(ctx->o_comp.ensure(comp_bytes));
+            a.comp_stats = as<int32_t>(ctx->o_comp);
+        } else {
+            a.comp_stats = out->comp_stats;
+        }
+        a.comp_stats_cap = comp_cap;
+        CK(cudaMemsetAsync(a.comp_stats, 0, comp_bytes, st));
+    }
 
     const bool plain = opts->sched == ZDX_SCHED_PLAIN;
     if (plain) {
@@ -435,6 +448,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         CK(cudaMemcpyAsync(out->pair_ncontact, a.pair_ncontact, sizeof(int32_t) * NP, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(out->pair_contact_off, coff, sizeof(int64_t) * (NP + 1), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(out->pair_stats, pstats, sizeof(int32_t) * 4 * NP, cudaMemcpyDeviceToHost, st));
+        if (comp_bytes) CK(cudaMemcpyAsync(out->comp_stats, a.comp_stats, comp_bytes, cudaMemcpyDeviceToHost, st));
         if (nct) {
             CK(cudaMemcpyAsync(out->contact_geom, cg, sizeof(double) * 20 * nct, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(out->contact_info, ci, sizeof(int32_t) * 4 * nct, cudaMemcpyDeviceToHost, st));

@@ -1093,6 +1093,14 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
             ne2 = __shfl_sync(FULL, ne2, 0);
             status = __shfl_sync(FULL, status, 0);
             if (status & PAIR_EDGE_OVERFLOW) break;
+            if (lane == 0 && a.comp_stats && c < a.comp_stats_cap) {
+                // the counts of the component line printed by polyline.py main (polyline.py:809); its
+                // accepted loops are the contacts whose component index is c
+                int32_t* cs = a.comp_stats + 3 * ((int64_t)p * a.comp_stats_cap + c);
+                cs[0] = m;
+                cs[1] = nv;
+                cs[2] = ne2;
+            }
 
             // ---- extract_loops (src/main.cpp:963-1025), then each loop's integrals, filters and
             // force (src/main.cpp:1027-1052, 2187-2219; polyline.py:799-822, 655-701)

@@ -96,6 +96,10 @@ struct PairArgs {
     int32_t* pair_ncomp;
     int32_t* pair_nloop;
     int* err;
+    // null, or per pair comp_stats_cap x 3: each component's segments, snapped vertices and edges after
+    // the T-junction split, in component order
+    int32_t* comp_stats;
+    int64_t comp_stats_cap;
 };
 
 // Bytes of one rebuild slot able to hold a pair of n segments.

@@ -52,7 +52,7 @@ class PairResult(C.Structure):
     _fields_ = [("pair_ncontact", C.c_void_p), ("pair_contact_off", C.c_void_p), ("pair_stats", C.c_void_p),
                 ("contact_cap", C.c_int64), ("contact_geom", C.c_void_p), ("contact_info", C.c_void_p),
                 ("loop_point_cap", C.c_int64), ("loop_points", C.c_void_p), ("contact_point_off", C.c_void_p),
-                ("totals", C.c_int64 * 4)]
+                ("totals", C.c_int64 * 4), ("comp_stats_cap", C.c_int64), ("comp_stats", C.c_void_p)]
 
 
 class ZdxError(RuntimeError):
@@ -207,8 +207,10 @@ def _ptr(a) -> int:
 
 def pair_contacts_raw(ctx: Context, mesh_tris, tri_off, mean_edge, bbox_diag, pair_mesh, pair_pose, *,
                       mode=MODE_ZDEM, split=True, tol=0.0, k=1.0, want_points=False, sched=SCHED_BATCHED,
-                      contact_cap=None, point_cap=None, max_seg_per_pair=0):
-    """Host-memory batched pair call.  Returns a dict of numpy arrays (CSR over pairs)."""
+                      contact_cap=None, point_cap=None, max_seg_per_pair=0, comp_cap=0):
+    """Host-memory batched pair call.  Returns a dict of numpy arrays (CSR over pairs).  With comp_cap > 0
+    it also holds "comp_stats" (pairs x comp_cap x 3: each component's segments, snapped vertices and edges
+    after the T-junction split)."""
     tris = np.ascontiguousarray(mesh_tris, dtype=np.float64)
     off = np.ascontiguousarray(tri_off, dtype=np.int64)
     me = np.ascontiguousarray(mean_edge, dtype=np.float64)
@@ -228,11 +230,13 @@ def pair_contacts_raw(ctx: Context, mesh_tris, tri_off, mean_edge, bbox_diag, pa
         info = np.zeros((max(contact_cap, 1), 4), np.int32)
         pts = np.zeros((max(point_cap, 1), 3))
         cpo = np.zeros(max(contact_cap, 1) + 1, np.int64)
+        comp = np.zeros((max(npairs, 1), max(comp_cap, 1), 3), np.int32)
         opts = PairOpts(mode, int(split), float(tol), float(k), MEM_HOST, sched, int(want_points), int(max_seg_per_pair))
         ms = MeshSet(len(off) - 1, tris.ctypes.data, off.ctypes.data, me.ctypes.data, bd.ctypes.data)
         pb = PairBatch(npairs, pm.ctypes.data, pp.ctypes.data)
         res = PairResult(ncontact.ctypes.data, coff.ctypes.data, stats.ctypes.data, contact_cap, geom.ctypes.data,
-                         info.ctypes.data, point_cap, pts.ctypes.data, cpo.ctypes.data)
+                         info.ctypes.data, point_cap, pts.ctypes.data, cpo.ctypes.data, (C.c_int64 * 4)(),
+                         int(comp_cap), comp.ctypes.data if comp_cap > 0 else None)
         st = lib().zdx_pair_contacts(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), C.byref(res))
         totals = list(res.totals)
         if st == ZDX_ERR_CAPACITY and attempt == 0 and (totals[0] > contact_cap or totals[3] > point_cap):
@@ -244,7 +248,8 @@ def pair_contacts_raw(ctx: Context, mesh_tris, tri_off, mean_edge, bbox_diag, pa
     nct = int(totals[0])
     return {"ncontact": ncontact[:npairs], "contact_off": coff, "stats": stats[:npairs], "geom": geom[:nct],
             "info": info[:nct], "points": pts[: int(totals[3])] if want_points else None,
-            "point_off": cpo[: nct + 1] if want_points else None, "totals": totals}
+            "point_off": cpo[: nct + 1] if want_points else None, "totals": totals,
+            "comp_stats": comp[:npairs] if comp_cap > 0 else None}
 
 
 def pair_contacts_device(ctx: Context, meshes: dict, pairs: dict, out: dict, *, mode=MODE_ZDEM, split=True, tol=0.0,

@@ -100,6 +100,17 @@ def pair_contacts(trisA, trisB, tA=(0.0, 0.0, 0.0), qA=(1.0, 0.0, 0.0, 0.0), tB=
                   qB=(1.0, 0.0, 0.0, 0.0), k=1.0, tol=1e-6, split_contacts=False, idA=0, idB=1, ctx=None):
     """Contacts between mesh A at pose (tA, qA) and mesh B at (tB, qB), as polyline.py main computes
     them (polyline.py:743-829).  Returns (manifold, loops_pts, xc0s, contact_ids)."""
+    return _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, ctx)[:4]
+
+
+# components recorded by the command line: at most one per segment, and a pair holds at most the
+# library's default segment capacity
+_COMP_CAP = 16384
+
+
+def _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, ctx, comp_cap=0):
+    """pair_contacts, plus the pair's segment and component counts and (comp_cap > 0) the per-component
+    counts (segments, snapped vertices, edges, loops) main prints."""
     A = np.ascontiguousarray(trisA, dtype=float).reshape(-1, 3, 3)
     B = np.ascontiguousarray(trisB, dtype=float).reshape(-1, 3, 3)
     tris = np.concatenate([A.reshape(-1), B.reshape(-1)])
@@ -107,7 +118,7 @@ def pair_contacts(trisA, trisB, tA=(0.0, 0.0, 0.0), qA=(1.0, 0.0, 0.0, 0.0), tB=
     pose = np.concatenate([np.asarray(tA, float), np.asarray(qA, float), np.asarray(tB, float), np.asarray(qB, float)])
     r = _lib.pair_contacts_raw(ctx or _ctx(), tris, off, np.zeros(2), np.zeros(2), np.array([[0, 1]], np.int32),
                                pose[None, :], mode=_lib.MODE_POLYLINE, split=split_contacts, tol=tol, k=k,
-                               want_points=True)
+                               want_points=True, comp_cap=comp_cap)
     loops, xc0s, cids = [], [], []
     for c in range(len(r["geom"])):
         pts = r["points"][r["point_off"][c]: r["point_off"][c + 1]]
@@ -116,7 +127,13 @@ def pair_contacts(trisA, trisB, tA=(0.0, 0.0, 0.0), qA=(1.0, 0.0, 0.0, 0.0), tB=
         xc0s.append(None if g[12] == 0.0 else g[6:9].copy())
         cids.append(int(r["info"][c, 1]))
     manifold = _manifold(idA, idB, r["geom"], r["info"], k)
-    return manifold, loops, xc0s, cids
+    nseg, ncomp = int(r["stats"][0, 0]), int(r["stats"][0, 1])
+    comps = None
+    if comp_cap > 0:
+        # (segments, snapped vertices, edges, loops) per component; its loops are its contacts
+        nloop = np.bincount(r["info"][:, 3], minlength=ncomp)[:ncomp]
+        comps = [tuple(int(x) for x in r["comp_stats"][0, c]) + (int(nloop[c]),) for c in range(ncomp)]
+    return manifold, loops, xc0s, cids, nseg, ncomp, comps
 
 
 def _manifold(idA, idB, geom, info, k):
@@ -270,16 +287,27 @@ def main(argv=None):
     write_vtk_polydata_tris(args.outA, trisA, comment="Mesh A (transformed)")
     write_vtk_polydata_tris(args.outB, trisB, comment="Mesh B (transformed)")
     print(f"Transformed meshes written: {args.outA}, {args.outB}")
-    manifold, loops, xc0s, cids = pair_contacts(trisA0, trisB0, args.tA, args.qA, args.tB, args.qB, k=args.k,
-                                                tol=args.tol, split_contacts=args.split_contacts)
-    if not loops and not manifold["contacts"]:
+    manifold, loops, xc0s, cids, nseg, ncomp, comps = _pair_call(
+        trisA0, trisB0, args.tA, args.qA, args.tB, args.qB, args.k, args.tol, args.split_contacts, 0, 1, None,
+        comp_cap=_COMP_CAP)
+    if nseg == 0:
         print("No intersection segments found.")
         return
-    for c, (lp, x) in enumerate(zip(loops, xc0s)):
-        cc = manifold["contacts"][c]
-        print(f"  [Contact {cc['cid']}] nVert={len(lp)} |Sn|={cc['area']}")
-        print(f"    nA={cc['nA']}")
-        print(f"    xc(0)={None if x is None else x.tolist()}")
+    print(f"Raw intersection segments: {nseg}")
+    tol = float(args.tol)
+    if args.split_contacts:
+        print(f"Coarse components: {ncomp} (tol={tol})")
+    else:
+        print("Coarse components: 1 (no split)")
+    c = 0
+    for comp_idx, (raw_seg, snapped_v, edges, nloop) in enumerate(comps):
+        print(f"\n[Component {comp_idx}] rawSeg={raw_seg} snappedV={snapped_v} edges={edges} loops={nloop}")
+        for _ in range(nloop):
+            cc, x = manifold["contacts"][c], xc0s[c]
+            print(f"  [Contact {cc['cid']}] nVert={len(loops[c])} |Sn|={cc['area']}")
+            print(f"    nA={cc['nA']}")
+            print(f"    xc(0)={None if x is None else x.tolist()}")
+            c += 1
     write_vtk_polydata_polylines(args.vtk, loops, xc0s, cids)
     print(f"\nReconstructed-loop VTK written: {args.vtk}")
     print('ParaView: color by CELL "contact_id". Each loop is one polyline cell.')
