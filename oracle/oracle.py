@@ -84,6 +84,7 @@ class Oracle:
         L.zo_pair_free.argtypes = [C.POINTER(_OracleOut)]
         L.zo_build_mesh.argtypes = [_dp, C.c_int, C.c_int, _dp, _dp]
         L.zo_sort.argtypes = [C.c_int, _ip, C.c_int, _ip, _dp, C.c_int]
+        L.zo_pyset_order.argtypes = [_ip, C.c_int, _ip]
         L.zo_wall_contact.argtypes = [_dp, C.c_int, _dp, _dp, _dp, C.c_double, C.c_double, _dp, _dp, _dp]
         L.zo_integrate.argtypes = [_dp, _dp, _dp, _dp, C.c_double]
 
@@ -108,6 +109,12 @@ class Oracle:
         r["tol"] = o.tol
         self.lib.zo_pair_free(C.byref(o))
         return r
+
+    def pyset_order(self, keys):
+        k = np.ascontiguousarray(keys, dtype=np.int32)
+        out = np.zeros(max(len(k), 1), np.int32)
+        self.lib.zo_pyset_order(k.ctypes.data_as(_ip), len(k), out.ctypes.data_as(_ip))
+        return out[: len(k)]
 
     def sort(self, kind, n, ikey=None, dkey=None, stable=False):
         idx = np.arange(n, dtype=np.int32)

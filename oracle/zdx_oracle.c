@@ -463,10 +463,67 @@ static double seg_seg_dist2(V3 p1, V3 q1, V3 p2, V3 q2) {
     return vdot(df, df);
 }
 
-/* label_segments_by_contact_greedy, src/main.cpp:804-898 (polyline.py:267-341).  The reference visits
+/* The iteration order of a CPython set of non-negative ints built by adding keys[0..n) in order (all
+ * distinct): the slot order of its open-addressing table (CPython 3.12 Objects/setobject.c: hash(j) = j,
+ * an 8-slot table to start, each probe looks at slot i and, when i + 9 <= mask, the 9 slots after it,
+ * then i = (5 i + 1 + perturb) & mask with perturb = j shifted right by 5 each round; after an insert
+ * that makes fill * 5 >= mask * 3 the table is rebuilt at the smallest power of two above 4 x used,
+ * the old entries inserted again in slot order).  polyline.py iterates such a set of candidate
+ * segments (polyline.py:293-303, 324).  tab needs 8 n + 8 ints, old n + 1; out receives the keys. */
+static void pyset_insert(int* tab, unsigned mask, int k) {
+    unsigned i = (unsigned)k & mask;
+    unsigned perturb = (unsigned)k;
+    for (;;) {
+        unsigned probes = (i + 9 <= mask) ? 9u : 0u;
+        for (unsigned e = i;; ++e) {
+            if (tab[e] < 0) {
+                tab[e] = k;
+                return;
+            }
+            if (probes-- == 0) break;
+        }
+        perturb >>= 5;
+        i = (i * 5u + 1u + perturb) & mask;
+    }
+}
+static void pyset_order(const int* keys, int n, int* tab, int* old, int* out) {
+    unsigned mask = 7;
+    for (unsigned x = 0; x <= mask; ++x) tab[x] = -1;
+    long used = 0;
+    for (int q = 0; q < n; ++q) {
+        pyset_insert(tab, mask, keys[q]);
+        ++used;
+        if ((unsigned long)used * 5 >= (unsigned long)mask * 3) {
+            long minused = used > 50000 ? used * 2 : used * 4;
+            unsigned long size = 8;
+            while (size <= (unsigned long)minused) size <<= 1;
+            int no = 0;
+            for (unsigned x = 0; x <= mask; ++x)
+                if (tab[x] >= 0) old[no++] = tab[x];
+            mask = (unsigned)size - 1;
+            for (unsigned x = 0; x <= mask; ++x) tab[x] = -1;
+            for (int o = 0; o < no; ++o) pyset_insert(tab, mask, old[o]);
+        }
+    }
+    int m = 0;
+    for (unsigned x = 0; x <= mask; ++x)
+        if (tab[x] >= 0) out[m++] = tab[x];
+}
+
+int zo_pyset_order(const int* keys, int n, int* out) {
+    int* tab = (int*)malloc(sizeof(int) * (8 * (size_t)n + 8));
+    int* old = (int*)malloc(sizeof(int) * ((size_t)n + 1));
+    pyset_order(keys, n, tab, old, out);
+    free(tab);
+    free(old);
+    return n;
+}
+
+/* label_segments_by_contact_greedy, src/main.cpp:804-898 (polyline.py:267-368).  The reference visits
  * the candidates of segment i in hash-grid order: rep point r of i (p0, p1, mid), then the 27
  * neighbour cells in dx,dy,dz order, then the cell's list in insertion order.  That order is exactly
- * (smallest r*27+cell-offset over all rep points of j, then j), which is what is sorted here. */
+ * (smallest r*27+cell-offset over all rep points of j, then j), which is what is sorted here.
+ * polyline.py (py != 0) collects the same candidates into a set and visits them in the set's order. */
 static void label_components(const V3* s0, const V3* s1, int nseg, double h, int stable, IBuf* comp_off,
                              IBuf* comp_idx) {
     V3* rep = (V3*)malloc(sizeof(V3) * 3 * (size_t)nseg);
@@ -487,6 +544,8 @@ static void label_components(const V3* s0, const V3* s1, int nseg, double h, int
     int* stack = (int*)malloc(sizeof(int) * (size_t)nseg);
     int* cand = (int*)malloc(sizeof(int) * (size_t)nseg);
     int* ckey = (int*)malloc(sizeof(int) * (size_t)nseg);
+    int* ptab = stable ? (int*)malloc(sizeof(int) * (8 * (size_t)nseg + 8)) : NULL;
+    int* pold = stable ? (int*)malloc(sizeof(int) * ((size_t)nseg + 1)) : NULL;
     IBuf raw_off = {0}, raw_idx = {0};
     ib_push(&raw_off, 0);
     for (int seed = 0; seed < nseg; ++seed) {
@@ -522,6 +581,11 @@ static void label_components(const V3* s0, const V3* s1, int nseg, double h, int
                 ckey[pos] = best;
                 ++nc;
             }
+            if (stable) {
+                /* the set's order; ckey is free now and takes it */
+                pyset_order(cand, nc, ptab, pold, ckey);
+                memcpy(cand, ckey, sizeof(int) * (size_t)nc);
+            }
             for (int k = 0; k < nc; ++k) {
                 int j = cand[k];
                 if (visited[j]) continue;
@@ -550,6 +614,7 @@ static void label_components(const V3* s0, const V3* s1, int nseg, double h, int
     }
     free(order); free(sizes); free(raw_off.p); free(raw_idx.p);
     free(rep); free(cel); free(bmn); free(bmx); free(visited); free(stack); free(cand); free(ckey);
+    free(ptab); free(pold);
 }
 
 static int uf_find(int* parent, int x) {

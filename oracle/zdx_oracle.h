@@ -65,6 +65,10 @@ void zo_pair_free(ZoPairOut* out);
  * zdx_ref_std_sort.  stable != 0 gives Python's stable order instead. */
 void zo_sort(int kind, int* idx, int n, const int* ikey, const double* dkey, int stable);
 
+/* Iteration order of a CPython 3.12 set of the distinct non-negative ints keys[0..n) added in order
+ * (the order polyline.py visits a segment's candidates in); out receives the n keys.  Returns n. */
+int zo_pyset_order(const int* keys, int n, int* out);
+
 /* compute_wall_contact (src/main.cpp:1205-1258). */
 int zo_wall_contact(const double* tris, int ntri, const double* pose, const double* wall_tri9,
                     const double* wall_normal, double radius, double tol, double* area, double* point3,

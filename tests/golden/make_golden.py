@@ -20,6 +20,9 @@ the tests that use them never touch the reference.
                      its argv, stdout and the three VTK files it writes (no split, split into two
                      components, no intersection, segments whose loops all snap away).
 
+* polyline_split_ref.npz  the same pipeline with --split-contacts (label_segments_by_contact_greedy,
+                     polyline.py:267-368) on pairs whose contact splits into several components.
+
 `python tests/golden/make_golden.py vtk` regenerates only the named fixtures.
 """
 from __future__ import annotations
@@ -229,6 +232,79 @@ def make_vtk():
     np.savez_compressed(os.path.join(HERE, "vtk_ref.npz"), **d)
 
 
+def make_polyline_split():
+    sys.path.insert(0, REF_PY)
+    import polyline as P  # the reference module, imported read-only
+
+    rng = np.random.default_rng(123)
+    d = {}
+    n_cases = 6
+    for ci in range(n_cases):
+        A = synth.noised_icosphere(2, 1e-3, 0.15, rng)
+        # B: two or three blobs around A, so that the contact splits
+        nb = 2 + ci % 2
+        blobs = []
+        for b in range(nb):
+            u = synth.random_dirs(rng, 1)[0]
+            blobs.append(synth.noised_icosphere(1 + (b + ci) % 2, 0.6e-3, 0.1, rng) + u * rng.uniform(1.35e-3, 1.5e-3))
+        B = np.concatenate(blobs)
+        q = synth.random_unit_quat(rng)
+        pose = np.r_[rng.normal(size=3) * 1e-5, q, np.zeros(3), [1.0, 0.0, 0.0, 0.0]]
+        tol = 1e-5
+        trisA = P.transform_points(A.reshape(-1, 3), pose[0:3], pose[3:7]).reshape(-1, 3, 3)
+        trisB = P.transform_points(B.reshape(-1, 3), pose[7:10], pose[10:14]).reshape(-1, 3, 3)
+        nA_all, nB_all = P.tri_normals(trisA), P.tri_normals(trisB)
+        planesA = [P.plane_from_tri(trisA[i]) for i in range(len(trisA))]
+        planesB = [P.plane_from_tri(trisB[i]) for i in range(len(trisB))]
+        aminA, amaxA = trisA.min(axis=1), trisA.max(axis=1)
+        aminB, amaxB = trisB.min(axis=1), trisB.max(axis=1)
+        segs = []
+        for i in range(len(trisA)):
+            nAi, dAi = planesA[i]
+            if nAi is None:
+                continue
+            for j in range(len(trisB)):
+                if (amaxA[i, 0] < aminB[j, 0] or aminA[i, 0] > amaxB[j, 0] or amaxA[i, 1] < aminB[j, 1] or
+                        aminA[i, 1] > amaxB[j, 1] or amaxA[i, 2] < aminB[j, 2] or aminA[i, 2] > amaxB[j, 2]):
+                    continue
+                nBj, dBj = planesB[j]
+                if nBj is None:
+                    continue
+                sg = P.tri_tri_intersection_segment(trisA[i], nA_all[i], dAi, trisB[j], nB_all[j], dBj)
+                if sg is not None:
+                    segs.append(sg)
+        _, ncomp, comps = P.label_segments_by_contact_greedy(segs, tol=tol) if segs else (None, 0, [])
+        loops, comp_of, comp_sz = [], [], []
+        for c, comp in enumerate(comps):
+            comp_sz.append(len(comp))
+            V, E = P.snap_endpoints([segs[i] for i in comp], tol=tol)
+            V2, E2 = P.split_t_junctions(V, E, tol=tol)
+            for lv in P.extract_loops(V2, E2):
+                if len(lv) < 3:
+                    continue
+                pts = [V2[i] for i in lv]
+                if np.linalg.norm(np.max(pts, axis=0) - np.min(pts, axis=0)) < tol * 2:
+                    continue
+                loops.append(np.asarray(pts))
+                comp_of.append(c)
+        man = P.build_contacts_from_loops(0, 1, loops, list(range(len(loops))), k_stiff=1e7)
+        d[f"c{ci}_A"] = A
+        d[f"c{ci}_B"] = B
+        d[f"c{ci}_pose"] = pose
+        d[f"c{ci}_tol"] = np.array(tol)
+        d[f"c{ci}_nseg"] = np.array(len(segs))
+        d[f"c{ci}_ncomp"] = np.array(ncomp)
+        d[f"c{ci}_comp_sz"] = np.array(comp_sz, np.int64)
+        d[f"c{ci}_loop_comp"] = np.array(comp_of, np.int64)
+        d[f"c{ci}_loop_len"] = np.array([len(x) for x in loops], np.int64)
+        d[f"c{ci}_loop_pts"] = np.concatenate(loops) if loops else np.zeros((0, 3))
+        geo = [c["Sn"] + c["Gn"] + (c["xc0"] or [0, 0, 0]) + c["nA"] + [c["area"], c["Fn"]] + c["F_A"]
+               for c in man["contacts"]]
+        d[f"c{ci}_geom"] = np.asarray(geo, float).reshape(-1, 17)
+    d["ncase"] = np.array(n_cases)
+    np.savez_compressed(os.path.join(HERE, "polyline_split_ref.npz"), **d)
+
+
 CLI_CASES = [
     # (name, mesh A spec, mesh B spec, extra argv); a spec is a list of (subdivision, centre) blobs
     ("plain", [(2, (0, 0, 0))], [(2, (0, 0, 0))], ["--tB", "1.9e-3", "1e-4", "0", "--qB", "0.9", "0.1", "0.3", "0.2",
@@ -305,6 +381,8 @@ if __name__ == "__main__":
             make_sort(R)
     if want("polyline"):
         make_polyline()
+    if want("polyline_split"):
+        make_polyline_split()
     if want("vtk"):
         make_vtk()
     if want("cli"):

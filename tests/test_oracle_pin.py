@@ -117,3 +117,49 @@ def test_oracle_wall_and_integrate_live(oracle, ref):
         f, t, g = rng.normal(size=3), rng.normal(size=3), np.array([0.0, 0.0, -9.81])
         assert np.array_equal(ref.integrate(st, f, t, g, 1e-5)[:16], oracle.integrate(st, f, t, g, 1e-5)[:16])
     assert hits > 5
+
+
+@pytest.mark.parametrize("fixture,split", [("polyline_ref.npz", False), ("polyline_split_ref.npz", True)])
+def test_oracle_polyline_mode_matches_polyline_py(oracle, fixture, split):
+    """The oracle's polyline mode against polyline.py's own pipeline (polyline.py:743-822, with
+    --split-contacts for the second fixture): the same segment count, components (sizes in order),
+    loops (vertex counts, component of each) and loop points; the FP64 numbers within 1e-9 relative,
+    since polyline.py computes them with numpy."""
+    from _helpers import expected_contacts
+
+    z = np.load(os.path.join(GOLDEN, fixture))
+    for ci in range(int(z["ncase"])):
+        A, B, pose, tol = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], float(z[f"c{ci}_tol"])
+        r = oracle.pair(A, 0.0, 0.0, B, pose[:7], pose[7:], split=split, mode=1, tol=tol)
+        e = expected_contacts(r, polyline=True)
+        assert r["nseg"] == int(z[f"c{ci}_nseg"]), ci
+        lens = list(z[f"c{ci}_loop_len"])
+        assert list(e["nvert"]) == lens, ci
+        if split:
+            assert r["ncomp"] == int(z[f"c{ci}_ncomp"]), ci
+            assert list(np.diff(r["comp_off"])) == list(z[f"c{ci}_comp_sz"]), ci
+            assert list(e["comp"]) == list(z[f"c{ci}_loop_comp"]), ci
+        pts = np.split(z[f"c{ci}_loop_pts"], np.cumsum(lens)[:-1]) if lens else []
+        for c, p in enumerate(pts):
+            assert np.allclose(e["points"][c], p, rtol=1e-9, atol=1e-15), (ci, c)
+        ref = z[f"c{ci}_geom"]
+        for c in range(len(e["geom"])):
+            g = e["geom"][c]
+            Fn = 0.5 * 1e7 * g[12]
+            got = np.r_[g, Fn, Fn * g[9:12]]
+            assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)
+
+
+def test_pyset_order_matches_cpython(oracle):
+    """The oracle's restatement of CPython's set table (the order polyline.py visits a segment's
+    candidates in) against real sets of this interpreter: distinct ints added in a random order, small
+    and large, dense and sparse (collisions, linear probes, perturbed probes, resizes)."""
+    rng = np.random.default_rng(8)
+    for t in range(3000):
+        n = int(rng.integers(0, 400))
+        hi = int(rng.choice([16, 64, 500, 4000, 1 << 20]))
+        keys = list(dict.fromkeys(int(x) for x in rng.integers(0, hi, size=n)))
+        s = set()
+        for k in keys:
+            s.add(k)
+        assert list(oracle.pyset_order(keys)) == list(s), (t, keys[:10])

@@ -163,7 +163,37 @@ def test_polyline_mode_matches_oracle_and_python_reference(ctx, oracle):
             assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)
 
 
-@pytest.mark.parametrize("split,mode", [(True, 0), (False, 0), (False, 1)])
+def test_polyline_split_matches_oracle_and_python_reference(ctx, oracle):
+    """--split-contacts in polyline mode: components searched in the iteration order of polyline.py's
+    candidate sets, so loops start and run as polyline.py's do.  GPU == oracle bit for bit; against
+    polyline.py itself (tests/golden/polyline_split_ref.npz) the same components, loops and loop points,
+    numbers within 1e-9."""
+    from zdemx import polyline
+
+    z = np.load(os.path.join(GOLDEN, "polyline_split_ref.npz"))
+    for ci in range(int(z["ncase"])):
+        A, B, pose, tol = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], float(z[f"c{ci}_tol"])
+        man, loops, xc0s, cids = polyline.pair_contacts(A, B, pose[0:3], pose[3:7], pose[7:10], pose[10:14], k=1e7,
+                                                        tol=tol, split_contacts=True, ctx=ctx)
+        o = oracle.pair(A, 0.0, 0.0, B, pose[:7], pose[7:], split=True, mode=1, tol=tol)
+        e = expected_contacts(o, polyline=True)
+        assert len(man["contacts"]) == len(e["geom"]), ci
+        for c, cc in enumerate(man["contacts"]):
+            got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"]]
+            assert np.array_equal(got, e["geom"][c]), (ci, c)
+            assert np.array_equal(np.asarray(loops[c]), e["points"][c]), (ci, c)
+        lens = list(z[f"c{ci}_loop_len"])
+        assert [len(x) for x in loops] == lens, ci
+        pts = np.split(z[f"c{ci}_loop_pts"], np.cumsum(lens)[:-1])
+        for c, p in enumerate(pts):
+            assert np.allclose(np.asarray(loops[c]), p, rtol=1e-9, atol=1e-15), (ci, c)
+        ref = z[f"c{ci}_geom"]
+        for c, cc in enumerate(man["contacts"]):
+            got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"], cc["Fn"], cc["F_A"]]
+            assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)
+
+
+@pytest.mark.parametrize("split,mode", [(True, 0), (False, 0), (False, 1), (True, 1)])
 def test_large_pairs(ctx, oracle, split, mode):
     """Pairs of 1,280- and 5,120-triangle meshes (160 to 560 segments and up to 17 contacts a pair: long
     component searches, large snap classes, many T-junction candidates) against the oracle, bit for bit;

@@ -739,6 +739,136 @@ __device__ int uf_find_ro(const int* parent, int x) {
     return x;
 }
 
+// ---- polyline.py's candidate order
+// polyline.py collects the grid candidates of a segment into a Python set of ints and visits them in the
+// set's iteration order (polyline.py:293-303, 324), the slot order of CPython's open-addressing table
+// (CPython 3.12 Objects/setobject.c): hash(j) = j; a probe looks at slot i and, when i + 9 <= mask, the
+// 9 slots after it, then moves to i = (5 i + 1 + perturb) & mask with perturb = j shifted right by 5
+// each round; the table starts with 8 slots and, after an insert that makes used * 5 >= mask * 3, is
+// rebuilt at the smallest power of two above 4 x used with the old entries inserted again in slot
+// order.  The table is at most 60 % full, so a free slot is always found; the round limit only bounds
+// the loop.
+__device__ bool pyset_insert(int* tab, unsigned mask, int k) {
+    unsigned i = (unsigned)k & mask, perturb = (unsigned)k;
+    for (unsigned round = 0; round < 2u * (mask + 1u) + 8u; ++round) {
+        const unsigned probes = (i + 9u <= mask) ? 9u : 0u;
+        for (unsigned e = i; e <= i + probes; ++e)
+            if (tab[e] < 0) {
+                tab[e] = k;
+                return true;
+            }
+        perturb >>= 5;
+        i = (i * 5u + 1u + perturb) & mask;
+    }
+    return false;
+}
+
+// The table after inserting the n distinct keys (all >= 0) in order; returns its mask.  tab holds
+// 8 n + 8 ints, old n.
+__device__ unsigned pyset_build(const int* keys, int n, int* tab, int* old, bool* ok) {
+    unsigned mask = 7;
+    for (unsigned x = 0; x <= mask; ++x) tab[x] = -1;
+    for (int q = 0; q < n; ++q) {
+        *ok = pyset_insert(tab, mask, keys[q]) && *ok;
+        const unsigned used = (unsigned)q + 1u;
+        if (used * 5u >= mask * 3u) {
+            const unsigned minused = used > 50000u ? used * 2u : used * 4u;
+            unsigned size = 8;
+            while (size <= minused) size <<= 1;
+            int no = 0;
+            for (unsigned x = 0; x <= mask; ++x)
+                if (tab[x] >= 0) old[no++] = tab[x];
+            mask = size - 1u;
+            for (unsigned x = 0; x <= mask; ++x) tab[x] = -1;
+            for (int o = 0; o < no; ++o) *ok = pyset_insert(tab, mask, old[o]) && *ok;
+        }
+    }
+    return mask;
+}
+
+// One pop of polyline.py's component search for segment i (the whole warp): every grid candidate j
+// (some rep point of j in a cell next to one of i's, in the grid walk's order, as in the zdem search), the
+// accepted ones (not visited, padded boxes overlapping, seg_seg_dist2 <= tol2) pushed in the set's order.
+// Returns how many were pushed (on every lane).  The table lives in the snap's point buffer (12 n ints)
+// and its rebuild list in the union-find parents (2 n ints), both unused until the snap.
+__device__ __forceinline__ int py_neighbours(const PostBufs& B, const double* S, int n, int i, const I3* ci, V3 imn,
+                                             V3 imx, V3 p1, V3 q1, double tol2, int sp, int cnt, int lane,
+                                             int* status) {
+    int nc = 0;
+    for (int jb = 0; jb < n; jb += 32) {
+        const int j = jb + lane;
+        int best = 1 << 30;
+        bool acc = false;
+        if (j < n && j != i) {
+            for (int r = 0; r < 3; ++r)
+                for (int rj = 0; rj < 3; ++rj) {
+                    I3 cj = ld_cell(B.rcell + 9 * j + 3 * rj);
+                    int dx = cj.x - ci[r].x, dy = cj.y - ci[r].y, dz = cj.z - ci[r].z;
+                    if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+                    int k = r * 27 + (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+                    if (k < best) best = k;
+                }
+            if (best != (1 << 30) && !B.visited[j]) {
+                V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
+                bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y || imx.z < jmn.z ||
+                            imn.z > jmx.z);
+                acc = ov && seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2;
+            }
+        }
+        const bool cand = best != (1 << 30);
+        unsigned bal = __ballot_sync(FULL, cand);
+        if (cand) {
+            int pos = nc + __popc(bal & ((1u << lane) - 1u));
+            B.el_j[pos] = j;
+            B.el_k[pos] = best | (acc ? 0x10000 : 0);
+        }
+        nc += __popc(bal);
+    }
+    __syncwarp();
+    int nel = 0;
+    if (lane == 0 && nc > 0) {
+        // insertion order: (first grid key, then j); the scan gave j ascending
+        for (int x = 1; x < nc; ++x) {
+            int kj = B.el_j[x], kk = B.el_k[x], y = x - 1;
+            while (y >= 0 && (B.el_k[y] & 0xffff) > (kk & 0xffff)) {
+                B.el_j[y + 1] = B.el_j[y];
+                B.el_k[y + 1] = B.el_k[y];
+                --y;
+            }
+            B.el_j[y + 1] = kj;
+            B.el_k[y + 1] = kk;
+        }
+        for (int x = 0; x < nc; ++x)
+            if (B.el_k[x] & 0x10000) B.visited[B.el_j[x]] = 2;
+        int* tab = reinterpret_cast<int*>(B.pts);
+        bool ok = true;
+        const unsigned mask = pyset_build(B.el_j, nc, tab, B.parent, &ok);
+        if (!ok) *status |= PAIR_SET_PROBE;
+        for (unsigned x = 0; x <= mask; ++x) {
+            const int j = tab[x];
+            if (j >= 0 && B.visited[j] == 2) {
+                B.visited[j] = 1;
+                B.stack[sp + nel] = j;
+                B.raw_idx[cnt + nel] = j;
+                ++nel;
+            }
+        }
+        // an accepted candidate the table lost (only after a failed insert) is still pushed
+        for (int x = 0; x < nc; ++x) {
+            const int j = B.el_j[x];
+            if (B.visited[j] == 2) {
+                B.visited[j] = 1;
+                B.stack[sp + nel] = j;
+                B.raw_idx[cnt + nel] = j;
+                ++nel;
+            }
+        }
+    }
+    nel = __shfl_sync(FULL, nel, 0);
+    __syncwarp();
+    return nel;
+}
+
 // The post-triangle part of the reference's per-pair body (src/main.cpp:2148-2219) for one pair, by
 // one warp.  Component / loop / contact order follows the reference exactly.
 __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, const int lane) {
@@ -795,55 +925,60 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     for (int r = 0; r < 3; ++r) ci[r] = ld_cell(B.rcell + 9 * i + 3 * r);
                     const V3 imn = ld3(B.bmn + 3 * i), imx = ld3(B.bmx + 3 * i);
                     int nel = 0;
-                    for (int jb = 0; jb < n; jb += 32) {
-                        const int j = jb + lane;
-                        bool el = false;
-                        int best = 1 << 30;
-                        if (j < n && j != i && !B.visited[j]) {
-                            // the padded-box overlap is necessary too; test it first (cheapest reject)
-                            V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
-                            bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y ||
-                                        imx.z < jmn.z || imn.z > jmx.z);
-                            if (ov) {
-                                // first visit of j in the reference's hash-grid walk: smallest
-                                // r*27 + neighbour-cell rank over the rep points (p0, p1, mid)
-                                for (int r = 0; r < 3; ++r)
-                                    for (int rj = 0; rj < 3; ++rj) {
-                                        I3 cj = ld_cell(B.rcell + 9 * j + 3 * rj);
-                                        int dx = cj.x - ci[r].x, dy = cj.y - ci[r].y, dz = cj.z - ci[r].z;
-                                        if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
-                                        int k = r * 27 + (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
-                                        if (k < best) best = k;
-                                    }
-                                if (best != (1 << 30) && seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2)
-                                    el = true;
+                    if (py) {
+                        nel = py_neighbours(B, S, n, i, ci, imn, imx, p1, q1, tol2, sp, cnt, lane, &status);
+                    } else {
+                        for (int jb = 0; jb < n; jb += 32) {
+                            const int j = jb + lane;
+                            bool el = false;
+                            int best = 1 << 30;
+                            if (j < n && j != i && !B.visited[j]) {
+                                // the padded-box overlap is necessary too; test it first (cheapest reject)
+                                V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
+                                bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y ||
+                                            imx.z < jmn.z || imn.z > jmx.z);
+                                if (ov) {
+                                    // first visit of j in the reference's hash-grid walk: smallest
+                                    // r*27 + neighbour-cell rank over the rep points (p0, p1, mid)
+                                    for (int r = 0; r < 3; ++r)
+                                        for (int rj = 0; rj < 3; ++rj) {
+                                            I3 cj = ld_cell(B.rcell + 9 * j + 3 * rj);
+                                            int dx = cj.x - ci[r].x, dy = cj.y - ci[r].y, dz = cj.z - ci[r].z;
+                                            if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+                                            int k = r * 27 + (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+                                            if (k < best) best = k;
+                                        }
+                                    if (best != (1 << 30) &&
+                                        seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2)
+                                        el = true;
+                                }
                             }
-                        }
-                        unsigned bal = __ballot_sync(FULL, el);
-                        if (el) {
-                            int pos = nel + __popc(bal & ((1u << lane) - 1u));
-                            B.el_j[pos] = j;
-                            B.el_k[pos] = best;
-                        }
-                        nel += __popc(bal);
-                    }
-                    __syncwarp();
-                    if (lane == 0) {
-                        for (int x = 1; x < nel; ++x) {
-                            int kj = B.el_j[x], kk = B.el_k[x], y = x - 1;
-                            while (y >= 0 && B.el_k[y] > kk) {
-                                B.el_j[y + 1] = B.el_j[y];
-                                B.el_k[y + 1] = B.el_k[y];
-                                --y;
+                            unsigned bal = __ballot_sync(FULL, el);
+                            if (el) {
+                                int pos = nel + __popc(bal & ((1u << lane) - 1u));
+                                B.el_j[pos] = j;
+                                B.el_k[pos] = best;
                             }
-                            B.el_j[y + 1] = kj;
-                            B.el_k[y + 1] = kk;
+                            nel += __popc(bal);
                         }
-                        for (int x = 0; x < nel; ++x) {
-                            int j = B.el_j[x];
-                            B.visited[j] = 1;
-                            B.stack[sp + x] = j;
-                            B.raw_idx[cnt + x] = j;
+                        __syncwarp();
+                        if (lane == 0) {
+                            for (int x = 1; x < nel; ++x) {
+                                int kj = B.el_j[x], kk = B.el_k[x], y = x - 1;
+                                while (y >= 0 && B.el_k[y] > kk) {
+                                    B.el_j[y + 1] = B.el_j[y];
+                                    B.el_k[y + 1] = B.el_k[y];
+                                    --y;
+                                }
+                                B.el_j[y + 1] = kj;
+                                B.el_k[y + 1] = kk;
+                            }
+                            for (int x = 0; x < nel; ++x) {
+                                int j = B.el_j[x];
+                                B.visited[j] = 1;
+                                B.stack[sp + x] = j;
+                                B.raw_idx[cnt + x] = j;
+                            }
                         }
                     }
                     sp += nel;

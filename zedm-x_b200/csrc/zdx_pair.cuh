@@ -13,6 +13,7 @@ enum : int {
     PAIR_EDGE_OVERFLOW = 2,  // the T-junction split produced more edges than the rebuild slot holds
     PAIR_TAPE_OVERFLOW = 4,  // the adjoint tape of the pair did not fit its slot
     PAIR_NO_ARENA = 8,       // the pair's segments did not fit the call's segment arena (not rebuilt)
+    PAIR_SET_PROBE = 16,     // polyline mode's set-order table found no free slot (not expected)
 };
 // Call-wide error bits (*err).
 enum : int {

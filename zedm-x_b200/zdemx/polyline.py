@@ -9,9 +9,9 @@ Sn/Gn/xc0 and the minimal law Fn = k/2 |Sn|) runs in libzdemx.so; there is no CP
 Semantics follow polyline.py, not zdem_cpu: the tolerance is the --tol argument (default 1e-6), loops
 are dropped when shorter than 3 vertices or when their bounding-box diagonal is below 2 tol, sorts are
 stable, nA = -Sn/|Sn| is not flipped, and a loop with |Sn| < 1e-14 is still a contact with xc0 None.
-The one order polyline.py leaves to CPython (iteration of a ``set`` of candidate segments when
---split-contacts is on) is replaced by the C++ program's grid order; it only changes vertex numbering
-inside a component, never which loops are found.
+With --split-contacts, polyline.py visits each segment's candidates in the iteration order of a Python
+set of ints; the kernel rebuilds CPython 3.12's set table to visit them in the same order, so loops
+start, run and are numbered as polyline.py's.
 """
 from __future__ import annotations
 
