@@ -22,6 +22,9 @@ the tests that use them never touch the reference.
 
 * polyline_split_ref.npz  the same pipeline with --split-contacts (label_segments_by_contact_greedy,
                      polyline.py:267-368) on pairs whose contact splits into several components.
+* polyline_hard_ref.npz   the same pipeline, with and without the split, on flat faces and sharp edges:
+                     offset, coplanar, rotated and tilted cubes, a sphere in a face and on an edge,
+                     hulls, a T-junction in a mesh, grazing spheres.
 
 `python tests/golden/make_golden.py vtk` regenerates only the named fixtures.
 """
@@ -232,6 +235,58 @@ def make_vtk():
     np.savez_compressed(os.path.join(HERE, "vtk_ref.npz"), **d)
 
 
+def polyline_pipeline(P, A, B, pose, tol, split):
+    """polyline.py main's pipeline (polyline.py:743-822) on mesh-local triangles A, B at pose (14 values),
+    recorded as the fixture fields of one case."""
+    trisA = P.transform_points(A.reshape(-1, 3), pose[0:3], pose[3:7]).reshape(-1, 3, 3)
+    trisB = P.transform_points(B.reshape(-1, 3), pose[7:10], pose[10:14]).reshape(-1, 3, 3)
+    nA_all, nB_all = P.tri_normals(trisA), P.tri_normals(trisB)
+    planesA = [P.plane_from_tri(trisA[i]) for i in range(len(trisA))]
+    planesB = [P.plane_from_tri(trisB[i]) for i in range(len(trisB))]
+    aminA, amaxA = trisA.min(axis=1), trisA.max(axis=1)
+    aminB, amaxB = trisB.min(axis=1), trisB.max(axis=1)
+    segs = []
+    for i in range(len(trisA)):
+        nAi, dAi = planesA[i]
+        if nAi is None:
+            continue
+        for j in range(len(trisB)):
+            if (amaxA[i, 0] < aminB[j, 0] or aminA[i, 0] > amaxB[j, 0] or amaxA[i, 1] < aminB[j, 1] or
+                    aminA[i, 1] > amaxB[j, 1] or amaxA[i, 2] < aminB[j, 2] or aminA[i, 2] > amaxB[j, 2]):
+                continue
+            nBj, dBj = planesB[j]
+            if nBj is None:
+                continue
+            sg = P.tri_tri_intersection_segment(trisA[i], nA_all[i], dAi, trisB[j], nB_all[j], dBj)
+            if sg is not None:
+                segs.append(sg)
+    if split:
+        _, ncomp, comps = P.label_segments_by_contact_greedy(segs, tol=tol) if segs else (None, 0, [])
+    else:
+        ncomp, comps = (1, [list(range(len(segs)))]) if segs else (0, [])
+    loops, comp_of, comp_sz = [], [], []
+    for c, comp in enumerate(comps):
+        comp_sz.append(len(comp))
+        V, E = P.snap_endpoints([segs[i] for i in comp], tol=tol)
+        V2, E2 = P.split_t_junctions(V, E, tol=tol)
+        for lv in P.extract_loops(V2, E2):
+            if len(lv) < 3:
+                continue
+            pts = [V2[i] for i in lv]
+            if np.linalg.norm(np.max(pts, axis=0) - np.min(pts, axis=0)) < tol * 2:
+                continue
+            loops.append(np.asarray(pts))
+            comp_of.append(c)
+    man = P.build_contacts_from_loops(0, 1, loops, list(range(len(loops))), k_stiff=1e7)
+    geo = [c["Sn"] + c["Gn"] + (c["xc0"] or [0, 0, 0]) + c["nA"] + [c["area"], c["Fn"]] + c["F_A"]
+           for c in man["contacts"]]
+    return {"A": A, "B": B, "pose": pose, "tol": np.array(tol), "split": np.array(int(split)),
+            "nseg": np.array(len(segs)), "ncomp": np.array(ncomp), "comp_sz": np.array(comp_sz, np.int64),
+            "loop_comp": np.array(comp_of, np.int64), "loop_len": np.array([len(x) for x in loops], np.int64),
+            "loop_pts": np.concatenate(loops) if loops else np.zeros((0, 3)),
+            "geom": np.asarray(geo, float).reshape(-1, 17)}
+
+
 def make_polyline_split():
     sys.path.insert(0, REF_PY)
     import polyline as P  # the reference module, imported read-only
@@ -250,59 +305,74 @@ def make_polyline_split():
         B = np.concatenate(blobs)
         q = synth.random_unit_quat(rng)
         pose = np.r_[rng.normal(size=3) * 1e-5, q, np.zeros(3), [1.0, 0.0, 0.0, 0.0]]
-        tol = 1e-5
-        trisA = P.transform_points(A.reshape(-1, 3), pose[0:3], pose[3:7]).reshape(-1, 3, 3)
-        trisB = P.transform_points(B.reshape(-1, 3), pose[7:10], pose[10:14]).reshape(-1, 3, 3)
-        nA_all, nB_all = P.tri_normals(trisA), P.tri_normals(trisB)
-        planesA = [P.plane_from_tri(trisA[i]) for i in range(len(trisA))]
-        planesB = [P.plane_from_tri(trisB[i]) for i in range(len(trisB))]
-        aminA, amaxA = trisA.min(axis=1), trisA.max(axis=1)
-        aminB, amaxB = trisB.min(axis=1), trisB.max(axis=1)
-        segs = []
-        for i in range(len(trisA)):
-            nAi, dAi = planesA[i]
-            if nAi is None:
-                continue
-            for j in range(len(trisB)):
-                if (amaxA[i, 0] < aminB[j, 0] or aminA[i, 0] > amaxB[j, 0] or amaxA[i, 1] < aminB[j, 1] or
-                        aminA[i, 1] > amaxB[j, 1] or amaxA[i, 2] < aminB[j, 2] or aminA[i, 2] > amaxB[j, 2]):
-                    continue
-                nBj, dBj = planesB[j]
-                if nBj is None:
-                    continue
-                sg = P.tri_tri_intersection_segment(trisA[i], nA_all[i], dAi, trisB[j], nB_all[j], dBj)
-                if sg is not None:
-                    segs.append(sg)
-        _, ncomp, comps = P.label_segments_by_contact_greedy(segs, tol=tol) if segs else (None, 0, [])
-        loops, comp_of, comp_sz = [], [], []
-        for c, comp in enumerate(comps):
-            comp_sz.append(len(comp))
-            V, E = P.snap_endpoints([segs[i] for i in comp], tol=tol)
-            V2, E2 = P.split_t_junctions(V, E, tol=tol)
-            for lv in P.extract_loops(V2, E2):
-                if len(lv) < 3:
-                    continue
-                pts = [V2[i] for i in lv]
-                if np.linalg.norm(np.max(pts, axis=0) - np.min(pts, axis=0)) < tol * 2:
-                    continue
-                loops.append(np.asarray(pts))
-                comp_of.append(c)
-        man = P.build_contacts_from_loops(0, 1, loops, list(range(len(loops))), k_stiff=1e7)
-        d[f"c{ci}_A"] = A
-        d[f"c{ci}_B"] = B
-        d[f"c{ci}_pose"] = pose
-        d[f"c{ci}_tol"] = np.array(tol)
-        d[f"c{ci}_nseg"] = np.array(len(segs))
-        d[f"c{ci}_ncomp"] = np.array(ncomp)
-        d[f"c{ci}_comp_sz"] = np.array(comp_sz, np.int64)
-        d[f"c{ci}_loop_comp"] = np.array(comp_of, np.int64)
-        d[f"c{ci}_loop_len"] = np.array([len(x) for x in loops], np.int64)
-        d[f"c{ci}_loop_pts"] = np.concatenate(loops) if loops else np.zeros((0, 3))
-        geo = [c["Sn"] + c["Gn"] + (c["xc0"] or [0, 0, 0]) + c["nA"] + [c["area"], c["Fn"]] + c["F_A"]
-               for c in man["contacts"]]
-        d[f"c{ci}_geom"] = np.asarray(geo, float).reshape(-1, 17)
+        for k, v in polyline_pipeline(P, A, B, pose, 1e-5, True).items():
+            if k != "split":
+                d[f"c{ci}_{k}"] = v
     d["ncase"] = np.array(n_cases)
     np.savez_compressed(os.path.join(HERE, "polyline_split_ref.npz"), **d)
+
+
+def _t_junction_box(a):
+    """A cube of side a whose top face has a T-junction: one of its two triangles is split at the
+    midpoint of the shared diagonal, the other is not."""
+    from _dem_helpers import box_tris
+
+    tris = [t for t in box_tris(a, a, a) if not np.allclose(t[:, 2], a / 2)]
+    h = a / 2
+    v0, v1, v2, v3 = np.array([[-h, -h, h], [h, -h, h], [h, h, h], [-h, h, h]])
+    m = (v0 + v2) / 2
+    tris += [np.array([v0, v1, m]), np.array([m, v1, v2]), np.array([v0, v2, v3])]
+    return np.asarray(tris)
+
+
+def _hard_cases(rng):
+    """(name, A, B, pose, tol, split): contacts of flat faces and sharp edges, where segments meet at
+    triangle corners, run along edges or lie in coplanar faces."""
+    from _dem_helpers import box_tris
+
+    a = 1e-3
+    cube = box_tris(a, a, a)
+    ident = [1.0, 0.0, 0.0, 0.0]
+    qz45 = [np.cos(np.pi / 8), 0.0, 0.0, np.sin(np.pi / 8)]
+    qtilt = synth.random_unit_quat(rng)
+    sphere = synth.noised_icosphere(2, 0.6e-3, 0.0, rng)
+    rough = synth.noised_icosphere(2, 0.6e-3, 0.15, rng)
+    hullA = synth.ellipsoid_hull(64, (1.0, 0.8, 0.6), 1e-3, rng)
+    hullB = synth.ellipsoid_hull(64, (1.0, 0.8, 0.6), 1e-3, rng)
+    tbox = _t_junction_box(a)
+    P = lambda tA, qA, tB, qB: np.r_[tA, qA, tB, qB].astype(float)
+    cases = [
+        ("cubes_offset", cube, cube, P([0, 0, 0], ident, [0.6 * a, 0.3 * a, 0.2 * a], ident)),
+        ("cubes_coplanar", cube, cube, P([0, 0, 0], ident, [0.5 * a, 0, 0], ident)),
+        ("cubes_rotated", cube, cube, P([0, 0, 0], ident, [0.8 * a, 0.1 * a, 0.05 * a], qz45)),
+        ("cubes_tilted", cube, cube, P([0, 0, 0], ident, [0.9 * a, 0.2 * a, -0.1 * a], qtilt)),
+        ("sphere_in_cube_face", cube, sphere, P([0, 0, 0], ident, [0.0, 0.0, 0.9e-3], ident)),
+        ("sphere_on_cube_edge", cube, rough, P([0, 0, 0], ident, [0.85e-3, 0.0, 0.85e-3], qtilt)),
+        ("hulls", hullA, hullB, P([0, 0, 0], ident, [1.7e-3, 0.2e-3, 0.0], qtilt)),
+        ("t_junction_box", tbox, sphere, P([0, 0, 0], ident, [0.05e-3, 0.05e-3, 0.95e-3], ident)),
+        ("grazing_spheres", rough, sphere, P([0, 0, 0], ident, [0.0, 0.0, 1.1995e-3], qtilt)),
+    ]
+    out = []
+    for name, A, B, pose in cases:
+        for tol, split in ((1e-6, False), (1e-5, True)):
+            out.append((name, A, B, pose, tol, split))
+    return out
+
+
+def make_polyline_hard():
+    sys.path.insert(0, REF_PY)
+    sys.path.insert(0, os.path.dirname(HERE))
+    import polyline as P  # the reference module, imported read-only
+
+    rng = np.random.default_rng(321)
+    d = {}
+    cases = _hard_cases(rng)
+    for ci, (name, A, B, pose, tol, split) in enumerate(cases):
+        d[f"c{ci}_name"] = np.array(name)
+        for k, v in polyline_pipeline(P, np.asarray(A, float), np.asarray(B, float), pose, tol, split).items():
+            d[f"c{ci}_{k}"] = v
+    d["ncase"] = np.array(len(cases))
+    np.savez_compressed(os.path.join(HERE, "polyline_hard_ref.npz"), **d)
 
 
 CLI_CASES = [
@@ -383,6 +453,8 @@ if __name__ == "__main__":
         make_polyline()
     if want("polyline_split"):
         make_polyline_split()
+    if want("polyline_hard"):
+        make_polyline_hard()
     if want("vtk"):
         make_vtk()
     if want("cli"):

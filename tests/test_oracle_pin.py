@@ -119,17 +119,21 @@ def test_oracle_wall_and_integrate_live(oracle, ref):
     assert hits > 5
 
 
-@pytest.mark.parametrize("fixture,split", [("polyline_ref.npz", False), ("polyline_split_ref.npz", True)])
+@pytest.mark.parametrize("fixture,split", [("polyline_ref.npz", False), ("polyline_split_ref.npz", True),
+                                           ("polyline_hard_ref.npz", None)])
 def test_oracle_polyline_mode_matches_polyline_py(oracle, fixture, split):
     """The oracle's polyline mode against polyline.py's own pipeline (polyline.py:743-822, with
-    --split-contacts for the second fixture): the same segment count, components (sizes in order),
-    loops (vertex counts, component of each) and loop points; the FP64 numbers within 1e-9 relative,
-    since polyline.py computes them with numpy."""
+    --split-contacts for the second fixture and per case for the third, whose cases are flat faces and
+    sharp edges): the same segment count, components (sizes in order), loops (vertex counts, component
+    of each) and loop points; the FP64 numbers within 1e-9 relative, since polyline.py computes them
+    with numpy."""
     from _helpers import expected_contacts
 
     z = np.load(os.path.join(GOLDEN, fixture))
     for ci in range(int(z["ncase"])):
         A, B, pose, tol = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], float(z[f"c{ci}_tol"])
+        if fixture == "polyline_hard_ref.npz":
+            split = bool(z[f"c{ci}_split"])
         r = oracle.pair(A, 0.0, 0.0, B, pose[:7], pose[7:], split=split, mode=1, tol=tol)
         e = expected_contacts(r, polyline=True)
         assert r["nseg"] == int(z[f"c{ci}_nseg"]), ci
@@ -163,3 +167,43 @@ def test_pyset_order_matches_cpython(oracle):
         for k in keys:
             s.add(k)
         assert list(oracle.pyset_order(keys)) == list(s), (t, keys[:10])
+
+
+def test_oracle_matches_reference_flat_shapes(oracle, ref):
+    """zdem mode on flat faces and sharp edges against the reference C++ itself, bit for bit: offset,
+    coplanar, rotated and tilted cubes, spheres in a face and on an edge, hulls, a mesh with a
+    T-junction, grazing spheres; with and without the split."""
+    from _dem_helpers import box_tris
+    from zdemx import synth
+
+    rng = np.random.default_rng(321)
+    a = 1e-3
+    cube = box_tris(a, a, a)
+    h = a / 2
+    v0, v1, v2, v3 = np.array([[-h, -h, h], [h, -h, h], [h, h, h], [-h, h, h]])
+    m = (v0 + v2) / 2
+    tbox = np.asarray([t for t in cube if not np.allclose(t[:, 2], h)] +
+                      [np.array([v0, v1, m]), np.array([m, v1, v2]), np.array([v0, v2, v3])])
+    ident = [1.0, 0.0, 0.0, 0.0]
+    qz45 = [np.cos(np.pi / 8), 0.0, 0.0, np.sin(np.pi / 8)]
+    qtilt = synth.random_unit_quat(rng)
+    sphere = synth.noised_icosphere(2, 0.6e-3, 0.0, rng)
+    rough = synth.noised_icosphere(2, 0.6e-3, 0.15, rng)
+    hullA = synth.ellipsoid_hull(64, (1.0, 0.8, 0.6), 1e-3, rng)
+    hullB = synth.ellipsoid_hull(64, (1.0, 0.8, 0.6), 1e-3, rng)
+    cases = [(cube, cube, [0.6 * a, 0.3 * a, 0.2 * a], ident), (cube, cube, [0.5 * a, 0, 0], ident),
+             (cube, cube, [0.8 * a, 0.1 * a, 0.05 * a], qz45), (cube, cube, [0.9 * a, 0.2 * a, -0.1 * a], qtilt),
+             (cube, sphere, [0.0, 0.0, 0.9e-3], ident), (cube, rough, [0.85e-3, 0.0, 0.85e-3], qtilt),
+             (hullA, hullB, [1.7e-3, 0.2e-3, 0.0], qtilt), (tbox, sphere, [0.05e-3, 0.05e-3, 0.95e-3], ident),
+             (rough, sphere, [0.0, 0.0, 1.1995e-3], qtilt)]
+    contacts = 0
+    for k, (A, B, tB, qB) in enumerate(cases):
+        Ab, pA = ref.build_mesh(np.asarray(A, float))
+        Bb, pB = ref.build_mesh(np.asarray(B, float))
+        poseA, poseB = np.r_[0.0, 0.0, 0.0, ident], np.r_[tB, qB].astype(float)
+        for split in (False, True):
+            r = ref.pair(Ab, pA[5], pA[6], Bb, poseA, poseB, split=split)
+            o = oracle.pair(Ab, pA[5], pA[6], Bb, poseA, poseB, split=split)
+            assert compare_pair(r, o, exact=True) == [], (k, split)
+            contacts += r["nloop"]
+    assert contacts >= 10
