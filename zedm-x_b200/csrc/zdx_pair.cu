@@ -20,6 +20,7 @@
 
 #include "zdx_math.cuh"
 #include "zdx_pair.cuh"
+#include "zdx_pyset.cuh"
 #include "zdx_radix.cuh"
 #include "zdx_sortrep.cuh"
 
@@ -739,58 +740,13 @@ __device__ int uf_find_ro(const int* parent, int x) {
     return x;
 }
 
-// ---- polyline.py's candidate order
-// polyline.py collects the grid candidates of a segment into a Python set of ints and visits them in the
-// set's iteration order (polyline.py:293-303, 324), the slot order of CPython's open-addressing table
-// (CPython 3.12 Objects/setobject.c): hash(j) = j; a probe looks at slot i and, when i + 9 <= mask, the
-// 9 slots after it, then moves to i = (5 i + 1 + perturb) & mask with perturb = j shifted right by 5
-// each round; the table starts with 8 slots and, after an insert that makes used * 5 >= mask * 3, is
-// rebuilt at the smallest power of two above 4 x used with the old entries inserted again in slot
-// order.  The table is at most 60 % full, so a free slot is always found; the round limit only bounds
-// the loop.
-__device__ bool pyset_insert(int* tab, unsigned mask, int k) {
-    unsigned i = (unsigned)k & mask, perturb = (unsigned)k;
-    for (unsigned round = 0; round < 2u * (mask + 1u) + 8u; ++round) {
-        const unsigned probes = (i + 9u <= mask) ? 9u : 0u;
-        for (unsigned e = i; e <= i + probes; ++e)
-            if (tab[e] < 0) {
-                tab[e] = k;
-                return true;
-            }
-        perturb >>= 5;
-        i = (i * 5u + 1u + perturb) & mask;
-    }
-    return false;
-}
-
-// The table after inserting the n distinct keys (all >= 0) in order; returns its mask.  tab holds
-// 8 n + 8 ints, old n.
-__device__ unsigned pyset_build(const int* keys, int n, int* tab, int* old, bool* ok) {
-    unsigned mask = 7;
-    for (unsigned x = 0; x <= mask; ++x) tab[x] = -1;
-    for (int q = 0; q < n; ++q) {
-        *ok = pyset_insert(tab, mask, keys[q]) && *ok;
-        const unsigned used = (unsigned)q + 1u;
-        if (used * 5u >= mask * 3u) {
-            const unsigned minused = used > 50000u ? used * 2u : used * 4u;
-            unsigned size = 8;
-            while (size <= minused) size <<= 1;
-            int no = 0;
-            for (unsigned x = 0; x <= mask; ++x)
-                if (tab[x] >= 0) old[no++] = tab[x];
-            mask = size - 1u;
-            for (unsigned x = 0; x <= mask; ++x) tab[x] = -1;
-            for (int o = 0; o < no; ++o) *ok = pyset_insert(tab, mask, old[o]) && *ok;
-        }
-    }
-    return mask;
-}
-
 // One pop of polyline.py's component search for segment i (the whole warp): every grid candidate j
 // (some rep point of j in a cell next to one of i's, in the grid walk's order, as in the zdem search), the
 // accepted ones (not visited, padded boxes overlapping, seg_seg_dist2 <= tol2) pushed in the set's order.
-// Returns how many were pushed (on every lane).  The table lives in the snap's point buffer (12 n ints)
-// and its rebuild list in the union-find parents (2 n ints), both unused until the snap.
+// Returns how many were pushed (on every lane).  The set's table (zdx_pyset.cuh) lives in the snap's
+// point buffer (12 n ints) and its rebuild list in the union-find parents (2 n ints), both unused until
+// the snap.  Lane 0 orders the candidates by an insertion sort, O(nc^2) for nc candidates: fine for the
+// tens a pop has when tol is small against the segments, slow when tol spans many of them.
 __device__ __forceinline__ int py_neighbours(const PostBufs& B, const double* S, int n, int i, const I3* ci, V3 imn,
                                              V3 imx, V3 p1, V3 q1, double tol2, int sp, int cnt, int lane,
                                              int* status) {
