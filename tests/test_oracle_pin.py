@@ -207,3 +207,47 @@ def test_oracle_matches_reference_flat_shapes(oracle, ref):
             assert compare_pair(r, o, exact=True) == [], (k, split)
             contacts += r["nloop"]
     assert contacts >= 10
+
+
+def test_oracle_wall_contact_flat_shapes(oracle, ref):
+    """compute_wall_contact (src/main.cpp:1205-1258: plane section, Sutherland-Hodgman clip, area and
+    centroid) on degenerate sections, against the reference C++ bit for bit: a cube face-down on the
+    wall plane (coplanar with it, and just above and below), on an edge, on a corner, tilted, a cube
+    straddling the wall triangle's edge, and icospheres touching at a vertex."""
+    from _dem_helpers import box_tris
+    from zdemx import synth
+
+    rng = np.random.default_rng(9)
+    a = 1e-3
+    cube, cp = ref.build_mesh(box_tris(a, a, a))
+    ball, bp = ref.build_mesh(synth.noised_icosphere(1, 1e-3, 0.0, rng))
+    wall = np.array([-0.01, -0.01, 0.0, 0.01, -0.01, 0.0, 0.01, 0.01, 0.0])
+    small = np.array([-4e-4, -4e-4, 0.0, 4e-4, -4e-4, 0.0, -4e-4, 4e-4, 0.0])  # edge under the cube
+    wn = np.array([0.0, 0.0, 1.0])
+    q_edge = [np.cos(np.pi / 8), np.sin(np.pi / 8), 0.0, 0.0]  # 45 deg about x: an edge down
+    v = np.array([1.0, 1.0, 0.0]) / np.sqrt(2.0)
+    ang = np.arccos(1.0 / np.sqrt(3.0))  # a body diagonal down: a corner
+    q_corner = [np.cos(ang / 2), *(np.sin(ang / 2) * v)]
+    ident = [1.0, 0.0, 0.0, 0.0]
+    h = a / 2
+    poses = []
+    for dz in (0.0, 1e-9, -1e-9, -1e-5, -1e-4):
+        poses.append((cube, cp, [0.0, 0.0, h + dz], ident, wall))
+        poses.append((cube, cp, [1e-4, -2e-4, h + dz], ident, small))
+    for dz in (0.0, -1e-6, -5e-5):
+        poses.append((cube, cp, [0.0, 0.0, h * np.sqrt(2.0) + dz], q_edge, wall))
+        poses.append((cube, cp, [0.0, 0.0, h * np.sqrt(3.0) + dz], q_corner, wall))
+    for _ in range(8):
+        poses.append((cube, cp, [0.0, 0.0, h * rng.uniform(0.9, 1.6)], list(synth.random_unit_quat(rng)), wall))
+    poses.append((ball, bp, [0.0, 0.0, 1e-3 - 1e-7], ident, wall))
+    poses.append((ball, bp, [0.0, 0.0, 1e-3], ident, wall))
+    hits = 0
+    for k, (tris, props, t, q, wt) in enumerate(poses):
+        pose = np.r_[t, q].astype(float)
+        ra = ref.wall_contact(tris, pose, wt, wn, props[4], props[5] * 0.1)
+        rb = oracle.wall_contact(tris, pose, wt, wn, props[4], props[5] * 0.1)
+        assert ra[0] == rb[0], k
+        if ra[0]:
+            hits += 1
+            assert ra[1] == rb[1] and np.array_equal(ra[2], rb[2]) and np.array_equal(ra[3], rb[3]), k
+    assert hits >= 12
