@@ -1,6 +1,7 @@
-"""The polyline mirror's two VTK writers against the text polyline.py's own writers gave for the same
-inputs (polyline.py:544-649; fixture tests/golden/vtk_ref.npz): byte for byte, including the 1e-9 point
-merge, skipped one-point loops, None contact points and contact lists shorter than the loop list."""
+"""The polyline mirror's host code against polyline.py's own: its two VTK writers against the text
+polyline.py's writers gave for the same inputs (polyline.py:544-649; fixture tests/golden/vtk_ref.npz),
+byte for byte, including the 1e-9 point merge, skipped one-point loops, None contact points and contact
+lists shorter than the loop list; and build_contacts_from_loops on polyline.py's traced loops."""
 import os
 
 import numpy as np
@@ -42,3 +43,23 @@ def test_triangle_writer_matches_reference_text(tmp_path):
         polyline.write_vtk_polydata_tris(out, z[f"t{ti}_tris"], comment=f"mesh {ti}")
         with open(out, encoding="utf-8") as f:
             assert f.read() == str(z[f"t{ti}_text"]), ti
+
+
+def test_build_contacts_from_loops_matches_reference_bit_for_bit():
+    """The mirror's host build_contacts_from_loops (polyline.py:655-701, for loops a caller already holds)
+    on the loops polyline.py traced in the three polyline fixtures: the same numpy expressions, so Sn,
+    Gn, xc0, nA, |Sn|, Fn and F_A are identical to the bit."""
+    from zdemx import polyline
+
+    n = 0
+    for fixture in ("polyline_ref.npz", "polyline_split_ref.npz", "polyline_hard_ref.npz"):
+        z = np.load(os.path.join(GOLDEN, fixture))
+        for ci in range(int(z["ncase"])):
+            lens = list(z[f"c{ci}_loop_len"])
+            loops = np.split(z[f"c{ci}_loop_pts"], np.cumsum(lens)[:-1]) if lens else []
+            man = polyline.build_contacts_from_loops(0, 1, loops, list(range(len(loops))), k_stiff=1e7)
+            geo = np.asarray([c["Sn"] + c["Gn"] + (c["xc0"] or [0, 0, 0]) + c["nA"] + [c["area"], c["Fn"]] +
+                              c["F_A"] for c in man["contacts"]], float).reshape(-1, 17)
+            assert np.array_equal(geo, z[f"c{ci}_geom"]), (fixture, ci)
+            n += len(geo)
+    assert n >= 40
