@@ -469,7 +469,7 @@ static double seg_seg_dist2(V3 p1, V3 q1, V3 p2, V3 q2) {
  * then i = (5 i + 1 + perturb) & mask with perturb = j shifted right by 5 each round; after an insert
  * that makes fill * 5 >= mask * 3 the table is rebuilt at the smallest power of two above 4 x used,
  * the old entries inserted again in slot order).  polyline.py iterates such a set of candidate
- * segments (polyline.py:293-303, 324).  tab needs 8 n + 8 ints, old n + 1; out receives the keys. */
+ * segments (polyline.py:288-299, 324).  tab needs 8 n + 8 ints, old n + 1; out receives the keys. */
 static void pyset_insert(int* tab, unsigned mask, int k) {
     unsigned i = (unsigned)k & mask;
     unsigned perturb = (unsigned)k;

@@ -1,6 +1,6 @@
 """The rebuild kernel's polyline-mode candidate order (zedm-x_b200/csrc/zdx_pyset.cuh), host build,
 against this interpreter itself: the slot order of a CPython set of ints built by adding distinct keys
-(polyline.py:293-303, 324)."""
+(polyline.py:288-299, 324)."""
 import os
 import shutil
 import subprocess

@@ -2,7 +2,7 @@
 // segments into components (label_segments_by_contact_greedy, polyline.py:267-368), for the polyline
 // mode of the rebuild kernel.  Host and device code; the host build is what the CPU tests check.
 //
-// polyline.py adds the grid candidates of a segment to a Python set of ints (polyline.py:293-303) and
+// polyline.py adds the grid candidates of a segment to a Python set of ints (polyline.py:288-299) and
 // iterates the set (:324).  CPython's set iterates its open-addressing table in slot order (CPython 3.12
 // Objects/setobject.c): hash(j) = j; a probe looks at slot i and, when i + 9 <= mask, the 9 slots after
 // it, then moves to i = (5 i + 1 + perturb) & mask with perturb = j shifted right by 5 each round; the
