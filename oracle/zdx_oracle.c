@@ -519,7 +519,7 @@ int zo_pyset_order(const int* keys, int n, int* out) {
     return n;
 }
 
-/* label_segments_by_contact_greedy, src/main.cpp:804-898 (polyline.py:267-368).  The reference visits
+/* label_segments_by_contact_greedy, src/main.cpp:804-898 (polyline.py:267-341).  The reference visits
  * the candidates of segment i in hash-grid order: rep point r of i (p0, p1, mid), then the 27
  * neighbour cells in dx,dy,dz order, then the cell's list in insertion order.  That order is exactly
  * (smallest r*27+cell-offset over all rep points of j, then j), which is what is sorted here.

@@ -21,7 +21,7 @@ the tests that use them never touch the reference.
                      components, no intersection, segments whose loops all snap away).
 
 * polyline_split_ref.npz  the same pipeline with --split-contacts (label_segments_by_contact_greedy,
-                     polyline.py:267-368) on pairs whose contact splits into several components.
+                     polyline.py:267-341) on pairs whose contact splits into several components.
 * polyline_hard_ref.npz   the same pipeline, with and without the split, on flat faces and sharp edges:
                      offset, coplanar, rotated and tilted cubes, a sphere in a face and on an edge,
                      hulls, a T-junction in a mesh, grazing spheres.

@@ -1,5 +1,5 @@
 // zdx_pyset.cuh -- the order in which polyline.py visits a segment's candidates when it splits the
-// segments into components (label_segments_by_contact_greedy, polyline.py:267-368), for the polyline
+// segments into components (label_segments_by_contact_greedy, polyline.py:267-341), for the polyline
 // mode of the rebuild kernel.  Host and device code; the host build is what the CPU tests check.
 //
 // polyline.py adds the grid candidates of a segment to a Python set of ints (polyline.py:288-299) and
