@@ -251,3 +251,40 @@ def test_oracle_wall_contact_flat_shapes(oracle, ref):
             hits += 1
             assert ra[1] == rb[1] and np.array_equal(ra[2], rb[2]) and np.array_equal(ra[3], rb[3]), k
     assert hits >= 12
+
+
+def test_oracle_matches_reference_on_its_own_meshes(oracle, ref):
+    """The oracle against the reference C++, bit for bit, on the reference's own sample meshes (its
+    geometry/ folder: a convex particle, a low-poly banana and pug, a table; non-convex, with long thin
+    triangles), each pair at seeded overlapping poses, with and without the split.  Runs where the
+    reference tree is present (its path is recorded by oracle/Makefile in oracle/_ref/REF_ROOT)."""
+    from zdemx import synth
+
+    root_file = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                             "REF_ROOT")
+    geo = os.path.join(open(root_file).read().strip(), "geometry") if os.path.exists(root_file) else ""
+    if not (geo and os.path.isdir(geo)):
+        pytest.skip("the reference's geometry folder is not here")
+    names = ["convex-particle.stl", "low-poly-banbana.stl", "pug-lowpoly.stl", "table.stl"]
+    meshes = []
+    for f in names:
+        p = os.path.join(geo, f)
+        if not os.path.exists(p):
+            pytest.skip(f"{f} missing")
+        t = np.asarray(ref.load_stl(p), float).reshape(-1, 3, 3)
+        t = t / np.max(np.linalg.norm(t.reshape(-1, 3) - t.reshape(-1, 3).mean(0), axis=1)) * 1e-3  # 1 mm scale
+        meshes.append(ref.build_mesh(t))
+    rng = np.random.default_rng(4)
+    loops = 0
+    for a in range(len(meshes)):
+        for b in range(len(meshes)):
+            (Ab, pA), (Bb, pB) = meshes[a], meshes[b]
+            for trial in range(4):
+                pose = synth.pair_poses(rng, 1, 0.5 * (pA[4] + pB[4]), 0.3, 1.2)[0]
+                pose[3:7] = synth.random_unit_quat(rng)
+                split = bool(trial % 2)
+                r = ref.pair(Ab, pA[5], pA[6], Bb, pose[:7], pose[7:], split=split)
+                o = oracle.pair(Ab, pA[5], pA[6], Bb, pose[:7], pose[7:], split=split)
+                assert compare_pair(r, o, exact=True) == [], (names[a], names[b], trial)
+                loops += r["nloop"]
+    assert loops >= 40
