@@ -101,3 +101,33 @@ def test_config_counts(tmp_path):
         rc, msg, counts = _lib.config_check(cfg)
         assert rc == 0, (name, msg)
         assert counts[:3] == w, (name, counts)
+
+
+def test_reference_sample_configs(tmp_path):
+    """The reference's own sample configs (its config/ folder), with their STL paths made absolute, the
+    output folder moved here and steps = 0: accepted by both, with the same particle, wall and mesh
+    counts as the files describe.  Runs where the reference tree is present (oracle/_ref/REF_ROOT)."""
+    import re
+
+    from zdemx import _lib
+
+    root_file = os.path.join(ROOT, "oracle", "_ref", "REF_ROOT")
+    ref_root = open(root_file).read().strip() if os.path.exists(root_file) else ""
+    cfg_dir = os.path.join(ref_root, "config")
+    if not (ref_root and os.path.isdir(cfg_dir)):
+        pytest.skip("the reference's config folder is not here")
+    names = sorted(f for f in os.listdir(cfg_dir) if f.endswith(".txt"))
+    assert names
+    for name in names:
+        text = open(os.path.join(cfg_dir, name)).read()
+        text = re.sub(r"(?m)^(\s*stl\s*=?\s*)(\S+)", lambda m: m.group(1) + os.path.join(ref_root, m.group(2)), text)
+        text = re.sub(r"(?m)^(\s*output_dir\s*=?\s*)(\S+)", lambda m: m.group(1) + str(tmp_path / "out"), text)
+        text = re.sub(r"(?m)^(\s*steps\s*=?\s*)(\S+)", lambda m: m.group(1) + "0", text)
+        cfg = str(tmp_path / name)
+        open(cfg, "w").write(text)
+        rc, msg, counts = _lib.config_check(cfg)
+        ref_rc, ref_err = _reference(cfg)
+        assert rc == 0 and ref_rc == 0, (name, msg, ref_err)
+        nblocks = len(re.findall(r"(?m)^\s*particle\s*$", text))
+        nwalls = len(re.findall(r"(?m)^\s*wall\s*$", text))
+        assert counts[0] == nblocks and counts[1] == nwalls, (name, counts)
