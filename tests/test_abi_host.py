@@ -104,6 +104,12 @@ def test_stl_loader_matches_reference(tmp_path, ref):
                 a = ref.load_stl(os.path.join(ref_geo, f))
                 b = _lib.stl_load(os.path.join(ref_geo, f))
                 assert np.array_equal(a, b), f
+                # and build_mesh on them, at the reference configs' scale and unscaled
+                for scale in (1.0, 1e-3):
+                    for center in (True, False):
+                        ma, pa = ref.build_mesh(a * scale, center)
+                        mb, pb = _lib.mesh_build(b * scale, center)
+                        assert np.array_equal(ma, mb) and np.array_equal(pa, pb["raw"]), (f, scale, center)
 
 
 def test_stl_loader_errors(tmp_path):
