@@ -9,6 +9,7 @@ check or time against the CUDA path.  The product (zedm-x_b200/) never imports i
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -38,6 +39,159 @@ class _OracleOut(C.Structure):
 
 
 LOOP_SHORT, LOOP_TINY, LOOP_SMALL, LOOP_ACCEPT, LOOP_BBOX, LOOP_DEGEN = range(6)
+
+_i64p = C.POINTER(C.c_int64)
+
+
+class _ZoScene(C.Structure):
+    _fields_ = [("nmesh", C.c_int), ("mesh_tris", _dp), ("mesh_off", _i64p), ("mesh_props", _dp), ("np", C.c_int),
+                ("p_mesh", _ip), ("p_state", _dp), ("p_mat", _dp), ("nwall", C.c_int), ("w_mesh", _ip),
+                ("w_pose", _dp), ("w_mat", _dp), ("gravity", C.c_double * 3), ("dt", C.c_double),
+                ("split_contacts", C.c_int), ("nhist", C.c_int), ("hist_key", _i64p), ("hist_ds", _dp),
+                ("nwhist", C.c_int), ("whist_key", _i64p), ("whist_ds", _dp), ("force", _dp), ("torque", _dp),
+                ("contact_count", _ip), ("contacts", C.c_int), ("loops", C.c_int), ("comps", C.c_int),
+                ("segments", C.c_int), ("tri_checks", C.c_int64)]
+
+
+# ---- zdem_cpu's particle set-up (src/main.cpp:1936-1987), in Python floats (IEEE doubles) with the
+# reference's operation order, so that the scene handed to zo_dem_step is the reference's to the bit
+def _quat_normalize(q):
+    n = math.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+    if n < 1e-14:
+        return (1.0, 0.0, 0.0, 0.0)
+    return (q[0] / n, q[1] / n, q[2] / n, q[3] / n)
+
+
+def _quat_to_mat3(q):  # src/main.cpp:150-163
+    w, x, y, z = _quat_normalize(q)
+    return [[1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w)],
+            [2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w)],
+            [2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)]]
+
+
+def _mat3_mul(a, b):  # src/main.cpp:173-184
+    r = [[0.0] * 3 for _ in range(3)]
+    for i in range(3):
+        for j in range(3):
+            acc = 0.0
+            for k in range(3):
+                acc += a[i][k] * b[k][j]
+            r[i][j] = acc
+    return r
+
+
+def _mat3_inverse(a):  # src/main.cpp:196-217
+    det = (a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0])
+           + a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]))
+    if abs(det) < 1e-18:
+        return [[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]]
+    inv = 1.0 / det
+    return [[(a[1][1] * a[2][2] - a[1][2] * a[2][1]) * inv, -(a[0][1] * a[2][2] - a[0][2] * a[2][1]) * inv,
+             (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * inv],
+            [-(a[1][0] * a[2][2] - a[1][2] * a[2][0]) * inv, (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * inv,
+             -(a[0][0] * a[1][2] - a[0][2] * a[1][0]) * inv],
+            [(a[1][0] * a[2][1] - a[1][1] * a[2][0]) * inv, -(a[0][0] * a[2][1] - a[0][1] * a[2][0]) * inv,
+             (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * inv]]
+
+
+class DemScene:
+    """A zdem_cpu scene for zo_dem_step (the oracle's DEM step, src/main.cpp:2034-2468).  particles: dicts
+    with tris (raw, as loaded), scale, pos, quat, vel, omega, density, young, poisson, mu, restitution;
+    walls: dicts with tris, scale, pos, quat, mu, restitution.  Meshes are built with the oracle's
+    build_mesh; masses, inertias and L0 as src/main.cpp:1936-1987."""
+
+    def __init__(self, oracle, particles, walls=(), gravity=(0.0, 0.0, 0.0), dt=1e-6, split=True, center=True):
+        self.o = oracle
+        tris, offs, props = [], [0], []
+
+        def add_mesh(t, scale):
+            t = np.asarray(t, float).reshape(-1, 3, 3) * float(scale)
+            out, pr = oracle.build_mesh(t, center)
+            tris.append(out.reshape(-1, 9))
+            offs.append(offs[-1] + len(out))
+            props.append(pr)
+            return len(props) - 1
+
+        p_mesh, state, mat = [], [], []
+        for p in particles:
+            m = add_mesh(p["tris"], p.get("scale", 1.0))
+            pr = props[m]
+            vol, radius = float(pr[0]), float(pr[4])
+            dens = float(p.get("density", 1.0))
+            dens = dens if dens > 0.0 else 1.0
+            if vol > 0.0:
+                mass = dens * vol
+                Ib = [[float(pr[7 + 3 * i + j]) * dens for j in range(3)] for i in range(3)]
+            else:
+                mass = dens
+                I = 0.4 * mass * radius * radius
+                Ib = [[I, 0.0, 0.0], [0.0, I, 0.0], [0.0, 0.0, I]]
+            Ibi = _mat3_inverse(Ib)
+            eq = math.cbrt(3.0 * vol / (4.0 * 3.141592653589793)) if vol > 0.0 else radius
+            q = [float(x) for x in p.get("quat", (1.0, 0.0, 0.0, 0.0))]
+            om = [float(x) for x in p.get("omega", (0.0, 0.0, 0.0))]
+            R = _quat_to_mat3(q)
+            Rt = [[R[j][i] for j in range(3)] for i in range(3)]
+            Iw = _mat3_mul(_mat3_mul(R, Ib), Rt)
+            L = [Iw[i][0] * om[0] + Iw[i][1] * om[1] + Iw[i][2] * om[2] for i in range(3)]
+            p_mesh.append(m)
+            state.append(list(map(float, p.get("pos", (0, 0, 0)))) + q + list(map(float, p.get("vel", (0, 0, 0))))
+                         + om + L)
+            mat.append([mass, 1.0 / mass, radius, eq, float(p.get("young", 1e7)), float(p.get("poisson", 0.25)),
+                        float(p.get("mu", 0.5)), float(p.get("restitution", 0.5))] + [Ibi[i][j] for i in range(3)
+                                                                                    for j in range(3)])
+        w_mesh, w_pose, w_mat = [], [], []
+        for w in walls:
+            w_mesh.append(add_mesh(w["tris"], w.get("scale", 1.0)))
+            w_pose.append(list(map(float, w.get("pos", (0, 0, 0)))) + list(map(float, w.get("quat", (1, 0, 0, 0)))))
+            w_mat.append([float(w.get("mu", 0.5)), float(w.get("restitution", 0.5))])
+        n = len(particles)
+        self.mesh_tris = np.ascontiguousarray(np.concatenate(tris) if tris else np.zeros((0, 9)))
+        self.mesh_off = np.asarray(offs, np.int64)
+        self.mesh_props = np.ascontiguousarray(np.asarray(props, float).reshape(-1, 17))
+        self.p_mesh = np.asarray(p_mesh, np.int32)
+        self.state = np.ascontiguousarray(np.asarray(state, float).reshape(-1, 16))
+        self.mat = np.ascontiguousarray(np.asarray(mat, float).reshape(-1, 17))
+        self.w_mesh = np.asarray(w_mesh or [0], np.int32)
+        self.w_pose = np.ascontiguousarray(np.asarray(w_pose or [[0] * 7], float))
+        self.w_mat = np.ascontiguousarray(np.asarray(w_mat or [[0, 0]], float))
+        self.force = np.zeros((max(n, 1), 3))
+        self.torque = np.zeros((max(n, 1), 3))
+        self.count = np.zeros(max(n, 1), np.int32)
+        sc = _ZoScene()
+        sc.nmesh = len(props)
+        sc.mesh_tris = self.mesh_tris.ctypes.data_as(_dp)
+        sc.mesh_off = self.mesh_off.ctypes.data_as(_i64p)
+        sc.mesh_props = self.mesh_props.ctypes.data_as(_dp)
+        sc.np = n
+        sc.p_mesh = self.p_mesh.ctypes.data_as(_ip)
+        sc.p_state = self.state.ctypes.data_as(_dp)
+        sc.p_mat = self.mat.ctypes.data_as(_dp)
+        sc.nwall = len(walls)
+        sc.w_mesh = self.w_mesh.ctypes.data_as(_ip)
+        sc.w_pose = self.w_pose.ctypes.data_as(_dp)
+        sc.w_mat = self.w_mat.ctypes.data_as(_dp)
+        for k in range(3):
+            sc.gravity[k] = float(gravity[k])
+        sc.dt = float(dt)
+        sc.split_contacts = int(bool(split))
+        sc.force = self.force.ctypes.data_as(_dp)
+        sc.torque = self.torque.ctypes.data_as(_dp)
+        sc.contact_count = self.count.ctypes.data_as(_ip)
+        self.sc = sc
+
+    def step(self, n=1):
+        for _ in range(n):
+            self.o.lib.zo_dem_step(C.byref(self.sc))
+        s = self.sc
+        return {"contacts": s.contacts, "tri_checks": int(s.tri_checks), "segments": s.segments, "comps": s.comps,
+                "loops": s.loops}
+
+    def __del__(self):
+        try:
+            self.o.lib.zo_scene_free_history(C.byref(self.sc))
+        except Exception:
+            pass
 
 
 def _arr(ptr, n, dtype):
@@ -85,6 +239,8 @@ class Oracle:
         L.zo_build_mesh.argtypes = [_dp, C.c_int, C.c_int, _dp, _dp]
         L.zo_sort.argtypes = [C.c_int, _ip, C.c_int, _ip, _dp, C.c_int]
         L.zo_pyset_order.argtypes = [_ip, C.c_int, _ip]
+        L.zo_dem_step.argtypes = [C.POINTER(_ZoScene)]
+        L.zo_scene_free_history.argtypes = [C.POINTER(_ZoScene)]
         L.zo_wall_contact.argtypes = [_dp, C.c_int, _dp, _dp, _dp, C.c_double, C.c_double, _dp, _dp, _dp]
         L.zo_integrate.argtypes = [_dp, _dp, _dp, _dp, C.c_double]
 

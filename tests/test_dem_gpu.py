@@ -8,8 +8,8 @@ import os
 import numpy as np
 import pytest
 
-from _dem_helpers import (box_tris, out_file, parse_log, parse_state_txt, plane_tris, run_reference, write_binary_stl,
-                          write_config)
+from _dem_helpers import (box_tris, fmt, out_file, parse_log, parse_state_txt, plane_tris, run_reference,
+                          write_binary_stl, write_config)
 
 pytestmark = pytest.mark.gpu
 
@@ -72,9 +72,9 @@ def test_cluster_with_spin_and_split_off(tmp_path):
     for i in range(8):
         pos = np.array([(i % 2) * 1.85e-3, ((i // 2) % 2) * 1.85e-3, (i // 4) * 1.85e-3]) + rng.uniform(-5e-5, 5e-5, 3)
         q = synth.random_unit_quat(rng)
-        parts.append(dict(stl=str(tmp_path / ("a.stl" if i % 3 else "b.stl")), pos=" ".join(map(repr, pos)),
-                          vel=" ".join(map(repr, rng.normal(size=3) * 0.02)), quat=" ".join(map(repr, q)),
-                          omega=" ".join(map(repr, rng.normal(size=3) * 5.0)), scale=1, **MAT))
+        parts.append(dict(stl=str(tmp_path / ("a.stl" if i % 3 else "b.stl")), pos=fmt(pos),
+                          vel=fmt(rng.normal(size=3) * 0.02), quat=fmt(q), omega=fmt(rng.normal(size=3) * 5.0),
+                          scale=1, **MAT))
     _compare_run(tmp_path, {"steps": 40, "dt": 1e-6, "split_contacts": 0, "gravity": "0 0 -9.81",
                             "output_interval": 2}, parts, min_contact_steps=5)
 

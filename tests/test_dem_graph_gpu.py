@@ -8,7 +8,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from _dem_helpers import box_tris, out_file, parse_state_txt, plane_tris, write_binary_stl, write_config
+from _dem_helpers import box_tris, fmt, out_file, parse_state_txt, plane_tris, write_binary_stl, write_config
 
 pytestmark = pytest.mark.gpu
 
@@ -28,10 +28,9 @@ def _cluster_config(tmp_path, n=8, walls=True, seed=2):
     for i in range(n):
         pos = np.array([(i % 2) * 1.85e-3, ((i // 2) % 2) * 1.85e-3, 1.05e-3 + (i // 4) * 1.85e-3])
         pos += rng.uniform(-5e-5, 5e-5, 3)
-        parts.append(dict(stl=str(tmp_path / ("a.stl" if i % 3 else "b.stl")), pos=" ".join(map(repr, pos)),
-                          vel=" ".join(map(repr, rng.normal(size=3) * 0.02)),
-                          quat=" ".join(map(repr, synth.random_unit_quat(rng))),
-                          omega=" ".join(map(repr, rng.normal(size=3) * 5.0)), scale=1, **MAT))
+        parts.append(dict(stl=str(tmp_path / ("a.stl" if i % 3 else "b.stl")), pos=fmt(pos),
+                          vel=fmt(rng.normal(size=3) * 0.02), quat=fmt(synth.random_unit_quat(rng)),
+                          omega=fmt(rng.normal(size=3) * 5.0), scale=1, **MAT))
     wl = []
     if walls:
         wl = [dict(stl=str(tmp_path / "plane.stl"), pos="0 0 0", quat="1 0 0 0", scale=1, mu=0.4, restitution=0.3),
