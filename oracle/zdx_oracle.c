@@ -22,7 +22,14 @@ static inline V3 vadd(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); 
 static inline V3 vsub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
 static inline V3 vmul(V3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
 static inline V3 vdiv(V3 a, double s) { return v3(a.x / s, a.y / s, a.z / s); }
-static inline double vdot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* numpy's arithmetic (ZO_MODE_NUMPY, set for the duration of one zo_pair call): on this platform np.dot
+ * of two 3-vectors is fma(a2, b2, fma(a1, b1, a0 b0)) and np.linalg.norm of a 3- or 4-vector the square
+ * root of that chain; elementwise ufuncs and np.cross are the plain IEEE operations. */
+static int g_np = 0;
+static inline double vdot(V3 a, V3 b) {
+    if (g_np) return fma(a.z, b.z, fma(a.y, b.y, a.x * b.x));
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
 static inline V3 vcross(V3 a, V3 b) {
     return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
@@ -76,7 +83,8 @@ static inline V3 qrotate(Q4 q, V3 v) {
 }
 /* quat_rotate, polyline.py:36-53: v + w t + qv x t with t = 2 qv x v. */
 static inline V3 qrotate_py(Q4 q, V3 v) {
-    double n = sqrt(q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z);
+    double n = g_np ? sqrt(fma(q.z, q.z, fma(q.y, q.y, fma(q.x, q.x, q.w * q.w))))
+                    : sqrt(q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z);
     Q4 qn = {1.0, 0.0, 0.0, 0.0};
     if (!(n < 1e-30)) { qn.w = q.w / n; qn.x = q.x / n; qn.y = q.y / n; qn.z = q.z / n; }
     V3 qv = v3(qn.x, qn.y, qn.z);
@@ -837,7 +845,8 @@ static void loop_integrals(const V3* P, int m, V3* Sn, V3* Gn) {
 int zo_pair(const double* trisA, int nA, double mean_edgeA, double bbox_diagA, const double* trisB, int nB,
             const double* poseA, const double* poseB, int split, int mode, double tol_in, ZoPairOut* out) {
     memset(out, 0, sizeof(*out));
-    int py = (mode == ZO_MODE_POLYLINE);
+    int py = (mode == ZO_MODE_POLYLINE || mode == ZO_MODE_NUMPY);
+    g_np = (mode == ZO_MODE_NUMPY);
     V3* wa = (V3*)malloc(sizeof(V3) * 3 * (size_t)(nA + 1));
     V3* wb = (V3*)malloc(sizeof(V3) * 3 * (size_t)(nB + 1));
     Q4 qa = {poseA[3], poseA[4], poseA[5], poseA[6]}, qb = {poseB[3], poseB[4], poseB[5], poseB[6]};
@@ -859,6 +868,21 @@ int zo_pair(const double* trisA, int nA, double mean_edgeA, double bbox_diagA, c
     for (int i = 0; i < nB; ++i) {
         okB[i] = (char)plane_from_tri(wb + 3 * i, &nBv[i], &dBv[i]);
         if (!okB[i]) { nBv[i] = v3(0, 0, 0); dBv[i] = 0.0; }
+    }
+    if (g_np) {
+        /* polyline.py main hands tri_tri the normals of tri_normals (polyline.py:99-109: row norms, a plain
+         * sum of squares) and the offsets of plane_from_tri (:112-119, np.linalg.norm) */
+        for (int s2 = 0; s2 < 2; ++s2) {
+            const V3* w = s2 ? wb : wa;
+            V3* nv = s2 ? nBv : nAv;
+            const char* ok = s2 ? okB : okA;
+            for (int i = 0; i < (s2 ? nB : nA); ++i) {
+                if (!ok[i]) continue;
+                V3 c = vcross(vsub(w[3 * i + 1], w[3 * i]), vsub(w[3 * i + 2], w[3 * i]));
+                double ln = sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
+                nv[i] = ln > 1e-30 ? vdiv(c, ln) : c;
+            }
+        }
     }
     /* per-triangle AABBs, src/main.cpp:2093-2116 */
     V3* amnA = (V3*)malloc(sizeof(V3) * (size_t)(nA + 1));
@@ -1014,6 +1038,7 @@ int zo_pair(const double* trisA, int nA, double mean_edgeA, double bbox_diagA, c
     out->contact_loop = ib_take(&contact_loop);
     free(wa); free(wb); free(nAv); free(nBv); free(dAv); free(dBv); free(okA); free(okB);
     free(amnA); free(amxA); free(amnB); free(amxB); free(s0); free(s1);
+    g_np = 0;
     return 0;
 }
 

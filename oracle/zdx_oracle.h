@@ -15,7 +15,9 @@
 extern "C" {
 #endif
 
-enum { ZO_MODE_ZDEM = 0, ZO_MODE_POLYLINE = 1 };
+enum { ZO_MODE_ZDEM = 0, ZO_MODE_POLYLINE = 1, ZO_MODE_NUMPY = 2 };
+/* ZO_MODE_NUMPY: polyline mode in numpy's own arithmetic (its np.dot / np.linalg.norm FMA chains and
+ * tri_normals' normals), to be bit-exact with polyline.py itself. */
 
 /* Loop status codes (both modes). */
 enum {

@@ -288,3 +288,29 @@ def test_oracle_matches_reference_on_its_own_meshes(oracle, ref):
                 assert compare_pair(r, o, exact=True) == [], (names[a], names[b], trial)
                 loops += r["nloop"]
     assert loops >= 40
+
+
+@pytest.mark.parametrize("fixture", ["polyline_ref.npz", "polyline_split_ref.npz", "polyline_hard_ref.npz"])
+def test_oracle_numpy_mode_is_bit_exact_with_polyline_py(oracle, fixture):
+    """The oracle's numpy-arithmetic polyline mode (mode 2: np.dot and np.linalg.norm as this platform's
+    FMA chains, tri_normals' normals for the triangle test) against polyline.py's own pipeline: every
+    loop's points and Sn, Gn, xc0, nA, |Sn|, Fn, F_A identical to the bit, split or not."""
+    from _helpers import expected_contacts
+
+    z = np.load(os.path.join(GOLDEN, fixture))
+    loops = 0
+    for ci in range(int(z["ncase"])):
+        A, B, pose, tol = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], float(z[f"c{ci}_tol"])
+        split = bool(z[f"c{ci}_split"]) if f"c{ci}_split" in z.files else fixture == "polyline_split_ref.npz"
+        r = oracle.pair(A, 0.0, 0.0, B, pose[:7], pose[7:], split=split, mode=2, tol=tol)
+        e = expected_contacts(r, polyline=True)
+        lens = list(z[f"c{ci}_loop_len"])
+        assert r["nseg"] == int(z[f"c{ci}_nseg"]) and list(e["nvert"]) == lens, ci
+        pts = np.split(z[f"c{ci}_loop_pts"], np.cumsum(lens)[:-1]) if lens else []
+        for c, p in enumerate(pts):
+            g = e["geom"][c]
+            Fn = 0.5 * 1e7 * g[12]
+            assert np.array_equal(e["points"][c], p), (ci, c)
+            assert np.array_equal(np.r_[g, Fn, Fn * g[9:12]], z[f"c{ci}_geom"][c]), (ci, c)
+            loops += 1
+    assert loops >= 3

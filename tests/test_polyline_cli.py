@@ -3,7 +3,8 @@ pairs of tests/golden/cli_ref.npz (its argv, stdout and the three VTK files it w
 
 * CPU: the transformed-mesh VTK files byte for byte (host code only), and main's printing and file
   logic, with the pair call replaced by the counts polyline.py printed, byte for byte on the cases
-  without contacts (no segments; segments whose loops all snap away).
+  without contacts (no segments; segments whose loops all snap away).  With the pair call computed in
+  numpy's own arithmetic (the oracle's mode 2), stdout and all three files byte for byte on every case.
 * GPU: the whole command line.  Lines and files are identical except for FP64 numbers, which polyline.py
   computes with numpy (its own rounding) and which agree within 1e-9 relative."""
 import contextlib
@@ -102,6 +103,36 @@ def test_main_without_contacts_matches_reference(tmp_path, monkeypatch):
         assert (va, vb, loops) == (case["vtkA"], case["vtkB"], case["loops"]), case["name"]
         checked += 1
     assert checked == 2
+
+
+def test_main_with_numpy_arithmetic_is_byte_identical(tmp_path, monkeypatch, oracle):
+    """With the pair call computed in numpy's own arithmetic (the oracle's mode 2), main's stdout and all
+    three VTK files are byte-identical with polyline.py's, so its command line is reproduced exactly.
+    (The GPU's polyline mode follows the C++ arithmetic and agrees to 1e-9: test_main_matches_reference.)"""
+    from _helpers import expected_contacts
+    from zdemx import polyline
+
+    def pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split, idA, idB, ctx, comp_cap=0):
+        A, B = np.asarray(trisA, float).reshape(-1, 3, 3), np.asarray(trisB, float).reshape(-1, 3, 3)
+        r = oracle.pair(A, 0.0, 0.0, B, np.r_[tA, qA], np.r_[tB, qB], split=split, mode=2, tol=tol)
+        e = expected_contacts(r, polyline=True)
+        geom = np.asarray([np.r_[g, 0.5 * k * g[12], g[9:12] * (0.5 * k * g[12]), -(g[9:12] * (0.5 * k * g[12]))]
+                           for g in e["geom"]]).reshape(-1, 20)
+        info = np.array([[0, c, e["nvert"][c], e["comp"][c]] for c in range(len(geom))], np.int32).reshape(-1, 4)
+        man = polyline._manifold(idA, idB, geom, info, k)
+        comps = [(int(r["comp_off"][c + 1] - r["comp_off"][c]), int(r["v_off"][c + 1] - r["v_off"][c]),
+                  int(r["e2_off"][c + 1] - r["e2_off"][c]), int(np.sum(e["comp"] == c))) for c in range(r["ncomp"])]
+        loops = [[p.copy() for p in pts] for pts in e["points"]]
+        xc0s = [None if g[12] == 0.0 else g[6:9].copy() for g in geom]
+        return man, loops, xc0s, list(range(len(geom))), int(r["nseg"]), r["ncomp"], comps
+
+    monkeypatch.setattr(polyline, "_pair_call", pair_call)
+    for case in _cases():
+        d = tmp_path / case["name"]
+        d.mkdir()
+        stdout, va, vb, loops = _run_main(case, str(d))
+        assert stdout == case["stdout"], case["name"]
+        assert (va, vb, loops) == (case["vtkA"], case["vtkB"], case["loops"]), case["name"]
 
 
 @pytest.mark.gpu
