@@ -48,7 +48,7 @@ def _compare_run(tmp_path, glob, particles, walls=(), rtol=1e-9, min_contact_ste
 
 
 def test_two_noised_icospheres_config1_like(tmp_path):
-    """BASELINE config 1 shape: two 320-triangle noised icospheres, 1 mm, 1.9 mm apart, +-0.05 m/s."""
+    """The two-particle workload's shape: two 320-triangle noised icospheres, 1 mm, 1.9 mm apart, +-0.05 m/s."""
     from zdemx import synth
 
     rng = np.random.default_rng(1)
