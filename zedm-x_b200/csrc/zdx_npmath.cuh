@@ -41,5 +41,152 @@ ZDX_HD_NP void cross3(const double* a, const double* b, double* out) {
     out[2] = z;
 }
 
+// ---- polyline.py's triangle stage in numpy's arithmetic (points and vectors as double[3])
+
+// quat_rotate + translation of transform_points (polyline.py:36-56): v + w t + qv x t, t = 2 qv x v, the
+// quaternion normalised by np.linalg.norm (threshold 1e-30)
+ZDX_HD_NP void transform_point(const double* q, const double* tr, const double* v, double* out) {
+    const double n = norm4(q);
+    double w = 1.0, qv[3] = {0.0, 0.0, 0.0};
+    if (!(n < 1e-30)) {
+        w = q[0] / n;
+        qv[0] = q[1] / n;
+        qv[1] = q[2] / n;
+        qv[2] = q[3] / n;
+    }
+    double t[3], c[3];
+    cross3(qv, v, t);
+    for (int k = 0; k < 3; ++k) t[k] = 2.0 * t[k];
+    cross3(qv, t, c);
+    for (int k = 0; k < 3; ++k) out[k] = ((v[k] + w * t[k]) + c[k]) + tr[k];
+}
+
+// tri_normals (polyline.py:99-109) for one triangle: the cross product divided by its row norm when that
+// is above 1e-30, else left as it is
+ZDX_HD_NP void tri_normal(const double* t, double* n) {
+    double e1[3], e2[3];
+    for (int k = 0; k < 3; ++k) {
+        e1[k] = t[3 + k] - t[k];
+        e2[k] = t[6 + k] - t[k];
+    }
+    cross3(e1, e2, n);
+    const double ln = row_norm3(n);
+    if (ln > 1e-30)
+        for (int k = 0; k < 3; ++k) n[k] = n[k] / ln;
+}
+
+// plane_from_tri (polyline.py:112-119); false when the triangle has no plane
+ZDX_HD_NP bool plane_from_tri(const double* t, double* n, double* d) {
+    double e1[3], e2[3];
+    for (int k = 0; k < 3; ++k) {
+        e1[k] = t[3 + k] - t[k];
+        e2[k] = t[6 + k] - t[k];
+    }
+    cross3(e1, e2, n);
+    const double ln = norm3(n);
+    if (ln < 1e-30) return false;
+    for (int k = 0; k < 3; ++k) n[k] = n[k] / ln;
+    *d = -dot3(n, t);
+    return true;
+}
+
+// point_in_tri (polyline.py:121-128)
+ZDX_HD_NP bool point_in_tri(const double* p, const double* t, const double* n) {
+    const double* a = t;
+    const double* b = t + 3;
+    const double* c = t + 6;
+    double ab[3], bc[3], ca[3], ap[3], bp[3], cp[3], x[3];
+    for (int k = 0; k < 3; ++k) {
+        ab[k] = b[k] - a[k];
+        bc[k] = c[k] - b[k];
+        ca[k] = a[k] - c[k];
+        ap[k] = p[k] - a[k];
+        bp[k] = p[k] - b[k];
+        cp[k] = p[k] - c[k];
+    }
+    cross3(ab, ap, x);
+    const double c1 = dot3(x, n);
+    cross3(bc, bp, x);
+    const double c2 = dot3(x, n);
+    cross3(ca, cp, x);
+    const double c3 = dot3(x, n);
+    return (c1 >= -1e-10) && (c2 >= -1e-10) && (c3 >= -1e-10);
+}
+
+// seg_plane_intersection (polyline.py:130-140); t is clamped as Python's min(1.0, max(0.0, t))
+ZDX_HD_NP bool seg_plane(const double* p0, const double* p1, const double* n, double d, double* out) {
+    double u[3];
+    for (int k = 0; k < 3; ++k) u[k] = p1[k] - p0[k];
+    const double denom = dot3(n, u);
+    const double num = -(dot3(n, p0) + d);
+    if (fabs(denom) < 1e-30) return false;
+    double t = num / denom;
+    if (t < -1e-10 || t > 1.0 + 1e-10) return false;
+    t = 0.0 < t ? t : 0.0;
+    t = t < 1.0 ? t : 1.0;
+    for (int k = 0; k < 3; ++k) out[k] = p0[k] + t * u[k];
+    return true;
+}
+
+// tri_tri_intersection_segment (polyline.py:154-190) with unique_points (:142-152, tol 1e-9): true and the
+// segment (p0, p1) oriented along nA x nB, or false
+ZDX_HD_NP bool tri_tri(const double* tA, const double* nA, double dA, const double* tB, const double* nB, double dB,
+                       double* p0, double* p1) {
+    double tau[3];
+    cross3(nA, nB, tau);
+    const double lt = norm3(tau);
+    if (lt < 1e-20) return false;
+    for (int k = 0; k < 3; ++k) tau[k] = tau[k] / lt;
+    double cand[6][3];
+    int nc = 0;
+    for (int side = 0; side < 2; ++side) {
+        const double* t = side ? tB : tA;
+        const double* other = side ? tA : tB;
+        const double* n = side ? nA : nB;
+        const double d = side ? dA : dB;
+        for (int e = 0; e < 3; ++e) {
+            double p[3];
+            if (seg_plane(t + 3 * e, t + 3 * ((e + 1) % 3), n, d, p) && point_in_tri(p, other, n)) {
+                bool keep = true;
+                for (int q = 0; q < nc && keep; ++q) {
+                    double df[3] = {p[0] - cand[q][0], p[1] - cand[q][1], p[2] - cand[q][2]};
+                    if (norm3(df) <= 1e-9) keep = false;
+                }
+                if (keep) {
+                    cand[nc][0] = p[0];
+                    cand[nc][1] = p[1];
+                    cand[nc][2] = p[2];
+                    ++nc;
+                }
+            }
+        }
+    }
+    if (nc < 2) return false;
+    int i0 = 0, i1 = 0;
+    double tmin = dot3(cand[0], tau), tmax = tmin;
+    for (int q = 1; q < nc; ++q) {
+        const double tq = dot3(cand[q], tau);
+        if (tq < tmin) {
+            tmin = tq;
+            i0 = q;
+        }
+        if (tq > tmax) {
+            tmax = tq;
+            i1 = q;
+        }
+    }
+    if (i0 == i1) return false;
+    double df[3] = {cand[i1][0] - cand[i0][0], cand[i1][1] - cand[i0][1], cand[i1][2] - cand[i0][2]};
+    if (norm3(df) < 1e-18) return false;
+    const bool swap = dot3(df, tau) < 0.0;
+    const double* a = swap ? cand[i1] : cand[i0];
+    const double* b = swap ? cand[i0] : cand[i1];
+    for (int k = 0; k < 3; ++k) {
+        p0[k] = a[k];
+        p1[k] = b[k];
+    }
+    return true;
+}
+
 }  // namespace np
 }  // namespace zdx
