@@ -188,5 +188,108 @@ ZDX_HD_NP bool tri_tri(const double* tA, const double* nA, double dA, const doub
     return true;
 }
 
+// ---- polyline.py's rebuild arithmetic
+
+// np.clip(x, 0.0, 1.0): max first, then min, each taking its second operand unless the first is
+// strictly beyond it (so -0.0 clips to +0.0)
+ZDX_HD_NP double clip01(double x) {
+    const double m = x > 0.0 ? x : 0.0;
+    return m < 1.0 ? m : 1.0;
+}
+
+// seg_seg_dist2 (polyline.py:227-265), EPS = 1e-12
+ZDX_HD_NP double seg_seg_dist2(const double* p1, const double* q1, const double* p2, const double* q2) {
+    double d1[3], d2[3], r[3];
+    for (int k = 0; k < 3; ++k) {
+        d1[k] = q1[k] - p1[k];
+        d2[k] = q2[k] - p2[k];
+        r[k] = p1[k] - p2[k];
+    }
+    const double a = dot3(d1, d1), e = dot3(d2, d2), f = dot3(d2, r);
+    double c_[3];
+    if (a <= 1e-12 && e <= 1e-12) {
+        for (int k = 0; k < 3; ++k) c_[k] = p1[k] - p2[k];
+        return dot3(c_, c_);
+    }
+    if (a <= 1e-12) {
+        const double t = clip01(f / e);
+        for (int k = 0; k < 3; ++k) c_[k] = p1[k] - (p2[k] + t * d2[k]);
+        return dot3(c_, c_);
+    }
+    if (e <= 1e-12) {
+        const double s = clip01(-dot3(d1, r) / a);
+        for (int k = 0; k < 3; ++k) c_[k] = (p1[k] + s * d1[k]) - p2[k];
+        return dot3(c_, c_);
+    }
+    const double b = dot3(d1, d2), c = dot3(d1, r);
+    const double denom = a * e - b * b;
+    double s = fabs(denom) > 0.0 ? clip01((b * f - c * e) / denom) : 0.0;
+    double t = (b * s + f) / e;
+    if (t < 0.0) {
+        t = 0.0;
+        s = clip01(-c / a);
+    } else if (t > 1.0) {
+        t = 1.0;
+        s = clip01((b - c) / a);
+    }
+    for (int k = 0; k < 3; ++k) c_[k] = (p1[k] + s * d1[k]) - (p2[k] + t * d2[k]);
+    return dot3(c_, c_);
+}
+
+// point_segment_dist2_and_t (polyline.py:420-431): dist2, with t (clamped) in *t
+ZDX_HD_NP double point_seg_dist2_t(const double* p, const double* a, const double* b, double* t_out) {
+    double ab[3], pa[3];
+    for (int k = 0; k < 3; ++k) {
+        ab[k] = b[k] - a[k];
+        pa[k] = p[k] - a[k];
+    }
+    const double denom = dot3(ab, ab);
+    if (denom <= 1e-12) {
+        *t_out = 0.0;
+        return dot3(pa, pa);
+    }
+    const double t = dot3(pa, ab) / denom;
+    double tc = 0.0 < t ? t : 0.0;  // min(1.0, max(0.0, t))
+    tc = tc < 1.0 ? tc : 1.0;
+    double d[3];
+    for (int k = 0; k < 3; ++k) d[k] = p[k] - (a[k] + tc * ab[k]);
+    *t_out = tc;
+    return dot3(d, d);
+}
+
+// accumulate_Sn_Gn_from_polyline (polyline.py:193-209) over m points (3 doubles each)
+ZDX_HD_NP void loop_sn_gn(const double* P, int m, double* Sn, double* Gn) {
+    for (int k = 0; k < 3; ++k) Sn[k] = Gn[k] = 0.0;
+    for (int i = 0; i < m; ++i) {
+        const double* p0 = P + 3 * i;
+        const double* p1 = P + 3 * ((i + 1) % m);
+        double c[3], dx[3];
+        cross3(p0, p1, c);
+        for (int k = 0; k < 3; ++k) {
+            Sn[k] = Sn[k] + 0.5 * c[k];
+            dx[k] = p1[k] - p0[k];
+        }
+        const double s = dot3(p0, p1) + (1.0 / 3.0) * dot3(dx, dx);
+        const double g = -(1.0 / 3.0) * s;
+        for (int k = 0; k < 3; ++k) Gn[k] = Gn[k] + g * dx[k];
+    }
+}
+
+// contact_point_xc0 (polyline.py:211-218): |Sn|, with nA and xc0 (false: |Sn| < 1e-14, xc0 None, nA 0)
+ZDX_HD_NP bool contact_xc0(const double* Sn, const double* Gn, double* area, double* nA, double* xc0) {
+    const double a = norm3(Sn);
+    if (a < 1e-14) {
+        *area = 0.0;
+        nA[0] = nA[1] = nA[2] = 0.0;
+        return false;
+    }
+    for (int k = 0; k < 3; ++k) nA[k] = -Sn[k] / a;
+    double c[3];
+    cross3(nA, Gn, c);
+    for (int k = 0; k < 3; ++k) xc0[k] = c[k] / a;
+    *area = a;
+    return true;
+}
+
 }  // namespace np
 }  // namespace zdx
