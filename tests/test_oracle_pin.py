@@ -314,3 +314,51 @@ def test_oracle_numpy_mode_is_bit_exact_with_polyline_py(oracle, fixture):
             assert np.array_equal(np.r_[g, Fn, Fn * g[9:12]], z[f"c{ci}_geom"][c]), (ci, c)
             loops += 1
     assert loops >= 3
+
+
+def test_oracle_numpy_mode_on_the_reference_meshes(oracle, ref):
+    """The numpy-arithmetic mode against polyline.py itself, imported live from the reference tree where it
+    is present, on the reference's own non-convex sample meshes at seeded overlapping poses, split and
+    not: every loop's points and numbers identical to the bit."""
+    import importlib.util
+    import sys
+
+    from _helpers import expected_contacts
+    from zdemx import synth
+
+    root_file = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                             "REF_ROOT")
+    root = open(root_file).read().strip() if os.path.exists(root_file) else ""
+    if not (root and os.path.exists(os.path.join(root, "polyline.py"))):
+        pytest.skip("the reference tree is not here")
+    spec = importlib.util.spec_from_file_location("_ref_polyline", os.path.join(root, "polyline.py"))
+    P = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(P)
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import polyline_pipeline
+
+    meshes = []
+    for f in ("convex-particle.stl", "low-poly-banbana.stl", "pug-lowpoly.stl"):
+        t = np.asarray(ref.load_stl(os.path.join(root, "geometry", f)), float).reshape(-1, 3, 3)
+        c = t.reshape(-1, 3).mean(0)
+        meshes.append((t - c) / np.max(np.linalg.norm(t.reshape(-1, 3) - c, axis=1)) * 1e-3)
+    rng = np.random.default_rng(6)
+    loops = 0
+    for a in range(3):
+        for b in range(3):
+            pose = synth.pair_poses(rng, 1, 1e-3, 0.3, 1.0)[0]
+            pose[3:7] = synth.random_unit_quat(rng)
+            for split in (False, True):
+                want = polyline_pipeline(P, meshes[a], meshes[b], pose, 1e-5, split)
+                r = oracle.pair(meshes[a], 0.0, 0.0, meshes[b], pose[:7], pose[7:], split=split, mode=2, tol=1e-5)
+                e = expected_contacts(r, polyline=True)
+                lens = list(want["loop_len"])
+                assert r["nseg"] == int(want["nseg"]) and list(e["nvert"]) == lens, (a, b, split)
+                pts = np.split(want["loop_pts"], np.cumsum(lens)[:-1]) if lens else []
+                for c, p in enumerate(pts):
+                    g = e["geom"][c]
+                    Fn = 0.5 * 1e7 * g[12]
+                    assert np.array_equal(e["points"][c], p), (a, b, split, c)
+                    assert np.array_equal(np.r_[g, Fn, Fn * g[9:12]], want["geom"][c]), (a, b, split, c)
+                    loops += 1
+    assert loops >= 10
