@@ -16,6 +16,7 @@
  */
 #ifndef ZDEMX_H
 #define ZDEMX_H
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus

@@ -125,3 +125,25 @@ def test_stl_loader_errors(tmp_path):
     q.write_text("solid nothing here\n" * 10)
     with pytest.raises(ValueError):
         polyline.load_stl(str(q))
+
+
+def test_header_is_self_contained_c_and_cpp(tmp_path):
+    """include/zdemx.h compiles on its own as C99 and as C++11 (pedantic, warnings as errors): a caller
+    in either language includes it first and needs nothing else."""
+    import shutil
+    import subprocess
+
+    src = tmp_path / "use.c"
+    src.write_text('#include "zdemx.h"\n'
+                   "int main(void) {\n"
+                   "    zdx_pair_opts o = {ZDX_MODE_POLYLINE, 1, 1e-6, 1.0, ZDX_MEM_HOST, ZDX_SCHED_BATCHED, 1, 0};\n"
+                   "    (void)o;\n"
+                   "    return zdx_version() ? 0 : 1;\n"
+                   "}\n")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    for cc, args in (("gcc", ["-std=c99"]), ("g++", ["-std=c++11", "-x", "c++"])):
+        if shutil.which(cc) is None:
+            continue
+        p = subprocess.run([cc] + args + ["-Wall", "-Wextra", "-pedantic", "-Werror", "-I", inc, "-fsyntax-only",
+                                          str(src)], capture_output=True, text=True, timeout=120)
+        assert p.returncode == 0, (cc, p.stderr)
