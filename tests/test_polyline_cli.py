@@ -144,3 +144,28 @@ def test_main_matches_reference(tmp_path):
         assert (va, vb) == (case["vtkA"], case["vtkB"]), case["name"]
         _same_up_to_rounding(stdout, case["stdout"], (case["name"], "stdout"))
         _same_up_to_rounding(loops, case["loops"], (case["name"], "loops vtk"))
+
+
+@pytest.mark.parametrize("argv", [[], ["a.stl"], ["a.stl", "b.stl", "--tol"], ["a.stl", "b.stl", "--tA", "1", "2"],
+                                  ["a.stl", "b.stl", "--bogus"], ["--help"]])
+def test_argument_errors_match_reference_script(tmp_path, argv):
+    """`python -m zdemx.polyline` against the reference's own `python polyline.py` on bad or missing
+    arguments: the same stdout, stderr and exit status (argparse's usage and messages).  Runs where the
+    reference tree is present (oracle/_ref/REF_ROOT)."""
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    root_file = os.path.join(root, "oracle", "_ref", "REF_ROOT")
+    ref_root = open(root_file).read().strip() if os.path.exists(root_file) else ""
+    ref_py = os.path.join(ref_root, "polyline.py")
+    if not (ref_root and os.path.exists(ref_py)):
+        pytest.skip("the reference tree is not here")
+    env = dict(os.environ, PYTHONPATH=os.path.join(root, "zedm-x_b200"))
+    got = subprocess.run([sys.executable, "-m", "zdemx.polyline"] + argv, capture_output=True, text=True,
+                         timeout=120, cwd=str(tmp_path), env=env)
+    want = subprocess.run([sys.executable, ref_py] + argv, capture_output=True, text=True, timeout=120,
+                          cwd=str(tmp_path))
+    assert got.returncode == want.returncode, (got.stderr, want.stderr)
+    assert got.stderr == want.stderr
+    assert got.stdout == want.stdout
