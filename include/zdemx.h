@@ -62,6 +62,11 @@ int zdx_mesh_build(const double* tris, int64_t ntri, int center_mesh, double* tr
  * with build_contacts_from_loops, :655-701), for many pairs at once. */
 #define ZDX_MODE_ZDEM 0      /* zdem_cpu semantics: tol from mesh A, |Sn| filters, nA flipped toward B   */
 #define ZDX_MODE_POLYLINE 1  /* polyline.py semantics: tol given, bbox filter, stable orders, no flip    */
+/* ZDX_MODE_POLYLINE in numpy's own arithmetic, as polyline.py rounds on an x86-64 numpy whose 3-vector
+ * np.dot is the fused chain fma(a2, b2, fma(a1, b1, a0 b0)): np.linalg.norm as the root of that chain,
+ * tri_normals' row norms for the triangle test's normals.  Meant to give polyline.py's numbers to the
+ * bit.  zdx_pair_contacts only (not the adjoint, not zdx_pair_contacts_noalloc). */
+#define ZDX_MODE_POLYLINE_NUMPY 2
 #define ZDX_MEM_HOST 0
 #define ZDX_MEM_DEVICE 1
 #define ZDX_SCHED_BATCHED 0  /* one launch per stage over the whole batch, cost-ordered work queue       */

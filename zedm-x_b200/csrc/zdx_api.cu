@@ -153,7 +153,8 @@ int stage_in(zdx_ctx* ctx, bool host, const T* src, size_t count, DevBuf& buf, c
 extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const zdx_mesh_set* ms,
                                  const zdx_pair_batch* pb, zdx_pair_result* out) {
     if (!ctx || !opts || !ms || !pb || !out) return ZDX_ERR_INVALID;
-    if (ms->n_mesh < 0 || pb->n_pairs < 0 || (opts->mode != ZDX_MODE_ZDEM && opts->mode != ZDX_MODE_POLYLINE))
+    if (ms->n_mesh < 0 || pb->n_pairs < 0 ||
+        (opts->mode != ZDX_MODE_ZDEM && opts->mode != ZDX_MODE_POLYLINE && opts->mode != ZDX_MODE_POLYLINE_NUMPY))
         return ctx_fail(ctx, ZDX_ERR_INVALID, "bad mesh/pair count or mode");
     if (pb->n_pairs > 0x7fffffffLL) return ctx_fail(ctx, ZDX_ERR_INVALID, "at most 2^31-1 pairs per call");
     if (ms->n_mesh > 0 && (!ms->tris || !ms->tri_off || !ms->mean_edge || !ms->bbox_diag))
@@ -200,7 +201,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     a.n_pairs = NP;
     a.mode = opts->mode;
     a.split = opts->split_contacts ? 1 : 0;
-    a.tol_in = opts->mode == ZDX_MODE_POLYLINE ? (opts->tol > 0.0 ? opts->tol : 1e-6) : opts->tol;
+    a.tol_in = opts->mode != ZDX_MODE_ZDEM ? (opts->tol > 0.0 ? opts->tol : 1e-6) : opts->tol;
     a.k = opts->k;
     a.want_pts = opts->want_loop_points ? 1 : 0;
     a.cap_seg = opts->max_seg_per_pair > 0 ? opts->max_seg_per_pair : 16384;
@@ -486,6 +487,8 @@ extern "C" int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts
                                          double* grad_tris, double* grad_pose) {
     if (!ctx || !opts || !ms || !pb || (n_contacts > 0 && !grad_contact) || !grad_tris || !grad_pose)
         return ZDX_ERR_INVALID;
+    if (opts->mode == ZDX_MODE_POLYLINE_NUMPY)
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "the adjoint runs in ZDX_MODE_ZDEM or ZDX_MODE_POLYLINE");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const bool host = opts->mem == ZDX_MEM_HOST;

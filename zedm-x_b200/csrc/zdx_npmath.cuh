@@ -45,15 +45,11 @@ ZDX_HD_NP void cross3(const double* a, const double* b, double* out) {
 
 // quat_rotate + translation of transform_points (polyline.py:36-56): v + w t + qv x t, t = 2 qv x v, the
 // quaternion normalised by np.linalg.norm (threshold 1e-30)
+ZDX_HD_NP void quat_normalize(const double* q, double* out);
 ZDX_HD_NP void transform_point(const double* q, const double* tr, const double* v, double* out) {
-    const double n = norm4(q);
-    double w = 1.0, qv[3] = {0.0, 0.0, 0.0};
-    if (!(n < 1e-30)) {
-        w = q[0] / n;
-        qv[0] = q[1] / n;
-        qv[1] = q[2] / n;
-        qv[2] = q[3] / n;
-    }
+    double qn[4];
+    quat_normalize(q, qn);
+    const double w = qn[0], qv[3] = {qn[1], qn[2], qn[3]};
     double t[3], c[3];
     cross3(qv, v, t);
     for (int k = 0; k < 3; ++k) t[k] = 2.0 * t[k];
@@ -257,22 +253,34 @@ ZDX_HD_NP double point_seg_dist2_t(const double* p, const double* a, const doubl
     return dot3(d, d);
 }
 
-// accumulate_Sn_Gn_from_polyline (polyline.py:193-209) over m points (3 doubles each)
+// one edge (p0, p1) of accumulate_Sn_Gn_from_polyline (polyline.py:193-209) added to Sn, Gn
+ZDX_HD_NP void loop_edge(const double* p0, const double* p1, double* Sn, double* Gn) {
+    double c[3], dx[3];
+    cross3(p0, p1, c);
+    for (int k = 0; k < 3; ++k) {
+        Sn[k] = Sn[k] + 0.5 * c[k];
+        dx[k] = p1[k] - p0[k];
+    }
+    const double s = dot3(p0, p1) + (1.0 / 3.0) * dot3(dx, dx);
+    const double g = -(1.0 / 3.0) * s;
+    for (int k = 0; k < 3; ++k) Gn[k] = Gn[k] + g * dx[k];
+}
+
+// accumulate_Sn_Gn_from_polyline over m points (3 doubles each)
 ZDX_HD_NP void loop_sn_gn(const double* P, int m, double* Sn, double* Gn) {
     for (int k = 0; k < 3; ++k) Sn[k] = Gn[k] = 0.0;
-    for (int i = 0; i < m; ++i) {
-        const double* p0 = P + 3 * i;
-        const double* p1 = P + 3 * ((i + 1) % m);
-        double c[3], dx[3];
-        cross3(p0, p1, c);
-        for (int k = 0; k < 3; ++k) {
-            Sn[k] = Sn[k] + 0.5 * c[k];
-            dx[k] = p1[k] - p0[k];
-        }
-        const double s = dot3(p0, p1) + (1.0 / 3.0) * dot3(dx, dx);
-        const double g = -(1.0 / 3.0) * s;
-        for (int k = 0; k < 3; ++k) Gn[k] = Gn[k] + g * dx[k];
+    for (int i = 0; i < m; ++i) loop_edge(P + 3 * i, P + 3 * ((i + 1) % m), Sn, Gn);
+}
+
+// quat_normalize (polyline.py:36-41): q / np.linalg.norm(q), the identity below 1e-30
+ZDX_HD_NP void quat_normalize(const double* q, double* out) {
+    const double n = norm4(q);
+    if (n < 1e-30) {
+        out[0] = 1.0;
+        out[1] = out[2] = out[3] = 0.0;
+        return;
     }
+    for (int k = 0; k < 4; ++k) out[k] = q[k] / n;
 }
 
 // contact_point_xc0 (polyline.py:211-218): |Sn|, with nA and xc0 (false: |Sn| < 1e-14, xc0 None, nA 0)

@@ -19,6 +19,7 @@
 #include <cstdio>
 
 #include "zdx_math.cuh"
+#include "zdx_npmath.cuh"
 #include "zdx_pair.cuh"
 #include "zdx_pyset.cuh"
 #include "zdx_radix.cuh"
@@ -202,7 +203,9 @@ __host__ __device__ inline int next_pow2(int n) {
 }
 
 // tri_tri_intersection_segment on one queued (A survivor, B survivor) entry; the segment and its
-// (ta, tb) key go to the CTA's segment list.
+// (ta, tb) key go to the CTA's segment list.  NPX: in numpy's arithmetic (zdx_npmath.cuh), with no
+// candidate provenance (that mode has no adjoint).
+template <bool NPX>
 __device__ __forceinline__ void eval_entry(const PairArgs& a, const K1Slot& S, const K1Side& SA, const K1Side& SB,
                                            int cap, int2 e, int* nseg) {
     V3 TA[3], TB[3];
@@ -214,7 +217,13 @@ __device__ __forceinline__ void eval_entry(const PairArgs& a, const K1Slot& S, c
     V3 nb{SB.pl[e.y], SB.pl[cap + e.y], SB.pl[2 * cap + e.y]};
     V3 o0, o1;
     int c0 = 0, c1 = 0;
-    if (tri_tri_src(TA, na, SA.pl[3 * cap + e.x], TB, nb, SB.pl[3 * cap + e.y], o0, o1, &c0, &c1)) {
+    bool hit;
+    if constexpr (NPX) {
+        hit = np::tri_tri(&TA[0].x, &na.x, SA.pl[3 * cap + e.x], &TB[0].x, &nb.x, SB.pl[3 * cap + e.y], &o0.x, &o1.x);
+    } else {
+        hit = tri_tri_src(TA, na, SA.pl[3 * cap + e.x], TB, nb, SB.pl[3 * cap + e.y], o0, o1, &c0, &c1);
+    }
+    if (hit) {
         int si = atomicAdd(nseg, 1);
         if (si < a.cap_seg) {
             st3(S.seg + 6 * si, o0);
@@ -226,6 +235,7 @@ __device__ __forceinline__ void eval_entry(const PairArgs& a, const K1Slot& S, c
     }
 }
 
+template <bool NPX>
 __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     __shared__ double sh_red[2][K1_THREADS / 32];
     __shared__ double sh_slab[3];  // hi(A.d), lo(B.d), slack of the certificate (the slab cull uses them)
@@ -248,7 +258,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     K1Slot S;
     carve_k1(a.k1_slots + (size_t)blockIdx.x * a.k1_slot_bytes, a.cap_side, a.cap_seg, &S);
     const int cap = a.cap_side;
-    const bool py = a.mode == 1;
+    const bool py = NPX || a.mode == 1;
     const int64_t iend = item_end_of(a);
 
     for (;;) {
@@ -266,7 +276,15 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         V3 tpos[2] = {V3{ps[0], ps[1], ps[2]}, V3{ps[7], ps[8], ps[9]}};
         Q4 qraw[2] = {Q4{ps[3], ps[4], ps[5], ps[6]}, Q4{ps[10], ps[11], ps[12], ps[13]}};
         Q4 qn[2];
-        for (int k = 0; k < 2; ++k) qn[k] = py ? qnormalize_py(qraw[k]) : qnormalize(qraw[k]);
+        for (int k = 0; k < 2; ++k) {
+            if constexpr (NPX) {
+                double q4[4] = {qraw[k].w, qraw[k].x, qraw[k].y, qraw[k].z}, o4[4];
+                np::quat_normalize(q4, o4);
+                qn[k] = Q4{o4[0], o4[1], o4[2], o4[3]};
+            } else {
+                qn[k] = py ? qnormalize_py(qraw[k]) : qnormalize(qraw[k]);
+            }
+        }
         const int mesh[2] = {a.pmesh[2 * (int64_t)p], a.pmesh[2 * (int64_t)p + 1]};
         const int64_t off[2] = {a.tri_off[mesh[0]], a.tri_off[mesh[1]]};
         const int nt[2] = {(int)(a.tri_off[mesh[0] + 1] - off[0]), (int)(a.tri_off[mesh[1] + 1] - off[1])};
@@ -377,8 +395,15 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 }
                 V3 n;
                 double d;
-                if (!plane_from_tri(w[0], w[1], w[2], n, d)) continue;
-                if (norm2(n) < 1e-30) continue;
+                if constexpr (NPX) {
+                    // polyline.py main: the offset of plane_from_tri, the normal of tri_normals
+                    V3 np_n;
+                    if (!np::plane_from_tri(&w[0].x, &np_n.x, &d)) continue;
+                    np::tri_normal(&w[0].x, &n.x);
+                } else {
+                    if (!plane_from_tri(w[0], w[1], w[2], n, d)) continue;
+                    if (norm2(n) < 1e-30) continue;
+                }
                 int i = atomicAdd(&sh_n[s], 1);
                 for (int k = 0; k < 3; ++k) {
                     D.tri[(3 * k + 0) * cap + i] = w[k].x;
@@ -505,7 +530,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                         wq_n += __popc(hb);
                         if (wq_n >= 32) {
                             __syncwarp();
-                            for (int q = lane; q < wq_n; q += 32) eval_entry(a, S, SA, SB, cap, wq[q], &sh_nseg);
+                            for (int q = lane; q < wq_n; q += 32) eval_entry<NPX>(a, S, SA, SB, cap, wq[q], &sh_nseg);
                             __syncwarp();
                             wq_n = 0;
                         }
@@ -513,7 +538,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 }
             }
             __syncwarp();
-            for (int q = lane; q < wq_n; q += 32) eval_entry(a, S, SA, SB, cap, wq[q], &sh_nseg);
+            for (int q = lane; q < wq_n; q += 32) eval_entry<NPX>(a, S, SA, SB, cap, wq[q], &sh_nseg);
             __syncthreads();
         } else if (nB > 0) {
             int ia = 0, ib = 0, dA = 0, dB = 0;
@@ -546,7 +571,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 }
                 __syncthreads();
                 const int nq = sh_nq;
-                for (int qi = tid; qi < nq; qi += K1_THREADS) eval_entry(a, S, SA, SB, cap, sh_q[qi], &sh_nseg);
+                for (int qi = tid; qi < nq; qi += K1_THREADS) eval_entry<NPX>(a, S, SA, SB, cap, sh_q[qi], &sh_nseg);
                 __syncthreads();
                 if (tid == 0) sh_nq = 0;
                 __syncthreads();
@@ -597,8 +622,13 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
 void launch_segments(const PairArgs& a, int grid, cudaStream_t s) {
     if (grid <= 0) return;
     // per device and cheap: set it on every launch
-    cudaFuncSetAttribute(k_segments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
-    k_segments<<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
+    if (a.mode == 2) {
+        cudaFuncSetAttribute(k_segments<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+        k_segments<true><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
+    } else {
+        cudaFuncSetAttribute(k_segments<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+        k_segments<false><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
+    }
 }
 
 // --------------------------------------------------------------------------------------------- stage 2
@@ -747,6 +777,7 @@ __device__ int uf_find_ro(const int* parent, int x) {
 // point buffer (12 n ints) and its rebuild list in the union-find parents (2 n ints), both unused until
 // the snap.  Lane 0 orders the candidates by an insertion sort, O(nc^2) for nc candidates: fine for the
 // tens a pop has when tol is small against the segments, slow when tol spans many of them.
+template <bool NPX>
 __device__ __forceinline__ int py_neighbours(const PostBufs& B, const double* S, int n, int i, const I3* ci, V3 imn,
                                              V3 imx, V3 p1, V3 q1, double tol2, int sp, int cnt, int lane,
                                              int* status) {
@@ -768,7 +799,11 @@ __device__ __forceinline__ int py_neighbours(const PostBufs& B, const double* S,
                 V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
                 bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y || imx.z < jmn.z ||
                             imn.z > jmx.z);
-                acc = ov && seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2;
+                if constexpr (NPX) {
+                    acc = ov && np::seg_seg_dist2(&p1.x, &q1.x, S + 6 * j, S + 6 * j + 3) <= tol2;
+                } else {
+                    acc = ov && seg_seg_dist2(p1, q1, ld3(S + 6 * j), ld3(S + 6 * j + 3)) <= tol2;
+                }
             }
         }
         const bool cand = best != (1 << 30);
@@ -827,12 +862,13 @@ __device__ __forceinline__ int py_neighbours(const PostBufs& B, const double* S,
 
 // The post-triangle part of the reference's per-pair body (src/main.cpp:2148-2219) for one pair, by
 // one warp.  Component / loop / contact order follows the reference exactly.
+template <bool NPX>
 __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, const int lane) {
     const int n = a.pair_nseg[p];
     int status = a.pair_status[p];
     const double* S = a.seg + 6 * a.pair_seg_off[p];
     const int mA = a.pmesh[2 * (int64_t)p];
-    const bool py = a.mode == 1;
+    const bool py = NPX || a.mode == 1;
     const double* ps = a.pose + 14 * (int64_t)p;
     const V3 dirAB = V3{ps[7], ps[8], ps[9]} - V3{ps[0], ps[1], ps[2]};
     const double me = a.mean_edge[mA];
@@ -882,7 +918,7 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     const V3 imn = ld3(B.bmn + 3 * i), imx = ld3(B.bmx + 3 * i);
                     int nel = 0;
                     if (py) {
-                        nel = py_neighbours(B, S, n, i, ci, imn, imx, p1, q1, tol2, sp, cnt, lane, &status);
+                        nel = py_neighbours<NPX>(B, S, n, i, ci, imn, imx, p1, q1, tol2, sp, cnt, lane, &status);
                     } else {
                         for (int jb = 0; jb < n; jb += 32) {
                             const int j = jb + lane;
@@ -991,7 +1027,11 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     bool close = false;
                     if (j < i && adjacent(ld_cell(B.pcell + 3 * j), ci)) {
                         V3 d = pi - ld3(B.pts + 3 * j);
-                        close = py ? (sqrt(dot(d, d)) <= h) : (dot(d, d) <= h * h);
+                        if constexpr (NPX) {
+                            close = np::norm3(&d.x) <= h;
+                        } else {
+                            close = py ? (sqrt(dot(d, d)) <= h) : (dot(d, d) <= h * h);
+                        }
                     }
                     unsigned bal = __ballot_sync(FULL, close);
                     if (lane == 0) {
@@ -1078,7 +1118,12 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     if (cv.x < cmin.x || cv.x > cmax.x || cv.y < cmin.y || cv.y > cmax.y || cv.z < cmin.z || cv.z > cmax.z)
                         continue;
                     double t = 0.0;
-                    const double d2 = pt_seg_d2t(ld3(B.V + 3 * v), pa, pb, t);
+                    double d2;
+                    if constexpr (NPX) {
+                        d2 = np::point_seg_dist2_t(B.V + 3 * v, &pa.x, &pb.x, &t);
+                    } else {
+                        d2 = pt_seg_d2t(ld3(B.V + 3 * v), pa, pb, t);
+                    }
                     hit = (d2 <= tol2 && t > 1e-6 && t < 1.0 - 1e-6) ? 1 : 0;
                 }
                 split_flag[e] = hit;
@@ -1114,7 +1159,12 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                         I3 cv = ld_cell(B.vcell + 3 * v);
                         if (!(cv.x < cmin.x || cv.x > cmax.x || cv.y < cmin.y || cv.y > cmax.y || cv.z < cmin.z ||
                               cv.z > cmax.z)) {
-                            double d2 = pt_seg_d2t(ld3(B.V + 3 * v), pa, pb, t);
+                            double d2;
+                            if constexpr (NPX) {
+                                d2 = np::point_seg_dist2_t(B.V + 3 * v, &pa.x, &pb.x, &t);
+                            } else {
+                                d2 = pt_seg_d2t(ld3(B.V + 3 * v), pa, pb, t);
+                            }
                             ok = d2 <= tol2 && t > 1e-6 && t < 1.0 - 1e-6;
                         }
                     }
@@ -1271,15 +1321,22 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     const int* lv = B.loop_vid + B.loop_off[l];
                     if (len < 3) continue;
                     V3 Sn{0.0, 0.0, 0.0}, Gn{0.0, 0.0, 0.0};
-                    for (int q = 0; q < len; ++q) {
-                        V3 p0 = ld3(B.V + 3 * lv[q]);
-                        V3 p1 = ld3(B.V + 3 * lv[(q + 1) % len]);
-                        Sn = Sn + cross(p0, p1) * 0.5;
-                        V3 dx = p1 - p0;
-                        double s = dot(p0, p1) + (1.0 / 3.0) * dot(dx, dx);
-                        Gn = Gn + dx * (-(1.0 / 3.0) * s);
+                    double area;
+                    if constexpr (NPX) {
+                        for (int q = 0; q < len; ++q)
+                            np::loop_edge(B.V + 3 * lv[q], B.V + 3 * lv[(q + 1) % len], &Sn.x, &Gn.x);
+                        area = np::norm3(&Sn.x);
+                    } else {
+                        for (int q = 0; q < len; ++q) {
+                            V3 p0 = ld3(B.V + 3 * lv[q]);
+                            V3 p1 = ld3(B.V + 3 * lv[(q + 1) % len]);
+                            Sn = Sn + cross(p0, p1) * 0.5;
+                            V3 dx = p1 - p0;
+                            double s = dot(p0, p1) + (1.0 / 3.0) * dot(dx, dx);
+                            Gn = Gn + dx * (-(1.0 / 3.0) * s);
+                        }
+                        area = norm(Sn);
                     }
-                    double area = norm(Sn);
                     V3 nA{0.0, 0.0, 0.0}, xc0{0.0, 0.0, 0.0};
                     bool contact = false;
                     if (!py) {
@@ -1298,7 +1355,14 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                             lo = V3{fmin(lo.x, pq.x), fmin(lo.y, pq.y), fmin(lo.z, pq.z)};
                             hi = V3{fmax(hi.x, pq.x), fmax(hi.y, pq.y), fmax(hi.z, pq.z)};
                         }
-                        if (!(norm(hi - lo) < tol * 2)) {
+                        const V3 ext = hi - lo;
+                        double diag;
+                        if constexpr (NPX) {
+                            diag = np::norm3(&ext.x);
+                        } else {
+                            diag = norm(ext);
+                        }
+                        if (!(diag < tol * 2)) {
                             contact = true;
                             if (area < 1e-14) {
                                 area = 0.0;
@@ -1410,6 +1474,7 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
     __syncwarp();
 }
 
+template <bool NPX>
 __global__ __launch_bounds__(K2_WARPS * 32) void k_rebuild(PairArgs a) {
     const int lane = threadIdx.x & 31;
     const int64_t wslot = (int64_t)blockIdx.x * K2_WARPS + (threadIdx.x >> 5);
@@ -1422,14 +1487,15 @@ __global__ __launch_bounds__(K2_WARPS * 32) void k_rebuild(PairArgs a) {
         if (lane == 0) item = (int)(a.item_begin + atomicAdd(a.queue2, 1));
         item = __shfl_sync(FULL, item, 0);
         if (item >= iend) break;
-        rebuild_pair(a, a.order[item], B, lane);
+        rebuild_pair<NPX>(a, a.order[item], B, lane);
     }
 }
 
 void launch_rebuild(const PairArgs& a, int warps, cudaStream_t s) {
     if (warps <= 0) return;
     int blocks = (warps + K2_WARPS - 1) / K2_WARPS;
-    k_rebuild<<<blocks, K2_WARPS * 32, 0, s>>>(a);
+    if (a.mode == 2) k_rebuild<true><<<blocks, K2_WARPS * 32, 0, s>>>(a);
+    else k_rebuild<false><<<blocks, K2_WARPS * 32, 0, s>>>(a);
 }
 
 // --------------------------------------------------------------------------------------------- stage 3

@@ -24,6 +24,7 @@ ZDX_ERR_STATE = 7
 
 MODE_ZDEM = 0
 MODE_POLYLINE = 1
+MODE_POLYLINE_NUMPY = 2  # polyline mode in numpy's own arithmetic
 MEM_HOST = 0
 MEM_DEVICE = 1
 SCHED_BATCHED = 0
