@@ -64,8 +64,9 @@ int zdx_mesh_build(const double* tris, int64_t ntri, int center_mesh, double* tr
 #define ZDX_MODE_POLYLINE 1  /* polyline.py semantics: tol given, bbox filter, stable orders, no flip    */
 /* ZDX_MODE_POLYLINE in numpy's own arithmetic, as polyline.py rounds on an x86-64 numpy whose 3-vector
  * np.dot is the fused chain fma(a2, b2, fma(a1, b1, a0 b0)): np.linalg.norm as the root of that chain,
- * tri_normals' row norms for the triangle test's normals.  Meant to give polyline.py's numbers to the
- * bit.  zdx_pair_contacts only (not the adjoint, not zdx_pair_contacts_noalloc). */
+ * tri_normals' row norms for the triangle test's normals.  Gives polyline.py's numbers to the bit (its
+ * fixtures, split and not, on a B200).  zdx_pair_contacts only (not the adjoint, not
+ * zdx_pair_contacts_noalloc). */
 #define ZDX_MODE_POLYLINE_NUMPY 2
 #define ZDX_MEM_HOST 0
 #define ZDX_MEM_DEVICE 1
@@ -237,8 +238,12 @@ int zdx_run_config_graph(const char* config_path, int device);
  *     opts->sched ZDX_SCHED_BATCHED, opts->want_loop_points 0.
  *   - Limits (larger inputs are rejected with ZDX_ERR_INVALID and a message): ZDX_NOALLOC_MAX_* below;
  *     more than 65536 segments in one call reports ZDX_ERR_CAPACITY.
- *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
- *     device current; make that first call before any stream capture.
+ *   - zdx_create looks up the array's device address (cudaGetSymbolAddress) with its device current,
+ *     which is also when the CUDA runtime loads the array onto that GPU.  Create the context before
+ *     reserving a pool that takes the rest of the device, and before any stream capture.
+ *   - Triangle-stage CTAs and rebuild warps share what the fixed buffers leave of the array (7.9 MiB):
+ *     their slots are sized for the call's largest mesh and largest segment count, so calls on small
+ *     meshes run on more CTAs and warps (4 triangle-stage CTAs at 5120 triangles, 18 at 1280, 51 at 320).
  *   - Every call on a device shares the one array and leaves its contents there (what must start at zero
  *     is cleared by each call); calls that overlap on the GPU race on it. */
 #define ZDX_NOALLOC_SCRATCH_BYTES (16u << 20)

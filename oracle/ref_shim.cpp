@@ -271,6 +271,45 @@ extern "C" int64_t zdx_ref_pair_batch(const double* tris, const int64_t* tri_off
     return total.load();
 }
 
+// The same as zdx_ref_pair_batch, keeping what the bench compares with the GPU's output of the same
+// pairs: per pair its segments, components, raw loops and contacts, and the first `geom_cap` accepted
+// loops' 13 values (Sn Gn xc0 nA area) in the reference's order.
+extern "C" int64_t zdx_ref_pair_batch_rec(const double* tris, const int64_t* tri_off, const double* mean_edge,
+                                          const double* bbox_diag, int n_mesh, int64_t n_pairs,
+                                          const int32_t* pair_mesh, const double* pose, int split_contacts,
+                                          int nthreads, int32_t* stats4, int geom_cap, double* geom13) {
+    std::vector<Mesh> meshes(n_mesh);
+    for (int m = 0; m < n_mesh; ++m) {
+        meshes[m].tris = tris_from(tris + 9 * tri_off[m], static_cast<int>(tri_off[m + 1] - tri_off[m]));
+        meshes[m].mean_edge = mean_edge[m];
+        meshes[m].bbox_diag = bbox_diag[m];
+    }
+    std::atomic<int64_t> next{0}, total{0};
+    auto work = [&]() {
+        for (;;) {
+            int64_t p = next.fetch_add(1);
+            if (p >= n_pairs) break;
+            ZdxRefPairOut o;
+            int c = run_pair(meshes[pair_mesh[2 * p]], meshes[pair_mesh[2 * p + 1]], pose_from(pose + 14 * p),
+                             pose_from(pose + 14 * p + 7), split_contacts, &o);
+            stats4[4 * p + 0] = o.nseg;
+            stats4[4 * p + 1] = o.ncomp;
+            stats4[4 * p + 2] = o.nloop;
+            stats4[4 * p + 3] = c;
+            int k = 0;
+            for (int l = 0; l < o.nloop && k < geom_cap; ++l)
+                if (o.loop_status[l] == 3) std::memcpy(geom13 + 13 * (p * geom_cap + k++), o.loop_geom + 13 * l, 13 * sizeof(double));
+            zdx_ref_pair_free(&o);
+            total.fetch_add(c);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(nthreads, 1); ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    return total.load();
+}
+
 extern "C" void zdx_ref_pair_free(ZdxRefPairOut* o) {
     void* ps[] = {o->seg, o->comp_off, o->comp_idx, o->v_off, o->V, o->e_off, o->E, o->e2_off, o->E2,
                   o->loop_comp, o->loop_off, o->loop_vid, o->loop_status, o->loop_geom};

@@ -55,6 +55,13 @@ int64_t zdx_ref_pair_batch(const double* tris, const int64_t* tri_off, const dou
                            const double* bbox_diag, int n_mesh, int64_t n_pairs, const int32_t* pair_mesh,
                            const double* pose, int split_contacts, int nthreads, int32_t* ncontact);
 
+/* zdx_ref_pair_batch that also keeps, per pair, stats4 = segments, components, raw loops, contacts and,
+ * in geom13 (n_pairs x geom_cap x 13), the first geom_cap accepted loops' Sn Gn xc0 nA area. */
+int64_t zdx_ref_pair_batch_rec(const double* tris, const int64_t* tri_off, const double* mean_edge,
+                               const double* bbox_diag, int n_mesh, int64_t n_pairs, const int32_t* pair_mesh,
+                               const double* pose, int split_contacts, int nthreads, int32_t* stats4, int geom_cap,
+                               double* geom13);
+
 /* compute_wall_contact (src/main.cpp:1205-1258).  Returns 1 on contact. */
 int zdx_ref_wall_contact(const double* tris, int ntri, const double* pose, const double* wall_tri9,
                          const double* wall_normal, double radius, double tol, double* area,

@@ -42,7 +42,7 @@ sys.path[:0] = [os.path.join(ROOT, "zedm-x_b200"), os.path.join(ROOT, "oracle")]
 from oracle import Reference  # noqa: E402
 from zdemx import synth  # noqa: E402
 
-REF_PY = "/root/reference"
+REF_PY = os.environ.get("ZDX_REFERENCE_ROOT", "/root/reference")
 
 
 def pack(prefix, r, d):

@@ -1,8 +1,7 @@
 """The spinning 8-particle cluster on the GPU against the reference program (the comparison of
-tests/test_dem_gpu.py): broad phase, multi-pair scatter order and history with split_contacts off.  Its
-scene was corrected (plain floats in the config) after the last B200 run, and the oracle's DEM step
-reproduces the reference on it bit for bit (tests/test_oracle_dem_cpu.py); collected last, after the
-rest of the GPU suite."""
+tests/test_dem_gpu.py): broad phase, multi-pair scatter order and history with split_contacts off.  The
+scene's config holds plain floats (numpy 2 reprs would not parse in either program), and the oracle's
+DEM step reproduces the reference on it bit for bit (tests/test_oracle_dem_cpu.py)."""
 import numpy as np
 import pytest
 

@@ -2,7 +2,7 @@
 offset, coplanar, rotated and tilted cubes, spheres in a face and on an edge, hulls, a mesh with a
 T-junction, grazing spheres (the shapes of tests/golden/polyline_hard_ref.npz, whose polyline-mode
 results come from polyline.py itself).  The oracle is pinned to the reference on the same shapes on the
-CPU (tests/test_oracle_pin.py).  Collected last, after the rest of the GPU suite."""
+CPU (tests/test_oracle_pin.py)."""
 import os
 
 import numpy as np

@@ -1,8 +1,7 @@
 """ZDX_MODE_POLYLINE_NUMPY on the GPU: the pair kernels in numpy's own arithmetic (zdx_npmath.cuh)
 against the oracle's numpy mode, bit for bit, on the three polyline fixtures, split and not.  The
 oracle's numpy mode is itself bit-exact with polyline.py on them (tests/test_oracle_pin.py), so this is
-the GPU against polyline.py's own numbers.  Written after the last B200 run of this build; collected
-last, after the rest of the GPU suite."""
+the GPU against polyline.py's own numbers."""
 import os
 
 import numpy as np

@@ -2,24 +2,24 @@
 whose own pool allocator owns the device, a real-time loop that cannot take cudaMalloc's device-wide
 synchronisation).  Its scratch is a fixed __device__ array inside libzdemx.so; the caller owns inputs
 and outputs.  Checked here against zdx_pair_contacts on the same inputs, bit-exact, on two calls in a
-row (the second call reuses the array the first one left behind).  Kept in its own file, collected last."""
+row (the second call reuses the array the first one left behind), with the device's free memory the
+same before and after the second call.  Kept in its own file, collected last."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def _setup():
+def _setup(levels=(1, 2, 2, 3, 3), npairs=200, depth=0.1):
     import torch
 
     from zdemx import synth
     from zdemx.contact import MeshLibrary
 
     rng = np.random.default_rng(77)
-    lib = MeshLibrary.build([synth.noised_icosphere(s, 1e-3, 0.15, rng) for s in (1, 2, 2, 3, 3)])
-    npairs = 200
+    lib = MeshLibrary.build([synth.noised_icosphere(s, 1e-3, 0.15, rng) for s in levels])
     pm = rng.integers(0, lib.n_mesh, size=(npairs, 2)).astype(np.int32)
-    pp = synth.pair_poses(rng, npairs, 1e-3, 0.0, 0.1)
+    pp = synth.pair_poses(rng, npairs, 1e-3, 0.0, depth)
     dev = torch.device("cuda", 0)
     meshes = {"tris": torch.from_numpy(lib.tris).to(dev), "tri_off": torch.from_numpy(lib.tri_off).to(dev),
               "mean_edge": torch.from_numpy(lib.mean_edge).to(dev),
@@ -39,12 +39,14 @@ def _outputs(npairs, cap):
             "info": torch.full((cap, 4), -1, dtype=torch.int32, device=dev)}
 
 
-def test_noalloc_matches_allocating_call_twice():
+@pytest.mark.parametrize("levels,npairs,depth", [((1, 2, 2, 3, 3), 200, 0.1), ((1, 4), 24, 0.05)],
+                         ids=["to1280", "to5120"])
+def test_noalloc_matches_allocating_call_twice(levels, npairs, depth):
     import torch
 
     from zdemx import _lib
 
-    meshes, pairs, npairs = _setup()
+    meshes, pairs, npairs = _setup(levels, npairs, depth)
     ctx = _lib.Context(0)
     try:
         cap = 16 * npairs
@@ -52,11 +54,17 @@ def test_noalloc_matches_allocating_call_twice():
         torch.cuda.synchronize()
         tot_ref = _lib.pair_contacts_device(ctx, meshes, pairs, ref, k=1e7, split=True)
         assert tot_ref[0] > npairs // 2
+        # within the no-allocation call's per-pair segment limit, so both calls must agree
+        assert int(ref["stats"][:, 0].max()) <= 1024
         for call in range(2):
             got = _outputs(npairs, cap)
             torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             tot = _lib.pair_contacts_noalloc(ctx, meshes, pairs, got, k=1e7, split=True)
             torch.cuda.synchronize()
+            if call == 1:
+                # the point of the entry: nothing on the device was allocated (or freed) by the call
+                assert torch.cuda.mem_get_info()[0] == free_before
             assert tot[:3] == tot_ref[:3], (call, tot, tot_ref)
             n = int(tot[0])
             for key in ("ncontact", "contact_off", "stats"):

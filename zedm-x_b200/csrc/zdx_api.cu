@@ -98,6 +98,7 @@ extern "C" int zdx_create(zdx_ctx** out, int device) {
         return ZDX_ERR_CUDA;
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
+    noalloc_setup(ctx);
     *out = ctx;
     return ZDX_OK;
 }
@@ -173,7 +174,11 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     std::vector<int64_t> off_h(NM + 1, 0);
     if (NM > 0) {
         if (host) std::memcpy(off_h.data(), ms->tri_off, sizeof(int64_t) * (NM + 1));
-        else CK(cudaMemcpy(off_h.data(), ms->tri_off, sizeof(int64_t) * (NM + 1), cudaMemcpyDeviceToHost));
+        else {
+            // on the context stream: a caller may have written tri_off there without waiting for it
+            CK(cudaMemcpyAsync(off_h.data(), ms->tri_off, sizeof(int64_t) * (NM + 1), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
     }
     int64_t total_tris = NM > 0 ? off_h[NM] : 0;
     int max_ntri = 0;
@@ -497,7 +502,10 @@ extern "C" int zdx_pair_contacts_adjoint(zdx_ctx* ctx, const zdx_pair_opts* opts
     int64_t total_tris = 0;
     if (ms->n_mesh > 0) {
         if (host) total_tris = ms->tri_off[ms->n_mesh];
-        else CK(cudaMemcpy(&total_tris, ms->tri_off + ms->n_mesh, sizeof(int64_t), cudaMemcpyDeviceToHost));
+        else {
+            CK(cudaMemcpyAsync(&total_tris, ms->tri_off + ms->n_mesh, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
     }
     // forward with the tape, into the context's own device buffers
     zdx_pair_opts fo = *opts;

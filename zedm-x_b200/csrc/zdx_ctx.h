@@ -18,6 +18,8 @@ struct DevBuf {
 };
 
 int ctx_fail(::zdx_ctx* c, int status, const char* fmt, ...);
+// Looks up the no-allocation call's scratch array on the context's device (zdx_noalloc.cu).
+void noalloc_setup(::zdx_ctx* c);
 
 struct Scene;  // DEM scene (zdx_scene.cu)
 

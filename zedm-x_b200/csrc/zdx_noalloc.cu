@@ -29,8 +29,6 @@ namespace {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[ZDX_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 128;
-constexpr int kTritestSlots = 2;   // CTAs of the triangle stage
-constexpr int kRebuildWarps = 4;   // warps of the rebuild stage
 constexpr int kSegArena = 65536;   // segments per call
 
 std::mutex g_mu;
@@ -38,7 +36,8 @@ unsigned char* g_scratch_addr[kMaxDevices] = {};
 
 // Device address of the scratch array on the context's device.  In host code g_noalloc_scratch names a
 // host-side stand-in, not device memory, so the address is looked up once per device (with that device
-// current) and cached; the first call on a device does this set-up.
+// current) and cached.  zdx_create does this set-up for its device (noalloc_setup below), which also
+// makes the CUDA runtime load the module and reserve the array then, not inside a later call.
 int scratch_address(zdx_ctx* ctx, unsigned char** out) {
     if (ctx->device < 0 || ctx->device >= kMaxDevices) return ctx_fail(ctx, ZDX_ERR_INVALID, "device index too large");
     std::lock_guard<std::mutex> lock(g_mu);
@@ -65,6 +64,18 @@ struct Carver {
 };
 
 }  // namespace
+
+namespace zdx {
+// Called by zdx_create with the context's device current: look the scratch array up now.  A failure is
+// not fatal here; zdx_pair_contacts_noalloc retries the lookup and reports it.
+void noalloc_setup(zdx_ctx* ctx) {
+    unsigned char* p = nullptr;
+    if (scratch_address(ctx, &p) != ZDX_OK) {
+        cudaGetLastError();
+        ctx->last_error.clear();
+    }
+}
+}  // namespace zdx
 
 #define CKN(call)                                                                                     \
     do {                                                                                              \
@@ -105,7 +116,11 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
     // sizes, read into host stack buffers
     int64_t off_h[ZDX_NOALLOC_MAX_MESHES + 1];
     off_h[0] = 0;
-    if (NM > 0) CKN(cudaMemcpy(off_h, ms->tri_off, sizeof(int64_t) * (NM + 1), cudaMemcpyDeviceToHost));
+    // read on the context stream, after whatever the caller queued there (it may have written these)
+    if (NM > 0) {
+        CKN(cudaMemcpyAsync(off_h, ms->tri_off, sizeof(int64_t) * (NM + 1), cudaMemcpyDeviceToHost, st));
+        CKN(cudaStreamSynchronize(st));
+    }
     int max_ntri = 0;
     for (int m = 0; m < NM; ++m) {
         int64_t c = off_h[m + 1] - off_h[m];
@@ -120,7 +135,10 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
         return ctx_fail(ctx, ZDX_ERR_INVALID, "noalloc call: %lld triangles in the mesh set, at most %d",
                         (long long)total_tris, ZDX_NOALLOC_MAX_TRIS);
     int32_t pm_h[2 * ZDX_NOALLOC_MAX_PAIRS];
-    if (NP > 0) CKN(cudaMemcpy(pm_h, pb->mesh, sizeof(int32_t) * 2 * NP, cudaMemcpyDeviceToHost));
+    if (NP > 0) {
+        CKN(cudaMemcpyAsync(pm_h, pb->mesh, sizeof(int32_t) * 2 * NP, cudaMemcpyDeviceToHost, st));
+        CKN(cudaStreamSynchronize(st));
+    }
     for (int64_t i = 0; i < 2 * NP; ++i)
         if (pm_h[i] < 0 || pm_h[i] >= NM) return ctx_fail(ctx, ZDX_ERR_INVALID, "pair mesh index out of range");
 
@@ -161,10 +179,9 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
     a.err = reinterpret_cast<int*>(cnt + 7);
     a.item_begin = 0;
     a.item_end = NP;
-    a.cap_side = ZDX_NOALLOC_MAX_TRIS_PER_MESH;
+    a.cap_side = std::max(max_ntri, 1);
     a.cap_seg = seg_cap;
-    a.k1_slot_bytes = (tritest_slot_bytes(a.cap_side, ZDX_NOALLOC_MAX_SEG_PER_PAIR) + 255) & ~size_t(255);
-    a.k1_slots = cv.take<char>(a.k1_slot_bytes * kTritestSlots);
+    a.mesh_infl_bits = cv.take<unsigned long long>(ZDX_NOALLOC_MAX_MESHES);
     a.seg = cv.take<double>(6 * (size_t)kSegArena);
     a.seg_cap = kSegArena;
     a.pair_seg_off = cv.take<int64_t>(ZDX_NOALLOC_MAX_PAIRS);
@@ -177,10 +194,6 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
     a.pair_ncontact = cv.take<int32_t>(ZDX_NOALLOC_MAX_PAIRS);
     a.pair_ncomp = cv.take<int32_t>(ZDX_NOALLOC_MAX_PAIRS);
     a.pair_nloop = cv.take<int32_t>(ZDX_NOALLOC_MAX_PAIRS);
-    a.k2_nmax = ZDX_NOALLOC_MAX_SEG_PER_PAIR;
-    a.k2_slot_bytes = (rebuild_slot_bytes(a.k2_nmax) + 255) & ~size_t(255);
-    a.k2_nslots = kRebuildWarps;
-    a.k2_slots = cv.take<char>(a.k2_slot_bytes * kRebuildWarps);
     a.contact_cap = std::max<int64_t>(out->contact_cap, 0);
     a.cgeom_stage = cv.take<double>(20 * (size_t)ZDX_NOALLOC_MAX_CONTACTS);
     a.cinfo_stage = cv.take<int32_t>(4 * (size_t)ZDX_NOALLOC_MAX_CONTACTS);
@@ -188,24 +201,56 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
     a.pts_stage = nullptr;
     a.pts_cap = 0;
     int64_t* poff = cv.take<int64_t>(ZDX_NOALLOC_MAX_PAIRS + 1);
-    if (cv.off > ZDX_NOALLOC_SCRATCH_BYTES)
-        return ctx_fail(ctx, ZDX_ERR_INVALID, "noalloc scratch layout needs %zu bytes", cv.off);
+    // The rest of the array holds the per-CTA slots of the triangle stage and, once that stage is done,
+    // the per-warp slots of the rebuild stage (the same bytes; the stream orders the two).  Slots are
+    // sized for this call's largest mesh and, after the triangle stage, for its largest segment count,
+    // so small meshes get more CTAs and warps out of the same fixed bytes.
+    const size_t var_off = cv.off;
+    if (var_off >= ZDX_NOALLOC_SCRATCH_BYTES)
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "noalloc scratch layout needs %zu bytes", var_off);
+    const size_t room = ZDX_NOALLOC_SCRATCH_BYTES - var_off;
+    char* var_base = reinterpret_cast<char*>(base + var_off);
+    a.k1_slot_bytes = (tritest_slot_bytes(a.cap_side, seg_cap) + 255) & ~size_t(255);
+    const int64_t k1_fit = (int64_t)(room / a.k1_slot_bytes);
+    if (k1_fit < 1) return ctx_fail(ctx, ZDX_ERR_INVALID, "noalloc call: a triangle-stage slot does not fit the scratch array");
+    const int k1_grid = (int)std::min<int64_t>(std::min<int64_t>(k1_fit, (int64_t)ctx->num_sms * k1_blocks_per_sm()),
+                                               std::max<int64_t>(NP, 1));
+    a.k1_slots = var_base;
 
     // clear what must start at zero; everything else is written before it is read
+    CKN(cudaEventRecord(ctx->ev[0], st));
     CKN(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
     CKN(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
     CKN(cudaMemsetAsync(a.mesh_R_bits, 0, sizeof(unsigned long long) * std::max(NM, 1), st));
     CKN(cudaMemsetAsync(a.mesh_valid, 0, sizeof(int) * std::max(NM, 1), st));
+    CKN(cudaMemsetAsync(a.mesh_infl_bits, 0, sizeof(unsigned long long) * std::max(NM, 1), st));
     launch_mesh_prep(a, total_tris, st);
     launch_cost_order(a, order, buckets, st);
     a.order = order;
     CKN(cudaGetLastError());
+    ctx->launches += total_tris > 0 ? 1 : 0;
+    ctx->launches += NP > 0 ? 3 : 0;
+    unsigned long long hc[8];
     if (NP > 0) {
-        launch_segments(a, (int)std::min<int64_t>(NP, kTritestSlots), st);
-        launch_rebuild(a, kRebuildWarps, st);
+        launch_segments(a, k1_grid, st);
+        ctx->launches += 1;
+        CKN(cudaGetLastError());
+        CKN(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        CKN(cudaStreamSynchronize(st));
+        if (static_cast<int>(hc[7] & 0xffffffffull) & ERR_SEG_ARENA)
+            return ctx_fail(ctx, ZDX_ERR_CAPACITY, "noalloc call: more than %d segments in one call", kSegArena);
+        a.k2_nmax = std::max(static_cast<int>(hc[6] & 0xffffffffull), 1);
+        a.k2_slot_bytes = (rebuild_slot_bytes(a.k2_nmax) + 255) & ~size_t(255);
+        const int64_t k2_fit = (int64_t)(room / a.k2_slot_bytes);
+        if (k2_fit < 1)
+            return ctx_fail(ctx, ZDX_ERR_INVALID, "noalloc call: a rebuild slot for %d segments does not fit the scratch array",
+                            a.k2_nmax);
+        a.k2_nslots = std::min<int64_t>(std::min<int64_t>(k2_fit, (int64_t)ctx->num_sms * 32), NP);
+        a.k2_slots = var_base;
+        launch_rebuild(a, (int)a.k2_nslots, st);
+        ctx->launches += 1;
         CKN(cudaGetLastError());
     }
-    unsigned long long hc[8];
     CKN(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CKN(cudaStreamSynchronize(st));
     const int err = static_cast<int>(hc[7] & 0xffffffffull);
@@ -213,19 +258,23 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
     out->totals[1] = (int64_t)hc[0];
     out->totals[2] = (int64_t)hc[3];
     out->totals[3] = 0;
-    if (err & ERR_SEG_ARENA)
-        return ctx_fail(ctx, ZDX_ERR_CAPACITY, "noalloc call: more than %d segments in one call", kSegArena);
     if (err & ERR_CONTACT_STAGE)
         return ctx_fail(ctx, ZDX_ERR_CAPACITY, "need contact_cap >= %lld", (long long)hc[1]);
     if (hc[1] > 0 && (!out->contact_geom || !out->contact_info))
         return ctx_fail(ctx, ZDX_ERR_INVALID, "result has null contact arrays");
     launch_gather(a, out->pair_contact_off, poff, out->contact_geom, out->contact_info, nullptr, nullptr,
                   out->pair_stats, nullptr, st);
+    ctx->launches += NP > 0 ? 2 : 0;
     CKN(cudaGetLastError());
     if (NP == 0) CKN(cudaMemsetAsync(out->pair_contact_off, 0, sizeof(int64_t), st));
     if (NP > 0)
         CKN(cudaMemcpyAsync(out->pair_ncontact, a.pair_ncontact, sizeof(int32_t) * NP, cudaMemcpyDeviceToDevice, st));
+    CKN(cudaEventRecord(ctx->ev[4], st));
     CKN(cudaStreamSynchronize(st));
+    float el = 0.f;
+    cudaEventElapsedTime(&el, ctx->ev[0], ctx->ev[4]);
+    for (int i = 0; i < 4; ++i) ctx->pair_ms[i] = 0.0;
+    ctx->pair_ms[4] = el;
     if (err & ERR_PAIR) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "some pair exceeded its segment or edge capacity (see pair_stats)");
     return ZDX_OK;
 }

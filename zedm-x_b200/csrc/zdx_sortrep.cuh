@@ -9,6 +9,13 @@
 // that the permutation is the one libstdc++ produces.  Disjoint sub-ranges are sorted in a different
 // order than the recursive original, which cannot change the result.  Python's stable sort (polyline
 // mode) is provided as stable_sort_idx.
+//
+// Attribution: the step sequence restated here is that of GNU libstdc++ (GCC 13), std::sort in
+// bits/stl_algo.h (__introsort_loop, __move_median_to_first, __unguarded_partition_pivot,
+// __final_insertion_sort) and the heap helpers in bits/stl_heap.h (__adjust_heap, __push_heap,
+// __make_heap, __sort_heap).  libstdc++ is licensed under the GPL-3.0 with the GCC Runtime Library
+// Exception.  The reference program links it; reproducing its tie order is what makes the loop starts,
+// loop order and contact ids bit-exact with the reference.
 #pragma once
 #include "zdx_math.cuh"
 
