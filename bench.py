@@ -62,10 +62,14 @@ def parse():
     ap.add_argument("--preroll", type=int, default=1500, help="pour: untimed steps before warm-up (collisions start)")
     ap.add_argument("--rollout-steps", type=int, default=2000, help="rollout: steps of the rollout")
     ap.add_argument("--rollout-side", type=int, default=10, help="rollout: particles per lattice side")
+    ap.add_argument("--tune-pairs", type=int, default=16384,
+                    help="sweep: pairs of the autotuner's calibration sample (0: keep the default launch parameters)")
     return ap.parse_args()
 
 
-def workload(args, rank):
+def workload(args, rank, builder="zdemx"):
+    """The sweep's mesh library and pairs.  builder="reference" builds the meshes with the reference's own
+    build_mesh (oracle/_ref), so that the reference arm loads nothing of this library."""
     from zdemx import synth
     from zdemx.contact import MeshLibrary
 
@@ -73,7 +77,18 @@ def workload(args, rank):
     raw = []
     for s in (1, 2, 3, 4):
         raw.extend(list(synth.noised_icospheres(s, args.lib_per_level, 1e-3, 0.15, rng)))
-    lib = MeshLibrary.build(raw)
+    if builder == "reference":
+        from oracle import Reference
+
+        ref = Reference()
+        built = [ref.build_mesh(t, True) for t in raw]
+        outs = [o.reshape(-1, 9) for o, _ in built]
+        props = np.asarray([p for _, p in built]).reshape(-1, 17)
+        off = np.zeros(len(outs) + 1, np.int64)
+        off[1:] = np.cumsum([len(o) for o in outs])
+        lib = MeshLibrary(np.ascontiguousarray(np.concatenate(outs)), off, props[:, 5].copy(), props[:, 6].copy(), props)
+    else:
+        lib = MeshLibrary.build(raw)
     from zdemx.replicas import rank_seed
 
     prng = np.random.default_rng(rank_seed(args.seed, rank))
@@ -155,46 +170,55 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_issue():
-    """Warp instructions per pair of the two pair kernels (profiles/issue.json, from one ncu capture)."""
-    p = os.path.join(ROOT, "profiles", "issue.json")
-    try:
-        return json.load(open(p))
-    except (OSError, ValueError):
-        return None
+# Per-pair counters of the two pair kernels from one ncu capture of the 4,096-pair sweep sample
+# (profiles/pair_kernels_pairsweep4096.md gives the command and the raw figures).  They hold only for the
+# kernel sources they were captured on: KERNEL_SOURCES hashed to `sources_sha256`.  When the sources
+# differ, the figures are reported as stale (null) rather than applied to other code.
+PROFILED = {
+    "sources_sha256": None,
+    "k_segments": {"warp_inst_per_pair": None, "dram_bytes_per_pair": None},
+    "k_rebuild": {"warp_inst_per_pair": None, "dram_bytes_per_pair": None},
+}
+KERNEL_SOURCES = ("zdx_pair.cu", "zdx_pair.cuh", "zdx_math.cuh", "zdx_npmath.cuh", "zdx_pyset.cuh",
+                  "zdx_sortrep.cuh", "zdx_radix.cuh")
+
+
+def kernel_sources_sha256():
+    import hashlib
+
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, "zedm-x_b200", "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def profiled_current():
+    """The profiled per-pair figures if they were captured on the kernel sources in this tree."""
+    return PROFILED if PROFILED["sources_sha256"] == kernel_sources_sha256() else None
 
 
 def issue_roofline(reb_s, seg_s, pairs, clocks):
     """Issue-rate roofline of the two pair kernels: profiled warp instructions per pair x pairs over the
     live kernel time, against 4 warp instructions per cycle per SM at the median SM clock of the run."""
-    iss = profiled_issue()
-    if not iss:
-        return None
     import torch
 
+    prof = profiled_current()
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
     peak = 4.0 * sms * mhz * 1e6
     out = {"unit": "warp-inst/s", "peak": peak, "peak_kind": f"4 per cycle per SM x {sms} SMs x {mhz:.0f} MHz"}
+    if prof is None:
+        out["stale"] = "kernel sources differ from the profiled ones: no instruction count for this code"
+        return out
+    out["profiled_sources_sha256"] = prof["sources_sha256"]
     for name, t in (("k_rebuild", reb_s), ("k_segments", seg_s)):
-        inst = float(iss[name]["warp_inst_per_pair"]) * pairs
+        inst = float(prof[name]["warp_inst_per_pair"]) * pairs
         out[name] = {"bound": "issue", "achieved": inst / t, "frac": inst / t / peak, "warp_inst_per_launch": inst}
     return out
 
 
-def profiled_traffic():
-    """DRAM bytes per pair of the pair kernels from the committed ncu summaries, if any."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        try:
-            return json.load(open(p))
-        except Exception:
-            return None
-    return None
-
-
-def cpu_reference_rate(lib, pm, pp, nthreads, seconds, rng_seed=5, fixed=None):
-    """Time the reference's own per-pair code (oracle/_ref) on a bounded random sample of the workload."""
+def _ref_batch_lib():
     import ctypes as C
 
     from oracle import LIB_REF
@@ -203,31 +227,141 @@ def cpu_reference_rate(lib, pm, pp, nthreads, seconds, rng_seed=5, fixed=None):
     L.zdx_ref_pair_batch.restype = C.c_int64
     L.zdx_ref_pair_batch.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                                         C.c_void_p]
+    L.zdx_ref_pair_batch_rec.restype = C.c_int64
+    L.zdx_ref_pair_batch_rec.argtypes = [C.c_void_p] * 4 + [C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_int,
+                                                            C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+    return L
+
+
+PARITY_GEOM_CAP = 64
+
+
+def cpu_reference_rate(lib, pm, pp, nthreads, seconds, rng_seed=5, fixed=None, record=False):
+    """Time the reference's own per-pair code (oracle/_ref) on a bounded random sample of the workload.
+    With record, the sample's per-pair results (segments, components, raw loops, contacts and the
+    accepted loops' Sn Gn xc0 nA area) come back too, for the parity check against the GPU."""
+    L = _ref_batch_lib()
     rng = np.random.default_rng(rng_seed)
     order = rng.permutation(len(pm))
+    rec = {}
 
     def run(sel):
         spm = np.ascontiguousarray(pm[sel])
         spp = np.ascontiguousarray(pp[sel])
-        t0 = time.perf_counter()
-        L.zdx_ref_pair_batch(lib.tris.ctypes.data, lib.tri_off.ctypes.data, lib.mean_edge.ctypes.data,
-                             lib.bbox_diag.ctypes.data, lib.n_mesh, len(sel), spm.ctypes.data, spp.ctypes.data, 1,
-                             nthreads, None)
+        args = (lib.tris.ctypes.data, lib.tri_off.ctypes.data, lib.mean_edge.ctypes.data, lib.bbox_diag.ctypes.data,
+                lib.n_mesh, len(sel), spm.ctypes.data, spp.ctypes.data, 1, nthreads)
+        if record:
+            rec["stats"] = np.zeros((len(sel), 4), np.int32)
+            rec["geom"] = np.zeros((len(sel), PARITY_GEOM_CAP, 13))
+            t0 = time.perf_counter()
+            L.zdx_ref_pair_batch_rec(*args, rec["stats"].ctypes.data, PARITY_GEOM_CAP, rec["geom"].ctypes.data)
+        else:
+            t0 = time.perf_counter()
+            L.zdx_ref_pair_batch(*args, None)
         return time.perf_counter() - t0
 
     if fixed is not None:
         dt = run(fixed)
-        return len(fixed) / dt, len(fixed), dt, fixed
+        return len(fixed) / dt, len(fixed), dt, fixed, rec
     n = 32 * nthreads
     dt = run(order[:n])
     n = int(min(len(pm), max(n, n * seconds / max(dt, 1e-3))))
     sel = order[:n]
     dt = run(sel)
-    return n / dt, n, dt, sel
+    return n / dt, n, dt, sel, rec
+
+
+def parity_check(sel, rec, stats, coff, geom):
+    """The GPU's results for the sampled pairs against the reference's: per pair the segment, component,
+    raw-loop and contact counts, and every contact's Sn Gn xc0 nA area, bit for bit."""
+    bad_pairs = 0
+    fields = {"segments": 0, "components": 0, "raw_loops": 0, "contacts": 0, "contact_geometry": 0}
+    checked_contacts = 0
+    for k, p in enumerate(sel):
+        r = rec["stats"][k]
+        g = stats[p]
+        nc = int(coff[p + 1] - coff[p])
+        bad = False
+        for f, a, b in (("segments", g[0], r[0]), ("components", g[1], r[1]), ("raw_loops", g[2], r[2]),
+                        ("contacts", nc, r[3])):
+            if int(a) != int(b):
+                fields[f] += 1
+                bad = True
+        if not bad:
+            m = min(nc, PARITY_GEOM_CAP)
+            checked_contacts += m
+            if m and not np.array_equal(geom[coff[p]:coff[p] + m, :13], rec["geom"][k, :m]):
+                fields["contact_geometry"] += 1
+                bad = True
+        bad_pairs += bad
+    return {"pairs": int(len(sel)), "contacts": int(checked_contacts), "mismatches": int(bad_pairs),
+            "mismatches_by_field": fields, "against": "oracle/_ref (the reference's src/main.cpp, unchanged)",
+            "compare": "bit for bit: segments, components, raw loops, contacts per pair; Sn Gn xc0 nA area per contact"}
 
 
 def emit(d):
     print(json.dumps(d), flush=True)
+
+
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
+def _sweep_buffers(dev, npairs, cap):
+    import torch
+
+    return {"ncontact": torch.zeros(npairs, dtype=torch.int32, device=dev),
+            "contact_off": torch.zeros(npairs + 1, dtype=torch.int64, device=dev),
+            "stats": torch.zeros(npairs, 4, dtype=torch.int32, device=dev),
+            "geom": torch.zeros(cap, 20, dtype=torch.float64, device=dev),
+            "info": torch.zeros(cap, 4, dtype=torch.int32, device=dev)}
+
+
+def _device_steps(ctx, call, flush, steps):
+    """Run `call` steps times (L2 flushed before each); the library's own CUDA-event times per call."""
+    import torch
+
+    ms, seg, reb = [], [], []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        tot = call()
+        t = ctx.timings()
+        ms.append(t["total"])
+        seg.append(t["segments"])
+        reb.append(t["rebuild"])
+    return tot, ms, seg, reb
+
+
+def run_reference_sweep(args, base_cfg):
+    """The reference's own C++ per-pair code on all host threads, over a bounded sample per step."""
+    from oracle import LIB_REF
+
+    if not os.path.exists(LIB_REF):
+        emit({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"})
+        return
+    lib, pm, pp = workload(args, 0, builder="reference")
+    nthreads = os.cpu_count() or 1
+    # size one step's sample to ~2 s of work on all threads
+    rate, n, dt, sel, _ = cpu_reference_rate(lib, pm, pp, nthreads, 2.0)
+    times = []
+    for i in range(args.warmup + args.steps):
+        r, _, d, _, _ = cpu_reference_rate(lib, pm, pp, nthreads, 0.0, fixed=sel)
+        if i >= args.warmup:
+            times.append(d)
+    T = sum(times)
+    value = len(sel) * len(times) / T
+    sample = f"{len(sel)} random pairs of the {args.pairs}-pair workload per step"
+    emit({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / len(times),
+          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+          "data": "synthetic (seeded noised icospheres)", "config": base_cfg,
+          "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "reference", "sample": sample},
+          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
 
 
 def main():
@@ -254,31 +388,8 @@ def main():
                 "parallelism": f"replicas x{world} (independent pair batches)", "seed": args.seed}
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        from oracle import LIB_REF
-
-        if not os.path.exists(LIB_REF):
-            emit({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"})
-            return
-        lib, pm, pp = workload(args, 0)
-        nthreads = os.cpu_count() or 1
-        # size one step's sample to ~2 s of work on all threads
-        rate, n, dt, sel = cpu_reference_rate(lib, pm, pp, nthreads, 2.0)
-        times = []
-        for i in range(args.warmup + args.steps):
-            r, _, d, _ = cpu_reference_rate(lib, pm, pp, nthreads, 0.0, fixed=sel)
-            if i >= args.warmup:
-                times.append(d)
-        T = sum(times)
-        value = len(sel) * len(times) / T
-        sample = f"{len(sel)} random pairs of the {args.pairs}-pair workload per step"
-        emit({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-              "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / len(times),
-              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-              "data": "synthetic (seeded noised icospheres)", "config": base_cfg,
-              "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "reference", "sample": sample},
-              "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        if rank == 0:
+            run_reference_sweep(args, base_cfg)
         return
 
     import torch
@@ -305,17 +416,28 @@ def main():
     d_pm = torch.from_numpy(pm).to(dev)
     d_pp = torch.from_numpy(pp).to(dev)
     cap = 16 * args.pairs
-    out = {"ncontact": torch.zeros(args.pairs, dtype=torch.int32, device=dev),
-           "contact_off": torch.zeros(args.pairs + 1, dtype=torch.int64, device=dev),
-           "stats": torch.zeros(args.pairs, 4, dtype=torch.int32, device=dev),
-           "geom": torch.zeros(cap, 20, dtype=torch.float64, device=dev),
-           "info": torch.zeros(cap, 4, dtype=torch.int32, device=dev)}
+    out = _sweep_buffers(dev, args.pairs, cap)
     meshes = {"tris": d_tris, "tri_off": d_off, "mean_edge": d_me, "bbox_diag": d_bd}
     pairs = {"mesh": d_pm, "pose": d_pp}
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
     def step():
         return _lib.pair_contacts_device(ctx, meshes, pairs, out, k=1e7, split=True)
+
+    # launch parameters from the autotuner, on a calibration sample of the same mix (another seed)
+    tuning = {"best": ctx.tuning(), "calibration_pairs": 0}
+    if args.tune_pairs > 0:
+        from zdemx import autotune
+
+        clib, cpm, cpp = autotune.sweep_sample(args.tune_pairs, args.seed + 1)
+        cm, cp, co = autotune.device_batch(clib, cpm, cpp, dev)
+        tres = autotune.tune(ctx, cm, cp, co, flush=flush)
+        tuning = {"best": tres["best"], "calibration_pairs": tres["pairs"], "calibration_ms": tres["best_ms"],
+                  "calibration_default_ms": tres["default_ms"], "trials": len(tres["trials"]),
+                  "tuner": "zdemx.autotune (coordinate descent over flat_max, tri_ctas_per_sm, rebuild_warps, "
+                           "split_tests)"}
+        del cm, cp, co
+        torch.cuda.empty_cache()
 
     for _ in range(args.warmup):
         totals = step()
@@ -324,17 +446,9 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = ctx.timings()["launches"]
-    step_ms, seg_ms, reb_ms = [], [], []
     wall0 = time.perf_counter()
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            totals = step()
-            t = ctx.timings()
-            step_ms.append(t["total"])
-            seg_ms.append(t["segments"])
-            reb_ms.append(t["rebuild"])
+        totals, step_ms, seg_ms, reb_ms = _device_steps(ctx, step, flush, args.steps)
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     launches = ctx.timings()["launches"] - launches0
@@ -345,15 +459,13 @@ def main():
         T = max_over_ranks(T, dev)
         dist.barrier()
     value = world * args.pairs * args.steps / T
+    # the last timed step's outputs, for the parity check and the comparisons below
+    res = {k: v.cpu().numpy() for k, v in out.items() if k != "info"}
 
     # e2e: the same call with pinned host buffers, copies inside the timed region
     h = {k: torch.from_numpy(v).pin_memory() for k, v in
          {"tris": lib.tris, "off": lib.tri_off, "me": lib.mean_edge, "bd": lib.bbox_diag, "pm": pm, "pp": pp}.items()}
-    hout = {"ncontact": torch.zeros(args.pairs, dtype=torch.int32).pin_memory(),
-            "contact_off": torch.zeros(args.pairs + 1, dtype=torch.int64).pin_memory(),
-            "stats": torch.zeros(args.pairs, 4, dtype=torch.int32).pin_memory(),
-            "geom": torch.zeros(cap, 20, dtype=torch.float64).pin_memory(),
-            "info": torch.zeros(cap, 4, dtype=torch.int32).pin_memory()}
+    hout = {k: v.cpu().pin_memory() for k, v in out.items()}
     hmeshes = {"tris": h["tris"], "tri_off": h["off"], "mean_edge": h["me"], "bbox_diag": h["bd"]}
     hpairs = {"mesh": h["pm"], "pose": h["pp"]}
 
@@ -378,24 +490,42 @@ def main():
     h2d = sum(int(v.numel() * v.element_size()) for v in h.values())
     nct = int(tot_e[0])
     d2h = args.pairs * (4 + 8 + 16) + 8 + nct * (160 + 16)
+    del h, hout, hmeshes, hpairs
 
-    # plain form on a subset (one launch per stage per pair)
-    plain_n = min(args.plain_pairs, args.pairs)
-    sub = {"mesh": d_pm[:plain_n].contiguous(), "pose": d_pp[:plain_n].contiguous()}
-    _lib.pair_contacts_device(ctx, meshes, sub, out, k=1e7, split=True, sched=_lib.SCHED_PLAIN)
-    torch.cuda.synchronize()
-    _lib.pair_contacts_device(ctx, meshes, sub, out, k=1e7, split=True, sched=_lib.SCHED_PLAIN)
-    plain_ms = ctx.timings()["total"]
-    _lib.pair_contacts_device(ctx, meshes, sub, out, k=1e7, split=True)
-    batched_sub_ms = ctx.timings()["total"]
-    plain_value = plain_n / (plain_ms / 1e3)
-
-    if rank != 0:
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
+    if world > 1:
+        # the scaling run reports the headline numbers only; the comparisons below run at N=1
+        dist.barrier()
+        if rank == 0:
+            emit(_sweep_line(args, world, value, T, totals, launches, clk, wall, e2e_value, h2d, d2h, lib, pm,
+                             seg_ms, reb_ms, step_ms, base_cfg, extras={"tuning": tuning}))
+        dist.barrier()
+        dist.destroy_process_group()
         return
 
+    log(f"sweep: {value:.4g} pairs/s device, {e2e_value:.4g} e2e")
+    extras = {"tuning": tuning}
+    # parity of this step's output with the reference's own code on the CPU baseline's sample
+    rate, n_cpu, dt_cpu, sel, rec = cpu_reference_rate(lib, pm, pp, 1, args.cpu_seconds, record=True)
+    extras["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
+                              "sample": f"{n_cpu} random pairs of the workload through oracle/_ref, {dt_cpu:.1f} s"}
+    extras["parity"] = parity_check(sel, rec, res["stats"], res["contact_off"], res["geom"])
+    log(f"parity: {extras['parity']['pairs']} pairs, {extras['parity']['mismatches']} mismatches")
+    extras.update(sweep_comparisons(args, ctx, dev, meshes, pairs, out, res, flush, step_ms))
+    del d_tris
+    log("comparisons done")
+    extras["independent_meshes"] = sweep_independent(args, ctx, dev, flush)
+    log("independent meshes done")
+    torch.cuda.empty_cache()
+    extras["dem"] = {"pour": measure_pour(args, ctx, steps=args.steps, cpu=False)}
+    log("pour done")
+    extras["dem"]["two_particles"] = measure_two(args, ctx, reps=3, extras=False)
+    log("two particles done")
+    emit(_sweep_line(args, world, value, T, totals, launches, clk, wall, e2e_value, h2d, d2h, lib, pm, seg_ms,
+                     reb_ms, step_ms, base_cfg, extras))
+
+
+def _sweep_line(args, world, value, T, totals, launches, clk, wall, e2e_value, h2d, d2h, lib, pm, seg_ms, reb_ms,
+                step_ms, base_cfg, extras):
     # roofline of the dominant kernel (the rebuild): it reads each segment of the arena once (6 doubles)
     # and writes each contact once (20 doubles + 4 ints); the triangle stage's line follows it
     peak, peak_kind = measured_peaks()
@@ -404,41 +534,163 @@ def main():
     abytes = algorithmic_bytes(lib, pm)
     seg_s = statistics.mean(seg_ms) / 1e3
     achieved = abytes / seg_s / 1e9
-    tr = profiled_traffic() or {}
-    traffic = float(tr["k_segments"]["dram_bytes_per_pair"]) * args.pairs if "k_segments" in tr else None
-    reb_traffic = float(tr["k_rebuild"]["dram_bytes_per_pair"]) * args.pairs if "k_rebuild" in tr else None
-
-    rate, n_cpu, dt_cpu, _ = cpu_reference_rate(lib, pm, pp, 1, args.cpu_seconds)
+    prof = profiled_current()
+    traffic = prof["k_segments"]["dram_bytes_per_pair"] * args.pairs if prof else None
+    reb_traffic = prof["k_rebuild"]["dram_bytes_per_pair"] * args.pairs if prof else None
     cfg = dict(base_cfg)
     cfg.update({"l2": "flushed (256 MB write) before every timed step", "inputs": "device-resident for value",
                 "contacts_per_step": int(totals[0]), "segments_per_step": int(totals[1]),
                 "tri_aabb_checks_per_step": int(totals[2])})
-    emit({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-          "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps, "higher_is_better": True, "scaling": "weak",
-          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded noised icospheres, 1024-mesh library)",
-          "config": cfg,
-          "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-          "gpu_launches": int(launches),
-          "roofline": {"bound": "hbm", "achieved": reb_bytes / reb_s / 1e9, "peak": peak, "unit": "GB/s",
-                       "frac": reb_bytes / reb_s / 1e9 / peak, "traffic": reb_traffic, "kernel": "k_rebuild",
-                       "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": reb_bytes,
-                       "kernel_ms": 1e3 * reb_s,
-                       "note": "latency bound (serial per-pair topology in the reference's order); see profiles/"},
-          "roofline_k_segments": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                                  "frac": achieved / peak, "traffic": traffic, "kernel": "k_segments",
-                                  "algorithmic_bytes_per_launch": abytes, "kernel_ms": 1e3 * seg_s,
-                                  "note": "FP64 compare/ALU issue and scratch latency bound; see profiles/"},
-          "roofline_issue": issue_roofline(reb_s, seg_s, args.pairs, clk.summary()),
-          "stages_ms": {"triangle_tests": statistics.mean(seg_ms), "rebuild": statistics.mean(reb_ms),
-                        "whole_call": statistics.mean(step_ms)},
-          "plain": {"value": plain_value, "unit": UNIT, "pairs": plain_n, "batched_same_pairs": plain_n / (batched_sub_ms / 1e3),
-                    "speedup_batched_vs_plain": (plain_n / (batched_sub_ms / 1e3)) / plain_value},
-          "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
-                           "sample": f"{n_cpu} random pairs of the workload through oracle/_ref, {dt_cpu:.1f} s"},
-          "clocks": clk.summary(), "wall_s_timed": wall})
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": f"synthetic (seeded noised icospheres, {4 * args.lib_per_level}-mesh library)", "config": cfg,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": reb_bytes / reb_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": reb_bytes / reb_s / 1e9 / peak, "traffic": reb_traffic, "kernel": "k_rebuild",
+                         "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": reb_bytes,
+                         "kernel_ms": 1e3 * reb_s,
+                         "note": "latency bound (serial per-pair topology in the reference's order); see profiles/"},
+            "roofline_k_segments": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                    "frac": achieved / peak, "traffic": traffic, "kernel": "k_segments",
+                                    "algorithmic_bytes_per_launch": abytes, "kernel_ms": 1e3 * seg_s,
+                                    "note": "FP64 compare/ALU issue and scratch latency bound; see profiles/"},
+            "roofline_issue": issue_roofline(reb_s, seg_s, args.pairs, clk.summary()),
+            "stages_ms": {"triangle_tests": statistics.mean(seg_ms), "rebuild": statistics.mean(reb_ms),
+                          "whole_call": statistics.mean(step_ms)},
+            "clocks": clk.summary(), "wall_s_timed": wall}
+    line.update(extras)
+    return line
+
+
+def sweep_comparisons(args, ctx, dev, meshes, pairs, out, res, flush, step_ms):
+    """The batched call against its plain forms and the no-allocation entry, each on the same pairs and
+    checked to give the same results."""
+    import torch
+
+    from zdemx import _lib
+
+    out_ = {}
+    batched_ms = statistics.mean(step_ms)
+    # plain per-stage form on the whole batch: one launch per stage, no work queue, no cost order, no culls
+    ps = _sweep_buffers(dev, args.pairs, out["geom"].shape[0])
+    _lib.pair_contacts_device(ctx, meshes, pairs, ps, k=1e7, split=True, sched=_lib.SCHED_PER_STAGE)
+    _, ps_ms, ps_seg, ps_reb = _device_steps(
+        ctx, lambda: _lib.pair_contacts_device(ctx, meshes, pairs, ps, k=1e7, split=True, sched=_lib.SCHED_PER_STAGE),
+        flush, 2)
+    same = all(np.array_equal(ps[k].cpu().numpy(), res[k]) for k in ("ncontact", "contact_off", "stats")) and \
+        np.array_equal(ps["geom"].cpu().numpy()[: int(res["contact_off"][-1])], res["geom"][: int(res["contact_off"][-1])])
+    out_["plain_per_stage"] = {
+        "value": args.pairs / (statistics.mean(ps_ms) / 1e3), "unit": UNIT, "pairs": args.pairs,
+        "ms_per_step": statistics.mean(ps_ms), "stages_ms": {"triangle_tests": statistics.mean(ps_seg),
+                                                             "rebuild": statistics.mean(ps_reb)},
+        "speedup_batched_vs_plain_per_stage": statistics.mean(ps_ms) / batched_ms, "results_identical": bool(same),
+        "form": "one launch per stage over the batch; pairs in a fixed grid-stride order (no work queue, no cost "
+                "order); every nA x nB triangle pair AABB-tested (no certificate, cube, slab or hierarchical culls)"}
+    del ps
+    # plain per-pair form on a subset (one launch per stage per pair)
+    plain_n = min(args.plain_pairs, args.pairs)
+    sub = {"mesh": pairs["mesh"][:plain_n].contiguous(), "pose": pairs["pose"][:plain_n].contiguous()}
+    sub_out = _sweep_buffers(dev, plain_n, 16 * plain_n)
+    _lib.pair_contacts_device(ctx, meshes, sub, sub_out, k=1e7, split=True, sched=_lib.SCHED_PLAIN)
+    torch.cuda.synchronize()
+    _lib.pair_contacts_device(ctx, meshes, sub, sub_out, k=1e7, split=True, sched=_lib.SCHED_PLAIN)
+    plain_ms = ctx.timings()["total"]
+    _lib.pair_contacts_device(ctx, meshes, sub, sub_out, k=1e7, split=True)
+    batched_sub_ms = ctx.timings()["total"]
+    plain_value = plain_n / (plain_ms / 1e3)
+    out_["plain"] = {"value": plain_value, "unit": UNIT, "pairs": plain_n,
+                     "batched_same_pairs": plain_n / (batched_sub_ms / 1e3),
+                     "speedup_batched_vs_plain": (plain_n / (batched_sub_ms / 1e3)) / plain_value,
+                     "form": "one launch per stage per pair"}
+    # the no-allocation entry against the allocating call: 384 pairs of the sweep's mix (about 40,000
+    # segments of its 65,536), over at most 65,536 triangles (16, 8, 16 and 8 meshes of subdivision 1 to 4)
+    nn = min(384, args.pairs)
+    per_level = (16, 8, 16, 8)
+    tri_off = meshes["tri_off"].cpu().numpy()
+    ids = [lv * args.lib_per_level + i for lv in range(4) for i in range(min(per_level[lv], args.lib_per_level))]
+    sub_tris = torch.cat([meshes["tris"][int(tri_off[m]):int(tri_off[m + 1])] for m in ids])
+    sub_off = np.zeros(len(ids) + 1, np.int64)
+    sub_off[1:] = np.cumsum([tri_off[m + 1] - tri_off[m] for m in ids])
+    first = np.cumsum([0] + [min(c, args.lib_per_level) for c in per_level])
+    srng = np.random.default_rng([args.seed, 0x4E])
+    slv = srng.integers(0, 4, size=(nn, 2))
+    spm = (first[slv] + srng.integers(0, 1 << 30, size=(nn, 2)) % np.minimum(per_level, args.lib_per_level)[slv])
+    idx_t = torch.as_tensor(np.asarray(ids), device=dev)
+    nmesh = {"tris": sub_tris.contiguous(), "tri_off": torch.from_numpy(sub_off).to(dev),
+             "mean_edge": meshes["mean_edge"][idx_t].contiguous(), "bbox_diag": meshes["bbox_diag"][idx_t].contiguous()}
+    sub = {"mesh": torch.from_numpy(spm.astype(np.int32)).to(dev), "pose": pairs["pose"][:nn].contiguous()}
+    a_out = _sweep_buffers(dev, nn, 16384)
+    b_out = _sweep_buffers(dev, nn, 16384)
+    _lib.pair_contacts_device(ctx, nmesh, sub, a_out, k=1e7, split=True)
+    _, a_ms, _, _ = _device_steps(ctx, lambda: _lib.pair_contacts_device(ctx, nmesh, sub, a_out, k=1e7, split=True),
+                                  flush, 3)
+    _lib.pair_contacts_noalloc(ctx, nmesh, sub, b_out, k=1e7, split=True)
+    _, b_ms, _, _ = _device_steps(ctx, lambda: _lib.pair_contacts_noalloc(ctx, nmesh, sub, b_out, k=1e7, split=True),
+                                  flush, 3)
+    n_c = int(a_out["contact_off"][-1])
+    same = all(torch.equal(a_out[k], b_out[k]) for k in ("ncontact", "contact_off", "stats")) and \
+        torch.equal(a_out["geom"][:n_c], b_out["geom"][:n_c])
+    out_["noalloc"] = {"value": nn / (statistics.mean(b_ms) / 1e3), "unit": UNIT, "pairs": nn,
+                       "allocating_call_same_pairs": nn / (statistics.mean(a_ms) / 1e3),
+                       "results_identical": bool(same),
+                       "meshes": len(ids), "triangles": int(sub_off[-1]),
+                       "note": "zdx_pair_contacts_noalloc: scratch in the library's fixed 16 MiB device array"}
+    return out_
+
+
+def sweep_independent(args, ctx, dev, flush):
+    """The sweep with every pair's two meshes its own (2 x pairs meshes), device-timed and end to end."""
+    import torch
+
+    from zdemx import _lib
+    from zdemx.workloads import independent_pair_library, independent_pair_sizes
+    from zdemx import synth
+
+    t0 = time.perf_counter()
+    _, off, _ = independent_pair_sizes(args.pairs, args.seed)
+    h_tris = torch.empty((int(off[-1]), 9), dtype=torch.float64, pin_memory=True)
+    lib, pm = independent_pair_library(args.pairs, args.seed, out_tris=h_tris.numpy())
+    pp = synth.pair_poses(np.random.default_rng([args.seed, 0x1E]), args.pairs, 1e-3, 0.0, 0.1)
+    build_s = time.perf_counter() - t0
+    h = {"tris": h_tris, "tri_off": torch.from_numpy(lib.tri_off).pin_memory(),
+         "mean_edge": torch.from_numpy(lib.mean_edge).pin_memory(),
+         "bbox_diag": torch.from_numpy(lib.bbox_diag).pin_memory()}
+    hp = {"mesh": torch.from_numpy(pm).pin_memory(), "pose": torch.from_numpy(pp).pin_memory()}
+    d = {k: v.to(dev) for k, v in h.items()}
+    dp = {k: v.to(dev) for k, v in hp.items()}
+    cap = 16 * args.pairs
+    out = _sweep_buffers(dev, args.pairs, cap)
+    call = lambda: _lib.pair_contacts_device(ctx, d, dp, out, k=1e7, split=True)
+    call()
+    tot, ms, seg, reb = _device_steps(ctx, call, flush, args.steps)
+    del d, dp
+    torch.cuda.empty_cache()
+    hout = {k: v.cpu().pin_memory() for k, v in out.items()}
+    del out
+    torch.cuda.empty_cache()
+    call_h = lambda: _lib.pair_contacts_device(ctx, h, hp, hout, k=1e7, split=True, mem=_lib.MEM_HOST)
+    call_h()
+    e2e = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        te = call_h()
+        e2e.append(time.perf_counter() - t1)
+    h2d = sum(int(v.numel() * v.element_size()) for v in list(h.values()) + list(hp.values()))
+    d2h = args.pairs * (4 + 8 + 16) + 8 + int(te[0]) * (160 + 16)
+    return {"value": args.pairs * args.steps / (sum(ms) / 1e3), "unit": UNIT, "meshes": int(lib.n_mesh),
+            "triangle_bytes": int(lib.tris.nbytes), "contacts_per_step": int(tot[0]),
+            "stages_ms": {"triangle_tests": statistics.mean(seg), "rebuild": statistics.mean(reb),
+                          "whole_call": statistics.mean(ms)},
+            "e2e": {"value": args.pairs * args.steps / sum(e2e), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "host_build_s": build_s,
+            "workload": "the same sweep with both meshes of every pair independent seeded noised icospheres "
+                        "(subdivision U{1..4}), built by zdx_mesh_build on all host threads"}
+
 
 def run_strong(args):
     """One sweep batch spread over the ranks: each rank takes a cost-balanced shard of the cost-ordered
@@ -642,41 +894,22 @@ def _timed_steps(sc, stream, flush, n, graph):
     return [a.elapsed_time(b) for a, b in ev]
 
 
-def run_pour(args):
-    """A 100,000-particle pour (five templates, closed box, gravity), the whole step as one CUDA graph."""
+def measure_pour(args, ctx, steps, cpu=True):
+    """The 100,000-particle pour (five templates, closed box, gravity), the whole step as one CUDA graph:
+    `steps` timed steps after the pre-roll.  Returns the measurement (steps/s, e2e, roofline, clocks)."""
     import tempfile
 
     import torch
 
-    from zdemx import _lib
     from zdemx.dem import Scene
     from zdemx.workloads import pour_scene
 
-    if int(os.environ.get("RANK", "0")) != 0:
-        return
     d = tempfile.mkdtemp(prefix="zdx_pour_")
     cfg_path = pour_scene(d, n=args.particles, seed=args.seed)
     desc = (f"pour: {args.particles} particles (3 ellipsoid hulls of 64 points + icospheres s=2,3; circumradius 1 mm), "
             "jittered lattice in a closed 12-triangle box (60 x 60 mm floor), g=-9.81 z, dt=2e-6, "
             "velocities N(0, 0.05 m/s), zdem force law, split_contacts=1, FP64")
-    if args.impl == "reference":
-        if not os.path.exists(_ref_exe()):
-            emit({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"})
-            return
-        ms, _ = _ref_step_ms(cfg_path, max(1, min(args.steps, 2)))
-        T = sum(ms) / 1e3
-        value = len(ms) / T
-        emit({"impl": "reference", "metric": "DEM steps/s", "value": value, "unit": "steps/s", "n_gpus": 1,
-              "steps": len(ms), "warmup": 0, "ms_per_step": 1e3 * T / len(ms), "higher_is_better": True,
-              "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pour scene)",
-              "config": {"workload": desc},
-              "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
-                               "sample": f"the first {len(ms)} steps of zdem_cpu on the same config (its step_ms)"},
-              "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
-        return
     dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
-    ctx = _lib.Context(0)
     t0 = time.perf_counter()
     sc = Scene(cfg_path, ctx)
     load_s = time.perf_counter() - t0
@@ -688,9 +921,9 @@ def run_pour(args):
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     launches0 = ctx.timings()["launches"]
     infos = []
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with ClockSampler(0) as clk:
-        for k in range(args.steps):
+        for k in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 ev[k][0].record(stream)
@@ -702,12 +935,12 @@ def run_pour(args):
     step_ms = [a.elapsed_time(b) for a, b in ev]
     launches = ctx.timings()["launches"] - launches0
     T = sum(step_ms) / 1e3
-    value = args.steps / T
+    value = steps / T
     # the same steps without the graph (one launch per kernel, the host reads the counts)
     plain_ms = _timed_steps(sc, stream, flush, 3, graph=False)
     # e2e: the graph step plus the whole state brought back to the host every step
     e2e = []
-    for k in range(args.steps):
+    for k in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         torch.cuda.synchronize()
@@ -723,71 +956,93 @@ def run_pour(args):
     pairs = int(np.mean([i["pairs"] for i in infos]))
     mean_tris = _mean_particle_tris(cfg_path)
     abytes = np_ * (2 * 128 + 136) + pairs * 72.0 * 2 * mean_tris
-    achieved = abytes / (T / args.steps) / 1e9
-    try:
-        if args.cpu_seconds <= 0:
-            raise RuntimeError("skipped (--cpu-seconds 0)")
-        ms_ref, _ = _ref_step_ms(cfg_path, 1)
-        cpu = {"value": 1e3 / ms_ref[0], "unit": "steps/s", "cores": 1, "kind": "reference",
-               "sample": f"step 0 of zdem_cpu on the same config ({ms_ref[0] / 1e3:.1f} s, its step_ms - output_ms)"}
-    except Exception as e:
-        cpu = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
+    achieved = abytes / (T / steps) / 1e9
+    cpu_line = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference",
+                "sample": "not run here (one zdem_cpu step of this scene takes about a minute): --workload pour"}
+    if cpu:
+        try:
+            if args.cpu_seconds <= 0:
+                raise RuntimeError("skipped (--cpu-seconds 0)")
+            ms_ref, _ = _ref_step_ms(cfg_path, 1)
+            cpu_line = {"value": 1e3 / ms_ref[0], "unit": "steps/s", "cores": 1, "kind": "reference",
+                        "sample": f"step 0 of zdem_cpu on the same config ({ms_ref[0] / 1e3:.1f} s, its step_ms - output_ms)"}
+        except Exception as e:
+            cpu_line["sample"] = f"unavailable: {e}"
     last = infos[-1]
-    emit({"metric": "DEM steps/s", "value": value, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
-          "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * T / args.steps, "higher_is_better": True,
-          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pour scene)",
-          "config": {"workload": desc, "particles": np_, "preroll_steps": args.preroll, "mean_tris": mean_tris,
-                     "l2": "flushed (256 MB write) before every timed step", "graph": "whole step, one CUDA graph",
-                     "pairs_per_step": pairs, "contacts_last_step": last["contacts"],
-                     "wall_contacts_last_step": last["wall_contacts"], "segments_last_step": last["segments"],
-                     "load_s": load_s, "preroll_s": preroll_s},
-          "e2e": {"value": args.steps / sum(e2e), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
-          "gpu_launches": int(launches),
-          "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                       "traffic": None, "kernel": "whole step (graph)", "peak_kind": f"{peak_kind} hbm_gbs",
-                       "algorithmic_bytes_per_launch": abytes},
-          "plain_step_ms": plain_ms, "cpu_baseline": cpu, "clocks": clk.summary()})
+    return {"metric": "DEM steps/s", "value": value, "unit": "steps/s", "steps": steps, "ms_per_step": 1e3 * T / steps,
+            "config": {"workload": desc, "particles": np_, "preroll_steps": args.preroll, "mean_tris": mean_tris,
+                       "l2": "flushed (256 MB write) before every timed step", "graph": "whole step, one CUDA graph",
+                       "pairs_per_step": pairs, "contacts_last_step": last["contacts"],
+                       "wall_contacts_last_step": last["wall_contacts"], "segments_last_step": last["segments"],
+                       "load_s": load_s, "preroll_s": preroll_s},
+            "e2e": {"value": steps / sum(e2e), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": "whole step (graph)", "peak_kind": f"{peak_kind} hbm_gbs",
+                         "algorithmic_bytes_per_launch": abytes},
+            "plain_step_ms": plain_ms, "cpu_baseline": cpu_line, "clocks": clk.summary()}
 
 
-def run_two(args):
-    """Two 320-triangle noised icospheres colliding (2000 steps, dt 1e-6), and the same pair held in
-    contact (dt 1e-15): steps/s of the whole DEM step, graph and plain, and the trajectory against the
-    reference program."""
+def run_pour(args):
+    """A 100,000-particle pour (five templates, closed box, gravity), the whole step as one CUDA graph."""
     import tempfile
 
     import torch
 
     from zdemx import _lib
-    from zdemx.dem import Scene
-    from zdemx.workloads import two_particle_scene
+    from zdemx.workloads import pour_scene
 
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    d = tempfile.mkdtemp(prefix="zdx_two_")
-    steps_run = 2000
-    cfg_path = two_particle_scene(d, seed=args.seed, steps=steps_run)
-    desc = ("two particles: 320-triangle noised icospheres (r 1 mm, +-15%), 1.9 mm apart, +-0.05 m/s, dt=1e-6, "
-            "2000 steps, split_contacts=1, zdem force law, FP64")
     if args.impl == "reference":
         if not os.path.exists(_ref_exe()):
             emit({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"})
             return
-        wall, _ = _ref_run_wall(cfg_path, steps_run)
-        value = steps_run / wall
+        d = tempfile.mkdtemp(prefix="zdx_pour_")
+        cfg_path = pour_scene(d, n=args.particles, seed=args.seed)
+        ms, _ = _ref_step_ms(cfg_path, max(1, min(args.steps, 2)))
+        T = sum(ms) / 1e3
+        value = len(ms) / T
         emit({"impl": "reference", "metric": "DEM steps/s", "value": value, "unit": "steps/s", "n_gpus": 1,
-              "steps": steps_run, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True,
-              "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-              "config": {"workload": desc},
+              "steps": len(ms), "warmup": 0, "ms_per_step": 1e3 * T / len(ms), "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pour scene)",
+              "config": {"workload": f"pour: {args.particles} particles (see --impl zdemx)"},
               "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
-                               "sample": f"the whole {steps_run}-step zdem_cpu run (wall clock)"},
+                               "sample": f"the first {len(ms)} steps of zdem_cpu on the same config (its step_ms)"},
               "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         return
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     ctx = _lib.Context(0)
+    m = measure_pour(args, ctx, args.steps, cpu=True)
+    line = {"metric": m.pop("metric"), "value": m.pop("value"), "unit": m.pop("unit"), "n_gpus": 1,
+            "steps": m.pop("steps"), "warmup": max(args.warmup, 3), "ms_per_step": m.pop("ms_per_step"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded pour scene)"}
+    line.update(m)
+    emit(line)
+
+
+def measure_two(args, ctx, reps, extras=True):
+    """Two 320-triangle noised icospheres colliding (2000 steps, dt 1e-6): steps/s of whole runs through
+    the graph step, the trajectory against the reference program and the run end to end.  With extras,
+    also the plain step, every step through the full step, the whole program with outputs and the same
+    pair held in contact (dt 1e-15)."""
+    import tempfile
+
+    import torch
+
+    from zdemx.dem import Scene
+    from zdemx.workloads import two_particle_scene
+
+    d = tempfile.mkdtemp(prefix="zdx_two_")
+    steps_run = 2000
+    cfg_path = two_particle_scene(d, seed=args.seed, steps=steps_run)
+    desc = ("two particles: 320-triangle noised icospheres (r 1 mm, +-15%), 1.9 mm apart, +-0.05 m/s, dt=1e-6, "
+            "2000 steps, split_contacts=1, zdem force law, FP64")
+    dev = torch.device("cuda", 0)
     stream = _lib_stream(ctx)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
-    reps = max(int(args.steps), 1)
 
     def whole_runs(graph, free_flight=True):
         """Device time of `reps` whole 2000-step runs from the initial state (L2 flushed before each).  One
@@ -819,10 +1074,6 @@ def run_two(args):
     with ClockSampler(0) as clk:
         g_ms, g_same, launches, sc, st0, fin = whole_runs(graph=True)
     final = fin[:, :13]
-    p_ms, p_same, _, sp, _, pfin = whole_runs(graph=False)
-    same = bool(np.array_equal(pfin, fin))
-    nf_ms, _, nf_launches, _, _, nffin = whole_runs(graph=True, free_flight=False)
-    same_nf = bool(np.array_equal(nffin, fin))
     # end to end through the public API: state in from host memory, the run, state back out (a context
     # holds one scene: load it again, with free flight, and run it once untimed)
     sc = Scene(cfg_path, ctx)
@@ -843,6 +1094,32 @@ def run_two(args):
             traj[name] = float(np.max(np.abs(final[:, cols] - ref[:, cols])) / scale)
     except Exception as e:
         traj = {"unavailable": str(e)[:200]}
+    cpu = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": "unavailable"}
+    try:
+        wall, _ = _ref_run_wall(cfg_path, steps_run)
+        cpu = {"value": steps_run / wall, "unit": "steps/s", "cores": 1, "kind": "reference",
+               "sample": f"the whole {steps_run}-step zdem_cpu run (wall clock, 1 thread)"}
+    except Exception as e:
+        cpu["sample"] = f"unavailable: {e}"
+    T = sum(g_ms) / 1e3
+    n_all = steps_run * reps
+    res = {"metric": "DEM steps/s", "value": n_all / T, "unit": "steps/s", "steps": n_all, "warmup": steps_run,
+           "ms_per_step": 1e3 * T / n_all,
+           "config": {"workload": desc, "timed": f"{reps} whole {steps_run}-step runs from the initial state",
+                      "l2": "flushed (256 MB write) before every timed run",
+                      "graph": "candidate-free steps in one single-block kernel, the others one CUDA graph each"},
+           "e2e": {"value": n_all / sum(e2e), "unit": "steps/s",
+                   "h2d_bytes_per_step": 2 * 16 * 8 / steps_run, "d2h_bytes_per_step": 2 * (16 * 8 + 6 * 8 + 4) / steps_run},
+           "gpu_launches": int(launches) * reps, "repeat_runs_identical": g_same,
+           "trajectory_rel_err_vs_reference": traj, "cpu_baseline": cpu, "clocks": clk.summary()}
+    if not extras:
+        return res
+    p_ms, p_same, _, sp, _, pfin = whole_runs(graph=False)
+    nf_ms, _, nf_launches, _, _, nffin = whole_runs(graph=True, free_flight=False)
+    res["repeat_runs_identical"] = g_same and p_same
+    res["plain"] = {"value": n_all / (sum(p_ms) / 1e3), "unit": "steps/s", "bit_identical_to_graph": bool(np.array_equal(pfin, fin))}
+    res["every_step_full"] = {"value": n_all / (sum(nf_ms) / 1e3), "unit": "steps/s", "gpu_launches": int(nf_launches) * reps,
+                              "bit_identical_to_free_flight": bool(np.array_equal(nffin, fin))}
     # sustained contact: the same pair with dt = 1e-15 (it stays in contact every step)
     sus_path = os.path.join(d, "sustained.txt")
     open(sus_path, "w").write(open(cfg_path).read().replace("dt = 1e-06", "dt = 1e-15"))
@@ -868,35 +1145,58 @@ def run_two(args):
         shutil.rmtree(rout, ignore_errors=True)
     except Exception as e:
         prog["unavailable"] = str(e)[:200]
-    cpu = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference", "sample": "unavailable"}
     sus_ref = None
     try:
-        wall, _ = _ref_run_wall(cfg_path, steps_run)
-        cpu = {"value": steps_run / wall, "unit": "steps/s", "cores": 1, "kind": "reference",
-               "sample": f"the whole {steps_run}-step zdem_cpu run (wall clock, 1 thread)"}
         wall_s, _ = _ref_run_wall(sus_path, 500)
         sus_ref = 500 / wall_s
-    except Exception as e:
-        cpu["sample"] = f"unavailable: {e}"
-    T = sum(g_ms) / 1e3
-    n_all = steps_run * reps
-    emit({"metric": "DEM steps/s", "value": n_all / T, "unit": "steps/s", "n_gpus": 1, "steps": n_all,
-          "warmup": steps_run, "ms_per_step": 1e3 * T / n_all, "higher_is_better": True, "scaling": "weak",
-          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-          "config": {"workload": desc, "timed": f"{reps} whole {steps_run}-step runs from the initial state",
-                     "l2": "flushed (256 MB write) before every timed run",
-                     "graph": "candidate-free steps in one single-block kernel, the others one CUDA graph each"},
-          "e2e": {"value": n_all / sum(e2e), "unit": "steps/s",
-                  "h2d_bytes_per_step": 2 * 16 * 8 / steps_run, "d2h_bytes_per_step": 2 * (16 * 8 + 6 * 8 + 4) / steps_run},
-          "gpu_launches": int(launches) * reps, "repeat_runs_identical": g_same and p_same,
-          "plain": {"value": n_all / (sum(p_ms) / 1e3), "unit": "steps/s", "bit_identical_to_graph": same},
-          "every_step_full": {"value": n_all / (sum(nf_ms) / 1e3), "unit": "steps/s", "gpu_launches": int(nf_launches) * reps,
-                              "bit_identical_to_free_flight": same_nf},
-          "trajectory_rel_err_vs_reference": traj,
-          "program_with_outputs": prog,
-          "sustained_contact": {"value": 500 / (sum(s_ms) / 1e3), "unit": "pair-contacts/s", "dt": 1e-15,
-                                "contacts_per_step": sus_contacts, "reference_value": sus_ref},
-          "cpu_baseline": cpu, "clocks": clk.summary()})
+    except Exception:
+        pass
+    res["program_with_outputs"] = prog
+    res["sustained_contact"] = {"value": 500 / (sum(s_ms) / 1e3), "unit": "pair-contacts/s", "dt": 1e-15,
+                                "contacts_per_step": sus_contacts, "reference_value": sus_ref}
+    return res
+
+
+def run_two(args):
+    """Two 320-triangle noised icospheres colliding (2000 steps, dt 1e-6), and the same pair held in
+    contact (dt 1e-15): steps/s of the whole DEM step, graph and plain, and the trajectory against the
+    reference program."""
+    import tempfile
+
+    import torch
+
+    from zdemx import _lib
+    from zdemx.workloads import two_particle_scene
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    steps_run = 2000
+    if args.impl == "reference":
+        if not os.path.exists(_ref_exe()):
+            emit({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"})
+            return
+        d = tempfile.mkdtemp(prefix="zdx_two_")
+        cfg_path = two_particle_scene(d, seed=args.seed, steps=steps_run)
+        wall, _ = _ref_run_wall(cfg_path, steps_run)
+        value = steps_run / wall
+        emit({"impl": "reference", "metric": "DEM steps/s", "value": value, "unit": "steps/s", "n_gpus": 1,
+              "steps": steps_run, "warmup": 0, "ms_per_step": 1e3 / value, "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+              "config": {"workload": "two particles, 2000 steps (see --impl zdemx)"},
+              "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
+                               "sample": f"the whole {steps_run}-step zdem_cpu run (wall clock)"},
+              "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctx = _lib.Context(0)
+    m = measure_two(args, ctx, reps=max(int(args.steps), 1), extras=True)
+    line = {"metric": m.pop("metric"), "value": m.pop("value"), "unit": m.pop("unit"), "n_gpus": 1,
+            "steps": m.pop("steps"), "warmup": m.pop("warmup"), "ms_per_step": m.pop("ms_per_step"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)"}
+    line.update(m)
+    emit(line)
 
 
 def run_adjoint(args):

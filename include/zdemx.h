@@ -72,6 +72,10 @@ int zdx_mesh_build(const double* tris, int64_t ntri, int center_mesh, double* tr
 #define ZDX_MEM_DEVICE 1
 #define ZDX_SCHED_BATCHED 0  /* one launch per stage over the whole batch, cost-ordered work queue       */
 #define ZDX_SCHED_PLAIN 1    /* one launch per stage per pair (the unbatched form, for comparison)      */
+/* One launch per stage over the whole batch with no work queue, no cost order and no culls: CTAs and
+ * warps take pairs in a fixed grid-stride order, and every nA x nB triangle pair gets the reference's
+ * AABB test (the plain GPU form, for comparison).  Same results as ZDX_SCHED_BATCHED. */
+#define ZDX_SCHED_PER_STAGE 2
 
 typedef struct zdx_pair_opts {
     int mode;             /* ZDX_MODE_*                                                               */
@@ -154,6 +158,25 @@ int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launches);
 /* The context's CUDA stream (a cudaStream_t), on which every call of the context runs: for callers that
  * order their own work after it or time it with their own events.  No reference counterpart. */
 int zdx_get_stream(const zdx_ctx* ctx, void** stream);
+
+/* Launch parameters of the pair kernels, chosen by the project's autotuner (zdemx.autotune) on a
+ * calibration sample of a workload, or left at their defaults.  No reference counterpart.  Results do not
+ * depend on them (tests check this); only times do.  zdx_create starts from the defaults and then reads
+ * the JSON file named by the environment variable ZDX_TUNING, if set (keys as the fields below; a file
+ * that cannot be read or parsed is ignored).  A scene's graph step keeps the values in force when the
+ * scene was loaded. */
+typedef struct zdx_tuning {
+    int32_t tri_ctas_per_sm;    /* triangle-stage CTAs per SM: 1 or 2 (default 2)                     */
+    int32_t rebuild_warps;      /* warps per rebuild block, 1..4 (default 4)                          */
+    int64_t flat_max;           /* survivor pairs nA' x nB' up to which the flat box test runs rather
+                                   than the hierarchical one (default 8192)                          */
+    int64_t split_tests;        /* a batch with fewer pairs than triangle-stage CTAs splits each pair
+                                   of nA x nB triangle tests into ceil(nA nB / split_tests) work items
+                                   (at most 64, at most nA) over ranges of A's triangles; 0: never
+                                   (default).  zdx_pair_contacts only                                 */
+} zdx_tuning;
+int zdx_set_tuning(zdx_ctx* ctx, const zdx_tuning* t);  /* ZDX_ERR_INVALID for values out of range */
+int zdx_get_tuning(const zdx_ctx* ctx, zdx_tuning* t);
 
 /* ---- the DEM scene (the zdem_cpu step loop) ------------------------------------------------------
  * zdx_scene_load replaces parse_config_file (src/main.cpp:1531-1689), load_mesh_for and the particle

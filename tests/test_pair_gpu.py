@@ -93,8 +93,12 @@ def test_batched_equals_plain(ctx):
     pp = synth.pair_poses(rng, 24, 1e-3, 0.0, 0.1)
     a = _run(ctx, lib, pm, pp, sched=_lib.SCHED_BATCHED)
     b = _run(ctx, lib, pm, pp, sched=_lib.SCHED_PLAIN)
+    c = _run(ctx, lib, pm, pp, sched=_lib.SCHED_PER_STAGE)
     for k in ("ncontact", "contact_off", "stats", "geom", "info", "points", "point_off"):
         assert np.array_equal(a[k], b[k]), k
+        assert np.array_equal(a[k], c[k]), k
+    # the per-stage form has no culls: it counts the same triangle tests as the reference
+    assert a["totals"][2] == c["totals"][2]
 
 
 def test_edge_cases(ctx, oracle):
@@ -161,6 +165,24 @@ def test_polyline_mode_matches_oracle_and_python_reference(ctx, oracle):
         for c, cc in enumerate(man["contacts"]):
             got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"], cc["Fn"], cc["F_A"]]
             assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)
+
+
+def test_polyline_tol_none_is_the_mean_edge_rule(ctx):
+    """pair_contacts(tol=None) snaps with the zdem_cpu step's tolerance, 0.1 x A's mean edge
+    (src/main.cpp:2118-2121): the same contacts as the explicit value."""
+    from zdemx import _lib, polyline, synth
+
+    rng = np.random.default_rng(31)
+    A = synth.noised_icosphere(2, 1e-3, 0.15, rng)
+    B = synth.noised_icosphere(2, 1e-3, 0.15, rng)
+    pose = synth.pair_poses(rng, 1, 1e-3, 0.05, 0.06)[0]
+    me = _lib.mesh_build(A, False)[1]["mean_edge"]
+    assert me > 0
+    a = polyline.pair_contacts(A, B, pose[0:3], pose[3:7], pose[7:10], pose[10:14], k=1e7, tol=None, ctx=ctx)
+    b = polyline.pair_contacts(A, B, pose[0:3], pose[3:7], pose[7:10], pose[10:14], k=1e7, tol=0.1 * me, ctx=ctx)
+    assert len(a[0]["contacts"]) == len(b[0]["contacts"]) > 0
+    for x, y in zip(a[0]["contacts"], b[0]["contacts"]):
+        assert np.array_equal(x["Sn"], y["Sn"]) and x["area"] == y["area"]
 
 
 def test_polyline_split_matches_oracle_and_python_reference(ctx, oracle):

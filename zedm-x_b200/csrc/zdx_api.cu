@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -73,6 +74,10 @@ extern "C" const char* zdx_status_string(int s) {
 
 extern "C" const char* zdx_last_error(const zdx_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
+namespace {
+void tuning_from_file(zdx_ctx* ctx, const char* path);
+}
+
 extern "C" int zdx_create(zdx_ctx** out, int device) {
     if (!out) return ZDX_ERR_INVALID;
     *out = nullptr;
@@ -99,6 +104,7 @@ extern "C" int zdx_create(zdx_ctx** out, int device) {
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
     noalloc_setup(ctx);
+    if (const char* tf = std::getenv("ZDX_TUNING")) tuning_from_file(ctx, tf);
     *out = ctx;
     return ZDX_OK;
 }
@@ -119,6 +125,72 @@ extern "C" int zdx_pair_timings(const zdx_ctx* ctx, double* ms5, int64_t* launch
     if (!ctx || !ms5) return ZDX_ERR_INVALID;
     for (int i = 0; i < 5; ++i) ms5[i] = ctx->pair_ms[i];
     if (launches) *launches = ctx->launches;
+    return ZDX_OK;
+}
+
+namespace {
+
+int tuning_check(const zdx_tuning* t) {
+    if (t->tri_ctas_per_sm < 1 || t->tri_ctas_per_sm > 2) return ZDX_ERR_INVALID;
+    if (t->rebuild_warps < 1 || t->rebuild_warps > K2_MAX_WARPS) return ZDX_ERR_INVALID;
+    if (t->flat_max < 0 || t->split_tests < 0) return ZDX_ERR_INVALID;
+    return ZDX_OK;
+}
+
+// The tuning file: one flat JSON object of integer fields, e.g. {"flat_max": 8192, "rebuild_warps": 4}.
+// Unknown keys are skipped; a malformed file changes nothing.
+void tuning_from_file(zdx_ctx* ctx, const char* path) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return;
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0 && text.size() < (1u << 20)) text.append(buf, got);
+    std::fclose(f);
+    zdx_tuning t{ctx->tune.tri_ctas_per_sm, ctx->tune.rebuild_warps, ctx->tune.flat_max, ctx->tune.split_tests};
+    struct Key {
+        const char* name;
+        int64_t* v64;
+        int32_t* v32;
+    } keys[] = {{"tri_ctas_per_sm", nullptr, &t.tri_ctas_per_sm}, {"rebuild_warps", nullptr, &t.rebuild_warps},
+                {"flat_max", &t.flat_max, nullptr}, {"split_tests", &t.split_tests, nullptr}};
+    for (const Key& k : keys) {
+        const std::string quoted = std::string("\"") + k.name + "\"";
+        const size_t at = text.find(quoted);
+        if (at == std::string::npos) continue;
+        const size_t colon = text.find(':', at + quoted.size());
+        if (colon == std::string::npos) return;
+        char* end = nullptr;
+        const long long v = std::strtoll(text.c_str() + colon + 1, &end, 10);
+        if (end == text.c_str() + colon + 1) return;
+        if (k.v64) *k.v64 = v;
+        else *k.v32 = (int32_t)v;
+    }
+    if (tuning_check(&t) != ZDX_OK) return;
+    ctx->tune.tri_ctas_per_sm = t.tri_ctas_per_sm;
+    ctx->tune.rebuild_warps = t.rebuild_warps;
+    ctx->tune.flat_max = t.flat_max;
+    ctx->tune.split_tests = t.split_tests;
+}
+
+}  // namespace
+
+extern "C" int zdx_set_tuning(zdx_ctx* ctx, const zdx_tuning* t) {
+    if (!ctx || !t) return ZDX_ERR_INVALID;
+    if (tuning_check(t) != ZDX_OK) return ctx_fail(ctx, ZDX_ERR_INVALID, "tuning value out of range");
+    ctx->tune.tri_ctas_per_sm = t->tri_ctas_per_sm;
+    ctx->tune.rebuild_warps = t->rebuild_warps;
+    ctx->tune.flat_max = t->flat_max;
+    ctx->tune.split_tests = t->split_tests;
+    return ZDX_OK;
+}
+
+extern "C" int zdx_get_tuning(const zdx_ctx* ctx, zdx_tuning* t) {
+    if (!ctx || !t) return ZDX_ERR_INVALID;
+    t->tri_ctas_per_sm = ctx->tune.tri_ctas_per_sm;
+    t->rebuild_warps = ctx->tune.rebuild_warps;
+    t->flat_max = ctx->tune.flat_max;
+    t->split_tests = ctx->tune.split_tests;
     return ZDX_OK;
 }
 
@@ -158,6 +230,8 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         (opts->mode != ZDX_MODE_ZDEM && opts->mode != ZDX_MODE_POLYLINE && opts->mode != ZDX_MODE_POLYLINE_NUMPY))
         return ctx_fail(ctx, ZDX_ERR_INVALID, "bad mesh/pair count or mode");
     if (pb->n_pairs > 0x7fffffffLL) return ctx_fail(ctx, ZDX_ERR_INVALID, "at most 2^31-1 pairs per call");
+    if (opts->sched != ZDX_SCHED_BATCHED && opts->sched != ZDX_SCHED_PLAIN && opts->sched != ZDX_SCHED_PER_STAGE)
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "bad schedule %d", opts->sched);
     if (ms->n_mesh > 0 && (!ms->tris || !ms->tri_off || !ms->mean_edge || !ms->bbox_diag))
         return ctx_fail(ctx, ZDX_ERR_INVALID, "mesh set has null arrays");
     if (pb->n_pairs > 0 && (!pb->mesh || !pb->pose)) return ctx_fail(ctx, ZDX_ERR_INVALID, "pair batch has null arrays");
@@ -211,6 +285,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     a.want_pts = opts->want_loop_points ? 1 : 0;
     a.cap_seg = opts->max_seg_per_pair > 0 ? opts->max_seg_per_pair : 16384;
     a.cap_side = std::max(max_ntri, 1);
+    a.flat_max = ctx->tune.flat_max;
 
     // stage 0: per-triangle spheres and mesh bounds
     CK(ctx->tri_sph.ensure(sizeof(double4) * std::max<int64_t>(total_tris, 1)));
@@ -220,7 +295,10 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     CK(cudaMemsetAsync(ctx->mesh_valid.p, 0, sizeof(int) * std::max(NM, 1), st));
     CK(ctx->mesh_infl.ensure(sizeof(unsigned long long) * std::max(NM, 1)));
     CK(cudaMemsetAsync(ctx->mesh_infl.p, 0, sizeof(unsigned long long) * std::max(NM, 1), st));
-    a.mesh_infl_bits = as<unsigned long long>(ctx->mesh_infl);
+    const bool per_stage = opts->sched == ZDX_SCHED_PER_STAGE;
+    // the plain per-stage form has no separation certificate (null bound disables it)
+    a.mesh_infl_bits = per_stage ? nullptr : as<unsigned long long>(ctx->mesh_infl);
+    a.per_stage = per_stage ? 1 : 0;
     a.tri_sph = as<double4>(ctx->tri_sph);
     a.mesh_R_bits = as<unsigned long long>(ctx->mesh_R);
     a.mesh_valid = as<int>(ctx->mesh_valid);
@@ -255,6 +333,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     a.queue2 = reinterpret_cast<int*>(cnt + 5);
     a.max_nseg = reinterpret_cast<int*>(cnt + 6);
     a.err = reinterpret_cast<int*>(cnt + 7);
+    a.seg_total = cnt + 9;
     CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
     CK(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
     // optional per-component counts, written by the rebuild stage
@@ -272,8 +351,8 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     }
 
     const bool plain = opts->sched == ZDX_SCHED_PLAIN;
-    if (plain) {
-        // identity order: the plain form walks the pairs as given
+    if (plain || per_stage) {
+        // identity order: the plain forms walk the pairs as given
         std::vector<int32_t> id((size_t)NP);
         for (int64_t p = 0; p < NP; ++p) id[(size_t)p] = (int32_t)p;
         if (NP) CK(cudaMemcpyAsync(ctx->order.p, id.data(), sizeof(int32_t) * NP, cudaMemcpyHostToDevice, st));
@@ -284,10 +363,61 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     }
     a.order = as<int32_t>(ctx->order);
     CK(cudaEventRecord(ctx->ev[1], st));
-    ctx->launches += plain ? 0 : 4;  // mesh prep + three cost-order kernels
+    ctx->launches += plain ? 0 : per_stage ? 1 : 4;  // mesh prep (+ three cost-order kernels)
 
     // stage 1: segments
-    const int k1_grid = plain ? 1 : (int)std::min<int64_t>(std::max<int64_t>(NP, 1), (int64_t)ctx->num_sms * k1_blocks_per_sm());
+    int k1_grid = plain ? 1 : (int)std::min<int64_t>(std::max<int64_t>(NP, 1), (int64_t)ctx->num_sms * ctx->tune.tri_ctas_per_sm);
+    // A batch with fewer pairs than triangle-stage CTAs splits its large pairs: a pair of nA x nB triangle
+    // tests becomes ceil(nA nB / split_tests) work items (at most 64, at most nA), each over a range of A's
+    // triangles, joined back in order on the device.  The items go most expensive pair first.
+    const int64_t ctas = (int64_t)ctx->num_sms * ctx->tune.tri_ctas_per_sm;
+    if (!plain && !per_stage && ctx->tune.split_tests > 0 && NP > 0 && NP < ctas) {
+        std::vector<int32_t> pm_h((size_t)(2 * NP));
+        if (host) {
+            std::memcpy(pm_h.data(), pb->mesh, sizeof(int32_t) * 2 * NP);
+        } else {
+            CK(cudaMemcpyAsync(pm_h.data(), pb->mesh, sizeof(int32_t) * 2 * NP, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (int64_t q = 0; q < 2 * NP; ++q)
+                if (pm_h[q] < 0 || pm_h[q] >= NM) return ctx_fail(ctx, ZDX_ERR_INVALID, "pair mesh index out of range");
+        }
+        auto ntri = [&](int m) { return off_h[m + 1] - off_h[m]; };
+        std::vector<int32_t> ord((size_t)NP);
+        for (int64_t q = 0; q < NP; ++q) ord[q] = (int32_t)q;
+        std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) {
+            return ntri(pm_h[2 * x]) * ntri(pm_h[2 * x + 1]) > ntri(pm_h[2 * y]) * ntri(pm_h[2 * y + 1]);
+        });
+        std::vector<int32_t> items, ichunk, first((size_t)NP, 0);
+        for (int32_t q : ord) {
+            const int64_t nA = ntri(pm_h[2 * q]), cost = nA * ntri(pm_h[2 * q + 1]);
+            int64_t c = (cost + ctx->tune.split_tests - 1) / ctx->tune.split_tests;
+            c = std::max<int64_t>(1, std::min<int64_t>({c, 64, std::max<int64_t>(nA, 1)}));
+            first[q] = (int32_t)items.size();
+            for (int64_t k = 0; k < c; ++k) {
+                items.push_back(q);
+                ichunk.push_back((int32_t)(k | (c << 16)));
+            }
+        }
+        const size_t ni = items.size();
+        CK(ctx->sp_items.ensure(sizeof(int32_t) * 3 * ni));
+        CK(ctx->sp_first.ensure(sizeof(int32_t) * 2 * (size_t)NP));
+        CK(ctx->sp_chunk.ensure((sizeof(int64_t) + 2 * sizeof(int32_t)) * ni));
+        int32_t* it = as<int32_t>(ctx->sp_items);
+        CK(cudaMemcpyAsync(it, items.data(), sizeof(int32_t) * ni, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(it + ni, ichunk.data(), sizeof(int32_t) * ni, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->sp_first.p, first.data(), sizeof(int32_t) * NP, cudaMemcpyHostToDevice, st));
+        a.items = it;
+        a.item_chunk = it + ni;
+        a.pair_first_item = as<int32_t>(ctx->sp_first);
+        a.pair_done = as<int32_t>(ctx->sp_first) + NP;
+        a.chunk_seg_off = as<int64_t>(ctx->sp_chunk);
+        a.chunk_nseg = reinterpret_cast<int32_t*>(a.chunk_seg_off + ni);
+        a.chunk_status = a.chunk_nseg + ni;
+        a.n_items = (int64_t)ni;
+        CK(cudaMemsetAsync(a.pair_done, 0, sizeof(int32_t) * NP, st));
+        k1_grid = (int)std::min<int64_t>((int64_t)ni, ctas);
+        CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
+    }
     a.k1_slot_bytes = tritest_slot_bytes(a.cap_side, a.cap_seg);
     CK(ctx->k1_slots.ensure(a.k1_slot_bytes * (size_t)k1_grid));
     a.k1_slots = as<char>(ctx->k1_slots);
@@ -336,7 +466,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         ctape_final = as<int64_t>(ctx->t_cfinal);
     }
 
-    unsigned long long hc[9];
+    unsigned long long hc[10];
     if (plain) {
         ctx->launches += 1 + 2 * NP;
         for (int64_t p = 0; p < NP; ++p) {
@@ -345,7 +475,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
             CK(cudaMemsetAsync(a.queue1, 0, sizeof(int), st));
             launch_segments(a, 1, st);
             CK(cudaMemsetAsync(a.queue2, 0, sizeof(int), st));
-            launch_rebuild(a, 1, st);
+            launch_rebuild(a, 1, 1, st);
         }
         CK(cudaGetLastError());
         CK(cudaEventRecord(ctx->ev[5], st));
@@ -382,6 +512,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
             }
             CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
             CK(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
+            if (a.pair_done) CK(cudaMemsetAsync(a.pair_done, 0, sizeof(int32_t) * NP, st));
         }
         // stage 2: rebuild, one warp per pair, slots sized for the largest pair
         const int nmax = std::max(((int*)&hc[6])[0], 1);
@@ -390,12 +521,12 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         const size_t budget = (size_t)2 << 30;
         int64_t warps = std::min<int64_t>(std::max<int64_t>(NP, 1), (int64_t)ctx->num_sms * 32);
         warps = std::min<int64_t>(warps, std::max<int64_t>(1, (int64_t)(budget / a.k2_slot_bytes)));
-        warps = (warps + k2_warps_per_block() - 1) / k2_warps_per_block() * k2_warps_per_block();
+        warps = (warps + ctx->tune.rebuild_warps - 1) / ctx->tune.rebuild_warps * ctx->tune.rebuild_warps;
         a.k2_nslots = warps;
         CK(ctx->k2_slots.ensure(a.k2_slot_bytes * (size_t)warps));
         a.k2_slots = as<char>(ctx->k2_slots);
         CK(cudaEventRecord(ctx->ev[2], st));
-        launch_rebuild(a, (int)warps, st);
+        launch_rebuild(a, (int)warps, ctx->tune.rebuild_warps, st);
         ctx->launches += 1;
         CK(cudaGetLastError());
         CK(cudaEventRecord(ctx->ev[3], st));
@@ -405,7 +536,7 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
     const int err = ((int*)&hc[7])[0];
     ctx->tape_need = (int64_t)hc[8];
     out->totals[0] = (int64_t)hc[1];
-    out->totals[1] = (int64_t)hc[0];
+    out->totals[1] = (int64_t)hc[9];
     out->totals[2] = (int64_t)hc[3];
     out->totals[3] = (int64_t)hc[2];
     if (err & ERR_TAPE) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "adjoint tape arena too small");

@@ -23,6 +23,15 @@ void noalloc_setup(::zdx_ctx* c);
 
 struct Scene;  // DEM scene (zdx_scene.cu)
 
+// Launch parameters of the pair kernels (zdx_set_tuning; defaults measured on the pair sweep).
+struct Tuning {
+    int tri_ctas_per_sm = 2;     // triangle-stage CTAs per SM (shared memory allows 1 or 2)
+    int64_t flat_max = 8192;     // survivor pairs up to which the flat box test beats the hierarchical one
+    int rebuild_warps = 4;       // warps per rebuild block
+    int64_t split_tests = 0;     // split a pair's triangle stage into chunks of about this many survivor
+                                 // tests when the batch has fewer pairs than CTAs (0: never)
+};
+
 }  // namespace zdx
 
 struct zdx_ctx {
@@ -34,12 +43,14 @@ struct zdx_ctx {
     std::string last_error;
     double pair_ms[5] = {0, 0, 0, 0, 0};
     long long launches = 0;  // kernels this context has launched
+    zdx::Tuning tune;
 
     // pair-call workspaces
     zdx::DevBuf in_tris, in_off, in_me, in_bd, in_pm, in_pose;
     zdx::DevBuf tri_sph, mesh_R, mesh_valid, mesh_infl;
     zdx::DevBuf order, buckets, pair_i64, pair_i32, counters;
     zdx::DevBuf k1_slots, seg_arena, k2_slots;
+    zdx::DevBuf sp_items, sp_first, sp_chunk;  // split of large pairs (items, per-pair first item, runs)
     zdx::DevBuf cstage, cistage, pstage;
     zdx::DevBuf g_off, o_cg, o_ci, o_pts, o_cpo, o_ps, o_comp;
     // adjoint tape (recorded when tape_on): segment provenance, per-contact records, final offsets
@@ -51,7 +62,8 @@ struct zdx_ctx {
 
     std::vector<zdx::DevBuf*> all_bufs() {
         return {&in_tris, &in_off, &in_me, &in_bd, &in_pm, &in_pose, &tri_sph, &mesh_R, &mesh_valid, &mesh_infl,
-                &order, &buckets, &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots,
+                &order, &buckets, &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &sp_items,
+                &sp_first, &sp_chunk,
                 &cstage, &cistage, &pstage, &g_off, &o_cg, &o_ci, &o_pts, &o_cpo, &o_ps, &o_comp, &t_segtri, &t_segcand,
                 &t_arena, &t_cstage, &t_cfinal, &a_nc, &a_coff, &a_stats, &a_geom, &a_info, &a_pts, &a_cpo, &a_gc,
                 &a_gt, &a_gp};

@@ -180,6 +180,7 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
     a.item_begin = 0;
     a.item_end = NP;
     a.cap_side = std::max(max_ntri, 1);
+    a.flat_max = ctx->tune.flat_max;
     a.cap_seg = seg_cap;
     a.mesh_infl_bits = cv.take<unsigned long long>(ZDX_NOALLOC_MAX_MESHES);
     a.seg = cv.take<double>(6 * (size_t)kSegArena);
@@ -213,7 +214,7 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
     a.k1_slot_bytes = (tritest_slot_bytes(a.cap_side, seg_cap) + 255) & ~size_t(255);
     const int64_t k1_fit = (int64_t)(room / a.k1_slot_bytes);
     if (k1_fit < 1) return ctx_fail(ctx, ZDX_ERR_INVALID, "noalloc call: a triangle-stage slot does not fit the scratch array");
-    const int k1_grid = (int)std::min<int64_t>(std::min<int64_t>(k1_fit, (int64_t)ctx->num_sms * k1_blocks_per_sm()),
+    const int k1_grid = (int)std::min<int64_t>(std::min<int64_t>(k1_fit, (int64_t)ctx->num_sms * ctx->tune.tri_ctas_per_sm),
                                                std::max<int64_t>(NP, 1));
     a.k1_slots = var_base;
 
@@ -247,7 +248,7 @@ extern "C" int zdx_pair_contacts_noalloc(zdx_ctx* ctx, const zdx_pair_opts* opts
                             a.k2_nmax);
         a.k2_nslots = std::min<int64_t>(std::min<int64_t>(k2_fit, (int64_t)ctx->num_sms * 32), NP);
         a.k2_slots = var_base;
-        launch_rebuild(a, (int)a.k2_nslots, st);
+        launch_rebuild(a, (int)a.k2_nslots, ctx->tune.rebuild_warps, st);
         ctx->launches += 1;
         CKN(cudaGetLastError());
     }

@@ -32,17 +32,9 @@ constexpr int K1_THREADS = 256;
 constexpr int K1_ITER = 8;
 constexpr int K1_QCAP = K1_THREADS * K1_ITER;
 constexpr int K1_HCAP = 2048;  // B survivors handled by the hierarchical test (shared memory)
-// Up to this many survivor pairs (nA' x nB') the flat test (every pair's AABBs, thread-strided) beats the
-// Morton sort and group boxes of the hierarchical one: measured 23.8 against 25.3 ms on the sweep and
-// 114 against 92 steps/s on the pour.
-constexpr int64_t K1_FLAT_MAX = 8192;
 constexpr size_t K1_DSMEM = sizeof(float) * 6 * K1_HCAP + sizeof(uint32_t) * K1_HCAP + sizeof(int) * K1_HCAP +
                             sizeof(float) * 6 * (K1_HCAP / 32) + sizeof(int2) * 64 * (K1_THREADS / 32);
 static_assert(sizeof(int2) * K1_QCAP <= (sizeof(uint32_t) + sizeof(int)) * K1_HCAP, "flat queue must fit the alias");
-constexpr int K2_WARPS = 4;
-
-int k1_blocks_per_sm() { return 2; }
-int k2_warps_per_block() { return K2_WARPS; }
 
 __device__ __forceinline__ V3 ld3(const double* p) { return V3{p[0], p[1], p[2]}; }
 __device__ __forceinline__ void st3(double* p, V3 v) {
@@ -54,33 +46,58 @@ __device__ __forceinline__ void st3(double* p, V3 v) {
 
 // --------------------------------------------------------------------------------------------- stage 0
 __global__ void k_mesh_prep(PairArgs a, int64_t total) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    int lo = 0, hi = a.n_mesh;
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (a.tri_off[mid] <= t) lo = mid;
-        else hi = mid;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool live = t < total;
+    // per triangle: its mesh, the bound |c| + r, whether it has a plane, its point_in_tri inflation
+    int lo = -1, valid = 0;
+    unsigned long long Rb = 0, ib = 0;
+    if (live) {
+        lo = 0;
+        int hi = a.n_mesh;
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (a.tri_off[mid] <= t) lo = mid;
+            else hi = mid;
+        }
+        const double* v = a.tris + 9 * t;
+        V3 p0 = ld3(v), p1 = ld3(v + 3), p2 = ld3(v + 6);
+        V3 c = (p0 + p1 + p2) * (1.0 / 3.0);
+        double r = sqrt(smax3(norm2(p0 - c), norm2(p1 - c), norm2(p2 - c))) * (1.0 + 1e-12);
+        a.tri_sph[t] = make_double4(c.x, c.y, c.z, r);
+        Rb = (unsigned long long)__double_as_longlong((norm(c) + r) * (1.0 + 1e-12));
+        valid = !(norm(cross(p1 - p0, p2 - p0)) < 1e-30) ? 1 : 0;
+        if (a.mesh_infl_bits && valid) {
+            // point_in_tri accepts c_k = |e_k| x (in-plane distance to edge line k) >= -1e-10: each edge line
+            // moves out by 1e-10 / |e_k| and a vertex by at most 2 max_k(1e-10 / |e_k|) / sin(its angle)
+            const V3 e0 = p1 - p0, e1 = p2 - p1, e2 = p0 - p2;
+            const double l0 = norm(e0), l1 = norm(e1), l2 = norm(e2);
+            const double cr = norm(cross(e0, e2));
+            const double smin_ang = smin3(cr / (l0 * l2), cr / (l0 * l1), cr / (l1 * l2));
+            const double dmax = 1e-10 / smin3(l0, l1, l2);
+            double infl = 2.0 * dmax / smin_ang;
+            if (!(infl < 1e300)) infl = 1e300;
+            ib = (unsigned long long)__double_as_longlong(infl * (1.0 + 1e-6));
+        }
     }
-    const double* v = a.tris + 9 * t;
-    V3 p0 = ld3(v), p1 = ld3(v + 3), p2 = ld3(v + 6);
-    V3 c = (p0 + p1 + p2) * (1.0 / 3.0);
-    double r = sqrt(smax3(norm2(p0 - c), norm2(p1 - c), norm2(p2 - c))) * (1.0 + 1e-12);
-    a.tri_sph[t] = make_double4(c.x, c.y, c.z, r);
-    double R = (norm(c) + r) * (1.0 + 1e-12);
-    atomicMax(a.mesh_R_bits + lo, (unsigned long long)__double_as_longlong(R));
-    if (!(norm(cross(p1 - p0, p2 - p0)) < 1e-30)) atomicAdd(a.mesh_valid + lo, 1);
-    if (a.mesh_infl_bits && !(norm(cross(p1 - p0, p2 - p0)) < 1e-30)) {
-        // point_in_tri accepts c_k = |e_k| x (in-plane distance to edge line k) >= -1e-10: each edge line
-        // moves out by 1e-10 / |e_k| and a vertex by at most 2 max_k(1e-10 / |e_k|) / sin(its angle)
-        const V3 e0 = p1 - p0, e1 = p2 - p1, e2 = p0 - p2;
-        const double l0 = norm(e0), l1 = norm(e1), l2 = norm(e2);
-        const double cr = norm(cross(e0, e2));
-        const double smin_ang = smin3(cr / (l0 * l2), cr / (l0 * l1), cr / (l1 * l2));
-        const double dmax = 1e-10 / smin3(l0, l1, l2);
-        double infl = 2.0 * dmax / smin_ang;
-        if (!(infl < 1e300)) infl = 1e300;
-        atomicMax(a.mesh_infl_bits + lo, (unsigned long long)__double_as_longlong(infl * (1.0 + 1e-6)));
+    // A mesh's triangles are consecutive, so they are runs of lanes: reduce each run (max, sum, max of
+    // non-negative doubles as bits) and let its first lane alone do the atomics.
+    for (int d = 1; d < 32; d <<= 1) {
+        const int lo_d = __shfl_down_sync(FULL, lo, d);
+        const unsigned long long R_d = __shfl_down_sync(FULL, Rb, d);
+        const unsigned long long i_d = __shfl_down_sync(FULL, ib, d);
+        const int v_d = __shfl_down_sync(FULL, valid, d);
+        if (lane + d < 32 && lo_d == lo) {
+            Rb = R_d > Rb ? R_d : Rb;
+            ib = i_d > ib ? i_d : ib;
+            valid += v_d;
+        }
+    }
+    const int lo_up = __shfl_up_sync(FULL, lo, 1);
+    if (live && (lane == 0 || lo_up != lo)) {
+        atomicMax(a.mesh_R_bits + lo, Rb);
+        if (valid) atomicAdd(a.mesh_valid + lo, valid);
+        if (a.mesh_infl_bits && ib) atomicMax(a.mesh_infl_bits + lo, ib);
     }
 }
 
@@ -245,6 +262,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     __shared__ int sh_nq;
     __shared__ int sh_nseg;
     __shared__ unsigned long long sh_base;
+    __shared__ int sh_last;
+    __shared__ long long sh_ftot;
     extern __shared__ __align__(16) unsigned char k1_dsm[];
     // dynamic shared memory: float boxes | keys | values (the flat path's queue aliases keys+values)
     //                        | group boxes | per-warp overlap queues
@@ -259,11 +278,12 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     carve_k1(a.k1_slots + (size_t)blockIdx.x * a.k1_slot_bytes, a.cap_side, a.cap_seg, &S);
     const int cap = a.cap_side;
     const bool py = NPX || a.mode == 1;
-    const int64_t iend = item_end_of(a);
+    const int64_t iend = a.items ? a.item_begin + a.n_items : item_end_of(a);
 
-    for (;;) {
+    for (int64_t round = 0;; ++round) {
         if (tid == 0) {
-            sh_item = (int)(a.item_begin + atomicAdd(a.queue1, 1));
+            sh_item = a.per_stage ? (int)(a.item_begin + blockIdx.x + round * gridDim.x)
+                                  : (int)(a.item_begin + atomicAdd(a.queue1, 1));
             sh_n[0] = sh_n[1] = 0;
             sh_nq = 0;
             sh_nseg = 0;
@@ -271,7 +291,13 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         __syncthreads();
         const int64_t item = sh_item;
         if (item >= iend) break;
-        const int p = a.order[item];
+        const int p = a.items ? a.items[item] : a.order[item];
+        int chunk = 0, nchunk = 1;
+        if (a.items) {
+            const int ic = a.item_chunk[item];
+            chunk = ic & 0xffff;
+            nchunk = ic >> 16;
+        }
         const double* ps = a.pose + 14 * (int64_t)p;
         V3 tpos[2] = {V3{ps[0], ps[1], ps[2]}, V3{ps[7], ps[8], ps[9]}};
         Q4 qraw[2] = {Q4{ps[3], ps[4], ps[5], ps[6]}, Q4{ps[10], ps[11], ps[12], ps[13]}};
@@ -288,6 +314,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         const int mesh[2] = {a.pmesh[2 * (int64_t)p], a.pmesh[2 * (int64_t)p + 1]};
         const int64_t off[2] = {a.tri_off[mesh[0]], a.tri_off[mesh[1]]};
         const int nt[2] = {(int)(a.tri_off[mesh[0] + 1] - off[0]), (int)(a.tri_off[mesh[1] + 1] - off[1])};
+        // this item's A triangles (all of them unless the pair is split)
+        const int a_lo = (int)((int64_t)nt[0] * chunk / nchunk), a_hi = (int)((int64_t)nt[0] * (chunk + 1) / nchunk);
+        bool separated = false;
         const double R[2] = {__longlong_as_double((long long)a.mesh_R_bits[mesh[0]]),
                              __longlong_as_double((long long)a.mesh_R_bits[mesh[1]])};
         auto inf = [](V3 v) { return smax3(fabs(v.x), fabs(v.y), fabs(v.z)); };
@@ -338,7 +367,10 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     sh_slab[2] = slack;
                 }
                 __syncthreads();
-                if (sh_sep) {
+                if (sh_sep && nchunk > 1) {
+                    // a split pair finishes through the joining below, with no segments from this item
+                    separated = true;
+                } else if (sh_sep) {
                     if (tid == 0) {
                         a.pair_seg_off[p] = 0;
                         a.pair_nseg[p] = 0;
@@ -374,7 +406,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 bound = s == 0 ? sh_slab[1] - sh_slab[2] - dot(tpos[0], dslab)
                                : sh_slab[0] + sh_slab[2] - dot(tpos[1], dslab);
             }
-            for (int t = tid; t < nt[s]; t += K1_THREADS) {
+            const int t_lo = s == 0 ? a_lo : 0, t_hi = separated ? t_lo : (s == 0 ? a_hi : nt[1]);
+            for (int t = t_lo + tid; t < t_hi; t += K1_THREADS) {
                 if (slab) {
                     const double* lv = a.tris + 9 * (off[s] + t);
                     const double p0 = lv[0] * dl.x + lv[1] * dl.y + lv[2] * dl.z;
@@ -382,11 +415,14 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     const double p2 = lv[6] * dl.x + lv[7] * dl.y + lv[8] * dl.z;
                     if (s == 0 ? (smax3(p0, p1, p2) < bound) : (smin3(p0, p1, p2) > bound)) continue;
                 }
-                double4 sp = a.tri_sph[off[s] + t];
-                V3 c = V3{sp.x, sp.y, sp.z};
-                V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];
-                double L = sp.w + lim;
-                if (!(fabs(cw.x - other.x) <= L && fabs(cw.y - other.y) <= L && fabs(cw.z - other.z) <= L)) continue;
+                if (!a.per_stage) {
+                    double4 sp = a.tri_sph[off[s] + t];
+                    V3 c = V3{sp.x, sp.y, sp.z};
+                    V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];
+                    double L = sp.w + lim;
+                    if (!(fabs(cw.x - other.x) <= L && fabs(cw.y - other.y) <= L && fabs(cw.z - other.z) <= L))
+                        continue;
+                }
                 const double* v = a.tris + 9 * (off[s] + t);
                 V3 w[3];
                 for (int k = 0; k < 3; ++k) {
@@ -428,7 +464,12 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         const int64_t total = (int64_t)nA * nB;
         const K1Side& SA = S.side[0];
         const K1Side& SB = S.side[1];
-        if (nA > 0 && nB > 0 && nB <= K1_HCAP && total > K1_FLAT_MAX) {
+        // the survivors' exact boxes (component-major, stride cap) stay in the CTA's slot: the tests' gathers
+        // hit in L1, which staging them in shared memory (measured: slower) would take away
+        const double* bA = SA.box;
+        const double* bB = SB.box;
+        const int sA = cap, sB = cap;
+        if (!a.per_stage && nA > 0 && nB > 0 && nB <= K1_HCAP && total > a.flat_max) {
             // ---- hierarchical test: B's survivors in Morton order, outward-rounded float AABBs and
             // 32-triangle group boxes in shared memory; one warp per A triangle rejects whole groups
             // first.  A float reject is exact (the float box contains the double one); every float
@@ -471,8 +512,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 }
             for (int m = tid; m < nB; m += K1_THREADS) {
                 int ib = sm_val[m];
-                for (int k = 0; k < 3; ++k) sm_box[k * K1_HCAP + m] = __double2float_rd(SB.box[k * cap + ib]);
-                for (int k = 3; k < 6; ++k) sm_box[k * K1_HCAP + m] = __double2float_ru(SB.box[k * cap + ib]);
+                for (int k = 0; k < 3; ++k) sm_box[k * K1_HCAP + m] = __double2float_rd(bB[k * sB + ib]);
+                for (int k = 3; k < 6; ++k) sm_box[k * K1_HCAP + m] = __double2float_ru(bB[k * sB + ib]);
             }
             __syncthreads();
             const int ng = (nB + 31) >> 5;
@@ -493,7 +534,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
             int wq_n = 0;
             for (int ia = warp; ia < nA; ia += K1_THREADS / 32) {
                 double da[6];
-                for (int k = 0; k < 6; ++k) da[k] = SA.box[k * cap + ia];
+                for (int k = 0; k < 6; ++k) da[k] = bA[k * sA + ia];
                 float fa[6];
                 for (int k = 0; k < 3; ++k) fa[k] = __double2float_rd(da[k]);
                 for (int k = 3; k < 6; ++k) fa[k] = __double2float_ru(da[k]);
@@ -520,9 +561,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                             if (fov) {
                                 ib = sm_val[m];
                                 // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
-                                hit = !(da[3] < SB.box[ib] || da[0] > SB.box[3 * cap + ib] || da[4] < SB.box[cap + ib] ||
-                                        da[1] > SB.box[4 * cap + ib] || da[5] < SB.box[2 * cap + ib] ||
-                                        da[2] > SB.box[5 * cap + ib]);
+                                hit = !(da[3] < bB[ib] || da[0] > bB[3 * sB + ib] || da[4] < bB[sB + ib] ||
+                                        da[1] > bB[4 * sB + ib] || da[5] < bB[2 * sB + ib] || da[2] > bB[5 * sB + ib]);
                             }
                         }
                         unsigned hb = __ballot_sync(FULL, hit);
@@ -554,9 +594,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     int64_t kk = base + (int64_t)it * K1_THREADS + tid;
                     if (kk < total) {
                         // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
-                        bool sep = SA.box[3 * cap + ia] < SB.box[0 * cap + ib] || SA.box[0 * cap + ia] > SB.box[3 * cap + ib] ||
-                                   SA.box[4 * cap + ia] < SB.box[1 * cap + ib] || SA.box[1 * cap + ia] > SB.box[4 * cap + ib] ||
-                                   SA.box[5 * cap + ia] < SB.box[2 * cap + ib] || SA.box[2 * cap + ia] > SB.box[5 * cap + ib];
+                        bool sep = bA[3 * sA + ia] < bB[0 * sB + ib] || bA[0 * sA + ia] > bB[3 * sB + ib] ||
+                                   bA[4 * sA + ia] < bB[1 * sB + ib] || bA[1 * sA + ia] > bB[4 * sB + ib] ||
+                                   bA[5 * sA + ia] < bB[2 * sB + ib] || bA[2 * sA + ia] > bB[5 * sB + ib];
                         if (!sep) {
                             int qi = atomicAdd(&sh_nq, 1);
                             sh_q[qi] = make_int2(ia, ib);
@@ -606,14 +646,80 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
             status |= PAIR_NO_ARENA;
             if (tid == 0) atomicOr(a.err, ERR_SEG_ARENA);
         }
+        if (nchunk == 1) {
+            if (tid == 0) {
+                if (a.seg_total) atomicAdd(a.seg_total, (unsigned long long)ns);
+                a.pair_seg_off[p] = (int64_t)sbase;
+                a.pair_nseg[p] = ns;
+                a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
+                a.pair_status[p] = status;
+                atomicMax(a.max_nseg, ns);
+                atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
+                if (status) atomicOr(a.err, ERR_PAIR);
+            }
+            __syncthreads();
+            continue;
+        }
+        // ---- a split pair: record this item's run; the pair's last item joins the runs in chunk order
         if (tid == 0) {
-            a.pair_seg_off[p] = (int64_t)sbase;
-            a.pair_nseg[p] = ns;
+            a.chunk_seg_off[item] = (int64_t)sbase;
+            a.chunk_nseg[item] = ns;
+            a.chunk_status[item] = status;
+            __threadfence();
+            sh_last = atomicAdd(a.pair_done + p, 1) == nchunk - 1;
+        }
+        __syncthreads();
+        if (!sh_last) continue;
+        __threadfence();
+        const int64_t first = a.pair_first_item[p];
+        if (tid == 0) {
+            long long tot = 0;
+            int st = 0;
+            for (int c = 0; c < nchunk; ++c) {
+                tot += __ldcg(a.chunk_nseg + first + c);
+                st |= __ldcg(a.chunk_status + first + c);
+            }
+            if (tot > a.cap_seg) st |= PAIR_SEG_OVERFLOW;
+            int keep = (int)(tot < a.cap_seg ? tot : a.cap_seg);
+            unsigned long long fb = 0;
+            if (!(st & PAIR_NO_ARENA)) {
+                fb = atomicAdd(a.seg_counter, (unsigned long long)keep);
+                if (fb + (unsigned long long)keep > (unsigned long long)a.seg_cap) {
+                    st |= PAIR_NO_ARENA;
+                    atomicOr(a.err, ERR_SEG_ARENA);
+                }
+            }
+            if (st & PAIR_NO_ARENA) keep = 0;
+            sh_base = fb;
+            sh_ftot = keep;
+            if (a.seg_total) atomicAdd(a.seg_total, (unsigned long long)keep);
+            a.pair_seg_off[p] = (int64_t)fb;
+            a.pair_nseg[p] = keep;
             a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
-            a.pair_status[p] = status;
-            atomicMax(a.max_nseg, ns);
+            a.pair_status[p] = st;
+            atomicMax(a.max_nseg, keep);
             atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
-            if (status) atomicOr(a.err, ERR_PAIR);
+            if (st) atomicOr(a.err, ERR_PAIR);
+        }
+        __syncthreads();
+        {
+            const unsigned long long fb = sh_base;
+            const long long keep = sh_ftot;
+            long long run = 0;
+            for (int c = 0; c < nchunk && run < keep; ++c) {
+                const long long src = __ldcg(a.chunk_seg_off + first + c);
+                const long long nc = __ldcg(a.chunk_nseg + first + c);
+                const long long take = nc < keep - run ? nc : keep - run;
+                for (long long q = tid; q < 6 * take; q += K1_THREADS)
+                    a.seg[6 * (fb + run) + q] = __ldcg(a.seg + 6 * src + q);
+                if (a.seg_tri) {
+                    for (long long q = tid; q < 2 * take; q += K1_THREADS) {
+                        a.seg_tri[2 * (fb + run) + q] = __ldcg(a.seg_tri + 2 * src + q);
+                        a.seg_cand[2 * (fb + run) + q] = a.seg_cand[2 * src + q];
+                    }
+                }
+                run += take;
+            }
         }
         __syncthreads();
     }
@@ -622,11 +728,16 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
 void launch_segments(const PairArgs& a, int grid, cudaStream_t s) {
     if (grid <= 0) return;
     // per device and cheap: set it on every launch
+    // shared memory for two CTAs per SM and the rest of the SM's 256 KB as L1 (the survivors' gathers hit
+    // there): the carveout, in percent of the largest shared memory, that holds 2 x (dynamic + static + 1 KB)
+    const int carve = (int)((200 * (K1_DSMEM + 2048) + 233471) / 233472);
     if (a.mode == 2) {
         cudaFuncSetAttribute(k_segments<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+        cudaFuncSetAttribute(k_segments<true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         k_segments<true><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
     } else {
         cudaFuncSetAttribute(k_segments<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+        cudaFuncSetAttribute(k_segments<false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         k_segments<false><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
     }
 }
@@ -770,6 +881,7 @@ __device__ int uf_find_ro(const int* parent, int x) {
     return x;
 }
 
+
 // One pop of polyline.py's component search for segment i (the whole warp): every grid candidate j
 // (some rep point of j in a cell next to one of i's, in the grid walk's order, as in the zdem search), the
 // accepted ones (not visited, padded boxes overlapping, seg_seg_dist2 <= tol2) pushed in the set's order.
@@ -898,6 +1010,11 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
             if (lane == 0) B.raw_off[0] = 0;
             __syncwarp();
             int cnt = 0, ncr = 0;
+            // zdem mode scans only the segments not yet visited: U = sp_v[ub, ub + u), ascending, kept
+            // compact by every pop's scan (polyline mode's candidate sets include visited segments)
+            int ub = 0, u = n;
+            if (!py)
+                for (int i = lane; i < n; i += 32) B.sp_v[i] = i;
             for (int seed = 0; seed < n; ++seed) {
                 if (B.visited[seed]) continue;
                 __syncwarp();
@@ -906,6 +1023,9 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     B.stack[0] = seed;
                     B.raw_idx[cnt] = seed;
                 }
+                // every index below seed is visited, so seed is U's first entry
+                ub += 1;
+                u -= 1;
                 int sp = 1;
                 cnt++;
                 __syncwarp();
@@ -920,11 +1040,13 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                     if (py) {
                         nel = py_neighbours<NPX>(B, S, n, i, ci, imn, imx, p1, q1, tol2, sp, cnt, lane, &status);
                     } else {
-                        for (int jb = 0; jb < n; jb += 32) {
-                            const int j = jb + lane;
+                        int w = 0;
+                        for (int jb = 0; jb < u; jb += 32) {
+                            const int uk = jb + lane;
+                            const int j = uk < u ? B.sp_v[ub + uk] : -1;
                             bool el = false;
                             int best = 1 << 30;
-                            if (j < n && j != i && !B.visited[j]) {
+                            if (uk < u) {
                                 // the padded-box overlap is necessary too; test it first (cheapest reject)
                                 V3 jmn = ld3(B.bmn + 3 * j), jmx = ld3(B.bmx + 3 * j);
                                 bool ov = !(imx.x < jmn.x || imn.x > jmx.x || imx.y < jmn.y || imn.y > jmx.y ||
@@ -952,7 +1074,12 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
                                 B.el_k[pos] = best;
                             }
                             nel += __popc(bal);
+                            // U keeps the rest, in order; writes land at or below this chunk's reads
+                            const unsigned keep = __ballot_sync(FULL, uk < u && !el);
+                            if (uk < u && !el) B.sp_v[ub + w + __popc(keep & ((1u << lane) - 1u))] = j;
+                            w += __popc(keep);
                         }
+                        u = w;
                         __syncwarp();
                         if (lane == 0) {
                             for (int x = 1; x < nel; ++x) {
@@ -1475,27 +1602,35 @@ __device__ void rebuild_pair(const PairArgs& a, const int p, const PostBufs& B, 
 }
 
 template <bool NPX>
-__global__ __launch_bounds__(K2_WARPS * 32) void k_rebuild(PairArgs a) {
+__global__ __launch_bounds__(K2_MAX_WARPS * 32) void k_rebuild(PairArgs a) {
     const int lane = threadIdx.x & 31;
-    const int64_t wslot = (int64_t)blockIdx.x * K2_WARPS + (threadIdx.x >> 5);
+    const int64_t wslot = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (wslot >= a.k2_nslots) return;
     PostBufs B;
     carve_post(a.k2_slots + (size_t)wslot * a.k2_slot_bytes, a.k2_nmax, &B);
     const int64_t iend = item_end_of(a);
-    for (;;) {
+    for (int64_t round = 0;; ++round) {
         int item = 0;
-        if (lane == 0) item = (int)(a.item_begin + atomicAdd(a.queue2, 1));
+        if (a.per_stage) item = (int)(a.item_begin + wslot + round * a.k2_nslots);
+        else if (lane == 0) item = (int)(a.item_begin + atomicAdd(a.queue2, 1));
         item = __shfl_sync(FULL, item, 0);
         if (item >= iend) break;
         rebuild_pair<NPX>(a, a.order[item], B, lane);
     }
 }
 
-void launch_rebuild(const PairArgs& a, int warps, cudaStream_t s) {
+void launch_rebuild(const PairArgs& a, int warps, int warps_per_block, cudaStream_t s) {
     if (warps <= 0) return;
-    int blocks = (warps + K2_WARPS - 1) / K2_WARPS;
-    if (a.mode == 2) k_rebuild<true><<<blocks, K2_WARPS * 32, 0, s>>>(a);
-    else k_rebuild<false><<<blocks, K2_WARPS * 32, 0, s>>>(a);
+    const int wpb = warps_per_block < 1 ? 1 : (warps_per_block > K2_MAX_WARPS ? K2_MAX_WARPS : warps_per_block);
+    int blocks = (warps + wpb - 1) / wpb;
+    // the rebuild keeps every slot array in L1: ask for the largest L1 (it uses no shared memory)
+    if (a.mode == 2) {
+        cudaFuncSetAttribute(k_rebuild<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+        k_rebuild<true><<<blocks, wpb * 32, 0, s>>>(a);
+    } else {
+        cudaFuncSetAttribute(k_rebuild<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+        k_rebuild<false><<<blocks, wpb * 32, 0, s>>>(a);
+    }
 }
 
 // --------------------------------------------------------------------------------------------- stage 3

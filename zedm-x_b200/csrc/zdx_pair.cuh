@@ -48,6 +48,10 @@ struct PairArgs {
     const double* pose;
     const int32_t* order;  // work item -> pair, most expensive first
     int mode;              // 0 zdem, 1 polyline
+    // 1: the plain per-stage form (ZDX_SCHED_PER_STAGE): CTAs and warps take pairs in a fixed
+    // grid-stride order instead of from the work queues, and the triangle stage tests every nA x nB
+    // triangle pair (no separation certificate, no bounding-cube or slab cull, no hierarchical test)
+    int per_stage;
     int split;
     double tol_in;
     double k;
@@ -57,11 +61,26 @@ struct PairArgs {
     int64_t item_begin, item_end;
     int cap_side;
     int cap_seg;
+    int64_t flat_max;  // survivor pairs nA' x nB' up to which the flat box test runs (tuning)
+    // Split of large pairs across CTAs (null items: one triangle-stage work item per pair, from order).
+    // A pair of nchunk items has them consecutive from pair_first_item[p]; item c tests the A triangles
+    // [c nA / nchunk, (c + 1) nA / nchunk) against all of B and writes its (ta, tb)-ordered segments as a
+    // temporary run; the last of the pair's items to finish joins the runs in chunk order, which is the
+    // pair's (ta, tb) order, into one run of the arena.
+    const int32_t* items;       // per work item: its pair
+    const int32_t* item_chunk;  // per work item: chunk index | chunk count << 16
+    const int32_t* pair_first_item;
+    int32_t* pair_done;         // per pair: chunks finished (zero at the start of the triangle stage)
+    int64_t* chunk_seg_off;     // per work item: its temporary run
+    int32_t* chunk_nseg;
+    int32_t* chunk_status;
+    int64_t n_items;
     char* k1_slots;
     size_t k1_slot_bytes;
     double* seg;  // arena: 6 doubles per segment
     int64_t seg_cap;
-    unsigned long long* seg_counter;
+    unsigned long long* seg_counter;  // arena entries taken (with split pairs, their temporary runs too)
+    unsigned long long* seg_total;    // null, or the segments of all pairs (the call's segment total)
     int64_t* pair_seg_off;
     int32_t* pair_nseg;
     int64_t* pair_checks;
@@ -111,7 +130,7 @@ size_t tritest_slot_bytes(int cap_side, int cap_seg);
 void launch_mesh_prep(const PairArgs& a, int64_t total_tris, cudaStream_t s);
 void launch_cost_order(const PairArgs& a, int32_t* order, int* buckets, cudaStream_t s);
 void launch_segments(const PairArgs& a, int grid, cudaStream_t s);
-void launch_rebuild(const PairArgs& a, int warps, cudaStream_t s);
+void launch_rebuild(const PairArgs& a, int warps, int warps_per_block, cudaStream_t s);
 void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_pts_off, double* cgeom,
                    int32_t* cinfo, double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* ctape_off,
                    cudaStream_t s);
@@ -142,7 +161,9 @@ struct AdjointArgs {
     double* grad_pose;           // 12 per pair
 };
 void launch_adjoint(const AdjointArgs& a, cudaStream_t s);
-int k1_blocks_per_sm();
-int k2_warps_per_block();
+// Largest rebuild block the kernel is compiled for, in warps.  Its launch bound (128 threads) is what
+// gives the kernel its register budget: 168 registers; a 256-thread bound made ptxas choose 128 with
+// four times the spills (rebuild 28.2 against 26.6 ms on the pair sweep).
+constexpr int K2_MAX_WARPS = 4;
 
 }  // namespace zdx

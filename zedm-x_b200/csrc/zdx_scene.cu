@@ -1450,13 +1450,13 @@ static int graph_alloc(zdx_ctx* ctx, Scene& s) {
     CKS(G.pair_i64.ensure(sizeof(int64_t) * 5 * P1));
     CKS(G.pair_i32.ensure(sizeof(int32_t) * 6 * P1));
     CKS(G.counters.ensure(sizeof(unsigned long long) * 16));
-    G.k1_grid = (int)std::min<int64_t>(P1, (int64_t)ctx->num_sms * k1_blocks_per_sm());
+    G.k1_grid = (int)std::min<int64_t>(P1, (int64_t)ctx->num_sms * ctx->tune.tri_ctas_per_sm);
     CKS(G.k1_slots.ensure(tritest_slot_bytes(max_ntri, G.cap_seg) * (size_t)G.k1_grid));
     CKS(G.seg_arena.ensure(sizeof(double) * 6 * (size_t)std::max<int64_t>(G.segcap, 1)));
     const size_t slot = rebuild_slot_bytes(G.cap_seg);
     int64_t warps = std::min<int64_t>((int64_t)P1, (int64_t)ctx->num_sms * 32);
     warps = std::min<int64_t>(warps, std::max<int64_t>(1, (int64_t)(((size_t)2 << 30) / slot)));
-    warps = (warps + k2_warps_per_block() - 1) / k2_warps_per_block() * k2_warps_per_block();
+    warps = (warps + ctx->tune.rebuild_warps - 1) / ctx->tune.rebuild_warps * ctx->tune.rebuild_warps;
     G.k2_warps = (int)warps;
     CKS(G.k2_slots.ensure(slot * (size_t)warps));
     CKS(G.cstage.ensure(sizeof(double) * 20 * C1));
@@ -1533,6 +1533,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
         for (int m = 0; m < nm; ++m) max_ntri = std::max<int>(max_ntri, (int)(s.mesh_off[m + 1] - s.mesh_off[m]));
         a.cap_side = max_ntri;
         a.cap_seg = G.cap_seg;
+        a.flat_max = ctx->tune.flat_max;
         const size_t P1 = (size_t)std::max<int64_t>(G.pcap, 1);
         int64_t* pi64 = as<int64_t>(G.pair_i64);
         int32_t* pi32 = as<int32_t>(G.pair_i32);
@@ -1581,7 +1582,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
         a.contact_cap = G.ccap;
         a.pts_stage = nullptr;
         a.pts_cap = 0;
-        launch_rebuild(a, G.k2_warps, st);
+        launch_rebuild(a, G.k2_warps, ctx->tune.rebuild_warps, st);
         launch_gather_dev(a, as<int64_t>(G.pr_coff), as<double>(G.pr_geom), as<int32_t>(G.pr_info),
                           as<int32_t>(G.pr_stats), G.scan_tmp.p, st);
         k_g_pair_done<<<1, 1, 0, st>>>(cnt, g);

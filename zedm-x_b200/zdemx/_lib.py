@@ -29,6 +29,7 @@ MEM_HOST = 0
 MEM_DEVICE = 1
 SCHED_BATCHED = 0
 SCHED_PLAIN = 1
+SCHED_PER_STAGE = 2  # one launch per stage over the batch, no work queue, no cost order, no culls
 
 _dp = C.POINTER(C.c_double)
 _i32p = C.POINTER(C.c_int32)
@@ -54,6 +55,11 @@ class PairResult(C.Structure):
                 ("contact_cap", C.c_int64), ("contact_geom", C.c_void_p), ("contact_info", C.c_void_p),
                 ("loop_point_cap", C.c_int64), ("loop_points", C.c_void_p), ("contact_point_off", C.c_void_p),
                 ("totals", C.c_int64 * 4), ("comp_stats_cap", C.c_int64), ("comp_stats", C.c_void_p)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("tri_ctas_per_sm", C.c_int32), ("rebuild_warps", C.c_int32), ("flat_max", C.c_int64),
+                ("split_tests", C.c_int64)]
 
 
 class ZdxError(RuntimeError):
@@ -106,6 +112,8 @@ def lib() -> C.CDLL:
                                             C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.zdx_pair_contacts_noalloc.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                             C.POINTER(PairResult)]
+    L.zdx_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    L.zdx_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
     _lib = L
     return L
 
@@ -188,6 +196,22 @@ class Context:
         v = C.c_void_p()
         check(lib().zdx_get_stream(self.handle, C.byref(v)), self.handle)
         return int(v.value or 0)
+
+    def tuning(self) -> dict:
+        """The pair kernels' launch parameters in force (zdx_get_tuning)."""
+        t = Tuning()
+        check(lib().zdx_get_tuning(self.handle, C.byref(t)), self.handle)
+        return {k: int(getattr(t, k)) for k, _ in Tuning._fields_}
+
+    def set_tuning(self, **kw) -> dict:
+        """Change some launch parameters (zdx_set_tuning); the others keep their values."""
+        cur = self.tuning()
+        unknown = set(kw) - set(cur)
+        if unknown:
+            raise ValueError(f"unknown tuning keys {sorted(unknown)}")
+        cur.update({k: int(v) for k, v in kw.items()})
+        check(lib().zdx_set_tuning(self.handle, C.byref(Tuning(**cur))), self.handle)
+        return cur
 
     def timings(self):
         t = np.zeros(5)

@@ -99,8 +99,21 @@ def tri_normals(tris):
 def pair_contacts(trisA, trisB, tA=(0.0, 0.0, 0.0), qA=(1.0, 0.0, 0.0, 0.0), tB=(0.0, 0.0, 0.0),
                   qB=(1.0, 0.0, 0.0, 0.0), k=1.0, tol=1e-6, split_contacts=False, idA=0, idB=1, ctx=None):
     """Contacts between mesh A at pose (tA, qA) and mesh B at (tB, qB), as polyline.py main computes
-    them (polyline.py:743-829).  Returns (manifold, loops_pts, xc0s, contact_ids)."""
+    them (polyline.py:743-829).  Returns (manifold, loops_pts, xc0s, contact_ids): manifold is the dict
+    of build_contacts_from_loops (polyline.py:681-701), the rest what main passes to its writers.
+    tol=None takes the snap tolerance as the zdem_cpu step does, from A's mean edge length
+    (src/main.cpp:2118-2121: 0.1 mean edge, else 1 % of the bounding-box diagonal, else 1e-6)."""
+    if tol is None:
+        tol = _mean_edge_tol(trisA)
     return _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, ctx)[:4]
+
+
+def _mean_edge_tol(tris) -> float:
+    """The snap tolerance rule of src/main.cpp:2118-2121 on build_mesh's mean edge and bbox diagonal."""
+    _, props = _lib.mesh_build(np.asarray(tris, dtype=float), False)
+    me, bd = props["mean_edge"], props["bbox_diag"]
+    tol = me * 0.1 if me > 0.0 else bd * 1e-2
+    return tol if tol > 0.0 else 1e-6
 
 
 # components recorded by the command line: at most one per segment, and a pair holds at most the

@@ -161,3 +161,61 @@ def calibration_scene(dirpath: str, n_side: int = 10, seed: int = 5, steps: int 
     with open(cfg, "w") as f:
         f.write("\n".join(lines) + "\n")
     return cfg
+
+
+def independent_pair_library(n_pairs: int, seed: int, radius: float = 1e-3, noise: float = 0.15,
+                             threads: int | None = None, out_tris=None):
+    """The pair sweep with every pair's two meshes its own: 2 n_pairs seeded noised icospheres, each
+    subdivision drawn from U{1..4}, built with build_mesh (zdx_mesh_build) on `threads` host threads.
+
+    Meshes are numbered level by level (pair sides of subdivision 1 first), so a pair's two meshes are
+    two distinct ids.  `out_tris`, if given, is a float64 array of shape (T, 9) (T = the total triangle
+    count, from ``independent_pair_sizes``) that receives the built triangles, e.g. a pinned host
+    buffer.  Returns (MeshLibrary, pair_mesh (n_pairs, 2) int32)."""
+    import ctypes as C
+    from concurrent.futures import ThreadPoolExecutor
+
+    from . import _lib
+    from .contact import MeshLibrary
+
+    side_level, off, pm = independent_pair_sizes(n_pairs, seed)
+    n_mesh = 2 * n_pairs
+    tris = out_tris if out_tris is not None else np.empty((int(off[-1]), 9))
+    if tris.shape != (int(off[-1]), 9) or tris.dtype != np.float64 or not tris.flags.c_contiguous:
+        raise ValueError("out_tris must be a C-contiguous float64 (T, 9) array")
+    props = np.empty((n_mesh, 17))
+    L = _lib.lib()
+    dp = C.POINTER(C.c_double)
+    chunks = []
+    for lvl in (1, 2, 3, 4):
+        ids = np.nonzero(side_level == lvl)[0]
+        for a in range(0, len(ids), 256):
+            chunks.append((lvl, int(ids[a]), min(len(ids), a + 256) - a))
+
+    def work(ci):
+        lvl, m0, cnt = chunks[ci]
+        raw = np.ascontiguousarray(synth.noised_icospheres(lvl, cnt, radius, noise, np.random.default_rng([seed, ci])))
+        nt = 20 * 4 ** lvl
+        for k in range(cnt):
+            m = m0 + k
+            _lib.check(L.zdx_mesh_build(raw[k].ctypes.data_as(dp), nt, 1, tris[off[m]:off[m + 1]].ctypes.data_as(dp),
+                                        props[m].ctypes.data_as(dp)))
+
+    with ThreadPoolExecutor(threads or os.cpu_count() or 1) as ex:
+        list(ex.map(work, range(len(chunks))))
+    return MeshLibrary(tris, off, props[:, 5].copy(), props[:, 6].copy(), props), pm
+
+
+def independent_pair_sizes(n_pairs: int, seed: int):
+    """Subdivision level of every mesh (level-major numbering), the triangle offsets and the pairs' mesh
+    ids of ``independent_pair_library``."""
+    rng = np.random.default_rng([seed, 0x1D])
+    lv = rng.integers(1, 5, size=(n_pairs, 2))
+    order = np.argsort(lv.ravel(), kind="stable")
+    side_level = lv.ravel()[order]
+    mesh_of_side = np.empty(2 * n_pairs, np.int64)
+    mesh_of_side[order] = np.arange(2 * n_pairs)
+    ntri = (20 * 4 ** side_level).astype(np.int64)
+    off = np.zeros(2 * n_pairs + 1, np.int64)
+    off[1:] = np.cumsum(ntri)
+    return side_level, off, mesh_of_side.reshape(n_pairs, 2).astype(np.int32)
