@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--preroll", type=int, default=1500, help="pour: untimed steps before warm-up (collisions start)")
     ap.add_argument("--rollout-steps", type=int, default=2000, help="rollout: steps of the rollout")
     ap.add_argument("--rollout-side", type=int, default=10, help="rollout: particles per lattice side")
+    ap.add_argument("--extras", type=int, default=1,
+                    help="sweep at N=1: 0 prints the headline line alone (no parity, comparisons, independent "
+                         "meshes or DEM legs), e.g. under a profiler")
     ap.add_argument("--tune-pairs", type=int, default=16384,
                     help="sweep: pairs of the autotuner's calibration sample (0: keep the default launch parameters)")
     return ap.parse_args()
@@ -175,9 +178,9 @@ def measured_peaks():
 # kernel sources they were captured on: KERNEL_SOURCES hashed to `sources_sha256`.  When the sources
 # differ, the figures are reported as stale (null) rather than applied to other code.
 PROFILED = {
-    "sources_sha256": None,
-    "k_segments": {"warp_inst_per_pair": None, "dram_bytes_per_pair": None},
-    "k_rebuild": {"warp_inst_per_pair": None, "dram_bytes_per_pair": None},
+    "sources_sha256": "aca7521edfde6c6fa86dff7a6fae681e76c009daeb14084fd74925b48fbbb56b",
+    "k_segments": {"warp_inst_per_pair": 124799.9, "dram_bytes_per_pair": 278945.5},
+    "k_rebuild": {"warp_inst_per_pair": 147346.3, "dram_bytes_per_pair": 17531.2},
 }
 KERNEL_SOURCES = ("zdx_pair.cu", "zdx_pair.cuh", "zdx_math.cuh", "zdx_npmath.cuh", "zdx_pyset.cuh",
                   "zdx_sortrep.cuh", "zdx_radix.cuh")
@@ -504,6 +507,10 @@ def main():
 
     log(f"sweep: {value:.4g} pairs/s device, {e2e_value:.4g} e2e")
     extras = {"tuning": tuning}
+    if not args.extras:
+        emit(_sweep_line(args, world, value, T, totals, launches, clk, wall, e2e_value, h2d, d2h, lib, pm, seg_ms,
+                         reb_ms, step_ms, base_cfg, extras))
+        return
     # parity of this step's output with the reference's own code on the CPU baseline's sample
     rate, n_cpu, dt_cpu, sel, rec = cpu_reference_rate(lib, pm, pp, 1, args.cpu_seconds, record=True)
     extras["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
