@@ -251,6 +251,79 @@ int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t contacts, int64
 int zdx_run_config(const char* config_path, int device);
 int zdx_run_config_graph(const char* config_path, int device);
 
+/* ---- particle-wall contacts for differentiable rollouts ----------------------------------------------
+ * No counterpart in the reference (which has no derivatives): the wall part of its step loop
+ * (src/main.cpp:2308-2447 with compute_wall_contact, :1205-1258), for a list of (particle, wall) items, and
+ * its reverse mode.  Per item: for each triangle of the wall in order, the AABB test, the plane section
+ * of the particle's mesh, unique_points, the Sutherland-Hodgman clip against the triangle, area and
+ * centroid, and the wall force law with the tangential history shared by the wall's triangles.  Outputs
+ * per item: the summed force and torque on the particle, the history after the wall, and flags
+ * (bit 0: some triangle touched, bits 1-15: contacts, bit 16: a section exceeded 256 crossings).
+ * The restitution e is one value for every contact (the rollout's calibration parameter); everything
+ * else comes from the arrays.  All pointers are device memory on the context's GPU; the calls run on
+ * the context stream and return when done.  zdx_wall_forces_adjoint takes the cotangents of the three
+ * outputs and writes those of x, q (the stored, unnormalised quaternion), v, omega, the history in and e
+ * per item, with the contact topology of the forward pass. */
+typedef struct zdx_wall_items {
+    int64_t n_items;
+    const double* x;            /* n x 3 particle position                                        */
+    const double* q;            /* n x 4 quaternion (w, x, y, z)                                  */
+    const double* v;            /* n x 3 velocity                                                 */
+    const double* w;            /* n x 3 angular velocity                                         */
+    const double* mat;          /* n x 17 the particle's material row (zdx_scene_array ZDX_SCENE_MAT) */
+    const int32_t* mesh;        /* n particle mesh                                                */
+    const int32_t* wall;        /* n wall                                                         */
+    const double* ds_in;        /* n x 3 tangential history of (particle, wall) before the step   */
+    double e, dt;
+    int32_t max_mesh_tris;      /* largest triangle count of the meshes the items use             */
+    const double* mesh_tris;    /* particle meshes as build_mesh leaves them, 9 doubles a triangle */
+    const int64_t* mesh_off;
+    const double* mesh_tol;     /* per mesh: 0.1 mean edge, else 1 % of the bbox diagonal, else 1e-6 */
+    const double* wall_tris;    /* wall triangles in world coordinates, walls back to back        */
+    const double* wall_normals; /* their unit normals                                             */
+    const int64_t* wall_off;    /* n_walls + 1                                                    */
+    const double* wall_mu;      /* per wall: friction coefficient                                 */
+} zdx_wall_items;
+int zdx_wall_forces(zdx_ctx* ctx, const zdx_wall_items* items, double* force3, double* torque3, double* ds_out3,
+                    int32_t* flags);
+int zdx_wall_forces_adjoint(zdx_ctx* ctx, const zdx_wall_items* items, const double* g_force3,
+                            const double* g_torque3, const double* g_ds_out3, double* g_x3, double* g_q4,
+                            double* g_v3, double* g_w3, double* g_ds_in3, double* g_e);
+
+/* The particle-particle force law of the step loop (src/main.cpp:2220-2287) for a list of candidate pairs
+ * and its reverse mode, for differentiable rollouts (no reference counterpart).  Pair p's contacts are
+ * [contact_off[p], contact_off[p+1]) in loop order (at most 64), each with its contact point xc0, its
+ * normal (pointing from A toward B) and its area, as zdx_pair_contacts returns them in zdem mode; they
+ * share the pair's tangential history.  law 0 is the reference's zdem law (kn (A^1.5)^(1/3)), 1 the
+ * feng_min law k/2 A.  Outputs per pair: the summed force on B (A receives its negative), the torques on
+ * A and on B, the history after its last contact.  zdx_pp_forces_adjoint takes their cotangents and
+ * writes per pair those of xa xb va vb wa wb ds_in (21), k and e, and per contact those of xc0, the
+ * normal and the area (7), with the regimes (Coulomb cap, positive normal force) of the forward pass.
+ * Device pointers, context stream; the calls return when done. */
+typedef struct zdx_pp_pairs {
+    int64_t n_pairs;
+    const int64_t* contact_off;   /* n_pairs + 1                                             */
+    const double* xa;             /* n x 3 each: positions, velocities, angular velocities   */
+    const double* xb;
+    const double* va;
+    const double* vb;
+    const double* wa;
+    const double* wb;
+    const double* mat_a;          /* n x 17 material rows of A and B                         */
+    const double* mat_b;
+    const double* ds_in;          /* n x 3 tangential history before the step                */
+    const double* xc0;            /* contacts x 3                                            */
+    const double* normal;         /* contacts x 3                                            */
+    const double* area;           /* contacts                                                */
+    int32_t law;
+    double k, e, dt;
+} zdx_pp_pairs;
+int zdx_pp_forces(zdx_ctx* ctx, const zdx_pp_pairs* pairs, double* force_b3, double* torque_a3, double* torque_b3,
+                  double* ds_out3);
+int zdx_pp_forces_adjoint(zdx_ctx* ctx, const zdx_pp_pairs* pairs, const double* g_force_b3, const double* g_torque_a3,
+                          const double* g_torque_b3, const double* g_ds_out3, double* g_pair21, double* g_k,
+                          double* g_e, double* g_contact7);
+
 /* ---- pair contacts without device allocation ------------------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate GPU memory (a host program whose
  * pool allocator owns the whole device, a real-time loop that cannot take the device-wide

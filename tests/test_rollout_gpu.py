@@ -120,3 +120,44 @@ def test_checkpointed_rollout_gives_the_same_gradients(tmp_path):
     assert l0 == l1
     np.testing.assert_allclose([k1, e1], [k0, e0], rtol=1e-10)
     np.testing.assert_allclose(v1a, v0a, rtol=1e-10, atol=1e-10 * np.max(np.abs(v0a)))
+
+
+def test_cuda_wall_contacts_match_the_torch_ones(tmp_path):
+    """The wall contacts through the CUDA kernels and their hand-written reverse mode against the same
+    computation in torch autograd (sections inside their triangle, where both apply): forces, torques,
+    histories and contact counts to rounding, and the gradients of a random linear functional of them
+    with respect to the state and e."""
+    import torch
+
+    from zdemx.rollout import DiffScene
+
+    sc = _scene(tmp_path, seed=7)
+    ds = DiffScene(sc)
+    st = torch.from_numpy(sc.state()[0]).cuda()
+    hk, hd, wk, wd = ds.initial_history()
+    k = torch.tensor(ds.feng_k, dtype=torch.float64, device="cuda")
+    e0 = torch.tensor(0.5, dtype=torch.float64, device="cuda")
+    with torch.no_grad():
+        for _ in range(25):
+            st, hk, hd, wk, wd, stats = ds.step(st, hk, hd, wk, wd, k, e0)
+    assert wk.numel() > 0, "no wall contact yet"
+    rng = np.random.default_rng(3)
+    res = []
+    for fn in (ds._walls, ds._walls_torch):
+        s = st.clone().requires_grad_(True)
+        e = e0.clone().requires_grad_(True)
+        wdd = wd.clone().requires_grad_(True)
+        Fw, Tw, key, dso, nwc = fn(s, wk, wdd, e)
+        a = torch.from_numpy(rng.normal(size=Fw.shape)).cuda()
+        b = torch.from_numpy(rng.normal(size=Tw.shape)).cuda() * 1e3
+        c = torch.from_numpy(rng.normal(size=dso.shape)).cuda() * 1e6
+        rng = np.random.default_rng(3)  # the same functional for both
+        L = (a * Fw).sum() + (b * Tw).sum() + (c * dso).sum()
+        L.backward()
+        res.append((Fw.detach(), Tw.detach(), key, dso.detach(), nwc, s.grad, e.grad, wdd.grad))
+    (F1, T1, k1, d1, n1, gs1, ge1, gw1), (F2, T2, k2, d2, n2, gs2, ge2, gw2) = res
+    assert n1 == n2 > 0 and torch.equal(k1, k2)
+    for x, y in ((F1, F2), (T1, T2), (d1, d2), (gs1, gs2), (gw1, gw2)):
+        scale = float(y.abs().max())
+        assert scale > 0 and float((x - y).abs().max()) <= 1e-9 * scale
+    assert abs(float(ge1) - float(ge2)) <= 1e-9 * abs(float(ge2))

@@ -51,6 +51,8 @@ struct zdx_ctx {
     zdx::DevBuf order, buckets, pair_i64, pair_i32, counters;
     zdx::DevBuf k1_slots, seg_arena, k2_slots;
     zdx::DevBuf sp_items, sp_first, sp_chunk;  // split of large pairs (items, per-pair first item, runs)
+    zdx::DevBuf w_scratch;                     // per-item tapes of the wall contacts (zdx_rollout.cu)
+    zdx::DevBuf p_err;                         // error flag of the pair force kernels (zdx_rollout.cu)
     zdx::DevBuf cstage, cistage, pstage;
     zdx::DevBuf g_off, o_cg, o_ci, o_pts, o_cpo, o_ps, o_comp;
     // adjoint tape (recorded when tape_on): segment provenance, per-contact records, final offsets
@@ -63,7 +65,7 @@ struct zdx_ctx {
     std::vector<zdx::DevBuf*> all_bufs() {
         return {&in_tris, &in_off, &in_me, &in_bd, &in_pm, &in_pose, &tri_sph, &mesh_R, &mesh_valid, &mesh_infl,
                 &order, &buckets, &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &sp_items,
-                &sp_first, &sp_chunk,
+                &sp_first, &sp_chunk, &w_scratch, &p_err,
                 &cstage, &cistage, &pstage, &g_off, &o_cg, &o_ci, &o_pts, &o_cpo, &o_ps, &o_comp, &t_segtri, &t_segcand,
                 &t_arena, &t_cstage, &t_cfinal, &a_nc, &a_coff, &a_stats, &a_geom, &a_info, &a_pts, &a_cpo, &a_gc,
                 &a_gt, &a_gp};

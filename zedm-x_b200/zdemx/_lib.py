@@ -62,6 +62,21 @@ class Tuning(C.Structure):
                 ("split_tests", C.c_int64)]
 
 
+class WallItems(C.Structure):
+    _fields_ = [("n_items", C.c_int64), ("x", C.c_void_p), ("q", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
+                ("mat", C.c_void_p), ("mesh", C.c_void_p), ("wall", C.c_void_p), ("ds_in", C.c_void_p),
+                ("e", C.c_double), ("dt", C.c_double), ("max_mesh_tris", C.c_int32), ("mesh_tris", C.c_void_p),
+                ("mesh_off", C.c_void_p), ("mesh_tol", C.c_void_p), ("wall_tris", C.c_void_p),
+                ("wall_normals", C.c_void_p), ("wall_off", C.c_void_p), ("wall_mu", C.c_void_p)]
+
+
+class PPPairs(C.Structure):
+    _fields_ = [("n_pairs", C.c_int64), ("contact_off", C.c_void_p), ("xa", C.c_void_p), ("xb", C.c_void_p),
+                ("va", C.c_void_p), ("vb", C.c_void_p), ("wa", C.c_void_p), ("wb", C.c_void_p), ("mat_a", C.c_void_p),
+                ("mat_b", C.c_void_p), ("ds_in", C.c_void_p), ("xc0", C.c_void_p), ("normal", C.c_void_p),
+                ("area", C.c_void_p), ("law", C.c_int32), ("k", C.c_double), ("e", C.c_double), ("dt", C.c_double)]
+
+
 class ZdxError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"zdemx status {status}: {msg}")
@@ -113,6 +128,10 @@ def lib() -> C.CDLL:
     L.zdx_pair_contacts_noalloc.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                             C.POINTER(PairResult)]
     L.zdx_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    L.zdx_wall_forces.argtypes = [C.c_void_p, C.POINTER(WallItems)] + [C.c_void_p] * 4
+    L.zdx_pp_forces.argtypes = [C.c_void_p, C.POINTER(PPPairs)] + [C.c_void_p] * 4
+    L.zdx_pp_forces_adjoint.argtypes = [C.c_void_p, C.POINTER(PPPairs)] + [C.c_void_p] * 8
+    L.zdx_wall_forces_adjoint.argtypes = [C.c_void_p, C.POINTER(WallItems)] + [C.c_void_p] * 9
     L.zdx_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
     _lib = L
     return L
@@ -316,3 +335,55 @@ def pair_contacts_adjoint(ctx: Context, meshes: dict, pairs: dict, grad_contact,
     n = int(grad_contact.shape[0])
     check(lib().zdx_pair_contacts_adjoint(ctx.handle, C.byref(opts), C.byref(ms), C.byref(pb), _ptr(grad_contact), n,
                                           _ptr(grad_tris), _ptr(grad_pose)), ctx.handle)
+
+
+def _wall_items(items: dict, e: float, dt: float, max_mesh_tris: int) -> WallItems:
+    n = int(items["x"].shape[0])
+    return WallItems(n, _ptr(items["x"]), _ptr(items["q"]), _ptr(items["v"]), _ptr(items["w"]), _ptr(items["mat"]),
+                     _ptr(items["mesh"]), _ptr(items["wall"]), _ptr(items["ds_in"]), float(e), float(dt),
+                     int(max_mesh_tris), _ptr(items["mesh_tris"]), _ptr(items["mesh_off"]), _ptr(items["mesh_tol"]),
+                     _ptr(items["wall_tris"]), _ptr(items["wall_normals"]), _ptr(items["wall_off"]),
+                     _ptr(items["wall_mu"]))
+
+
+def wall_forces(ctx: Context, items: dict, e: float, dt: float, max_mesh_tris: int, out: dict) -> None:
+    """zdx_wall_forces on CUDA tensors: items as the fields of zdx_wall_items, out["f"], out["t"], out["ds"]
+    (n x 3 float64) and out["flags"] (n int32) written."""
+    wi = _wall_items(items, e, dt, max_mesh_tris)
+    check(lib().zdx_wall_forces(ctx.handle, C.byref(wi), _ptr(out["f"]), _ptr(out["t"]), _ptr(out["ds"]),
+                                _ptr(out["flags"])), ctx.handle)
+
+
+def wall_forces_adjoint(ctx: Context, items: dict, e: float, dt: float, max_mesh_tris: int, grad_out: dict,
+                        grad_in: dict) -> None:
+    """zdx_wall_forces_adjoint: grad_out["f"], ["t"], ["ds"] in; grad_in["x"], ["q"], ["v"], ["w"], ["ds_in"],
+    ["e"] (per item) written."""
+    wi = _wall_items(items, e, dt, max_mesh_tris)
+    check(lib().zdx_wall_forces_adjoint(ctx.handle, C.byref(wi), _ptr(grad_out["f"]), _ptr(grad_out["t"]),
+                                        _ptr(grad_out["ds"]), _ptr(grad_in["x"]), _ptr(grad_in["q"]),
+                                        _ptr(grad_in["v"]), _ptr(grad_in["w"]), _ptr(grad_in["ds_in"]),
+                                        _ptr(grad_in["e"])), ctx.handle)
+
+
+def _pp_pairs(pairs: dict, law: int, k: float, e: float, dt: float) -> PPPairs:
+    return PPPairs(int(pairs["xa"].shape[0]), _ptr(pairs["contact_off"]), _ptr(pairs["xa"]), _ptr(pairs["xb"]),
+                   _ptr(pairs["va"]), _ptr(pairs["vb"]), _ptr(pairs["wa"]), _ptr(pairs["wb"]), _ptr(pairs["mat_a"]),
+                   _ptr(pairs["mat_b"]), _ptr(pairs["ds_in"]), _ptr(pairs["xc0"]), _ptr(pairs["normal"]),
+                   _ptr(pairs["area"]), int(law), float(k), float(e), float(dt))
+
+
+def pp_forces(ctx: Context, pairs: dict, law: int, k: float, e: float, dt: float, out: dict) -> None:
+    """zdx_pp_forces on CUDA tensors: out["fb"], ["ta"], ["tb"], ["ds"] (n x 3) written."""
+    pp = _pp_pairs(pairs, law, k, e, dt)
+    check(lib().zdx_pp_forces(ctx.handle, C.byref(pp), _ptr(out["fb"]), _ptr(out["ta"]), _ptr(out["tb"]),
+                              _ptr(out["ds"])), ctx.handle)
+
+
+def pp_forces_adjoint(ctx: Context, pairs: dict, law: int, k: float, e: float, dt: float, grad_out: dict,
+                      grad_in: dict) -> None:
+    """zdx_pp_forces_adjoint: grad_out["fb"], ["ta"], ["tb"], ["ds"] in; grad_in["pair"] (n x 21), ["k"], ["e"]
+    (n) and ["contact"] (contacts x 7) written."""
+    pp = _pp_pairs(pairs, law, k, e, dt)
+    check(lib().zdx_pp_forces_adjoint(ctx.handle, C.byref(pp), _ptr(grad_out["fb"]), _ptr(grad_out["ta"]),
+                                      _ptr(grad_out["tb"]), _ptr(grad_out["ds"]), _ptr(grad_in["pair"]),
+                                      _ptr(grad_in["k"]), _ptr(grad_in["e"]), _ptr(grad_in["contact"])), ctx.handle)

@@ -11,9 +11,12 @@ the device step's, so trajectories agree to rounding, not bit for bit.
 
 What is differentiable: everything continuous in the particle state and in the parameters k (feng_min
 stiffness) and e (restitution, one value for all particles).  Topology (which pairs, loops, wall
-contacts, Coulomb regime) is taken from the forward pass.  The wall section must lie inside the wall
-triangle it touches (then the clip returns it unchanged); a section that a triangle edge would clip
-raises NotImplementedError.
+contacts, Coulomb regime) is taken from the forward pass.  The wall contacts (section, clip, area,
+centroid, force law and history, every triangle of a wall in order) run in CUDA with a hand-written
+reverse mode (zdx_wall_forces / zdx_wall_forces_adjoint, one thread per particle near a wall); sections
+clipped by a wall triangle's edges are differentiated too.  ``DiffScene._walls_torch`` keeps the same
+computation in torch autograd (sections inside their triangle only), the check the kernels are tested
+against.
 
     ds = DiffScene(scene)                   # a loaded zdemx.dem.Scene
     x, aux = ds.rollout(state0, k, e, steps=2000, checkpoint_every=100)
@@ -75,6 +78,98 @@ def _lookup(keys, query):
     return torch.where(keys[pos] == query, pos, torch.full_like(pos, -1))
 
 
+class _WallForces(torch.autograd.Function):
+    """Per (particle, wall) item: summed force, torque, history after the wall (CUDA, zdx_wall_forces) and
+    their reverse (zdx_wall_forces_adjoint)."""
+
+    @staticmethod
+    def forward(ctx, x, q, v, w, ds_in, e, mat, mesh, wall, consts):
+        n = x.shape[0]
+        dev = x.device
+        items = dict(consts["items"])
+        items.update({"x": x.detach().contiguous(), "q": q.detach().contiguous(), "v": v.detach().contiguous(),
+                      "w": w.detach().contiguous(), "ds_in": ds_in.detach().contiguous(), "mat": mat, "mesh": mesh,
+                      "wall": wall})
+        out = {"f": torch.empty(n, 3, dtype=torch.float64, device=dev),
+               "t": torch.empty(n, 3, dtype=torch.float64, device=dev),
+               "ds": torch.empty(n, 3, dtype=torch.float64, device=dev),
+               "flags": torch.empty(n, dtype=torch.int32, device=dev)}
+        ev = float(e)
+        torch.cuda.synchronize(dev)
+        _lib.wall_forces(consts["ctx"], items, ev, consts["dt"], consts["max_tris"], out)
+        # per-call tensors through save_for_backward (a checkpointed rollout frees and recomputes them);
+        # the scene's constant arrays stay in consts
+        ctx.save_for_backward(items["x"], items["q"], items["v"], items["w"], items["ds_in"], items["mat"],
+                              items["mesh"], items["wall"])
+        ctx.consts = consts
+        ctx.ev = ev
+        ctx.mark_non_differentiable(out["flags"])
+        return out["f"], out["t"], out["ds"], out["flags"]
+
+    @staticmethod
+    def backward(ctx, gf, gt, gds, gflags):
+        consts = ctx.consts
+        items = dict(consts["items"])
+        for name, t in zip(("x", "q", "v", "w", "ds_in", "mat", "mesh", "wall"), ctx.saved_tensors):
+            items[name] = t
+        n = items["x"].shape[0]
+        dev = items["x"].device
+        z = lambda k: torch.zeros(n, k, dtype=torch.float64, device=dev)
+        grad_in = {"x": z(3), "q": z(4), "v": z(3), "w": z(3), "ds_in": z(3),
+                   "e": torch.zeros(n, dtype=torch.float64, device=dev)}
+        g = {"f": (gf if gf is not None else z(3)).contiguous(), "t": (gt if gt is not None else z(3)).contiguous(),
+             "ds": (gds if gds is not None else z(3)).contiguous()}
+        torch.cuda.synchronize(dev)
+        _lib.wall_forces_adjoint(consts["ctx"], items, ctx.ev, consts["dt"], consts["max_tris"], g, grad_in)
+        return (grad_in["x"], grad_in["q"], grad_in["v"], grad_in["w"], grad_in["ds_in"], grad_in["e"].sum(), None, None,
+                None, None)
+
+
+_PP_SAVED = ("contact_off", "mat_a", "mat_b", "xa", "xb", "va", "vb", "wa", "wb", "ds_in", "xc0", "normal", "area")
+
+
+class _PPForces(torch.autograd.Function):
+    """Per candidate pair: the summed force on B, the torques on A and B and the history after its contacts
+    (CUDA, zdx_pp_forces), and their reverse (zdx_pp_forces_adjoint)."""
+
+    @staticmethod
+    def forward(ctx, xa, xb, va, vb, wa, wb, ds_in, xc0, normal, area, k, e, contact_off, mat_a, mat_b, consts):
+        n = xa.shape[0]
+        dev = xa.device
+        pairs = {"contact_off": contact_off, "mat_a": mat_a, "mat_b": mat_b}
+        for name, t in (("xa", xa), ("xb", xb), ("va", va), ("vb", vb), ("wa", wa), ("wb", wb), ("ds_in", ds_in),
+                        ("xc0", xc0), ("normal", normal), ("area", area)):
+            pairs[name] = t.detach().contiguous()
+        out = {nm: torch.empty(n, 3, dtype=torch.float64, device=dev) for nm in ("fb", "ta", "tb", "ds")}
+        kv, ev = float(k), float(e)
+        torch.cuda.synchronize(dev)
+        _lib.pp_forces(consts["ctx"], pairs, consts["law"], kv, ev, consts["dt"], out)
+        ctx.save_for_backward(*(pairs[nm] for nm in _PP_SAVED))
+        ctx.consts, ctx.kv, ctx.ev = consts, kv, ev
+        ctx.k_is_tensor = torch.is_tensor(k)
+        return out["fb"], out["ta"], out["tb"], out["ds"]
+
+    @staticmethod
+    def backward(ctx, gfb, gta, gtb, gds):
+        consts = ctx.consts
+        pairs = dict(zip(_PP_SAVED, ctx.saved_tensors))
+        n = pairs["xa"].shape[0]
+        nc = pairs["area"].shape[0]
+        dev = pairs["xa"].device
+        z3 = lambda g: (g if g is not None else torch.zeros(n, 3, dtype=torch.float64, device=dev)).contiguous()
+        gout = {"fb": z3(gfb), "ta": z3(gta), "tb": z3(gtb), "ds": z3(gds)}
+        gin = {"pair": torch.zeros(n, 21, dtype=torch.float64, device=dev),
+               "k": torch.zeros(n, dtype=torch.float64, device=dev), "e": torch.zeros(n, dtype=torch.float64, device=dev),
+               "contact": torch.zeros(max(nc, 1), 7, dtype=torch.float64, device=dev)}
+        torch.cuda.synchronize(dev)
+        _lib.pp_forces_adjoint(consts["ctx"], pairs, consts["law"], ctx.kv, ctx.ev, consts["dt"], gout, gin)
+        g = gin["pair"]
+        gc = gin["contact"][:nc]
+        gk = gin["k"].sum() if ctx.k_is_tensor else None
+        return (g[:, 0:3], g[:, 3:6], g[:, 6:9], g[:, 9:12], g[:, 12:15], g[:, 15:18], g[:, 18:21], gc[:, 0:3],
+                gc[:, 3:6], gc[:, 6], gk, gin["e"].sum(), None, None, None, None)
+
+
 class DiffScene:
     """Constants of a loaded zdemx.dem.Scene on the GPU, and its differentiable step."""
 
@@ -116,6 +211,13 @@ class DiffScene:
         self.mesh_pad = T(pad).reshape(nm, -1, 3, 3)
         tolm = np.where(props[:, 5] > 0, props[:, 5] * 0.1, props[:, 6] * 1e-2)
         self.mesh_tol = T(np.where(tolm > 0, tolm, 1e-6))
+        # the wall kernels' constant arrays
+        self.mesh_off_t = T(off, torch.int64)
+        self.wall_off_t = T(self.woff, torch.int64)
+        self.wall_mu = self.wmat[:, 0].contiguous() if self.nw else T(np.zeros(1))
+        self.wtris_flat = self.wtris.reshape(-1, 9).contiguous()
+        self.wnorm_c = self.wnorm.contiguous()
+        self._wctx = None
 
     # ------------------------------------------------------------------------------------------------
     def initial_history(self):
@@ -155,58 +257,20 @@ class DiffScene:
             if nc > 0:
                 cpair = out["pair"]
                 coff = out["contact_off"]
-                rank = torch.arange(nc, device=dev) - coff[cpair]
                 key = (pi.to(torch.int64) << 32) | pj.to(torch.int64)
                 hpos = _lookup(hkey, key)
-                ds_pair = torch.where((hpos >= 0)[:, None], hds[hpos.clamp(min=0)] if hds.shape[0] else
-                                      torch.zeros(P, 3, dtype=torch.float64, device=dev),
-                                      torch.zeros(P, 3, dtype=torch.float64, device=dev))
-                ci, cj = pi[cpair], pj[cpair]
-                ma, mb = mat[ci], mat[cj]
-                f_all = torch.zeros(nc, 3, dtype=torch.float64, device=dev)
-                for rr in range(int(rank.max().item()) + 1):
-                    sel = torch.nonzero(rank == rr, as_tuple=True)[0]
-                    p_ = cpair[sel]
-                    a_, b_ = ci[sel], cj[sel]
-                    xc0, nA, A = out["xc0"][sel], out["nA"][sel], out["area"][sel]
-                    rA, rB = xc0 - x[a_], xc0 - x[b_]
-                    vA = v[a_] + _cross(w[a_], rA)
-                    vB = v[b_] + _cross(w[b_], rB)
-                    vrel = vB - vA
-                    vn = _dot(vrel, nA)
-                    R1 = ma[sel, 3].clamp(min=1e-12)
-                    R2 = mb[sel, 3].clamp(min=1e-12)
-                    E1 = ma[sel, 4].clamp(min=1e-12)
-                    E2 = mb[sel, 4].clamp(min=1e-12)
-                    nu1, nu2 = ma[sel, 5], mb[sel, 5]
-                    kt = (E1 / (2.0 * (1.0 + nu1) * R1) + E2 / (2.0 * (1.0 + nu2) * R2)) * A
-                    m_eff = 1.0 / (ma[sel, 1] + mb[sel, 1])
-                    ee = torch.clamp(e * torch.ones_like(A), 1e-6, 0.9999)
-                    loge = torch.log(ee)
-                    ct = torch.abs(2.0 * loge * torch.sqrt(kt * m_eff) / torch.sqrt(loge * loge + PI * PI))
-                    if self.law == 1:
-                        fn = 0.5 * k * A
-                    else:
-                        kn = (E1 / R1 + E2 / R2) * A
-                        fn = kn * torch.pow(torch.pow(A, 1.5), 1.0 / 3.0)
-                    fn = torch.clamp(fn, min=0.0)
-                    fnv = nA * fn[:, None]
-                    vt = vrel - nA * vn[:, None]
-                    ds = ds_pair[p_] + vt * self.dt
-                    ds = ds - nA * _dot(ds, nA)[:, None]
-                    ft = ds * (-kt)[:, None] + vt * (-ct)[:, None]
-                    mu = torch.minimum(ma[sel, 6], mb[sel, 6])
-                    ftn = torch.sqrt(_dot(ft, ft))
-                    ftmax = mu * fn
-                    cap = (ftn > ftmax) & (ftn > 1e-14)
-                    ft = torch.where(cap[:, None], ft * (ftmax / torch.where(cap, ftn, torch.ones_like(ftn)))[:, None], ft)
-                    ds = torch.where((cap & (kt > 1e-12))[:, None], ft * (-1.0 / torch.where(kt > 1e-12, kt, torch.ones_like(kt)))[:, None], ds)
-                    ds_pair = ds_pair.index_copy(0, p_, ds)
-                    f_all = f_all.index_copy(0, sel, fnv + ft)
-                rA_all = out["xc0"] - x[ci]
-                rB_all = out["xc0"] - x[cj]
-                F = F.index_add(0, ci, -f_all).index_add(0, cj, f_all)
-                Tq = Tq.index_add(0, ci, _cross(rA_all, -f_all)).index_add(0, cj, _cross(rB_all, f_all))
+                zero3 = torch.zeros(P, 3, dtype=torch.float64, device=dev)
+                ds_in = torch.where((hpos >= 0)[:, None], hds[hpos.clamp(min=0)] if hds.shape[0] else zero3, zero3)
+                if self._wctx is None:
+                    from .autograd import ctx_handle
+
+                    self._wctx = ctx_handle(dev)
+                consts = {"ctx": self._wctx, "law": self.law, "dt": self.dt}
+                fb, ta, tb, ds_pair = _PPForces.apply(x[pi], x[pj], v[pi], v[pj], w[pi], w[pj], ds_in, out["xc0"],
+                                                      out["nA"], out["area"], k, e, coff.contiguous(),
+                                                      mat[pi].contiguous(), mat[pj].contiguous(), consts)
+                F = F.index_add(0, pi, -fb).index_add(0, pj, fb)
+                Tq = Tq.index_add(0, pi, ta).index_add(0, pj, tb)
                 active = torch.bincount(cpair, minlength=P) > 0
                 new_hkey = key[active]
                 new_hds = ds_pair[active]
@@ -236,6 +300,48 @@ class DiffScene:
 
     # ------------------------------------------------------------------------------------------------
     def _walls(self, state, wkey, wds, e):
+        """Wall contacts of every particle near a wall, through the CUDA kernels (see _WallForces)."""
+        dev, N, mat = self.dev, self.np, self.mat
+        x, q, v, w = state[:, 0:3], state[:, 3:7], state[:, 7:10], state[:, 10:13]
+        r = mat[:, 2]
+        Fw = torch.zeros(N, 3, dtype=torch.float64, device=dev)
+        Tw = torch.zeros(N, 3, dtype=torch.float64, device=dev)
+        with torch.no_grad():
+            d = x.detach()[:, None, :] - self.wpose[None, :, 0:3]
+            dist2 = d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1] + d[..., 2] * d[..., 2]
+            rs = r[:, None] + self.wrad[None, :]
+            ci, cw = torch.nonzero(~(dist2 > rs * rs), as_tuple=True)
+        C = ci.numel()
+        if C == 0:
+            z = torch.zeros(0, dtype=torch.int64, device=dev)
+            return Fw, Tw, z, torch.zeros(0, 3, dtype=torch.float64, device=dev), 0
+        key = (ci.to(torch.int64) << 16) | cw.to(torch.int64)
+        hpos = _lookup(wkey, key)
+        zero3 = torch.zeros(C, 3, dtype=torch.float64, device=dev)
+        ds_c = torch.where((hpos >= 0)[:, None], wds[hpos.clamp(min=0)] if wds.shape[0] else zero3, zero3)
+        if self._wctx is None:
+            from .autograd import ctx_handle
+
+            self._wctx = ctx_handle(dev)
+        consts = {"ctx": self._wctx, "dt": self.dt, "max_tris": self.max_ntri,
+                  "items": {"mesh_tris": self.tris, "mesh_off": self.mesh_off_t, "mesh_tol": self.mesh_tol,
+                            "wall_tris": self.wtris_flat, "wall_normals": self.wnorm_c, "wall_off": self.wall_off_t,
+                            "wall_mu": self.wall_mu}}
+        f, t, ds_out, flags = _WallForces.apply(x[ci], q[ci], v[ci], w[ci], ds_c, e, mat[ci].contiguous(),
+                                                self.pmesh[ci].contiguous(), cw.to(torch.int32).contiguous(), consts)
+        with torch.no_grad():
+            fl = flags.to(torch.int64)
+            if bool(((fl >> 16) & 1).any()):
+                raise RuntimeError("a wall section exceeded 256 crossings")
+            touched = (fl & 1) != 0
+            nwc = int(((fl >> 1) & 0x7FFF).sum())
+        Fw = Fw.index_add(0, ci, f)
+        Tw = Tw.index_add(0, ci, t)
+        return Fw, Tw, key[touched], ds_out[touched], nwc
+
+    def _walls_torch(self, state, wkey, wds, e):
+        """The wall contacts in torch autograd (sections inside their wall triangle only); the kernels'
+        check."""
         dev, N, mat = self.dev, self.np, self.mat
         x, q, v, w = state[:, 0:3], state[:, 3:7], state[:, 7:10], state[:, 10:13]
         r = mat[:, 2]
