@@ -518,6 +518,9 @@ def main():
     extras["parity"] = parity_check(sel, rec, res["stats"], res["contact_off"], res["geom"])
     log(f"parity: {extras['parity']['pairs']} pairs, {extras['parity']['mismatches']} mismatches")
     extras.update(sweep_comparisons(args, ctx, dev, meshes, pairs, out, res, flush, step_ms))
+    extras["strong_shards"] = shard_balance(args, ctx, dev, meshes, pairs, flush, statistics.mean(step_ms))
+    log("strong shards: " + ", ".join(f"{k} {v['balance_mean_over_max']:.3f}" for k, v in extras["strong_shards"].items()
+                                      if isinstance(v, dict)))
     del d_tris
     log("comparisons done")
     extras["independent_meshes"] = sweep_independent(args, ctx, dev, flush)
@@ -645,6 +648,38 @@ def sweep_comparisons(args, ctx, dev, meshes, pairs, out, res, flush, step_ms):
                        "meshes": len(ids), "triangles": int(sub_off[-1]),
                        "note": "zdx_pair_contacts_noalloc: scratch in the library's fixed 16 MiB device array"}
     return out_
+
+
+def shard_balance(args, ctx, dev, meshes, pairs, flush, batch_ms):
+    """Strong-scaling shards of the sweep batch, run one after another on this GPU: per world size and
+    shard mode, every shard's device time as its own batch (no rank waits on another, so one GPU times
+    them all).  The slowest shard bounds a strong-scaling step; mean / max is that step's balance."""
+    import torch
+
+    from zdemx import _lib
+    from zdemx.replicas import strong_shards
+
+    tri_off = meshes["tri_off"].cpu().numpy()
+    pm = pairs["mesh"].cpu().numpy()
+    res = {}
+    for world in (2, 4, 8):
+        for mode in ("ranges", "dealt"):
+            shard_ms = []
+            for idx in strong_shards(tri_off, pm, world, mode=mode):
+                it = torch.from_numpy(idx).to(dev)
+                sub = {"mesh": pairs["mesh"][it].contiguous(), "pose": pairs["pose"][it].contiguous()}
+                so = _sweep_buffers(dev, len(idx), 16 * max(len(idx), 1))
+                call = lambda: _lib.pair_contacts_device(ctx, meshes, sub, so, k=1e7, split=True)
+                call()
+                _, ms, _, _ = _device_steps(ctx, call, flush, 2)
+                shard_ms.append(statistics.mean(ms))
+                del so
+            mx, mean = max(shard_ms), statistics.mean(shard_ms)
+            res[f"{mode}_x{world}"] = {"shard_ms": [round(x, 3) for x in shard_ms], "max_ms": mx,
+                                       "balance_mean_over_max": mean / mx, "speedup_bound": batch_ms / mx}
+    res["note"] = ("shards timed one after another on one GPU; speedup_bound = the whole batch's time over the "
+                   "slowest shard's (the all-gather not included)")
+    return res
 
 
 def sweep_independent(args, ctx, dev, flush):
@@ -777,7 +812,7 @@ def run_strong(args):
               "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
               "data": "synthetic (seeded noised icospheres, 1024-mesh library)",
               "config": {"workload": f"pair sweep: {args.pairs} pairs (one batch over {world} ranks), "
-                                     "cost-balanced shards of the cost-ordered pairs, one all-gather of the contacts",
+                                     "the cost-ordered pairs dealt to the ranks, one all-gather of the contacts",
                          "pairs_total": args.pairs, "shard_sizes": shard_sizes, "seed": args.seed,
                          "parallelism": f"pair shards x{world}", "l2": "flushed (256 MB write) before every timed step"},
               "gathered": {"contacts": contacts, "pairs": pairs_seen},

@@ -67,17 +67,45 @@ def test_cost_balanced_ranges(world):
     assert max(loads) - min(loads) <= 2 * costs.max() + 1
 
 
-@pytest.mark.parametrize("world", [1, 2, 4])
-def test_strong_shards_cover_every_pair_once(world):
+@pytest.mark.parametrize("mode", ["dealt", "ranges"])
+@pytest.mark.parametrize("world", [1, 2, 4, 7])
+def test_strong_shards_cover_every_pair_once(world, mode):
     from zdemx.replicas import pair_costs, strong_shards
 
     rng = np.random.default_rng(10 + world)
     tri_off = np.r_[0, np.cumsum(20 * 4 ** rng.integers(1, 5, size=64))]
     pm = rng.integers(0, 64, size=(3000, 2))
-    shards = strong_shards(tri_off, pm, world)
+    shards = strong_shards(tri_off, pm, world, mode=mode)
     assert len(shards) == world
     allp = np.sort(np.concatenate(shards))
     assert np.array_equal(allp, np.arange(len(pm)))
     costs = pair_costs(tri_off, pm)
+    for s in shards:  # each shard in the work queue's cost order
+        assert np.all(np.diff(costs[s]) <= 0)
     loads = [costs[s].sum() for s in shards]
     assert max(loads) - min(loads) <= 2 * costs.max() + 1
+    if mode == "dealt":
+        # the same mix of sizes on every rank: of each distinct cost, counts differ by at most 2
+        for v in np.unique(costs):
+            cnt = [int(np.sum(costs[s] == v)) for s in shards]
+            assert max(cnt) - min(cnt) <= 2
+        assert max(len(s) for s in shards) - min(len(s) for s in shards) <= 1
+
+
+def test_dealt_order_is_serpentine():
+    from zdemx.replicas import dealt
+
+    assert dealt(10, 3).tolist() == [0, 1, 2, 2, 1, 0, 0, 1, 2, 2]
+    assert dealt(4, 1).tolist() == [0, 0, 0, 0]
+
+
+def test_strong_shards_take_given_costs():
+    from zdemx.replicas import strong_shards
+
+    tri_off = np.array([0, 10, 20, 30])
+    pm = np.zeros((6, 2), np.int64)        # equal nA * nB everywhere
+    seg = np.array([5, 60, 1, 40, 9, 7])   # measured per-pair costs of an earlier call
+    shards = strong_shards(tri_off, pm, 2, costs=seg)
+    assert [s.tolist() for s in shards] == [[1, 5, 0], [3, 4, 2]]
+    with pytest.raises(ValueError):
+        strong_shards(tri_off, pm, 2, mode="other")

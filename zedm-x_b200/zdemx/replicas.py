@@ -1,8 +1,8 @@
 """Host logic of running the pair sweep on several GPUs, one process per GPU.
 
 Pairs are independent, so ranks never exchange data on the path: each rank either runs its own batch
-(weak scaling, what bench.py measures) or takes a contiguous range of one cost-ordered batch with an
-equal share of the triangle-test work (strong scaling).  The only collectives are host-side: the
+(weak scaling, what bench.py measures) or takes a share of one cost-ordered batch, dealt so that every
+rank holds the same mix of pair sizes (strong scaling).  The only collectives are host-side: the
 slowest rank's time, and one gather of the per-rank results.
 """
 from __future__ import annotations
@@ -66,12 +66,36 @@ def gather_counts(count: int, device=None) -> list[int]:
     return [int(x.item()) for x in out]
 
 
-def strong_shards(tri_off, pair_mesh, world: int) -> list[np.ndarray]:
-    """Pair indices of each rank for one batch spread over `world` ranks: the pairs in the work queue's
-    cost order (nA * nB, descending, ties by index), cut into contiguous ranges of equal cost."""
-    costs = pair_costs(tri_off, pair_mesh)
-    order = np.argsort(-costs, kind="stable")
-    return [order[a:b] for a, b in cost_balanced_ranges(costs[order], world)]
+def dealt(n: int, world: int) -> np.ndarray:
+    """Rank of each position 0..n-1 of a descending cost order, dealt serpentine-wise: 0, 1, .., W-1,
+    W-1, .., 0, 0, 1, ...  Every rank receives one pair of each run of W similar pairs, and the reversal
+    of every other run cancels the first-dealt rank's edge within a run."""
+    if world <= 1:
+        return np.zeros(n, np.int64)
+    i = np.arange(n, dtype=np.int64)
+    run, pos = i // world, i % world
+    return np.where(run % 2 == 0, pos, world - 1 - pos)
+
+
+def strong_shards(tri_off, pair_mesh, world: int, mode: str = "dealt", costs=None) -> list[np.ndarray]:
+    """Pair indices of each rank for one batch spread over `world` ranks, each rank's pairs in the work
+    queue's cost order (descending, ties by index).
+
+    mode "dealt": the cost-ordered pairs dealt to the ranks serpentine-wise, so that every rank holds the
+    same mix of pair sizes.  Its balance does not depend on how real time grows with the cost: the certificate
+    and culls leave about 1 % of nA * nB to test and the rebuild is linear in segments, so two ranges of
+    equal nA * nB can differ severalfold in time, while two dealt shards of the same mix cannot.  It also
+    keeps the largest pairs apart, one per rank, instead of leaving a few of them to one rank's SMs.
+    mode "ranges": contiguous ranges of equal total cost (the cost-balanced cut).
+    costs: per-pair costs to order by (for example a previous call's segment counts); nA * nB when None."""
+    c = pair_costs(tri_off, pair_mesh) if costs is None else np.asarray(costs, np.float64)
+    order = np.argsort(-c, kind="stable")
+    if mode == "ranges":
+        return [order[a:b] for a, b in cost_balanced_ranges(c[order], world)]
+    if mode != "dealt":
+        raise ValueError(f"unknown shard mode {mode!r}")
+    r = dealt(len(order), world)
+    return [order[r == k] for k in range(max(world, 1))]
 
 
 def gather_rows(t, device=None) -> list:
