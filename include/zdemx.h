@@ -324,6 +324,37 @@ int zdx_pp_forces_adjoint(zdx_ctx* ctx, const zdx_pp_pairs* pairs, const double*
                           const double* g_torque_b3, const double* g_ds_out3, double* g_pair21, double* g_k,
                           double* g_e, double* g_contact7);
 
+/* integrate_particle (src/main.cpp:1494-1510) for n particles and its reverse mode, for differentiable
+ * rollouts (no reference counterpart as a call).  state: n rows of 16 doubles (position, quaternion,
+ * velocity, angular velocity, angular momentum), mat: n rows of 17, force and torque: n x 3, all device
+ * memory; gravity and dt by value.  zdx_integrate writes the new state rows (the arithmetic of the device
+ * step); zdx_integrate_adjoint takes the cotangents of the new rows and writes those of the old rows (the
+ * angular-velocity columns 0: the step recomputes omega from L), of the force and of the torque.  Context
+ * stream; the calls return when done. */
+typedef struct zdx_integrate_args {
+    int64_t n;
+    const double* state;
+    const double* mat;
+    const double* force;
+    const double* torque;
+    double gravity[3];
+    double dt;
+} zdx_integrate_args;
+int zdx_integrate(zdx_ctx* ctx, const zdx_integrate_args* args, double* state_out);
+int zdx_integrate_adjoint(zdx_ctx* ctx, const zdx_integrate_args* args, const double* g_state_out, double* g_state,
+                          double* g_force, double* g_torque);
+
+/* The broad phase of the step loop (src/main.cpp:2049-2059: every pair i < j whose bounding spheres meet,
+ * dist^2 <= (r_i + r_j)^2) over caller arrays, for callers with their own step such as differentiable
+ * rollouts (the reference has it only inside its loop).  state: np rows of 16 doubles (position first),
+ * mat: np rows of 17 (column 2 the bounding radius), both device memory.  Writes the candidate pairs as
+ * (i, j) int32 pairs in the reference's order (i, then j increasing) to `pairs` (device, 8-byte aligned,
+ * room for cap pairs) and their number to *npair; more than cap returns ZDX_ERR_CAPACITY with *npair the
+ * number needed.  Binned on cells of twice the largest radius, so the work is O(np + pairs), not O(np^2).
+ * Runs on the context stream and returns when done. */
+int zdx_broad_phase(zdx_ctx* ctx, const double* state, const double* mat, int32_t np, int32_t* pairs, int64_t cap,
+                    int64_t* npair);
+
 /* ---- pair contacts without device allocation ------------------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate GPU memory (a host program whose
  * pool allocator owns the whole device, a real-time loop that cannot take the device-wide

@@ -53,6 +53,7 @@ struct zdx_ctx {
     zdx::DevBuf sp_items, sp_first, sp_chunk;  // split of large pairs (items, per-pair first item, runs)
     zdx::DevBuf w_scratch;                     // per-item tapes of the wall contacts (zdx_rollout.cu)
     zdx::DevBuf p_err;                         // error flag of the pair force kernels (zdx_rollout.cu)
+    zdx::DevBuf bp[11];                        // zdx_broad_phase's cells, sort, bounds, counts and radius
     zdx::DevBuf cstage, cistage, pstage;
     zdx::DevBuf g_off, o_cg, o_ci, o_pts, o_cpo, o_ps, o_comp;
     // adjoint tape (recorded when tape_on): segment provenance, per-contact records, final offsets
@@ -68,7 +69,7 @@ struct zdx_ctx {
                 &sp_first, &sp_chunk, &w_scratch, &p_err,
                 &cstage, &cistage, &pstage, &g_off, &o_cg, &o_ci, &o_pts, &o_cpo, &o_ps, &o_comp, &t_segtri, &t_segcand,
                 &t_arena, &t_cstage, &t_cfinal, &a_nc, &a_coff, &a_stats, &a_geom, &a_info, &a_pts, &a_cpo, &a_gc,
-                &a_gt, &a_gp};
+                &a_gt, &a_gp, &bp[0], &bp[1], &bp[2], &bp[3], &bp[4], &bp[5], &bp[6], &bp[7], &bp[8], &bp[9], &bp[10]};
     }
 
     zdx::Scene* scene = nullptr;

@@ -1,12 +1,14 @@
 // zdx_rollout.cu -- the force laws of a DEM step and their reverse modes, for differentiable rollouts:
 // zdx_wall_forces / zdx_wall_forces_adjoint, one thread per (particle, wall) item (zdx_wallad.cuh), and
-// zdx_pp_forces / zdx_pp_forces_adjoint, one thread per candidate pair and its contacts (zdx_ppad.cuh).
+// zdx_pp_forces / zdx_pp_forces_adjoint, one thread per candidate pair and its contacts (zdx_ppad.cuh), and
+// zdx_integrate / zdx_integrate_adjoint, one thread per particle (zdx_intad.cuh).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
 #include "../../include/zdemx.h"
 #include "zdx_ctx.h"
+#include "zdx_intad.cuh"
 #include "zdx_ppad.cuh"
 #include "zdx_wallad.cuh"
 
@@ -287,5 +289,85 @@ extern "C" int zdx_pp_forces_adjoint(zdx_ctx* ctx, const zdx_pp_pairs* a, const 
     CKW(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CKW(cudaStreamSynchronize(ctx->stream));
     if (herr) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "a pair has more than 64 contacts");
+    return ZDX_OK;
+}
+
+// ---------------------------------------------------------------- integration
+namespace {
+
+__device__ __forceinline__ intad::In make_in(const zdx_integrate_args& a, int64_t i) {
+    const double* s = a.state + 16 * i;
+    intad::In I;
+    I.x = V3{s[0], s[1], s[2]};
+    I.q = Q4{s[3], s[4], s[5], s[6]};
+    I.v = V3{s[7], s[8], s[9]};
+    I.L = V3{s[13], s[14], s[15]};
+    I.F = V3{a.force[3 * i], a.force[3 * i + 1], a.force[3 * i + 2]};
+    I.T = V3{a.torque[3 * i], a.torque[3 * i + 1], a.torque[3 * i + 2]};
+    I.m = a.mat + 17 * i;
+    I.g = V3{a.gravity[0], a.gravity[1], a.gravity[2]};
+    I.dt = a.dt;
+    return I;
+}
+
+__global__ void k_integrate_fwd(zdx_integrate_args a, double* out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    intad::fwd(make_in(a, i), out + 16 * i);
+}
+
+__global__ void k_integrate_bwd(zdx_integrate_args a, const double* g_out, double* g_state, double* g_force,
+                                double* g_torque) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const intad::Grad G = intad::bwd(make_in(a, i), g_out + 16 * i);
+    double* s = g_state + 16 * i;
+    const double row[16] = {G.x.x, G.x.y, G.x.z, G.q.w, G.q.x, G.q.y, G.q.z, G.v.x, G.v.y, G.v.z,
+                            0.0,   0.0,   0.0,   G.L.x, G.L.y, G.L.z};
+    for (int k = 0; k < 16; ++k) s[k] = row[k];
+    g_force[3 * i] = G.F.x;
+    g_force[3 * i + 1] = G.F.y;
+    g_force[3 * i + 2] = G.F.z;
+    g_torque[3 * i] = G.T.x;
+    g_torque[3 * i + 1] = G.T.y;
+    g_torque[3 * i + 2] = G.T.z;
+}
+
+int check_integrate(zdx_ctx* ctx, const zdx_integrate_args* a) {
+    if (!a || a->n < 0) return ctx_fail(ctx, ZDX_ERR_INVALID, "bad integration batch");
+    if (a->n > 0 && (!a->state || !a->mat || !a->force || !a->torque))
+        return ctx_fail(ctx, ZDX_ERR_INVALID, "integration batch has null arrays");
+    return ZDX_OK;
+}
+
+}  // namespace
+
+extern "C" int zdx_integrate(zdx_ctx* ctx, const zdx_integrate_args* a, double* state_out) {
+    if (!ctx) return ZDX_ERR_INVALID;
+    int rc = check_integrate(ctx, a);
+    if (rc) return rc;
+    if (a->n == 0) return ZDX_OK;
+    if (!state_out) return ctx_fail(ctx, ZDX_ERR_INVALID, "null output");
+    CKW(cudaSetDevice(ctx->device));
+    k_integrate_fwd<<<(unsigned)((a->n + 127) / 128), 128, 0, ctx->stream>>>(*a, state_out);
+    ctx->launches += 1;
+    CKW(cudaGetLastError());
+    CKW(cudaStreamSynchronize(ctx->stream));
+    return ZDX_OK;
+}
+
+extern "C" int zdx_integrate_adjoint(zdx_ctx* ctx, const zdx_integrate_args* a, const double* g_state_out,
+                                     double* g_state, double* g_force, double* g_torque) {
+    if (!ctx) return ZDX_ERR_INVALID;
+    int rc = check_integrate(ctx, a);
+    if (rc) return rc;
+    if (a->n == 0) return ZDX_OK;
+    if (!g_state_out || !g_state || !g_force || !g_torque) return ctx_fail(ctx, ZDX_ERR_INVALID, "null gradient array");
+    CKW(cudaSetDevice(ctx->device));
+    k_integrate_bwd<<<(unsigned)((a->n + 127) / 128), 128, 0, ctx->stream>>>(*a, g_state_out, g_state, g_force,
+                                                                            g_torque);
+    ctx->launches += 1;
+    CKW(cudaGetLastError());
+    CKW(cudaStreamSynchronize(ctx->stream));
     return ZDX_OK;
 }

@@ -1850,4 +1850,85 @@ int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps) {
     return ZDX_OK;
 }
 
+namespace {
+// The largest bounding radius (material column 2) of np particles, into *out; one block.
+__global__ void k_rmax(const double* mat, int np, double* out) {
+    __shared__ double red[256];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) m = fmax(m, mat[17 * (int64_t)i + 2]);
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+}  // namespace
+
+// The broad phase of the step alone (zdx_broad_phase): the same cells, sort, sphere test and (i, j) order
+// as scene_step's, over caller arrays, with the context's own buffers.
+int broad_phase(zdx_ctx* ctx, const double* state, const double* mat, int np, int2* pairs, int64_t cap,
+                int64_t* npair) {
+    cudaStream_t st = ctx->stream;
+    DevBuf* b = ctx->bp;  // cell, key, idx, key2, idx2, start, end, cnt, off, tmp, rmax
+    const size_t N1 = (size_t)std::max(np, 1);
+    CKS(b[10].ensure(sizeof(double)));
+    k_rmax<<<1, 256, 0, st>>>(mat, np, as<double>(b[10]));
+    double rmax = 0.0;
+    CKS(cudaMemcpyAsync(&rmax, b[10].p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CKS(cudaStreamSynchronize(st));
+    double h = 2.0 * rmax * (1.0 + 1e-9);
+    if (!(h > 0.0)) h = 1.0;
+    uint32_t T = 1;
+    while (T < (uint32_t)std::max(2 * np, 2)) T <<= 1;
+    int bits = 0;
+    while ((1u << bits) < T) bits++;
+    CKS(b[0].ensure(sizeof(int4) * N1));
+    CKS(b[1].ensure(sizeof(uint32_t) * N1));
+    CKS(b[2].ensure(sizeof(int32_t) * N1));
+    CKS(b[3].ensure(sizeof(uint32_t) * N1));
+    CKS(b[4].ensure(sizeof(int32_t) * N1));
+    CKS(b[5].ensure(sizeof(int) * T));
+    CKS(b[6].ensure(sizeof(int) * T));
+    CKS(b[7].ensure(sizeof(int32_t) * N1));
+    CKS(b[8].ensure(sizeof(int64_t) * (N1 + 1)));
+    CKS(b[9].ensure(radix_scratch_bytes(std::max<int64_t>(np, 1))));
+    k_bp_cells<<<grid(np), 256, 0, st>>>(state, np, 1.0 / h, T - 1, as<int4>(b[0]), as<uint32_t>(b[1]), as<int32_t>(b[2]));
+    CKS(radix_sort_u32(as<uint32_t>(b[1]), as<int32_t>(b[2]), as<uint32_t>(b[3]), as<int32_t>(b[4]), np, bits, b[9].p, st));
+    CKS(cudaMemsetAsync(b[5].p, 0, sizeof(int) * T, st));
+    CKS(cudaMemsetAsync(b[6].p, 0, sizeof(int) * T, st));
+    k_bp_bounds<<<grid(np), 256, 0, st>>>(as<uint32_t>(b[1]), np, as<int>(b[5]), as<int>(b[6]));
+    k_bp_pairs<false><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(b[0]), as<int32_t>(b[2]), as<int>(b[5]),
+                                                     as<int>(b[6]), T - 1, as<int32_t>(b[7]), nullptr, nullptr, INT64_MAX);
+    CKS(scan_counts_i32(as<int32_t>(b[7]), np, as<int64_t>(b[8]), st));
+    int64_t total = 0;
+    CKS(cudaMemcpyAsync(&total, as<int64_t>(b[8]) + np, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CKS(cudaStreamSynchronize(st));
+    ctx->launches += 6 + radix_kernels(np, bits);
+    *npair = total;
+    if (total > cap) return ctx_fail(ctx, ZDX_ERR_CAPACITY, "%lld candidate pairs, capacity %lld", (long long)total,
+                                     (long long)cap);
+    if (total > 0) {
+        k_bp_pairs<true><<<grid(np, 128), 128, 0, st>>>(state, mat, np, as<int4>(b[0]), as<int32_t>(b[2]), as<int>(b[5]),
+                                                        as<int>(b[6]), T - 1, nullptr, as<int64_t>(b[8]), pairs, cap);
+        ctx->launches += 1;
+        CKS(cudaGetLastError());
+        CKS(cudaStreamSynchronize(st));
+    }
+    return ZDX_OK;
+}
+
 }  // namespace zdx
+
+extern "C" int zdx_broad_phase(zdx_ctx* ctx, const double* state, const double* mat, int32_t np, int32_t* pairs,
+                               int64_t cap, int64_t* npair) {
+    if (!ctx || !npair || np < 0 || cap < 0) return ctx ? zdx::ctx_fail(ctx, ZDX_ERR_INVALID, "bad argument") : ZDX_ERR_INVALID;
+    *npair = 0;
+    if (np == 0) return ZDX_OK;
+    if (!state || !mat || (cap > 0 && !pairs)) return zdx::ctx_fail(ctx, ZDX_ERR_INVALID, "null array");
+    if (reinterpret_cast<uintptr_t>(pairs) % 8) return zdx::ctx_fail(ctx, ZDX_ERR_INVALID, "pairs not 8-byte aligned");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return zdx::ctx_fail(ctx, ZDX_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    return zdx::broad_phase(ctx, state, mat, np, reinterpret_cast<int2*>(pairs), cap, npair);
+}

@@ -77,6 +77,11 @@ class PPPairs(C.Structure):
                 ("area", C.c_void_p), ("law", C.c_int32), ("k", C.c_double), ("e", C.c_double), ("dt", C.c_double)]
 
 
+class IntegrateArgs(C.Structure):
+    _fields_ = [("n", C.c_int64), ("state", C.c_void_p), ("mat", C.c_void_p), ("force", C.c_void_p),
+                ("torque", C.c_void_p), ("gravity", C.c_double * 3), ("dt", C.c_double)]
+
+
 class ZdxError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"zdemx status {status}: {msg}")
@@ -133,6 +138,9 @@ def lib() -> C.CDLL:
     L.zdx_pp_forces_adjoint.argtypes = [C.c_void_p, C.POINTER(PPPairs)] + [C.c_void_p] * 8
     L.zdx_wall_forces_adjoint.argtypes = [C.c_void_p, C.POINTER(WallItems)] + [C.c_void_p] * 9
     L.zdx_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+    L.zdx_integrate.argtypes = [C.c_void_p, C.POINTER(IntegrateArgs), C.c_void_p]
+    L.zdx_integrate_adjoint.argtypes = [C.c_void_p, C.POINTER(IntegrateArgs)] + [C.c_void_p] * 4
+    L.zdx_broad_phase.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, _i64p]
     _lib = L
     return L
 
@@ -370,6 +378,45 @@ def _pp_pairs(pairs: dict, law: int, k: float, e: float, dt: float) -> PPPairs:
                    _ptr(pairs["va"]), _ptr(pairs["vb"]), _ptr(pairs["wa"]), _ptr(pairs["wb"]), _ptr(pairs["mat_a"]),
                    _ptr(pairs["mat_b"]), _ptr(pairs["ds_in"]), _ptr(pairs["xc0"]), _ptr(pairs["normal"]),
                    _ptr(pairs["area"]), int(law), float(k), float(e), float(dt))
+
+
+def _integrate_args(state, mat, force, torque, gravity, dt):
+    return IntegrateArgs(int(state.shape[0]), _ptr(state), _ptr(mat), _ptr(force), _ptr(torque),
+                         (C.c_double * 3)(*[float(g) for g in gravity]), float(dt))
+
+
+def integrate(ctx: Context, state, mat, force, torque, gravity, dt, out) -> None:
+    """zdx_integrate on contiguous CUDA float64 tensors: out (n, 16) receives the new state rows."""
+    a = _integrate_args(state, mat, force, torque, gravity, dt)
+    check(lib().zdx_integrate(ctx.handle, C.byref(a), _ptr(out)), ctx.handle)
+
+
+def integrate_adjoint(ctx: Context, state, mat, force, torque, gravity, dt, g_out, g_state, g_force, g_torque) -> None:
+    """zdx_integrate_adjoint: g_out (n, 16) in; g_state (n, 16), g_force and g_torque (n, 3) written."""
+    a = _integrate_args(state, mat, force, torque, gravity, dt)
+    check(lib().zdx_integrate_adjoint(ctx.handle, C.byref(a), _ptr(g_out), _ptr(g_state), _ptr(g_force),
+                                      _ptr(g_torque)), ctx.handle)
+
+
+def broad_phase(ctx: Context, state, mat, pairs=None):
+    """zdx_broad_phase on CUDA tensors: state (np, 16) and mat (np, 17) float64.  Returns (candidates,
+    buffer): an (n, 2) int32 tensor of the candidate pairs (i < j, in i then j order), a view of the
+    buffer, which is `pairs` (an (m, 2) int32 tensor) or, when that is missing or too small, a new one
+    to pass next time."""
+    import torch
+
+    np_ = int(state.shape[0])
+    dev = state.device
+    if pairs is None:
+        pairs = torch.empty(max(8 * np_, 64), 2, dtype=torch.int32, device=dev)
+    n = C.c_int64(0)
+    st, mt = state.contiguous(), mat.contiguous()
+    rc = lib().zdx_broad_phase(ctx.handle, _ptr(st), _ptr(mt), np_, _ptr(pairs), int(pairs.shape[0]), C.byref(n))
+    if rc == ZDX_ERR_CAPACITY:
+        pairs = torch.empty(int(n.value) + 64, 2, dtype=torch.int32, device=dev)
+        rc = lib().zdx_broad_phase(ctx.handle, _ptr(st), _ptr(mt), np_, _ptr(pairs), int(pairs.shape[0]), C.byref(n))
+    check(rc, ctx.handle)
+    return pairs[: int(n.value)], pairs
 
 
 def pp_forces(ctx: Context, pairs: dict, law: int, k: float, e: float, dt: float, out: dict) -> None:

@@ -125,6 +125,30 @@ class _WallForces(torch.autograd.Function):
                 None, None)
 
 
+class _Integrate(torch.autograd.Function):
+    """integrate_particle for every particle through zdx_integrate; backward through zdx_integrate_adjoint
+    (the cotangents of the old state, of the forces and of the torques)."""
+
+    @staticmethod
+    def forward(ctx, state, F, T, consts):
+        st, f, t = state.detach().contiguous(), F.detach().contiguous(), T.detach().contiguous()
+        out = torch.empty_like(st)
+        torch.cuda.synchronize(st.device)
+        _lib.integrate(consts["ctx"], st, consts["mat"], f, t, consts["g"], consts["dt"], out)
+        ctx.save_for_backward(st, f, t)
+        ctx.consts = consts
+        return out
+
+    @staticmethod
+    def backward(ctx, g_out):
+        st, f, t = ctx.saved_tensors
+        c = ctx.consts
+        g_st, g_f, g_t = torch.empty_like(st), torch.empty_like(f), torch.empty_like(t)
+        torch.cuda.synchronize(st.device)
+        _lib.integrate_adjoint(c["ctx"], st, c["mat"], f, t, c["g"], c["dt"], g_out.contiguous(), g_st, g_f, g_t)
+        return g_st, g_f, g_t, None
+
+
 _PP_SAVED = ("contact_off", "mat_a", "mat_b", "xa", "xb", "va", "vb", "wa", "wb", "ds_in", "xc0", "normal", "area")
 
 
@@ -195,6 +219,7 @@ class DiffScene:
         prm = scene.array("params")
         self.dt = float(prm[0])
         self.g = T(prm[1:4])
+        self.g_host = [float(a) for a in prm[1:4]]
         self.split = bool(prm[4] != 0)
         self.law = int(prm[5])
         self.feng_k = float(prm[6])
@@ -218,6 +243,7 @@ class DiffScene:
         self.wtris_flat = self.wtris.reshape(-1, 9).contiguous()
         self.wnorm_c = self.wnorm.contiguous()
         self._wctx = None
+        self._bp_buf = None
 
     # ------------------------------------------------------------------------------------------------
     def initial_history(self):
@@ -229,20 +255,19 @@ class DiffScene:
         """One step; returns (state, hkey, hds, wkey, wds, stats)."""
         dev, N = self.dev, self.np
         mat = self.mat
-        x, q, v, w, L = state[:, 0:3], state[:, 3:7], state[:, 7:10], state[:, 10:13], state[:, 13:16]
-        r = mat[:, 2]
+        x, v, w = state[:, 0:3], state[:, 7:10], state[:, 10:13]
         F = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         Tq = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         stats = {}
-        # ---- broad phase (no gradient: decides topology only)
+        # ---- broad phase (no gradient: decides topology only), binned on the GPU
         with torch.no_grad():
-            xd = x.detach()
-            d = xd[None, :, :] - xd[:, None, :]
-            dist2 = d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1] + d[..., 2] * d[..., 2]
-            rs = r[:, None] + r[None, :]
-            ok = ~(dist2 > rs * rs)
-            ok = torch.triu(ok, diagonal=1)
-            pi, pj = torch.nonzero(ok, as_tuple=True)
+            if self._wctx is None:
+                from .autograd import ctx_handle
+
+                self._wctx = ctx_handle(dev)
+            torch.cuda.synchronize(dev)
+            cand, self._bp_buf = _lib.broad_phase(self._wctx, state.detach(), mat, self._bp_buf)
+            pi, pj = cand[:, 0].long(), cand[:, 1].long()
         P = pi.numel()
         stats["pairs"] = P
         new_hkey = torch.zeros(0, dtype=torch.int64, device=dev)
@@ -283,7 +308,14 @@ class DiffScene:
             F = F + Fw
             Tq = Tq + Tw
         stats["wall_contacts"] = nwc
-        # ---- integrate_particle (src/main.cpp:1494-1510)
+        # ---- integrate_particle (src/main.cpp:1494-1510), in CUDA with its reverse mode
+        new_state = _Integrate.apply(state, F, Tq, {"ctx": self._wctx, "mat": mat, "g": self.g_host, "dt": self.dt})
+        return new_state, new_hkey, new_hds, new_wkey, new_wds, stats
+
+    def integrate_torch(self, state, F, Tq):
+        """integrate_particle in torch autograd (the kernels' check)."""
+        N, dev, mat = self.np, self.dev, self.mat
+        x, q, v, L = state[:, 0:3], state[:, 3:7], state[:, 7:10], state[:, 13:16]
         acc = F * mat[:, 1:2] + self.g
         vel = v + acc * self.dt
         pos = x + vel * self.dt
@@ -295,8 +327,17 @@ class DiffScene:
         om = (Iinv @ Ln[:, :, None])[:, :, 0]
         qd = _qmul(torch.cat([torch.zeros(N, 1, dtype=q.dtype, device=dev), om], 1), q)
         qq = _qnormalize(q + 0.5 * qd * self.dt)
-        new_state = torch.cat([pos, qq, vel, om, Ln], 1)
-        return new_state, new_hkey, new_hds, new_wkey, new_wds, stats
+        return torch.cat([pos, qq, vel, om, Ln], 1)
+
+    def broad_phase_torch(self, x):
+        """The candidate pairs by the O(np^2) all-pairs sphere test in torch (the binned kernel's check)."""
+        with torch.no_grad():
+            r = self.mat[:, 2]
+            d = x[None, :, :] - x[:, None, :]
+            dist2 = d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1] + d[..., 2] * d[..., 2]
+            rs = r[:, None] + r[None, :]
+            ok = torch.triu(~(dist2 > rs * rs), diagonal=1)
+            return torch.nonzero(ok, as_tuple=True)
 
     # ------------------------------------------------------------------------------------------------
     def _walls(self, state, wkey, wds, e):
