@@ -174,6 +174,19 @@ typedef struct zdx_tuning {
                                    of nA x nB triangle tests into ceil(nA nB / split_tests) work items
                                    (at most 64, at most nA) over ranges of A's triangles; 0: never
                                    (default).  zdx_pair_contacts only                                 */
+    int32_t rebuild_arena;      /* rebuild form of zdx_pair_contacts in zdem mode (without adjoint tape,
+                                   loop points or component stats), same results in every form: 0
+                                   (default) one warp per pair with its arrays in a global-memory slot;
+                                   1 pairs of at least arena_min_seg segments in arenas (one warp per
+                                   pair: the neighbour relation from a sorted sweep, a lock-free
+                                   union-find for the snap), on a second stream at the same time as
+                                   form 0 on the smaller pairs; 2 every pair in an arena (fastest when
+                                   most pairs have hundreds of segments); 3 an arena too small for any
+                                   pair, so that every pair with segments falls back to form 0 (a test
+                                   of that path)                                                     */
+    int32_t arena_warps;        /* warps per SM given arenas, 1..32 (default 8)                      */
+    int32_t arena_min_seg;      /* form 1: pairs of fewer segments take form 0 (default 192)        */
+    int32_t arena_pad;          /* reserved, 0                                                        */
 } zdx_tuning;
 int zdx_set_tuning(zdx_ctx* ctx, const zdx_tuning* t);  /* ZDX_ERR_INVALID for values out of range */
 int zdx_get_tuning(const zdx_ctx* ctx, zdx_tuning* t);

@@ -22,7 +22,8 @@ def test_tuning_file_and_range_checks(tmp_path):
     p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
     assert p.returncode == 0, p.stderr[-2000:]
     got = json.loads(p.stdout.strip().splitlines()[-1])
-    assert got == {"tri_ctas_per_sm": 1, "rebuild_warps": 2, "flat_max": 2048, "split_tests": 0}
+    assert got == {"tri_ctas_per_sm": 1, "rebuild_warps": 2, "flat_max": 2048, "split_tests": 0,
+                   "rebuild_arena": 0, "arena_warps": 8, "arena_min_seg": 192}
     # a value out of range leaves the defaults
     path.write_text(json.dumps({"flat_max": 2048, "rebuild_warps": 99}))
     p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
@@ -36,6 +37,10 @@ def test_tuning_file_and_range_checks(tmp_path):
             ctx.set_tuning(tri_ctas_per_sm=3)
         with pytest.raises(_lib.ZdxError):
             ctx.set_tuning(rebuild_warps=0)
+        with pytest.raises(_lib.ZdxError):
+            ctx.set_tuning(rebuild_arena=4)
+        with pytest.raises(_lib.ZdxError):
+            ctx.set_tuning(arena_warps=0)
         assert ctx.set_tuning(flat_max=0)["flat_max"] == 0
     finally:
         ctx.close()
@@ -56,15 +61,16 @@ def test_results_do_not_depend_on_launch_parameters():
             ref = {k: v.clone() for k, v in out.items()}
             n = int(tot[0])
             assert n > 0
-            for knob, values in autotune.GRID.items():
-                for v in values:
-                    ctx.set_tuning(**dict(autotune.DEFAULTS, **{knob: v}))
-                    t2 = _lib.pair_contacts_device(ctx, meshes, pairs, out, k=1e7, split=split)
-                    assert t2[:3] == tot[:3], (knob, v)
-                    for key in ("ncontact", "contact_off", "stats"):
-                        assert torch.equal(out[key], ref[key]), (knob, v, key)
-                    assert torch.equal(out["geom"][:n], ref["geom"][:n]), (knob, v)
-                    assert torch.equal(out["info"][:n], ref["info"][:n]), (knob, v)
+            # every knob value, and the arena form's test of its fallback path (rebuild_arena 3)
+            cases = [(knob, v) for knob, values in autotune.GRID.items() for v in values] + [("rebuild_arena", 3)]
+            for knob, v in cases:
+                ctx.set_tuning(**dict(autotune.DEFAULTS, **{knob: v}))
+                t2 = _lib.pair_contacts_device(ctx, meshes, pairs, out, k=1e7, split=split)
+                assert t2[:3] == tot[:3], (knob, v)
+                for key in ("ncontact", "contact_off", "stats"):
+                    assert torch.equal(out[key], ref[key]), (knob, v, key)
+                assert torch.equal(out["geom"][:n], ref["geom"][:n]), (knob, v)
+                assert torch.equal(out["info"][:n], ref["info"][:n]), (knob, v)
     finally:
         ctx.close()
 

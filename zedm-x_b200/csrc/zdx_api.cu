@@ -117,6 +117,10 @@ extern "C" int zdx_destroy(zdx_ctx* ctx) {
     ctx->scene_release();
     for (auto& e : ctx->ev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
+    if (ctx->stream2) {
+        for (auto& e : ctx->ev2) cudaEventDestroy(e);
+        cudaStreamDestroy(ctx->stream2);
+    }
     delete ctx;
     return ZDX_OK;
 }
@@ -134,6 +138,81 @@ int tuning_check(const zdx_tuning* t) {
     if (t->tri_ctas_per_sm < 1 || t->tri_ctas_per_sm > 2) return ZDX_ERR_INVALID;
     if (t->rebuild_warps < 1 || t->rebuild_warps > K2_MAX_WARPS) return ZDX_ERR_INVALID;
     if (t->flat_max < 0 || t->split_tests < 0) return ZDX_ERR_INVALID;
+    if (t->rebuild_arena < 0 || t->rebuild_arena > 3 || t->arena_warps < 1 || t->arena_warps > 32) return ZDX_ERR_INVALID;
+    if (t->arena_min_seg < 0 || t->arena_pad != 0) return ZDX_ERR_INVALID;
+    return ZDX_OK;
+}
+
+// The arena form of the rebuild (zdx_rebuild.cu).  Pairs of at least arena_min_seg segments run in
+// global-memory arenas on a second stream while the warp-per-pair kernel takes the smaller ones on the
+// context stream (the two are latency-bound and share the SMs); then the warp-per-pair kernel runs the
+// pairs that outgrew their arena.  Form 2 puts every pair in an arena; form 3 gives every arena 256
+// bytes, so that each pair with segments takes the fallback.
+int rebuild_by_arenas(zdx_ctx* ctx, PairArgs a, int64_t NP, int nmax, size_t budget, cudaStream_t st) {
+    ArenaPlan plan{};
+    const int64_t stride = std::max<int64_t>(NP, 1);
+    CK(ctx->ar_lists.ensure(sizeof(int32_t) * 3 * (size_t)stride));
+    CK(ctx->ar_counts.ensure(sizeof(int64_t) * 8));
+    plan.lists = static_cast<int32_t*>(ctx->ar_lists.p);
+    plan.counts = static_cast<int64_t*>(ctx->ar_counts.p);
+    plan.list_stride = stride;
+    const int mode = ctx->tune.rebuild_arena;
+    plan.min_seg = mode == 1 ? ctx->tune.arena_min_seg : 0;
+    // an arena per warp, sized for the call's largest pair (about 500 B a segment is ample)
+    plan.arena_bytes = mode == 3 ? 256
+                                 : (int)std::min<int64_t>(((int64_t)nmax * 500 + 32768 + 255) & ~int64_t(255), 64 << 20);
+    int64_t slots = (int64_t)ctx->num_sms * ctx->tune.arena_warps;
+    slots = std::min<int64_t>(slots, std::max<int64_t>(4, (int64_t)(((size_t)2 << 30) / (size_t)plan.arena_bytes)));
+    slots = std::max<int64_t>(4, slots / 4 * 4);
+    CK(ctx->ar_gslots.ensure((size_t)plan.arena_bytes * (size_t)slots));
+    plan.gslots = static_cast<char*>(ctx->ar_gslots.p);
+    plan.grid = (int)(slots / 4);
+    if (!ctx->stream2) {
+        CK(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+        for (auto& e : ctx->ev2) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    // meanwhile the small pairs on the warp-per-pair kernel, with slots sized for them; afterwards the
+    // pairs no arena held, with slots for the call's largest pair (one buffer, sized before either runs)
+    struct WarpLaunch {
+        PairArgs w;
+        int64_t warps;
+    } wl[2];
+    size_t slot_need = 0;
+    const int32_t* wlist[2] = {plan.lists + 2 * stride, plan.lists + stride};
+    const int64_t* wcount[2] = {plan.counts + 2, plan.counts + 1};
+    int* wqueue[2] = {a.queue2, reinterpret_cast<int*>(plan.counts + 5)};
+    const int wbig[2] = {plan.min_seg > 0 ? std::min(nmax, plan.min_seg - 1) : 1, nmax};
+    for (int k = 0; k < 2; ++k) {
+        PairArgs& w = wl[k].w;
+        w = a;
+        w.order = wlist[k];
+        w.n_dev = wcount[k];
+        w.item_begin = 0;
+        w.item_end = NP;
+        w.queue2 = wqueue[k];
+        w.k2_nmax = std::max(1, wbig[k]);
+        w.k2_slot_bytes = rebuild_slot_bytes(w.k2_nmax);
+        int64_t warps = std::min<int64_t>(std::max<int64_t>(NP, 1), (int64_t)ctx->num_sms * 32);
+        warps = std::min<int64_t>(warps, std::max<int64_t>(1, (int64_t)(budget / w.k2_slot_bytes)));
+        warps = (warps + ctx->tune.rebuild_warps - 1) / ctx->tune.rebuild_warps * ctx->tune.rebuild_warps;
+        w.k2_nslots = warps;
+        wl[k].warps = warps;
+        slot_need = std::max(slot_need, w.k2_slot_bytes * (size_t)warps);
+    }
+    CK(ctx->k2_slots.ensure(slot_need));
+    launch_rebuild_classes(a, plan, st);
+    CK(cudaEventRecord(ctx->ev2[0], st));
+    CK(cudaStreamWaitEvent(ctx->stream2, ctx->ev2[0], 0));
+    launch_rebuild_arena(a, plan, ctx->stream2);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev2[1], ctx->stream2));
+    for (int k = 0; k < 2; ++k) {
+        wl[k].w.k2_slots = static_cast<char*>(ctx->k2_slots.p);
+        if (k == 1) CK(cudaStreamWaitEvent(st, ctx->ev2[1], 0));
+        launch_rebuild(wl[k].w, (int)wl[k].warps, ctx->tune.rebuild_warps, st);
+    }
+    ctx->launches += 4;
+    CK(cudaGetLastError());
     return ZDX_OK;
 }
 
@@ -147,13 +226,16 @@ void tuning_from_file(zdx_ctx* ctx, const char* path) {
     size_t got;
     while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0 && text.size() < (1u << 20)) text.append(buf, got);
     std::fclose(f);
-    zdx_tuning t{ctx->tune.tri_ctas_per_sm, ctx->tune.rebuild_warps, ctx->tune.flat_max, ctx->tune.split_tests};
+    zdx_tuning t{ctx->tune.tri_ctas_per_sm, ctx->tune.rebuild_warps, ctx->tune.flat_max, ctx->tune.split_tests,
+                 ctx->tune.rebuild_arena, ctx->tune.arena_warps, ctx->tune.arena_min_seg, 0};
     struct Key {
         const char* name;
         int64_t* v64;
         int32_t* v32;
     } keys[] = {{"tri_ctas_per_sm", nullptr, &t.tri_ctas_per_sm}, {"rebuild_warps", nullptr, &t.rebuild_warps},
-                {"flat_max", &t.flat_max, nullptr}, {"split_tests", &t.split_tests, nullptr}};
+                {"flat_max", &t.flat_max, nullptr}, {"split_tests", &t.split_tests, nullptr},
+                {"rebuild_arena", nullptr, &t.rebuild_arena}, {"arena_warps", nullptr, &t.arena_warps},
+                {"arena_min_seg", nullptr, &t.arena_min_seg}};
     for (const Key& k : keys) {
         const std::string quoted = std::string("\"") + k.name + "\"";
         const size_t at = text.find(quoted);
@@ -171,6 +253,9 @@ void tuning_from_file(zdx_ctx* ctx, const char* path) {
     ctx->tune.rebuild_warps = t.rebuild_warps;
     ctx->tune.flat_max = t.flat_max;
     ctx->tune.split_tests = t.split_tests;
+    ctx->tune.rebuild_arena = t.rebuild_arena;
+    ctx->tune.arena_warps = t.arena_warps;
+    ctx->tune.arena_min_seg = t.arena_min_seg;
 }
 
 }  // namespace
@@ -182,6 +267,9 @@ extern "C" int zdx_set_tuning(zdx_ctx* ctx, const zdx_tuning* t) {
     ctx->tune.rebuild_warps = t->rebuild_warps;
     ctx->tune.flat_max = t->flat_max;
     ctx->tune.split_tests = t->split_tests;
+    ctx->tune.rebuild_arena = t->rebuild_arena;
+    ctx->tune.arena_warps = t->arena_warps;
+    ctx->tune.arena_min_seg = t->arena_min_seg;
     return ZDX_OK;
 }
 
@@ -191,6 +279,10 @@ extern "C" int zdx_get_tuning(const zdx_ctx* ctx, zdx_tuning* t) {
     t->rebuild_warps = ctx->tune.rebuild_warps;
     t->flat_max = ctx->tune.flat_max;
     t->split_tests = ctx->tune.split_tests;
+    t->rebuild_arena = ctx->tune.rebuild_arena;
+    t->arena_warps = ctx->tune.arena_warps;
+    t->arena_min_seg = ctx->tune.arena_min_seg;
+    t->arena_pad = 0;
     return ZDX_OK;
 }
 
@@ -525,9 +617,16 @@ extern "C" int zdx_pair_contacts(zdx_ctx* ctx, const zdx_pair_opts* opts, const 
         a.k2_nslots = warps;
         CK(ctx->k2_slots.ensure(a.k2_slot_bytes * (size_t)warps));
         a.k2_slots = as<char>(ctx->k2_slots);
+        const bool arena = ctx->tune.rebuild_arena != 0 && a.mode == 0 && !a.tape_stage && !a.want_pts &&
+                           !a.comp_stats && !a.per_stage;
         CK(cudaEventRecord(ctx->ev[2], st));
-        launch_rebuild(a, (int)warps, ctx->tune.rebuild_warps, st);
-        ctx->launches += 1;
+        if (arena) {
+            int st_code = rebuild_by_arenas(ctx, a, NP, nmax, budget, st);
+            if (st_code != ZDX_OK) return st_code;
+        } else {
+            launch_rebuild(a, (int)warps, ctx->tune.rebuild_warps, st);
+            ctx->launches += 1;
+        }
         CK(cudaGetLastError());
         CK(cudaEventRecord(ctx->ev[3], st));
         CK(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));

@@ -30,6 +30,9 @@ struct Tuning {
     int rebuild_warps = 4;       // warps per rebuild block
     int64_t split_tests = 0;     // split a pair's triangle stage into chunks of about this many survivor
                                  // tests when the batch has fewer pairs than CTAs (0: never)
+    int rebuild_arena = 0;       // rebuild form (zdx_tuning.rebuild_arena)
+    int arena_warps = 8;         // warps per SM of the arena kernel (one arena each)
+    int arena_min_seg = 192;     // smaller pairs stay on the warp-per-pair kernel
 };
 
 }  // namespace zdx
@@ -39,6 +42,8 @@ struct zdx_ctx {
     int num_sms = 148;
     int cc_major = 0, cc_minor = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;  // the arena rebuild's stream (created on first use)
+    cudaEvent_t ev2[2] = {};
     cudaEvent_t ev[8] = {};
     std::string last_error;
     double pair_ms[5] = {0, 0, 0, 0, 0};
@@ -50,6 +55,7 @@ struct zdx_ctx {
     zdx::DevBuf tri_sph, mesh_R, mesh_valid, mesh_infl;
     zdx::DevBuf order, buckets, pair_i64, pair_i32, counters;
     zdx::DevBuf k1_slots, seg_arena, k2_slots;
+    zdx::DevBuf ar_lists, ar_counts, ar_gslots;  // arena form of the rebuild: class lists, counts, slots
     zdx::DevBuf sp_items, sp_first, sp_chunk;  // split of large pairs (items, per-pair first item, runs)
     zdx::DevBuf w_scratch;                     // per-item tapes of the wall contacts (zdx_rollout.cu)
     zdx::DevBuf p_err;                         // error flag of the pair force kernels (zdx_rollout.cu)
@@ -65,7 +71,8 @@ struct zdx_ctx {
 
     std::vector<zdx::DevBuf*> all_bufs() {
         return {&in_tris, &in_off, &in_me, &in_bd, &in_pm, &in_pose, &tri_sph, &mesh_R, &mesh_valid, &mesh_infl,
-                &order, &buckets, &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &sp_items,
+                &order, &buckets, &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &ar_lists,
+                &ar_counts, &ar_gslots, &sp_items,
                 &sp_first, &sp_chunk, &w_scratch, &p_err,
                 &cstage, &cistage, &pstage, &g_off, &o_cg, &o_ci, &o_pts, &o_cpo, &o_ps, &o_comp, &t_segtri, &t_segcand,
                 &t_arena, &t_cstage, &t_cfinal, &a_nc, &a_coff, &a_stats, &a_geom, &a_info, &a_pts, &a_cpo, &a_gc,

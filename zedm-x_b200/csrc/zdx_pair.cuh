@@ -124,6 +124,23 @@ struct PairArgs {
 
 // Bytes of one rebuild slot able to hold a pair of n segments.
 size_t rebuild_slot_bytes(int n);
+
+// The arena form of the rebuild (zdx_rebuild.cu; zdem mode without the adjoint tape, loop points or
+// component stats): one warp per pair with all of the pair's arrays in the warp's arena (a global-memory
+// slot of arena_bytes).  launch_rebuild_classes sorts the pairs into the arena list (lists[0]) and, below
+// min_seg segments, the list of the warp-per-pair kernel (lists[2]); launch_rebuild_arena runs the arena
+// list and appends the pairs that outgrow their arena to lists[1], for the warp-per-pair kernel.
+struct ArenaPlan {
+    int min_seg;
+    int arena_bytes;
+    int grid;               // CTAs of 4 warps, one arena each
+    char* gslots;
+    int32_t* lists;         // 3 lists of list_stride pairs
+    int64_t list_stride;
+    int64_t* counts;        // [0..2]: list lengths; [4]: the arena list's work queue; [5]: spare queue
+};
+void launch_rebuild_classes(const PairArgs& a, const ArenaPlan& plan, cudaStream_t s);
+void launch_rebuild_arena(const PairArgs& a, const ArenaPlan& plan, cudaStream_t s);
 // Bytes of one triangle-stage slot.
 size_t tritest_slot_bytes(int cap_side, int cap_seg);
 

@@ -59,7 +59,8 @@ class PairResult(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("tri_ctas_per_sm", C.c_int32), ("rebuild_warps", C.c_int32), ("flat_max", C.c_int64),
-                ("split_tests", C.c_int64)]
+                ("split_tests", C.c_int64), ("rebuild_arena", C.c_int32), ("arena_warps", C.c_int32),
+                ("arena_min_seg", C.c_int32), ("arena_pad", C.c_int32)]
 
 
 class WallItems(C.Structure):
@@ -228,7 +229,7 @@ class Context:
         """The pair kernels' launch parameters in force (zdx_get_tuning)."""
         t = Tuning()
         check(lib().zdx_get_tuning(self.handle, C.byref(t)), self.handle)
-        return {k: int(getattr(t, k)) for k, _ in Tuning._fields_}
+        return {k: int(getattr(t, k)) for k, _ in Tuning._fields_ if k != "arena_pad"}
 
     def set_tuning(self, **kw) -> dict:
         """Change some launch parameters (zdx_set_tuning); the others keep their values."""

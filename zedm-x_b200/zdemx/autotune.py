@@ -7,7 +7,12 @@ The knobs change how the batched pair call is launched, never what it computes:
                        directly, above which it uses the Morton-ordered group boxes;
 * ``rebuild_warps``    warps per rebuild block (one warp per pair);
 * ``split_tests``      in a batch with fewer pairs than triangle-stage CTAs, the triangle tests per work
-                       item into which large pairs are split (0: no split).
+                       item into which large pairs are split (0: no split);
+* ``rebuild_arena``    the rebuild's form: one warp per pair over global-memory slots (0), the large
+                       pairs in arenas alongside form 0 on the small ones (1), or arenas for every
+                       pair (2);
+* ``arena_warps``      warps per SM given arenas;
+* ``arena_min_seg``    the segment count from which form 1 gives a pair an arena.
 
 On a seeded calibration sample of a workload the tuner times the call (the library's own CUDA events)
 for each candidate value of one knob with the others held, keeps the fastest, and goes over the knobs
@@ -31,8 +36,12 @@ GRID = {
     "tri_ctas_per_sm": (1, 2),
     "rebuild_warps": (1, 2, 4),
     "split_tests": (0, 16384, 131072),
+    "rebuild_arena": (0, 1, 2),
+    "arena_warps": (4, 8, 12, 16),
+    "arena_min_seg": (96, 192, 384),
 }
-DEFAULTS = {"tri_ctas_per_sm": 2, "rebuild_warps": 4, "flat_max": 8192, "split_tests": 0}
+DEFAULTS = {"tri_ctas_per_sm": 2, "rebuild_warps": 4, "flat_max": 8192, "split_tests": 0, "rebuild_arena": 0,
+            "arena_warps": 8, "arena_min_seg": 192}
 
 
 def _snapshot(out, n_contacts):
