@@ -868,16 +868,44 @@ __global__ __launch_bounds__(128) void k_rebuild_arena(PairArgs a, FastArgs f) {
 }
 
 // Pairs into the arena list (0), or, below min_seg segments, the list of the warp-per-pair kernel (2).
-// Pairs the triangle stage could not finish (overflow) have nothing to rebuild: the arena list.
-__global__ void k_rebuild_classes(PairArgs a, int min_seg, int32_t* lists, int64_t* counts, int64_t list_stride) {
+// Pairs the triangle stage could not finish (overflow) have nothing to rebuild: the arena list.  Each
+// block takes its run of each list with one atomic and keeps its pairs in work order (most expensive
+// first) inside the run, so both lists stay close to that order.
+__global__ __launch_bounds__(256) void k_rebuild_classes(PairArgs a, int min_seg, int32_t* lists, int64_t* counts,
+                                                         int64_t list_stride) {
+    __shared__ int wsum[2][8];
+    __shared__ long long base[2];
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t np = a.n_dev ? (*a.n_dev < a.n_pairs ? *a.n_dev : a.n_pairs) : a.n_pairs;
-    if (t >= np) return;
-    const int p = a.order ? a.order[t] : (int)t;
-    const int n = a.pair_nseg[p];
-    const int st = a.pair_status[p];
-    const int cls = (!(st & (PAIR_SEG_OVERFLOW | PAIR_NO_ARENA)) && n > 0 && n < min_seg) ? 2 : 0;
-    lists[cls * list_stride + bump64(counts + cls)] = p;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int p = -1, cls = 0;
+    if (t < np) {
+        p = a.order ? a.order[t] : (int)t;
+        const int n = a.pair_nseg[p];
+        const int st = a.pair_status[p];
+        cls = (!(st & (PAIR_SEG_OVERFLOW | PAIR_NO_ARENA)) && n > 0 && n < min_seg) ? 2 : 0;
+    }
+    int rank[2];
+    for (int c = 0; c < 2; ++c) {
+        const unsigned bal = __ballot_sync(FULL, p >= 0 && cls == 2 * c);
+        rank[c] = __popc(bal & ((1u << lane) - 1u));
+        if (lane == 0) wsum[c][w] = __popc(bal);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        int tot = 0;
+        for (int k = 0; k < 8; ++k) tot += wsum[threadIdx.x][k];
+        base[threadIdx.x] = tot ? (long long)atomicAdd(reinterpret_cast<unsigned long long*>(counts + 2 * threadIdx.x),
+                                                       (unsigned long long)tot)
+                                : 0;
+    }
+    __syncthreads();
+    if (p >= 0) {
+        const int c = cls >> 1;
+        int before = 0;
+        for (int k = 0; k < w; ++k) before += wsum[c][k];
+        lists[cls * list_stride + base[c] + before + rank[c]] = p;
+    }
 }
 
 }  // namespace
