@@ -202,6 +202,8 @@ class Context:
 
     def __init__(self, device: int = 0):
         self._h = C.c_void_p()
+        self.device = int(device)
+        self._ext = None
         check(lib().zdx_create(C.byref(self._h), int(device)))
 
     @property
@@ -224,6 +226,18 @@ class Context:
         v = C.c_void_p()
         check(lib().zdx_get_stream(self.handle, C.byref(v)), self.handle)
         return int(v.value or 0)
+
+    def after_torch(self):
+        """Make the context stream wait, on the device, for the work queued so far on torch's current stream:
+        a call that follows reads what torch wrote, with no host-side synchronisation.  (Each call returns
+        once the context stream is done, so torch may use its outputs straight away.)"""
+        import torch
+
+        if self._ext is None:
+            self._ext = torch.cuda.ExternalStream(self.stream_ptr(), device=torch.device("cuda", self.device))
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(torch.device("cuda", self.device)))
+        self._ext.wait_event(ev)
 
     def tuning(self) -> dict:
         """The pair kernels' launch parameters in force (zdx_get_tuning)."""

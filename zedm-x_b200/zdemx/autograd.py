@@ -59,7 +59,7 @@ class PairContactGeometry(torch.autograd.Function):
                    "info": torch.zeros(cap, 4, dtype=torch.int32, device=dev)}
             meshes = {"tris": tris.detach(), "tri_off": tri_off, "mean_edge": mean_edge, "bbox_diag": bbox_diag}
             pairs = {"mesh": pair_mesh, "pose": pose.detach()}
-            torch.cuda.synchronize(dev)
+            ctx_handle(dev).after_torch()
             try:
                 totals = _lib.pair_contacts_device(ctx_handle(dev), meshes, pairs, out, mode=mode, split=split, tol=tol)
                 break
@@ -92,7 +92,7 @@ class PairContactGeometry(torch.autograd.Function):
         gp12 = torch.zeros(max(P, 1), 12, dtype=torch.float64, device=tris.device)
         meshes = {"tris": tris.detach(), "tri_off": tri_off, "mean_edge": mean_edge, "bbox_diag": bbox_diag}
         pairs = {"mesh": pair_mesh, "pose": pose.detach()}
-        torch.cuda.synchronize(tris.device)
+        ctx_handle(tris.device).after_torch()
         if n > 0:
             _lib.pair_contacts_adjoint(ctx_handle(tris.device), meshes, pairs, gc, gt, gp12, mode=mode, split=split,
                                        tol=tol)

@@ -70,6 +70,29 @@ def _rotmat(qn):
                         2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1).reshape(*qn.shape[:-1], 3, 3)
 
 
+class _Rows(torch.autograd.Function):
+    """src[idx] along dim 0, with the cotangent scattered back by index_add_ (FP64 atomics: the sums'
+    order, and so their last bits, may vary between runs) rather than by the sorted scatter of an indexing
+    backward."""
+
+    @staticmethod
+    def forward(ctx, src, idx):
+        ctx.save_for_backward(idx)
+        ctx.n = src.shape[0]
+        return src.index_select(0, idx)
+
+    @staticmethod
+    def backward(ctx, g):
+        (idx,) = ctx.saved_tensors
+        out = torch.zeros((ctx.n,) + tuple(g.shape[1:]), dtype=g.dtype, device=g.device)
+        out.index_add_(0, idx, g)
+        return out, None
+
+
+def _rows(src, idx):
+    return _Rows.apply(src, idx) if src.requires_grad else src.index_select(0, idx)
+
+
 def _lookup(keys, query):
     """Index of each query key in the sorted key array, -1 where absent."""
     if keys.numel() == 0 or query.numel() == 0:
@@ -95,7 +118,7 @@ class _WallForces(torch.autograd.Function):
                "ds": torch.empty(n, 3, dtype=torch.float64, device=dev),
                "flags": torch.empty(n, dtype=torch.int32, device=dev)}
         ev = float(e)
-        torch.cuda.synchronize(dev)
+        consts["ctx"].after_torch()
         _lib.wall_forces(consts["ctx"], items, ev, consts["dt"], consts["max_tris"], out)
         # per-call tensors through save_for_backward (a checkpointed rollout frees and recomputes them);
         # the scene's constant arrays stay in consts
@@ -119,7 +142,7 @@ class _WallForces(torch.autograd.Function):
                    "e": torch.zeros(n, dtype=torch.float64, device=dev)}
         g = {"f": (gf if gf is not None else z(3)).contiguous(), "t": (gt if gt is not None else z(3)).contiguous(),
              "ds": (gds if gds is not None else z(3)).contiguous()}
-        torch.cuda.synchronize(dev)
+        consts["ctx"].after_torch()
         _lib.wall_forces_adjoint(consts["ctx"], items, ctx.ev, consts["dt"], consts["max_tris"], g, grad_in)
         return (grad_in["x"], grad_in["q"], grad_in["v"], grad_in["w"], grad_in["ds_in"], grad_in["e"].sum(), None, None,
                 None, None)
@@ -133,7 +156,7 @@ class _Integrate(torch.autograd.Function):
     def forward(ctx, state, F, T, consts):
         st, f, t = state.detach().contiguous(), F.detach().contiguous(), T.detach().contiguous()
         out = torch.empty_like(st)
-        torch.cuda.synchronize(st.device)
+        consts["ctx"].after_torch()
         _lib.integrate(consts["ctx"], st, consts["mat"], f, t, consts["g"], consts["dt"], out)
         ctx.save_for_backward(st, f, t)
         ctx.consts = consts
@@ -144,7 +167,7 @@ class _Integrate(torch.autograd.Function):
         st, f, t = ctx.saved_tensors
         c = ctx.consts
         g_st, g_f, g_t = torch.empty_like(st), torch.empty_like(f), torch.empty_like(t)
-        torch.cuda.synchronize(st.device)
+        c["ctx"].after_torch()
         _lib.integrate_adjoint(c["ctx"], st, c["mat"], f, t, c["g"], c["dt"], g_out.contiguous(), g_st, g_f, g_t)
         return g_st, g_f, g_t, None
 
@@ -166,7 +189,7 @@ class _PPForces(torch.autograd.Function):
             pairs[name] = t.detach().contiguous()
         out = {nm: torch.empty(n, 3, dtype=torch.float64, device=dev) for nm in ("fb", "ta", "tb", "ds")}
         kv, ev = float(k), float(e)
-        torch.cuda.synchronize(dev)
+        consts["ctx"].after_torch()
         _lib.pp_forces(consts["ctx"], pairs, consts["law"], kv, ev, consts["dt"], out)
         ctx.save_for_backward(*(pairs[nm] for nm in _PP_SAVED))
         ctx.consts, ctx.kv, ctx.ev = consts, kv, ev
@@ -185,7 +208,7 @@ class _PPForces(torch.autograd.Function):
         gin = {"pair": torch.zeros(n, 21, dtype=torch.float64, device=dev),
                "k": torch.zeros(n, dtype=torch.float64, device=dev), "e": torch.zeros(n, dtype=torch.float64, device=dev),
                "contact": torch.zeros(max(nc, 1), 7, dtype=torch.float64, device=dev)}
-        torch.cuda.synchronize(dev)
+        consts["ctx"].after_torch()
         _lib.pp_forces_adjoint(consts["ctx"], pairs, consts["law"], ctx.kv, ctx.ev, consts["dt"], gout, gin)
         g = gin["pair"]
         gc = gin["contact"][:nc]
@@ -255,7 +278,6 @@ class DiffScene:
         """One step; returns (state, hkey, hds, wkey, wds, stats)."""
         dev, N = self.dev, self.np
         mat = self.mat
-        x, v, w = state[:, 0:3], state[:, 7:10], state[:, 10:13]
         F = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         Tq = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         stats = {}
@@ -265,7 +287,7 @@ class DiffScene:
                 from .autograd import ctx_handle
 
                 self._wctx = ctx_handle(dev)
-            torch.cuda.synchronize(dev)
+            self._wctx.after_torch()
             cand, self._bp_buf = _lib.broad_phase(self._wctx, state.detach(), mat, self._bp_buf)
             pi, pj = cand[:, 0].long(), cand[:, 1].long()
         P = pi.numel()
@@ -273,7 +295,8 @@ class DiffScene:
         new_hkey = torch.zeros(0, dtype=torch.int64, device=dev)
         new_hds = torch.zeros(0, 3, dtype=torch.float64, device=dev)
         if P > 0:
-            pose = torch.cat([state[pi, 0:7], state[pj, 0:7]], 1)
+            sa, sb = _rows(state, pi), _rows(state, pj)  # each pair's two particles, once
+            pose = torch.cat([sa[:, 0:7], sb[:, 0:7]], 1)
             pm = torch.stack([self.pmesh[pi], self.pmesh[pj]], 1).contiguous()
             out = pair_contacts(self.tris, pose, self.tri_off, self.mean_edge, self.bbox_diag, pm, k=1.0,
                                 mode=_lib.MODE_ZDEM, split=self.split)
@@ -285,20 +308,21 @@ class DiffScene:
                 key = (pi.to(torch.int64) << 32) | pj.to(torch.int64)
                 hpos = _lookup(hkey, key)
                 zero3 = torch.zeros(P, 3, dtype=torch.float64, device=dev)
-                ds_in = torch.where((hpos >= 0)[:, None], hds[hpos.clamp(min=0)] if hds.shape[0] else zero3, zero3)
+                ds_in = torch.where((hpos >= 0)[:, None], _rows(hds, hpos.clamp(min=0)) if hds.shape[0] else zero3, zero3)
                 if self._wctx is None:
                     from .autograd import ctx_handle
 
                     self._wctx = ctx_handle(dev)
                 consts = {"ctx": self._wctx, "law": self.law, "dt": self.dt}
-                fb, ta, tb, ds_pair = _PPForces.apply(x[pi], x[pj], v[pi], v[pj], w[pi], w[pj], ds_in, out["xc0"],
+                fb, ta, tb, ds_pair = _PPForces.apply(sa[:, 0:3], sb[:, 0:3], sa[:, 7:10], sb[:, 7:10], sa[:, 10:13],
+                                                      sb[:, 10:13], ds_in, out["xc0"],
                                                       out["nA"], out["area"], k, e, coff.contiguous(),
                                                       mat[pi].contiguous(), mat[pj].contiguous(), consts)
                 F = F.index_add(0, pi, -fb).index_add(0, pj, fb)
                 Tq = Tq.index_add(0, pi, ta).index_add(0, pj, tb)
-                active = torch.bincount(cpair, minlength=P) > 0
-                new_hkey = key[active]
-                new_hds = ds_pair[active]
+                act = torch.nonzero(torch.bincount(cpair, minlength=P) > 0).squeeze(1)
+                new_hkey = key.index_select(0, act)
+                new_hds = _rows(ds_pair, act)
         # ---- walls
         new_wkey = torch.zeros(0, dtype=torch.int64, device=dev)
         new_wds = torch.zeros(0, 3, dtype=torch.float64, device=dev)
@@ -343,12 +367,11 @@ class DiffScene:
     def _walls(self, state, wkey, wds, e):
         """Wall contacts of every particle near a wall, through the CUDA kernels (see _WallForces)."""
         dev, N, mat = self.dev, self.np, self.mat
-        x, q, v, w = state[:, 0:3], state[:, 3:7], state[:, 7:10], state[:, 10:13]
         r = mat[:, 2]
         Fw = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         Tw = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         with torch.no_grad():
-            d = x.detach()[:, None, :] - self.wpose[None, :, 0:3]
+            d = state.detach()[:, None, 0:3] - self.wpose[None, :, 0:3]
             dist2 = d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1] + d[..., 2] * d[..., 2]
             rs = r[:, None] + self.wrad[None, :]
             ci, cw = torch.nonzero(~(dist2 > rs * rs), as_tuple=True)
@@ -359,7 +382,7 @@ class DiffScene:
         key = (ci.to(torch.int64) << 16) | cw.to(torch.int64)
         hpos = _lookup(wkey, key)
         zero3 = torch.zeros(C, 3, dtype=torch.float64, device=dev)
-        ds_c = torch.where((hpos >= 0)[:, None], wds[hpos.clamp(min=0)] if wds.shape[0] else zero3, zero3)
+        ds_c = torch.where((hpos >= 0)[:, None], _rows(wds, hpos.clamp(min=0)) if wds.shape[0] else zero3, zero3)
         if self._wctx is None:
             from .autograd import ctx_handle
 
@@ -368,7 +391,9 @@ class DiffScene:
                   "items": {"mesh_tris": self.tris, "mesh_off": self.mesh_off_t, "mesh_tol": self.mesh_tol,
                             "wall_tris": self.wtris_flat, "wall_normals": self.wnorm_c, "wall_off": self.wall_off_t,
                             "wall_mu": self.wall_mu}}
-        f, t, ds_out, flags = _WallForces.apply(x[ci], q[ci], v[ci], w[ci], ds_c, e, mat[ci].contiguous(),
+        sc = _rows(state, ci)
+        f, t, ds_out, flags = _WallForces.apply(sc[:, 0:3], sc[:, 3:7], sc[:, 7:10], sc[:, 10:13], ds_c, e,
+                                                mat[ci].contiguous(),
                                                 self.pmesh[ci].contiguous(), cw.to(torch.int32).contiguous(), consts)
         with torch.no_grad():
             fl = flags.to(torch.int64)
@@ -378,7 +403,8 @@ class DiffScene:
             nwc = int(((fl >> 1) & 0x7FFF).sum())
         Fw = Fw.index_add(0, ci, f)
         Tw = Tw.index_add(0, ci, t)
-        return Fw, Tw, key[touched], ds_out[touched], nwc
+        tidx = torch.nonzero(touched).squeeze(1)
+        return Fw, Tw, key.index_select(0, tidx), _rows(ds_out, tidx), nwc
 
     def _walls_torch(self, state, wkey, wds, e):
         """The wall contacts in torch autograd (sections inside their wall triangle only); the kernels'
@@ -389,7 +415,7 @@ class DiffScene:
         Fw = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         Tw = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         with torch.no_grad():
-            d = x.detach()[:, None, :] - self.wpose[None, :, 0:3]
+            d = state.detach()[:, None, 0:3] - self.wpose[None, :, 0:3]
             dist2 = d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1] + d[..., 2] * d[..., 2]
             rs = r[:, None] + self.wrad[None, :]
             ci, cw = torch.nonzero(~(dist2 > rs * rs), as_tuple=True)
@@ -400,7 +426,7 @@ class DiffScene:
         key = (ci.to(torch.int64) << 16) | cw.to(torch.int64)
         hpos = _lookup(wkey, key)
         zero3 = torch.zeros(C, 3, dtype=torch.float64, device=dev)
-        ds_c = torch.where((hpos >= 0)[:, None], wds[hpos.clamp(min=0)] if wds.shape[0] else zero3, zero3)
+        ds_c = torch.where((hpos >= 0)[:, None], _rows(wds, hpos.clamp(min=0)) if wds.shape[0] else zero3, zero3)
         touched = torch.zeros(C, dtype=torch.bool, device=dev)
         qn = _qnormalize(q[ci])
         xp = x[ci]
