@@ -1307,13 +1307,14 @@ def run_adjoint(args):
             adj.append(e0.elapsed_time(e1))
     launches = ctx.timings()["launches"] - launches0
     step_s = (sum(fwd) + sum(adj)) / 1e3 / args.steps
-    # the plain form (one launch per pair per stage) against the batched one on the same subset of pairs
+    # the plain forms -- one launch per stage over the subset (no queue, cost order or culls), and one
+    # launch per pair per stage -- against the batched one on the same subset of pairs
     ns = min(args.plain_pairs, npairs)
     sub_p = {"mesh": pairs["mesh"][:ns].contiguous(), "pose": pairs["pose"][:ns].contiguous()}
     sub_o = {kk: (v[:ns].contiguous() if kk in ("ncontact", "stats") else v) for kk, v in out.items()}
     sub_o["contact_off"] = out["contact_off"][: ns + 1].contiguous()
     forms = {}
-    for name, sched in (("batched", _lib.SCHED_BATCHED), ("plain", _lib.SCHED_PLAIN)):
+    for name, sched in (("batched", _lib.SCHED_BATCHED), ("per_stage", _lib.SCHED_PER_STAGE), ("plain", _lib.SCHED_PLAIN)):
         tt = []
         for rep in range(3):
             torch.cuda.synchronize()
@@ -1328,7 +1329,10 @@ def run_adjoint(args):
         forms[name] = (min(tt[1:]), gps.clone())
     plain_form = {"pairs": ns, "batched_pairs_per_s": ns / forms["batched"][0], "plain_pairs_per_s": ns / forms["plain"][0],
                   "speedup_batched_vs_plain": forms["plain"][0] / forms["batched"][0],
+                  "per_stage_pairs_per_s": ns / forms["per_stage"][0],
+                  "speedup_batched_vs_plain_per_stage": forms["per_stage"][0] / forms["batched"][0],
                   "grad_pose_max_abs_diff": float((forms["plain"][1] - forms["batched"][1]).abs().max()),
+                  "grad_pose_max_abs_diff_per_stage": float((forms["per_stage"][1] - forms["batched"][1]).abs().max()),
                   "note": "forward with tape + reverse, wall clock around each call (host syncs included)"}
     # batched central differences of the per-pair objective w.r.t. the 12 pose coordinates
     gpose = gp.cpu().numpy()
