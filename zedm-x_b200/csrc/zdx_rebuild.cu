@@ -1,27 +1,26 @@
-// zdx_rebuild.cu -- the rebuild stage (components, endpoint snap, T-junction split, loop trace, Sn/Gn/xc0,
-// filters, force) with each pair's working set in an arena of shared memory, zdem mode.
+// zdx_rebuild.cu -- the arena form of the rebuild stage (components, endpoint snap, T-junction split,
+// loop trace, Sn/Gn/xc0, filters, force) in zdem mode.
 //
-// The results are those of rebuild_pair in zdx_pair.cu bit for bit (it follows src/main.cpp:2148-2219);
-// what changes is how the work is laid out:
-//   * one warp per pair, every array of the pair in the warp's arena (shared memory; a global-memory slot
-//     for pairs too large for it), so that the serial decisions lane 0 must take in the reference's order
-//     chain shared-memory loads of ~30 cycles rather than L2 round trips;
+// The results are those of rebuild_pair in zdx_pair.cu bit for bit (both follow src/main.cpp:2148-2219);
+// what changes is how the work is laid out.  One warp per pair, with every array of the pair in the warp's
+// arena (a global-memory slot, carved by a bump allocator):
 //   * the neighbour relation of the component search (src/main.cpp:804-898) -- some pair of rep points in
-//     adjacent cells and overlapping padded boxes -- is built once for all segment pairs, in parallel
-//     (each unordered pair tested once, an outward-rounded float box as the first reject), as per-segment
-//     lists in the order the reference's hash-grid walk visits them.  The depth-first search then pops
-//     through those lists on lane 0: O(segments + list entries) instead of a scan of every unvisited
-//     segment per pop;
-//   * the endpoint snap (src/main.cpp:680-746) unites only endpoints of neighbouring segments: two
-//     endpoints within h lie in adjacent cells and inside each other's padded boxes, so their segments are
-//     neighbours in the relation above.  The union is lock-free over all lanes (the partition does not
-//     depend on the order of the unions); with every link pointing at the smaller index, a class's root is
-//     its first endpoint, so vertex ids by first appearance are a scan, and each vertex sums its members
-//     in endpoint order on its own lane;
+//     adjacent cells and overlapping padded boxes -- comes from a sort of the segments' boxes along the
+//     pair's longest axis and a sweep (each overlapping pair met once, an outward-rounded float box as the
+//     first reject); the pairs found are listed, lanes over the list take the segment distances both ways
+//     (the search's edges), and each segment's list is ordered as the reference's hash-grid walk visits
+//     it.  The depth-first search then pops through edges-only lists on lane 0: O(segments + edges)
+//     instead of a scan of every unvisited segment per pop;
+//   * the endpoint snap (src/main.cpp:680-746) of every component at once unites only endpoints of the
+//     same segment or of listed pairs: two endpoints within h lie in adjacent cells and inside each other's
+//     padded boxes, so their segments are listed.  The union is lock-free over the lanes (the partition
+//     does not depend on the order of the unions); with every link pointing at the smaller index, a class's
+//     root is its first endpoint, so vertex ids by first appearance are a scan, and each vertex sums its
+//     members in endpoint order on its own lane;
 //   * the std::sort replicas (components by size, loop starts by degree) sort packed (key, index) words,
 //     so a compare reads no key array.
-// Pairs whose arrays do not fit the arena go to a fallback list that the warp-per-pair kernel of
-// zdx_pair.cu (global-memory slots) processes afterwards.
+// A pair whose arrays outgrow its arena (or a fixed cap of the warp-per-pair kernel) is handed to that
+// kernel instead, so every result is the same in either form.
 //
 // Compiled with --fmad=false: see zdx_math.cuh.
 #include <cstdio>
@@ -163,7 +162,7 @@ __device__ __forceinline__ uint32_t entry(int key, int j, bool edge) {
     return ((uint32_t)key << 16) | ((uint32_t)j << 1) | (edge ? 1u : 0u);
 }
 
-struct FastArgs {
+struct ArenaLaunch {
     const int32_t* list;  // pairs of this launch
     const int64_t* list_count;
     int64_t* queue;
@@ -180,7 +179,7 @@ __device__ __forceinline__ int64_t bump64(int64_t* c) {
 // has been published then.
 __device__ bool rebuild_pair_arena(const PairArgs& a, const int p, char* arena, int arena_bytes, const int lane) {
     const int n = a.pair_nseg[p];
-    int status = a.pair_status[p];
+    const int status = a.pair_status[p];
     const double* S = a.seg + 6 * a.pair_seg_off[p];  // the arena copy once it is made
     const int mA = a.pmesh[2 * (int64_t)p];
     const double* ps = a.pose + 14 * (int64_t)p;
@@ -849,7 +848,7 @@ __device__ bool rebuild_pair_arena(const PairArgs& a, const int p, char* arena, 
     return true;
 }
 
-__global__ __launch_bounds__(128) void k_rebuild_arena(PairArgs a, FastArgs f) {
+__global__ __launch_bounds__(128) void k_rebuild_arena(PairArgs a, ArenaLaunch f) {
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     char* arena = f.gslots + ((size_t)blockIdx.x * 4 + w) * (size_t)f.arena_bytes;
@@ -920,7 +919,7 @@ void launch_rebuild_classes(const PairArgs& a, const ArenaPlan& plan, cudaStream
 
 void launch_rebuild_arena(const PairArgs& a, const ArenaPlan& plan, cudaStream_t s) {
     if (plan.grid <= 0) return;
-    FastArgs f;
+    ArenaLaunch f;
     f.list = plan.lists;
     f.list_count = plan.counts;
     f.queue = plan.counts + 4;
