@@ -437,8 +437,7 @@ def main():
         tres = autotune.tune(ctx, cm, cp, co, flush=flush)
         tuning = {"best": tres["best"], "calibration_pairs": tres["pairs"], "calibration_ms": tres["best_ms"],
                   "calibration_default_ms": tres["default_ms"], "trials": len(tres["trials"]),
-                  "tuner": "zdemx.autotune (coordinate descent over flat_max, tri_ctas_per_sm, rebuild_warps, "
-                           "split_tests)"}
+                  "tuner": "zdemx.autotune (coordinate descent over " + ", ".join(autotune.GRID) + ")"}
         del cm, cp, co
         torch.cuda.empty_cache()
 
