@@ -258,6 +258,13 @@ int zdx_scene_step_graph(zdx_ctx* ctx, int nsteps);
 /* Initial capacities of the graph step (0 keeps a default): candidate pairs, contacts, arena segments,
  * segments of one pair.  Growth on overflow still applies; call before the first graph step. */
 int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t contacts, int64_t segments, int seg_per_pair);
+/* The graph step's clearance cache (no reference counterpart; config key contact_cache, default 0): a
+ * candidate pair whose triangle stage found no segment keeps a clearance M with the two poses; while
+ * the vertices of the two bodies have moved by at most mu_A + mu_B < M since (mu <= |x - x0| +
+ * 2 R min(|q - q0|, |q + q0|), R the mesh's bounding radius), the pair is known to have no segment and
+ * its triangle stage is skipped.  Results are those of the step without the cache, bit for bit.
+ * *entries: the cache's entries after the last graph step; *skipped: the pairs that step skipped. */
+int zdx_scene_graph_cache(zdx_ctx* ctx, int64_t* entries, int64_t* skipped);
 /* The whole zdem_cpu run after argument parsing (src/main.cpp:1879-2503) on CUDA device `device`:
  * returns the process exit code (0, or 1 on a bad config / STL, as the reference).
  * zdx_run_config_graph runs the steps between outputs with zdx_scene_step_graph. */

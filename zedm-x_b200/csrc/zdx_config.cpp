@@ -222,6 +222,8 @@ bool parse_config(const std::string& path, SimConfig& cfg, std::string& err) {
             }
         } else if (key == "feng_k") {
             iss >> cfg.feng_k;
+        } else if (key == "contact_cache") {
+            iss >> cfg.contact_cache;
         }
         // unknown keys are ignored, as in the reference
     }

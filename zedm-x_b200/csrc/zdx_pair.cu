@@ -252,7 +252,19 @@ __device__ __forceinline__ void eval_entry(const PairArgs& a, const K1Slot& S, c
     }
 }
 
-template <bool NPX>
+// |q - q0| or |q + q0|, whichever is smaller (unit quaternions; a rotation and its negative are one)
+__device__ __forceinline__ double qdist(Q4 q, Q4 q0) {
+    const double m = sqrt((q.w - q0.w) * (q.w - q0.w) + (q.x - q0.x) * (q.x - q0.x) + (q.y - q0.y) * (q.y - q0.y) +
+                          (q.z - q0.z) * (q.z - q0.z));
+    const double p = sqrt((q.w + q0.w) * (q.w + q0.w) + (q.x + q0.x) * (q.x + q0.x) + (q.y + q0.y) * (q.y + q0.y) +
+                          (q.z + q0.z) * (q.z + q0.z));
+    return fmin(m, p);
+}
+__device__ __forceinline__ unsigned long long dbits(double v) { return (unsigned long long)__double_as_longlong(v); }
+
+// CACHE: the clearance cache of a DEM step (PairArgs::cache_*), a separate instantiation so that the
+// others compile as without it.
+template <bool NPX, bool CACHE>
 __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     __shared__ double sh_red[2][K1_THREADS / 32];
     __shared__ double sh_slab[3];  // hi(A.d), lo(B.d), slack of the certificate (the slab cull uses them)
@@ -264,6 +276,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     __shared__ unsigned long long sh_base;
     __shared__ int sh_last;
     __shared__ long long sh_ftot;
+    __shared__ unsigned long long sh_cmin, sh_gmin;  // CACHE: smallest cull clearance, smallest box gap (bits)
+    __shared__ int sh_hits, sh_cbad;
     extern __shared__ __align__(16) unsigned char k1_dsm[];
     // dynamic shared memory: float boxes | keys | values (the flat path's queue aliases keys+values)
     //                        | group boxes | per-warp overlap queues
@@ -287,6 +301,12 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
             sh_n[0] = sh_n[1] = 0;
             sh_nq = 0;
             sh_nseg = 0;
+            if constexpr (CACHE) {
+                sh_cmin = dbits(__builtin_huge_val());
+                sh_gmin = dbits(__builtin_huge_val());
+                sh_hits = 0;
+                sh_cbad = 0;
+            }
         }
         __syncthreads();
         const int64_t item = sh_item;
@@ -321,6 +341,36 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                              __longlong_as_double((long long)a.mesh_R_bits[mesh[1]])};
         auto inf = [](V3 v) { return smax3(fabs(v.x), fabs(v.y), fabs(v.z)); };
         const double pad = 1e-9 * (inf(tpos[0]) + inf(tpos[1]) + R[0] + R[1]);
+        if constexpr (CACHE) {
+            // A clearance M found at an earlier step still holds while the vertices' displacements since
+            // then add up to less than M: a vertex of body s moves by at most |x - x0| + 2 |v| |q - q0|
+            // (|R(q) v - R(q0) v| = 2 sin(theta / 2) |v| <= 2 |q - q0| |v| for unit quaternions, |v| <= R).
+            // The pair then has no segment, as when the certificate holds.
+            const int ci = a.cache_idx ? a.cache_idx[p] : -1;
+            if (ci >= 0) {
+                const double* e = a.cache_in + CACHE_W * (int64_t)ci;
+                double mv = 0.0;
+                for (int s2 = 0; s2 < 2; ++s2) {
+                    const double* o = e + 1 + 7 * s2;
+                    const Q4 q0 = qnormalize(Q4{o[3], o[4], o[5], o[6]});
+                    mv += norm(tpos[s2] - V3{o[0], o[1], o[2]}) + 2.0 * R[s2] * qdist(qn[s2], q0);
+                }
+                if (mv * (1.0 + 1e-9) + 8.0 * pad < e[0]) {
+                    if (tid == 0) {
+                        a.pair_seg_off[p] = 0;
+                        a.pair_nseg[p] = 0;
+                        a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
+                        a.pair_status[p] = 0;
+                        atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
+                    }
+                    // the entry carries over unchanged (word 15 marks a skip)
+                    for (int k = tid; k < CACHE_W; k += K1_THREADS)
+                        a.cache_out[CACHE_W * (int64_t)p + k] = k == CACHE_W - 1 ? 1.0 : e[k];
+                    __syncthreads();
+                    continue;
+                }
+            }
+        }
 
         // Separation certificate along the line of centres d: every point of A lies below the largest
         // corner projection max_v (v.d) of A's triangles, every point of B above B's smallest one.  A
@@ -378,6 +428,14 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                         a.pair_status[p] = 0;
                         atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
                     }
+                    if constexpr (CACHE) {
+                        // the certificate's gap along d: moved vertices shift the projections by their
+                        // displacement at most, and the slack by the change of pad (inside the allowance)
+                        double* c = a.cache_out + CACHE_W * (int64_t)p;
+                        if (tid == 0) c[0] = sh_slab[1] - sh_slab[0] - sh_slab[2];
+                        if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
+                        if (tid == 15) c[15] = 0.0;
+                    }
                     __syncthreads();
                     continue;
                 }
@@ -393,6 +451,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         // where the two bodies overlap along d: an A triangle whose corners all project below
         // lo(B.d) - slack, a B triangle whose corners all project above hi(A.d) + slack.  By the
         // certificate's argument neither can take part in a segment.
+        double cclear = __builtin_huge_val();  // CACHE: smallest clearance of a culled triangle
+        bool cbad = false;
         for (int s = 0; s < 2; ++s) {
             const V3 other = tpos[1 - s];
             const double lim = R[1 - s] + pad;
@@ -413,15 +473,23 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     const double p0 = lv[0] * dl.x + lv[1] * dl.y + lv[2] * dl.z;
                     const double p1 = lv[3] * dl.x + lv[4] * dl.y + lv[5] * dl.z;
                     const double p2 = lv[6] * dl.x + lv[7] * dl.y + lv[8] * dl.z;
-                    if (s == 0 ? (smax3(p0, p1, p2) < bound) : (smin3(p0, p1, p2) > bound)) continue;
+                    if (s == 0 ? (smax3(p0, p1, p2) < bound) : (smin3(p0, p1, p2) > bound)) {
+                        // CACHE: how far the triangle sits outside the slab along d
+                        if constexpr (CACHE) cclear = fmin(cclear, s == 0 ? bound - smax3(p0, p1, p2) : smin3(p0, p1, p2) - bound);
+                        continue;
+                    }
                 }
                 if (!a.per_stage) {
                     double4 sp = a.tri_sph[off[s] + t];
                     V3 c = V3{sp.x, sp.y, sp.z};
                     V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];
                     double L = sp.w + lim;
-                    if (!(fabs(cw.x - other.x) <= L && fabs(cw.y - other.y) <= L && fabs(cw.z - other.z) <= L))
+                    if (!(fabs(cw.x - other.x) <= L && fabs(cw.y - other.y) <= L && fabs(cw.z - other.z) <= L)) {
+                        // CACHE: how far the triangle's cube misses the other body's, on the widest axis
+                        if constexpr (CACHE)
+                            cclear = fmin(cclear, smax3(fabs(cw.x - other.x), fabs(cw.y - other.y), fabs(cw.z - other.z)) - L);
                         continue;
+                    }
                 }
                 const double* v = a.tris + 9 * (off[s] + t);
                 V3 w[3];
@@ -437,8 +505,16 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     if (!np::plane_from_tri(&w[0].x, &np_n.x, &d)) continue;
                     np::tri_normal(&w[0].x, &n.x);
                 } else {
-                    if (!plane_from_tri(w[0], w[1], w[2], n, d)) continue;
-                    if (norm2(n) < 1e-30) continue;
+                    if constexpr (CACHE) {
+                        // a triangle without a plane here might have one after a move: no clearance
+                        if (!plane_from_tri(w[0], w[1], w[2], n, d) || norm2(n) < 1e-30) {
+                            cbad = true;
+                            continue;
+                        }
+                    } else {
+                        if (!plane_from_tri(w[0], w[1], w[2], n, d)) continue;
+                        if (norm2(n) < 1e-30) continue;
+                    }
                 }
                 int i = atomicAdd(&sh_n[s], 1);
                 for (int k = 0; k < 3; ++k) {
@@ -458,6 +534,13 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 D.box[5 * cap + i] = smax3(w[0].z, w[1].z, w[2].z);
                 D.id[i] = t;
             }
+        }
+        if constexpr (CACHE) {
+            if (cclear < __builtin_huge_val()) {
+                if (cclear > 0.0) atomicMin(&sh_cmin, dbits(cclear));
+                else cbad = true;
+            }
+            if (cbad) sh_cbad = 1;
         }
         __syncthreads();
         const int nA = sh_n[0], nB = sh_n[1];
@@ -567,6 +650,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                         }
                         unsigned hb = __ballot_sync(FULL, hit);
                         if (hit) wq[wq_n + __popc(hb & ((1u << lane) - 1u))] = make_int2(ia, ib);
+                        if constexpr (CACHE) {
+                            if (hit) sh_hits = 1;
+                        }
                         wq_n += __popc(hb);
                         if (wq_n >= 32) {
                             __syncwarp();
@@ -598,6 +684,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                                    bA[4 * sA + ia] < bB[1 * sB + ib] || bA[1 * sA + ia] > bB[4 * sB + ib] ||
                                    bA[5 * sA + ia] < bB[2 * sB + ib] || bA[2 * sA + ia] > bB[5 * sB + ib];
                         if (!sep) {
+                            if constexpr (CACHE) sh_hits = 1;
                             int qi = atomicAdd(&sh_nq, 1);
                             sh_q[qi] = make_int2(ia, ib);
                         }
@@ -616,6 +703,37 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 if (tid == 0) sh_nq = 0;
                 __syncthreads();
             }
+        }
+        if constexpr (CACHE) {
+            // the pair's clearance: none unless no box met (so no segment) and no triangle lacked a plane;
+            // then the smaller of the culled triangles' clearances and the survivors' smallest box gap
+            // (the largest separation over the axes, for each pair of survivor boxes)
+            __syncthreads();
+            const bool ok = sh_hits == 0 && sh_nseg == 0 && sh_cbad == 0 && !separated;
+            if (ok && nA > 0 && nB > 0) {
+                double g = __builtin_huge_val();
+                for (int64_t q = tid; q < total; q += K1_THREADS) {
+                    const int ia = (int)(q / nB), ib = (int)(q - (int64_t)ia * nB);
+                    double gq = -__builtin_huge_val();
+                    for (int k = 0; k < 3; ++k) {
+                        gq = fmax(gq, bB[k * sB + ib] - bA[(3 + k) * sA + ia]);
+                        gq = fmax(gq, bA[k * sA + ia] - bB[(3 + k) * sB + ib]);
+                    }
+                    g = fmin(g, gq);
+                }
+                if (g < __builtin_huge_val()) {
+                    if (g > 0.0) atomicMin(&sh_gmin, dbits(g));
+                    else sh_cbad = 1;
+                }
+            }
+            __syncthreads();
+            double* c = a.cache_out + CACHE_W * (int64_t)p;
+            if (tid == 0) {
+                const double m = fmin(__longlong_as_double((long long)sh_cmin), __longlong_as_double((long long)sh_gmin));
+                c[0] = (ok && sh_cbad == 0 && m > 0.0) ? m : -1.0;
+            }
+            if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
+            if (tid == 15) c[15] = 0.0;
         }
         int ns = sh_nseg;
         int status = 0;
@@ -732,13 +850,17 @@ void launch_segments(const PairArgs& a, int grid, cudaStream_t s) {
     // there): the carveout, in percent of the largest shared memory, that holds 2 x (dynamic + static + 1 KB)
     const int carve = (int)((200 * (K1_DSMEM + 2048) + 233471) / 233472);
     if (a.mode == 2) {
-        cudaFuncSetAttribute(k_segments<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
-        cudaFuncSetAttribute(k_segments<true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
-        k_segments<true><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
+        cudaFuncSetAttribute(k_segments<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+        cudaFuncSetAttribute(k_segments<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        k_segments<true, false><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
+    } else if (a.cache_out && !a.items) {
+        cudaFuncSetAttribute(k_segments<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+        cudaFuncSetAttribute(k_segments<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        k_segments<false, true><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
     } else {
-        cudaFuncSetAttribute(k_segments<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
-        cudaFuncSetAttribute(k_segments<false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
-        k_segments<false><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
+        cudaFuncSetAttribute(k_segments<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
+        cudaFuncSetAttribute(k_segments<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        k_segments<false, false><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
     }
 }
 

@@ -120,7 +120,17 @@ struct PairArgs {
     // the T-junction split, in component order
     int32_t* comp_stats;
     int64_t comp_stats_cap;
+    // Clearance cache of a DEM step (null cache_out: none; pairs are never split then).  An entry is
+    // CACHE_W doubles: a clearance M > 0, then the pair's 14 pose values when M was found.  M certifies that
+    // the pair has no segment as long as every vertex of A has moved by at most mu_A and every vertex of B
+    // by mu_B with mu_A + mu_B < M (less the rounding allowance).  cache_idx[p] >= 0 names the entry of
+    // cache_in found for pair p, which k_segments uses to skip the pair while it holds; cache_out receives
+    // each pair's entry for the next step (M <= 0: none).
+    const int32_t* cache_idx;
+    const double* cache_in;
+    double* cache_out;
 };
+constexpr int CACHE_W = 16;
 
 // Bytes of one rebuild slot able to hold a pair of n segments.
 size_t rebuild_slot_bytes(int n);

@@ -1307,6 +1307,7 @@ namespace {
 
 __global__ void k_g_begin(GraphCounts* g) {
     g->flags = 0;
+    g->cache_skipped = 0;
     g->contacts = g->wall_contacts = g->tri_checks = g->segments = g->comps = g->loops = 0;
 }
 
@@ -1350,6 +1351,52 @@ __global__ void k_g_pair_stats(const int32_t* pstats, const GraphCounts* gc, Gra
         atomicAdd(&g->comps, c);
         atomicAdd(&g->loops, l);
     }
+}
+
+// ---- clearance cache (PairArgs::cache_*): the entry of each candidate pair, by binary search of its key
+__global__ void k_cache_lookup(const int2* pairs, int64_t cap, const int64_t* n_dev, const int64_t* ckey,
+                               const GraphCounts* g, int32_t* cidx) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= dev_count(cap, n_dev)) return;
+    const int64_t key = ((int64_t)pairs[p].x << 32) | (int64_t)(uint32_t)pairs[p].y;
+    int64_t lo = 0, hi = g->ncache;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (ckey[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    cidx[p] = (lo < g->ncache && ckey[lo] == key) ? (int32_t)lo : -1;
+}
+// pairs whose entry for the next step holds a clearance, and how many skipped this step (entry word 15)
+__global__ void k_cache_flags(const double* cout, int64_t cap, const int64_t* n_dev, int32_t* flag, GraphCounts* g) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t n = dev_count(cap, n_dev);
+    const bool live = p < n;
+    const bool f = live && cout[CACHE_W * p] > 0.0;
+    if (p < cap) flag[p] = f ? 1 : 0;
+    const unsigned b = __ballot_sync(FULLM, live && cout[CACHE_W * p + 15] != 0.0);
+    if ((threadIdx.x & 31) == 0 && b)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&g->cache_skipped), (unsigned long long)__popc(b));
+}
+__global__ void k_cache_write(const int32_t* flag, const int64_t* pos, int64_t cap, const int64_t* n_dev, const int2* pairs,
+                              const double* cout, int64_t* ckey2, double* cval2) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= dev_count(cap, n_dev) || !flag[p]) return;
+    const int64_t o = pos[p];
+    ckey2[o] = ((int64_t)pairs[p].x << 32) | (int64_t)(uint32_t)pairs[p].y;
+    for (int k = 0; k < CACHE_W; ++k) cval2[CACHE_W * o + k] = cout[CACHE_W * p + k];
+}
+// with the step complete, the next step's entries become the cache
+__global__ void k_cache_commit(GraphCounts* g, const int64_t* pos, const int64_t* ckey2, const double* cval2,
+                               int64_t* ckey, double* cval) {
+    if (g->flags) return;
+    const int64_t n = pos[g->npair];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += stride) {
+        ckey[k] = ckey2[k];
+        for (int c = 0; c < CACHE_W; ++c) cval[CACHE_W * k + c] = cval2[CACHE_W * k + c];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) g->ncache = n;
 }
 
 // The step completed: the compacted histories become the current ones.
@@ -1439,6 +1486,16 @@ static int graph_alloc(zdx_ctx* ctx, Scene& s) {
     CKS(G.whds.ensure(sizeof(double) * 3 * W1));
     CKS(G.whkey2.ensure(sizeof(int64_t) * W1));
     CKS(G.whds2.ensure(sizeof(double) * 3 * W1));
+    // clearance cache: at most one entry per pair of a step; emptied whenever the buffers are (re)sized
+    CKS(G.ckey.ensure(sizeof(int64_t) * P1));
+    CKS(G.cval.ensure(sizeof(double) * CACHE_W * P1));
+    CKS(G.ckey2.ensure(sizeof(int64_t) * P1));
+    CKS(G.cval2.ensure(sizeof(double) * CACHE_W * P1));
+    CKS(G.cidx.ensure(sizeof(int32_t) * P1));
+    CKS(G.cout.ensure(sizeof(double) * CACHE_W * P1));
+    CKS(G.cflag.ensure(sizeof(int32_t) * P1));
+    CKS(G.cscan.ensure(sizeof(int64_t) * (P1 + 1)));
+    CKS(cudaMemsetAsync(&as<GraphCounts>(G.g)->ncache, 0, sizeof(int64_t), ctx->stream));
     // pair kernels
     const int64_t total_tris = s.mesh_off.back();
     CKS(G.tri_sph.ensure(sizeof(double4) * (size_t)std::max<int64_t>(total_tris, 1)));
@@ -1509,6 +1566,10 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
                                                 as<int32_t>(G.tr_idx));
     CKS(radix_sort_u32(as<uint32_t>(G.tr_key), as<int32_t>(G.tr_idx), as<uint32_t>(G.tr_key2), as<int32_t>(G.tr_idx2),
                        G.pcap, G.pbits, G.rs_tmp.p, st, npair));
+    const bool cache = s.cfg.contact_cache != 0;
+    if (cache)
+        k_cache_lookup<<<grid(G.pcap), 256, 0, st>>>(as<int2>(G.bp_pairs), G.pcap, npair, as<int64_t>(G.ckey), g,
+                                                     as<int32_t>(G.cidx));
     {
         PairArgs a{};
         const int nm = (int)s.mesh_off.size() - 1;
@@ -1571,7 +1632,20 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
         a.k1_slots = as<char>(G.k1_slots);
         a.seg = as<double>(G.seg_arena);
         a.seg_cap = G.segcap;
+        if (cache) {
+            a.cache_idx = as<int32_t>(G.cidx);
+            a.cache_in = as<double>(G.cval);
+            a.cache_out = as<double>(G.cout);
+        }
         launch_segments(a, G.k1_grid, st);
+        if (cache) {
+            // the next step's cache: this step's clearances, in pair order (the keys stay sorted)
+            k_cache_flags<<<grid(G.pcap), 256, 0, st>>>(as<double>(G.cout), G.pcap, npair, as<int32_t>(G.cflag), g);
+            CKS(scan_offsets<int32_t>(as<int32_t>(G.cflag), G.pcap, npair, as<int64_t>(G.cscan), G.scan_tmp.p, st));
+            k_cache_write<<<grid(G.pcap), 256, 0, st>>>(as<int32_t>(G.cflag), as<int64_t>(G.cscan), G.pcap, npair,
+                                                        as<int2>(G.bp_pairs), as<double>(G.cout), as<int64_t>(G.ckey2),
+                                                        as<double>(G.cval2));
+        }
         a.k2_nmax = G.cap_seg;
         a.k2_slot_bytes = rebuild_slot_bytes(G.cap_seg);
         a.k2_nslots = G.k2_warps;
@@ -1647,6 +1721,10 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
                                                            as<int64_t>(G.hkey), as<double>(G.hds), as<int64_t>(G.hkey2),
                                                            as<double>(G.hds2), as<int64_t>(G.whkey), as<double>(G.whds),
                                                            as<int64_t>(G.whkey2), as<double>(G.whds2));
+    if (s.cfg.contact_cache)
+        k_cache_commit<<<std::max(1, ctx->num_sms), 256, 0, st>>>(g, as<int64_t>(G.cscan), as<int64_t>(G.ckey2),
+                                                                    as<double>(G.cval2), as<int64_t>(G.ckey),
+                                                                    as<double>(G.cval));
     CKS(cudaGetLastError());
     return ZDX_OK;
 }

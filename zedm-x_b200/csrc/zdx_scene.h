@@ -55,6 +55,9 @@ struct SimConfig {
     // with the zdem tangential, damping and Coulomb terms
     int force_law = 0;
     double feng_k = 1e7;
+    // addition: 1 lets the CUDA-graph step skip a candidate pair while a clearance it certified
+    // at an earlier step still holds (no segment either way); 0 (default) tests every candidate pair every step
+    int contact_cache = 0;
 };
 
 // parse_config_file, src/main.cpp:1531-1689 (same grammar, defaults and acceptance rule).
@@ -81,6 +84,8 @@ struct GraphCounts {
     int32_t flags, pad;                   // GRAPH_OVF_* bits of the last step (0: it completed)
     unsigned long long contacts, wall_contacts, tri_checks, segments, comps, loops;
     unsigned long long pair_counters[8];  // the pair kernels' counters (segments, contacts, ..., max nseg, err)
+    int64_t ncache;                       // clearance cache entries (sorted pair keys)
+    int64_t cache_skipped;                // pairs the last step skipped on a cached clearance
 };
 enum : int {
     GRAPH_OVF_PAIRS = 1,     // broad-phase pairs above the pair capacity
@@ -110,6 +115,8 @@ struct GraphStep {
     DevBuf pr_mesh, pr_pose, pr_coff, pr_stats, pr_geom, pr_info, pr_contrib, pr_active, pr_ds, pr_hscan;
     DevBuf w_active, w_scan, w_pairs, w_contrib, w_valid, w_act, w_ds, w_hscan, w_scratch;
     DevBuf hkey, hds, hkey2, hds2, whkey, whds, whkey2, whds2;
+    // clearance cache: sorted pair keys and entries (PairArgs::cache_*), the next step's, per-pair lookups
+    DevBuf ckey, cval, ckey2, cval2, cidx, cout, cflag, cscan;
     // pair kernels' workspaces
     DevBuf tri_sph, mesh_R, mesh_valid, mesh_infl, order, buckets, pair_i64, pair_i32, counters, k1_slots, seg_arena, k2_slots,
         cstage, cistage;
@@ -119,7 +126,8 @@ struct GraphStep {
                 &bp_pairs, &bp_pstart, &rs_tmp, &scan_tmp, &tr_key, &tr_idx, &tr_key2, &tr_idx2, &tr_start, &pr_mesh,
                 &pr_pose, &pr_coff, &pr_stats, &pr_geom, &pr_info, &pr_contrib, &pr_active, &pr_ds, &pr_hscan,
                 &w_active, &w_scan, &w_pairs, &w_contrib, &w_valid, &w_act, &w_ds, &w_hscan, &w_scratch, &hkey, &hds,
-                &hkey2, &hds2, &whkey, &whds, &whkey2, &whds2, &tri_sph, &mesh_R, &mesh_valid, &mesh_infl, &order, &buckets,
+                &hkey2, &hds2, &whkey, &whds, &whkey2, &whds2, &ckey, &cval, &ckey2, &cval2, &cidx, &cout, &cflag,
+                &cscan, &tri_sph, &mesh_R, &mesh_valid, &mesh_infl, &order, &buckets,
                 &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &cstage, &cistage};
     }
     void drop_graph() {

@@ -98,6 +98,16 @@ extern "C" int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t cont
     return ZDX_OK;
 }
 
+extern "C" int zdx_scene_graph_cache(zdx_ctx* ctx, int64_t* entries, int64_t* skipped) {
+    if (!ctx || !entries || !skipped) return ZDX_ERR_INVALID;
+    if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");
+    const GraphStep& G = ctx->scene->gs;
+    const bool g = G.active && G.host;
+    *entries = g ? G.host->ncache : 0;
+    *skipped = g ? G.host->cache_skipped : 0;
+    return ZDX_OK;
+}
+
 extern "C" int zdx_scene_array(zdx_ctx* ctx, int which, void* out, int64_t* count) {
     if (!ctx || !count) return ZDX_ERR_INVALID;
     if (!ctx->scene) return ctx_fail(ctx, ZDX_ERR_STATE, "no scene loaded");

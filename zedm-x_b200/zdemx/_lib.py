@@ -129,6 +129,7 @@ def lib() -> C.CDLL:
     L.zdx_run_config_graph.argtypes = [C.c_char_p, C.c_int]
     L.zdx_scene_step_graph.argtypes = [C.c_void_p, C.c_int]
     L.zdx_scene_graph_reserve.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int]
+    L.zdx_scene_graph_cache.argtypes = [C.c_void_p, _i64p, _i64p]
     L.zdx_pair_contacts_adjoint.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),
                                             C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.zdx_pair_contacts_noalloc.argtypes = [C.c_void_p, C.POINTER(PairOpts), C.POINTER(MeshSet), C.POINTER(PairBatch),

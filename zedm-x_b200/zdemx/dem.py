@@ -42,6 +42,12 @@ class Scene:
               "wall_normals": (6, np.float64, 3), "wall_off": (7, np.int64, 1), "wall_mat": (8, np.float64, 2),
               "wall_pose": (9, np.float64, 7), "wall_mesh": (10, np.int32, 1), "params": (11, np.float64, 1)}
 
+    def graph_cache(self) -> dict:
+        """The graph step's clearance cache: entries after the last graph step, pairs that step skipped."""
+        e, k = C.c_int64(0), C.c_int64(0)
+        _lib.check(_lib.lib().zdx_scene_graph_cache(self.ctx.handle, C.byref(e), C.byref(k)), self.ctx.handle)
+        return {"entries": int(e.value), "skipped": int(k.value)}
+
     def array(self, name: str) -> np.ndarray:
         """A set-up array of the scene (zdx_scene_array): mat, pmesh, mesh_tris, mesh_off, mesh_props,
         wall_tris, wall_normals, wall_off, wall_mat, wall_pose, wall_mesh, params (dt, gravity, split,
