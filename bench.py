@@ -949,7 +949,7 @@ def measure_pour(args, ctx, steps, cpu=True):
     cfg_path = pour_scene(d, n=args.particles, seed=args.seed)
     desc = (f"pour: {args.particles} particles (3 ellipsoid hulls of 64 points + icospheres s=2,3; circumradius 1 mm), "
             "jittered lattice in a closed 12-triangle box (60 x 60 mm floor), g=-9.81 z, dt=2e-6, "
-            "velocities N(0, 0.05 m/s), zdem force law, split_contacts=1, FP64")
+            "velocities N(0, 0.05 m/s), zdem force law, split_contacts=1, FP64, graph step's clearance cache on")
     dev = torch.device("cuda", 0)
     t0 = time.perf_counter()
     sc = Scene(cfg_path, ctx)
@@ -961,7 +961,7 @@ def measure_pour(args, ctx, steps, cpu=True):
     stream = _lib_stream(ctx)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     launches0 = ctx.timings()["launches"]
-    infos = []
+    infos, caches = [], []
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with ClockSampler(0) as clk:
         for k in range(steps):
@@ -972,6 +972,7 @@ def measure_pour(args, ctx, steps, cpu=True):
             with torch.cuda.stream(stream):
                 ev[k][1].record(stream)
             infos.append(sc.info())
+            caches.append(sc.graph_cache())
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     launches = ctx.timings()["launches"] - launches0
@@ -992,11 +993,13 @@ def measure_pour(args, ctx, steps, cpu=True):
     np_ = sc.n
     d2h = np_ * (16 * 8 + 3 * 8 * 2 + 4)
     peak, peak_kind = measured_peaks()
-    # algorithmic bytes of a step: particle state read + written, material read, and every candidate pair's
-    # two FP64 triangle soups (72 B per triangle) read once
+    # algorithmic bytes of a step: particle state read + written, material read, every candidate pair's
+    # two FP64 triangle soups (72 B per triangle) read once, except for the pairs skipped on the clearance
+    # cache, which read and write their 128-B entry instead
     pairs = int(np.mean([i["pairs"] for i in infos]))
+    skipped = int(np.mean([c["skipped"] for c in caches]))
     mean_tris = _mean_particle_tris(cfg_path)
-    abytes = np_ * (2 * 128 + 136) + pairs * 72.0 * 2 * mean_tris
+    abytes = np_ * (2 * 128 + 136) + (pairs - skipped) * 72.0 * 2 * mean_tris + skipped * 256.0
     achieved = abytes / (T / steps) / 1e9
     cpu_line = {"value": None, "unit": "steps/s", "cores": 1, "kind": "reference",
                 "sample": "not run here (one zdem_cpu step of this scene takes about a minute): --workload pour"}
@@ -1014,6 +1017,7 @@ def measure_pour(args, ctx, steps, cpu=True):
             "config": {"workload": desc, "particles": np_, "preroll_steps": args.preroll, "mean_tris": mean_tris,
                        "l2": "flushed (256 MB write) before every timed step", "graph": "whole step, one CUDA graph",
                        "pairs_per_step": pairs, "contacts_last_step": last["contacts"],
+                       "clearance_cache": {"pairs_skipped_per_step": skipped, "entries_last_step": caches[-1]["entries"]},
                        "wall_contacts_last_step": last["wall_contacts"], "segments_last_step": last["segments"],
                        "load_s": load_s, "preroll_s": preroll_s},
             "e2e": {"value": steps / sum(e2e), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},

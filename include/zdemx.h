@@ -258,7 +258,7 @@ int zdx_scene_step_graph(zdx_ctx* ctx, int nsteps);
 /* Initial capacities of the graph step (0 keeps a default): candidate pairs, contacts, arena segments,
  * segments of one pair.  Growth on overflow still applies; call before the first graph step. */
 int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t contacts, int64_t segments, int seg_per_pair);
-/* The graph step's clearance cache (no reference counterpart; config key contact_cache, default 0): a
+/* The graph step's clearance cache (no reference counterpart; config key contact_cache, default 1): a
  * candidate pair whose triangle stage found no segment keeps a clearance M with the two poses; while
  * the vertices of the two bodies have moved by at most mu_A + mu_B < M since (mu <= |x - x0| +
  * 2 R min(|q - q0|, |q + q0|), R the mesh's bounding radius), the pair is known to have no segment and

@@ -55,9 +55,9 @@ struct SimConfig {
     // with the zdem tangential, damping and Coulomb terms
     int force_law = 0;
     double feng_k = 1e7;
-    // addition: 1 lets the CUDA-graph step skip a candidate pair while a clearance it certified
-    // at an earlier step still holds (no segment either way); 0 (default) tests every candidate pair every step
-    int contact_cache = 0;
+    // addition: 1 (default) lets the CUDA-graph step skip a candidate pair while a clearance it certified
+    // at an earlier step still holds (no segment either way); 0 tests every candidate pair every step
+    int contact_cache = 1;
 };
 
 // parse_config_file, src/main.cpp:1531-1689 (same grammar, defaults and acceptance rule).
