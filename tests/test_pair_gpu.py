@@ -143,13 +143,17 @@ def test_capacity_is_reported_not_truncated(ctx):
 
 
 def test_polyline_mode_matches_oracle_and_python_reference(ctx, oracle):
-    from zdemx import polyline
+    """The mirror's pair call in the C++ program's arithmetic (MODE_POLYLINE): bit for bit the oracle's
+    polyline mode, within 1e-9 of polyline.py; in its default, numpy's arithmetic: polyline.py's numbers
+    bit for bit."""
+    from zdemx import _lib, polyline
 
     z = np.load(os.path.join(GOLDEN, "polyline_ref.npz"))
     for ci in range(int(z["ncase"])):
         A, B, pose, tol = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], float(z[f"c{ci}_tol"])
         man, loops, xc0s, cids = polyline.pair_contacts(A, B, pose[0:3], pose[3:7], pose[7:10], pose[10:14], k=1e7,
-                                                        tol=tol, split_contacts=False, ctx=ctx)
+                                                        tol=tol, split_contacts=False, ctx=ctx,
+                                                        mode=_lib.MODE_POLYLINE)
         o = oracle.pair(A, 0.0, 0.0, B, pose[:7], pose[7:], split=False, mode=1, tol=tol)
         e = expected_contacts(o, polyline=True)
         # GPU vs oracle in polyline mode: bit-exact
@@ -165,6 +169,22 @@ def test_polyline_mode_matches_oracle_and_python_reference(ctx, oracle):
         for c, cc in enumerate(man["contacts"]):
             got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"], cc["Fn"], cc["F_A"]]
             assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)
+        _same_as_polyline_py(polyline, z, ci, A, B, pose, tol, False, ctx)
+
+
+def _same_as_polyline_py(polyline, z, ci, A, B, pose, tol, split, ctx):
+    """The default mode against polyline.py's own loops and numbers, bit for bit."""
+    man, loops, _, _ = polyline.pair_contacts(A, B, pose[0:3], pose[3:7], pose[7:10], pose[10:14], k=1e7, tol=tol,
+                                              split_contacts=split, ctx=ctx)
+    lens = list(z[f"c{ci}_loop_len"])
+    assert [len(x) for x in loops] == lens, ci
+    pts = np.split(z[f"c{ci}_loop_pts"], np.cumsum(lens)[:-1]) if lens else []
+    for c, p in enumerate(pts):
+        assert np.array_equal(np.asarray(loops[c]), p), (ci, c)
+    ref = z[f"c{ci}_geom"]
+    for c, cc in enumerate(man["contacts"]):
+        got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"], cc["Fn"], cc["F_A"]]
+        assert np.array_equal(got, ref[c]), (ci, c)
 
 
 def test_polyline_tol_none_is_the_mean_edge_rule(ctx):
@@ -189,14 +209,15 @@ def test_polyline_split_matches_oracle_and_python_reference(ctx, oracle):
     """--split-contacts in polyline mode: components searched in the iteration order of polyline.py's
     candidate sets, so loops start and run as polyline.py's do.  GPU == oracle bit for bit; against
     polyline.py itself (tests/golden/polyline_split_ref.npz) the same components, loops and loop points,
-    numbers within 1e-9."""
-    from zdemx import polyline
+    numbers within 1e-9; in the default numpy arithmetic, polyline.py's numbers bit for bit."""
+    from zdemx import _lib, polyline
 
     z = np.load(os.path.join(GOLDEN, "polyline_split_ref.npz"))
     for ci in range(int(z["ncase"])):
         A, B, pose, tol = z[f"c{ci}_A"], z[f"c{ci}_B"], z[f"c{ci}_pose"], float(z[f"c{ci}_tol"])
         man, loops, xc0s, cids = polyline.pair_contacts(A, B, pose[0:3], pose[3:7], pose[7:10], pose[10:14], k=1e7,
-                                                        tol=tol, split_contacts=True, ctx=ctx)
+                                                        tol=tol, split_contacts=True, ctx=ctx,
+                                                        mode=_lib.MODE_POLYLINE)
         o = oracle.pair(A, 0.0, 0.0, B, pose[:7], pose[7:], split=True, mode=1, tol=tol)
         e = expected_contacts(o, polyline=True)
         assert len(man["contacts"]) == len(e["geom"]), ci
@@ -213,6 +234,7 @@ def test_polyline_split_matches_oracle_and_python_reference(ctx, oracle):
         for c, cc in enumerate(man["contacts"]):
             got = np.r_[cc["Sn"], cc["Gn"], cc["xc0"] or [0, 0, 0], cc["nA"], cc["area"], cc["Fn"], cc["F_A"]]
             assert np.allclose(got, ref[c], rtol=1e-9, atol=1e-9 * np.max(np.abs(ref[c]))), (ci, c)
+        _same_as_polyline_py(polyline, z, ci, A, B, pose, tol, True, ctx)
 
 
 @pytest.mark.parametrize("split,mode", [(True, 0), (False, 0), (False, 1), (True, 1)])

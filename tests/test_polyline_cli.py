@@ -5,8 +5,9 @@ pairs of tests/golden/cli_ref.npz (its argv, stdout and the three VTK files it w
   logic, with the pair call replaced by the counts polyline.py printed, byte for byte on the cases
   without contacts (no segments; segments whose loops all snap away).  With the pair call computed in
   numpy's own arithmetic (the oracle's mode 2), stdout and all three files byte for byte on every case.
-* GPU: the whole command line.  Lines and files are identical except for FP64 numbers, which polyline.py
-  computes with numpy (its own rounding) and which agree within 1e-9 relative."""
+* GPU: the whole command line, its pair call in numpy's arithmetic (the default): stdout and all three
+  files byte for byte.  In the C++ program's arithmetic (MODE_POLYLINE) lines and files are identical
+  except for FP64 numbers, which agree within 1e-9 relative."""
 import contextlib
 import io
 import os
@@ -137,6 +138,22 @@ def test_main_with_numpy_arithmetic_is_byte_identical(tmp_path, monkeypatch, ora
 
 @pytest.mark.gpu
 def test_main_matches_reference(tmp_path):
+    for case in _cases():
+        d = tmp_path / case["name"]
+        d.mkdir()
+        stdout, va, vb, loops = _run_main(case, str(d))
+        assert (va, vb) == (case["vtkA"], case["vtkB"]), case["name"]
+        assert stdout == case["stdout"], case["name"]
+        assert loops == case["loops"], case["name"]
+
+
+@pytest.mark.gpu
+def test_main_in_cpp_arithmetic_agrees_to_1e9(tmp_path, monkeypatch):
+    import functools
+
+    from zdemx import _lib, polyline
+
+    monkeypatch.setattr(polyline, "_pair_call", functools.partial(polyline._pair_call, mode=_lib.MODE_POLYLINE))
     for case in _cases():
         d = tmp_path / case["name"]
         d.mkdir()

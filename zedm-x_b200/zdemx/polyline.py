@@ -12,6 +12,11 @@ stable, nA = -Sn/|Sn| is not flipped, and a loop with |Sn| < 1e-14 is still a co
 With --split-contacts, polyline.py visits each segment's candidates in the iteration order of a Python
 set of ints; the kernel rebuilds CPython 3.12's set table to visit them in the same order, so loops
 start, run and are numbered as polyline.py's.
+
+The pair call computes in numpy's own arithmetic by default (``_lib.MODE_POLYLINE_NUMPY``: numpy's
+dot and norm chains, zdx_npmath.cuh), so the numbers, stdout and VTK files are polyline.py's bit for
+bit; ``mode=_lib.MODE_POLYLINE`` follows the reference C++ program's arithmetic instead (the same loops,
+numbers within 1e-9 of polyline.py's).
 """
 from __future__ import annotations
 
@@ -97,15 +102,18 @@ def tri_normals(tris):
 
 # ---------------------------------------------------------------- the pair call
 def pair_contacts(trisA, trisB, tA=(0.0, 0.0, 0.0), qA=(1.0, 0.0, 0.0, 0.0), tB=(0.0, 0.0, 0.0),
-                  qB=(1.0, 0.0, 0.0, 0.0), k=1.0, tol=1e-6, split_contacts=False, idA=0, idB=1, ctx=None):
+                  qB=(1.0, 0.0, 0.0, 0.0), k=1.0, tol=1e-6, split_contacts=False, idA=0, idB=1, ctx=None,
+                  mode=_lib.MODE_POLYLINE_NUMPY):
     """Contacts between mesh A at pose (tA, qA) and mesh B at (tB, qB), as polyline.py main computes
     them (polyline.py:743-829).  Returns (manifold, loops_pts, xc0s, contact_ids): manifold is the dict
     of build_contacts_from_loops (polyline.py:681-701), the rest what main passes to its writers.
     tol=None takes the snap tolerance as the zdem_cpu step does, from A's mean edge length
-    (src/main.cpp:2118-2121: 0.1 mean edge, else 1 % of the bounding-box diagonal, else 1e-6)."""
+    (src/main.cpp:2118-2121: 0.1 mean edge, else 1 % of the bounding-box diagonal, else 1e-6).
+    mode: _lib.MODE_POLYLINE_NUMPY (numpy's arithmetic, polyline.py's numbers bit for bit) or
+    _lib.MODE_POLYLINE (the C++ program's arithmetic)."""
     if tol is None:
         tol = _mean_edge_tol(trisA)
-    return _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, ctx)[:4]
+    return _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, ctx, mode=mode)[:4]
 
 
 def _mean_edge_tol(tris) -> float:
@@ -121,7 +129,8 @@ def _mean_edge_tol(tris) -> float:
 _COMP_CAP = 16384
 
 
-def _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, ctx, comp_cap=0):
+def _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, ctx, comp_cap=0,
+               mode=_lib.MODE_POLYLINE_NUMPY):
     """pair_contacts, plus the pair's segment and component counts and (comp_cap > 0) the per-component
     counts (segments, snapped vertices, edges, loops) main prints."""
     A = np.ascontiguousarray(trisA, dtype=float).reshape(-1, 3, 3)
@@ -130,7 +139,7 @@ def _pair_call(trisA, trisB, tA, qA, tB, qB, k, tol, split_contacts, idA, idB, c
     off = np.array([0, len(A), len(A) + len(B)], np.int64)
     pose = np.concatenate([np.asarray(tA, float), np.asarray(qA, float), np.asarray(tB, float), np.asarray(qB, float)])
     r = _lib.pair_contacts_raw(ctx or _ctx(), tris, off, np.zeros(2), np.zeros(2), np.array([[0, 1]], np.int32),
-                               pose[None, :], mode=_lib.MODE_POLYLINE, split=split_contacts, tol=tol, k=k,
+                               pose[None, :], mode=mode, split=split_contacts, tol=tol, k=k,
                                want_points=True, comp_cap=comp_cap)
     loops, xc0s, cids = [], [], []
     for c in range(len(r["geom"])):
