@@ -224,6 +224,8 @@ bool parse_config(const std::string& path, SimConfig& cfg, std::string& err) {
             iss >> cfg.feng_k;
         } else if (key == "contact_cache") {
             iss >> cfg.contact_cache;
+        } else if (key == "contact_cache_tau") {
+            iss >> cfg.contact_cache_tau;
         }
         // unknown keys are ignored, as in the reference
     }

@@ -276,8 +276,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     __shared__ unsigned long long sh_base;
     __shared__ int sh_last;
     __shared__ long long sh_ftot;
-    __shared__ unsigned long long sh_cmin, sh_gmin;  // CACHE: smallest cull clearance, smallest box gap (bits)
-    __shared__ int sh_hits, sh_cbad;
+    // CACHE: smallest cull clearance, smallest far box gap (bits); no clearance; near pairs; a re-test hit
+    __shared__ unsigned long long sh_cmin, sh_gmin;
+    __shared__ int sh_cbad, sh_nh, sh_rt;
     extern __shared__ __align__(16) unsigned char k1_dsm[];
     // dynamic shared memory: float boxes | keys | values (the flat path's queue aliases keys+values)
     //                        | group boxes | per-warp overlap queues
@@ -304,8 +305,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
             if constexpr (CACHE) {
                 sh_cmin = dbits(__builtin_huge_val());
                 sh_gmin = dbits(__builtin_huge_val());
-                sh_hits = 0;
                 sh_cbad = 0;
+                sh_nh = 0;
+                sh_rt = 0;
             }
         }
         __syncthreads();
@@ -345,7 +347,10 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
             // A clearance M found at an earlier step still holds while the vertices' displacements since
             // then add up to less than M: a vertex of body s moves by at most |x - x0| + 2 |v| |q - q0|
             // (|R(q) v - R(q0) v| = 2 sin(theta / 2) |v| <= 2 |q - q0| |v| for unit quaternions, |v| <= R).
-            // The pair then has no segment, as when the certificate holds.
+            // M covers every triangle pair but the entry's near pairs, which are tested again here as the
+            // full test does (world corners, plane, strict box compare, tri_tri).  With none of them
+            // meeting, the pair has no segment, as when the certificate holds; otherwise it takes the full
+            // test below.
             const int ci = a.cache_idx ? a.cache_idx[p] : -1;
             if (ci >= 0) {
                 const double* e = a.cache_in + CACHE_W * (int64_t)ci;
@@ -356,18 +361,48 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     mv += norm(tpos[s2] - V3{o[0], o[1], o[2]}) + 2.0 * R[s2] * qdist(qn[s2], q0);
                 }
                 if (mv * (1.0 + 1e-9) + 8.0 * pad < e[0]) {
-                    if (tid == 0) {
-                        a.pair_seg_off[p] = 0;
-                        a.pair_nseg[p] = 0;
-                        a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
-                        a.pair_status[p] = 0;
-                        atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
+                    const int nh = (int)e[CACHE_NH];
+                    const uint32_t* hin = a.cache_hin + CACHE_H * (int64_t)ci;
+                    for (int h = tid; h < nh; h += K1_THREADS) {
+                        const uint32_t code = hin[h];
+                        const int tt[2] = {(int)(code >> 16), (int)(code & 0xffffu)};
+                        V3 W[2][3], n[2];
+                        double d[2];
+                        bool ok = true;
+                        for (int s2 = 0; s2 < 2 && ok; ++s2) {
+                            const double* v = a.tris + 9 * (off[s2] + tt[s2]);
+                            for (int k = 0; k < 3; ++k) W[s2][k] = qrotate_n(qn[s2], ld3(v + 3 * k)) + tpos[s2];
+                            ok = plane_from_tri(W[s2][0], W[s2][1], W[s2][2], n[s2], d[s2]) && !(norm2(n[s2]) < 1e-30);
+                        }
+                        if (!ok) continue;  // a triangle without a plane: the full test drops it
+                        V3 lo[2], hi[2];
+                        for (int s2 = 0; s2 < 2; ++s2) {
+                            lo[s2] = V3{smin3(W[s2][0].x, W[s2][1].x, W[s2][2].x), smin3(W[s2][0].y, W[s2][1].y, W[s2][2].y),
+                                        smin3(W[s2][0].z, W[s2][1].z, W[s2][2].z)};
+                            hi[s2] = V3{smax3(W[s2][0].x, W[s2][1].x, W[s2][2].x), smax3(W[s2][0].y, W[s2][1].y, W[s2][2].y),
+                                        smax3(W[s2][0].z, W[s2][1].z, W[s2][2].z)};
+                        }
+                        const bool sep = hi[0].x < lo[1].x || lo[0].x > hi[1].x || hi[0].y < lo[1].y ||
+                                         lo[0].y > hi[1].y || hi[0].z < lo[1].z || lo[0].z > hi[1].z;
+                        V3 o0, o1;
+                        if (!sep && tri_tri(W[0], n[0], d[0], W[1], n[1], d[1], o0, o1)) sh_rt = 1;
                     }
-                    // the entry carries over unchanged (word 15 marks a skip)
-                    for (int k = tid; k < CACHE_W; k += K1_THREADS)
-                        a.cache_out[CACHE_W * (int64_t)p + k] = k == CACHE_W - 1 ? 1.0 : e[k];
                     __syncthreads();
-                    continue;
+                    if (sh_rt == 0) {
+                        if (tid == 0) {
+                            a.pair_seg_off[p] = 0;
+                            a.pair_nseg[p] = 0;
+                            a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
+                            a.pair_status[p] = 0;
+                            atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
+                        }
+                        // the entry carries over unchanged, marked as a skip
+                        for (int k = tid; k < CACHE_W; k += K1_THREADS)
+                            a.cache_out[CACHE_W * (int64_t)p + k] = k == CACHE_SKIP ? 1.0 : e[k];
+                        for (int h = tid; h < nh; h += K1_THREADS) a.cache_hout[CACHE_H * (int64_t)p + h] = hin[h];
+                        __syncthreads();
+                        continue;
+                    }
                 }
             }
         }
@@ -434,7 +469,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                         double* c = a.cache_out + CACHE_W * (int64_t)p;
                         if (tid == 0) c[0] = sh_slab[1] - sh_slab[0] - sh_slab[2];
                         if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
-                        if (tid == 15) c[15] = 0.0;
+                        if (tid >= 15 && tid < CACHE_W) c[tid] = 0.0;  // not a skip, no near pairs
                     }
                     __syncthreads();
                     continue;
@@ -453,6 +488,10 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         // certificate's argument neither can take part in a segment.
         double cclear = __builtin_huge_val();  // CACHE: smallest clearance of a culled triangle
         bool cbad = false;
+        // CACHE: the culls keep every triangle within tau more of the other body, so that each triangle
+        // they drop has a clearance of at least tau (the extra survivors meet nothing: the culls are
+        // conservative either way)
+        const double tau = CACHE ? a.cache_tau * (R[0] + R[1]) : 0.0;
         for (int s = 0; s < 2; ++s) {
             const V3 other = tpos[1 - s];
             const double lim = R[1 - s] + pad;
@@ -465,6 +504,7 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 // in the mesh frame: A keeps corners reaching lo(B.d) - slack, B corners below hi(A.d) + slack
                 bound = s == 0 ? sh_slab[1] - sh_slab[2] - dot(tpos[0], dslab)
                                : sh_slab[0] + sh_slab[2] - dot(tpos[1], dslab);
+                if constexpr (CACHE) bound = s == 0 ? bound - tau : bound + tau;
             }
             const int t_lo = s == 0 ? a_lo : 0, t_hi = separated ? t_lo : (s == 0 ? a_hi : nt[1]);
             for (int t = t_lo + tid; t < t_hi; t += K1_THREADS) {
@@ -475,7 +515,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     const double p2 = lv[6] * dl.x + lv[7] * dl.y + lv[8] * dl.z;
                     if (s == 0 ? (smax3(p0, p1, p2) < bound) : (smin3(p0, p1, p2) > bound)) {
                         // CACHE: how far the triangle sits outside the slab along d
-                        if constexpr (CACHE) cclear = fmin(cclear, s == 0 ? bound - smax3(p0, p1, p2) : smin3(p0, p1, p2) - bound);
+                        if constexpr (CACHE)
+                            cclear = fmin(cclear, (s == 0 ? bound - smax3(p0, p1, p2) : smin3(p0, p1, p2) - bound) + tau);
                         continue;
                     }
                 }
@@ -484,7 +525,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                     V3 c = V3{sp.x, sp.y, sp.z};
                     V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];
                     double L = sp.w + lim;
-                    if (!(fabs(cw.x - other.x) <= L && fabs(cw.y - other.y) <= L && fabs(cw.z - other.z) <= L)) {
+                    double Lc = L;
+                    if constexpr (CACHE) Lc = L + tau;
+                    if (!(fabs(cw.x - other.x) <= Lc && fabs(cw.y - other.y) <= Lc && fabs(cw.z - other.z) <= Lc)) {
                         // CACHE: how far the triangle's cube misses the other body's, on the widest axis
                         if constexpr (CACHE)
                             cclear = fmin(cclear, smax3(fabs(cw.x - other.x), fabs(cw.y - other.y), fabs(cw.z - other.z)) - L);
@@ -650,9 +693,6 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                         }
                         unsigned hb = __ballot_sync(FULL, hit);
                         if (hit) wq[wq_n + __popc(hb & ((1u << lane) - 1u))] = make_int2(ia, ib);
-                        if constexpr (CACHE) {
-                            if (hit) sh_hits = 1;
-                        }
                         wq_n += __popc(hb);
                         if (wq_n >= 32) {
                             __syncwarp();
@@ -684,7 +724,6 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                                    bA[4 * sA + ia] < bB[1 * sB + ib] || bA[1 * sA + ia] > bB[4 * sB + ib] ||
                                    bA[5 * sA + ia] < bB[2 * sB + ib] || bA[2 * sA + ia] > bB[5 * sB + ib];
                         if (!sep) {
-                            if constexpr (CACHE) sh_hits = 1;
                             int qi = atomicAdd(&sh_nq, 1);
                             sh_q[qi] = make_int2(ia, ib);
                         }
@@ -705,11 +744,13 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
             }
         }
         if constexpr (CACHE) {
-            // the pair's clearance: none unless no box met (so no segment) and no triangle lacked a plane;
-            // then the smaller of the culled triangles' clearances and the survivors' smallest box gap
-            // (the largest separation over the axes, for each pair of survivor boxes)
+            // the pair's clearance: none with a segment or a triangle without a plane.  Survivor pairs whose
+            // boxes are less than tau apart (those that met included) become the entry's near pairs,
+            // tested again at every skip; the clearance is the smallest of the culled triangles' and of
+            // the other pairs' box gaps (the largest separation over the axes), at least tau
             __syncthreads();
-            const bool ok = sh_hits == 0 && sh_nseg == 0 && sh_cbad == 0 && !separated;
+            const bool ok = sh_nseg == 0 && sh_cbad == 0 && !separated;
+            uint32_t* hout = a.cache_hout + CACHE_H * (int64_t)p;
             if (ok && nA > 0 && nB > 0) {
                 double g = __builtin_huge_val();
                 for (int64_t q = tid; q < total; q += K1_THREADS) {
@@ -719,12 +760,16 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                         gq = fmax(gq, bB[k * sB + ib] - bA[(3 + k) * sA + ia]);
                         gq = fmax(gq, bA[k * sA + ia] - bB[(3 + k) * sB + ib]);
                     }
-                    g = fmin(g, gq);
+                    if (gq < tau) {
+                        const int ta = SA.id[ia], tb = SB.id[ib];
+                        const int h = atomicAdd(&sh_nh, 1);
+                        if (ta < 65536 && tb < 65536 && h < CACHE_H) hout[h] = (uint32_t)ta << 16 | (uint32_t)tb;
+                        else sh_cbad = 1;
+                    } else {
+                        g = fmin(g, gq);
+                    }
                 }
-                if (g < __builtin_huge_val()) {
-                    if (g > 0.0) atomicMin(&sh_gmin, dbits(g));
-                    else sh_cbad = 1;
-                }
+                if (g < __builtin_huge_val()) atomicMin(&sh_gmin, dbits(g));
             }
             __syncthreads();
             double* c = a.cache_out + CACHE_W * (int64_t)p;
@@ -733,7 +778,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 c[0] = (ok && sh_cbad == 0 && m > 0.0) ? m : -1.0;
             }
             if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
-            if (tid == 15) c[15] = 0.0;
+            if (tid == CACHE_SKIP) c[CACHE_SKIP] = 0.0;
+            if (tid == CACHE_NH) c[CACHE_NH] = (double)(sh_nh < CACHE_H ? sh_nh : CACHE_H);
+            if (tid > CACHE_NH && tid < CACHE_W) c[tid] = 0.0;
         }
         int ns = sh_nseg;
         int status = 0;
@@ -853,7 +900,7 @@ void launch_segments(const PairArgs& a, int grid, cudaStream_t s) {
         cudaFuncSetAttribute(k_segments<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
         cudaFuncSetAttribute(k_segments<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         k_segments<true, false><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);
-    } else if (a.cache_out && !a.items) {
+    } else if (a.cache_out && !a.items && a.mode == 0) {
         cudaFuncSetAttribute(k_segments<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_DSMEM);
         cudaFuncSetAttribute(k_segments<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         k_segments<false, true><<<grid, K1_THREADS, K1_DSMEM, s>>>(a);

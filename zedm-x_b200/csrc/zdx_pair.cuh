@@ -120,17 +120,26 @@ struct PairArgs {
     // the T-junction split, in component order
     int32_t* comp_stats;
     int64_t comp_stats_cap;
-    // Clearance cache of a DEM step (null cache_out: none; pairs are never split then).  An entry is
-    // CACHE_W doubles: a clearance M > 0, then the pair's 14 pose values when M was found.  M certifies that
-    // the pair has no segment as long as every vertex of A has moved by at most mu_A and every vertex of B
-    // by mu_B with mu_A + mu_B < M (less the rounding allowance).  cache_idx[p] >= 0 names the entry of
-    // cache_in found for pair p, which k_segments uses to skip the pair while it holds; cache_out receives
-    // each pair's entry for the next step (M <= 0: none).
+    // Clearance cache of a DEM step (null cache_out: none; pairs are never split then; zdem mode).  An
+    // entry is CACHE_W doubles: a clearance M > 0, the pair's 14 pose values when M was found, a skip
+    // mark (1: carried over by a skip) and the count of its near pairs, plus CACHE_H codes (ta << 16 | tb)
+    // of those near pairs in the parallel cache_h* arrays.  M certifies that no other triangle pair of
+    // the pair can yield a segment as long as every vertex of A has moved by at most mu_A and every
+    // vertex of B by mu_B with mu_A + mu_B < M (less the rounding allowance); the near pairs are tested
+    // again.  cache_idx[p] >= 0 names the entry of cache_in found for pair p, which k_segments uses to
+    // skip the pair while it holds; cache_out / cache_hout receive each pair's entry for the next step
+    // (M <= 0: none).  cache_tau (times R_A + R_B) is the box gap below which a survivor pair is near.
     const int32_t* cache_idx;
     const double* cache_in;
     double* cache_out;
+    const uint32_t* cache_hin;
+    uint32_t* cache_hout;
+    double cache_tau;
 };
-constexpr int CACHE_W = 16;
+constexpr int CACHE_W = 18;
+constexpr int CACHE_SKIP = 15;  // entry word: skip mark
+constexpr int CACHE_NH = 16;    // entry word: near pairs
+constexpr int CACHE_H = 128;    // near pairs an entry holds at most
 
 // Bytes of one rebuild slot able to hold a pair of n segments.
 size_t rebuild_slot_bytes(int n);

@@ -1374,27 +1374,31 @@ __global__ void k_cache_flags(const double* cout, int64_t cap, const int64_t* n_
     const bool live = p < n;
     const bool f = live && cout[CACHE_W * p] > 0.0;
     if (p < cap) flag[p] = f ? 1 : 0;
-    const unsigned b = __ballot_sync(FULLM, live && cout[CACHE_W * p + 15] != 0.0);
+    const unsigned b = __ballot_sync(FULLM, live && cout[CACHE_W * p + CACHE_SKIP] != 0.0);
     if ((threadIdx.x & 31) == 0 && b)
         atomicAdd(reinterpret_cast<unsigned long long*>(&g->cache_skipped), (unsigned long long)__popc(b));
 }
 __global__ void k_cache_write(const int32_t* flag, const int64_t* pos, int64_t cap, const int64_t* n_dev, const int2* pairs,
-                              const double* cout, int64_t* ckey2, double* cval2) {
+                              const double* cout, const uint32_t* hout, int64_t* ckey2, double* cval2, uint32_t* chit2) {
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= dev_count(cap, n_dev) || !flag[p]) return;
     const int64_t o = pos[p];
     ckey2[o] = ((int64_t)pairs[p].x << 32) | (int64_t)(uint32_t)pairs[p].y;
     for (int k = 0; k < CACHE_W; ++k) cval2[CACHE_W * o + k] = cout[CACHE_W * p + k];
+    const int nh = (int)cout[CACHE_W * p + CACHE_NH];
+    for (int h = 0; h < nh; ++h) chit2[CACHE_H * o + h] = hout[CACHE_H * p + h];
 }
 // with the step complete, the next step's entries become the cache
 __global__ void k_cache_commit(GraphCounts* g, const int64_t* pos, const int64_t* ckey2, const double* cval2,
-                               int64_t* ckey, double* cval) {
+                               const uint32_t* chit2, int64_t* ckey, double* cval, uint32_t* chit) {
     if (g->flags) return;
     const int64_t n = pos[g->npair];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += stride) {
         ckey[k] = ckey2[k];
         for (int c = 0; c < CACHE_W; ++c) cval[CACHE_W * k + c] = cval2[CACHE_W * k + c];
+        const int nh = (int)cval2[CACHE_W * k + CACHE_NH];
+        for (int h = 0; h < nh; ++h) chit[CACHE_H * k + h] = chit2[CACHE_H * k + h];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) g->ncache = n;
 }
@@ -1495,6 +1499,9 @@ static int graph_alloc(zdx_ctx* ctx, Scene& s) {
     CKS(G.cout.ensure(sizeof(double) * CACHE_W * P1));
     CKS(G.cflag.ensure(sizeof(int32_t) * P1));
     CKS(G.cscan.ensure(sizeof(int64_t) * (P1 + 1)));
+    CKS(G.chit.ensure(sizeof(uint32_t) * CACHE_H * P1));
+    CKS(G.chit2.ensure(sizeof(uint32_t) * CACHE_H * P1));
+    CKS(G.chout.ensure(sizeof(uint32_t) * CACHE_H * P1));
     CKS(cudaMemsetAsync(&as<GraphCounts>(G.g)->ncache, 0, sizeof(int64_t), ctx->stream));
     // pair kernels
     const int64_t total_tris = s.mesh_off.back();
@@ -1636,6 +1643,9 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
             a.cache_idx = as<int32_t>(G.cidx);
             a.cache_in = as<double>(G.cval);
             a.cache_out = as<double>(G.cout);
+            a.cache_hin = as<uint32_t>(G.chit);
+            a.cache_hout = as<uint32_t>(G.chout);
+            a.cache_tau = s.cfg.contact_cache_tau;
         }
         launch_segments(a, G.k1_grid, st);
         if (cache) {
@@ -1643,8 +1653,8 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
             k_cache_flags<<<grid(G.pcap), 256, 0, st>>>(as<double>(G.cout), G.pcap, npair, as<int32_t>(G.cflag), g);
             CKS(scan_offsets<int32_t>(as<int32_t>(G.cflag), G.pcap, npair, as<int64_t>(G.cscan), G.scan_tmp.p, st));
             k_cache_write<<<grid(G.pcap), 256, 0, st>>>(as<int32_t>(G.cflag), as<int64_t>(G.cscan), G.pcap, npair,
-                                                        as<int2>(G.bp_pairs), as<double>(G.cout), as<int64_t>(G.ckey2),
-                                                        as<double>(G.cval2));
+                                                        as<int2>(G.bp_pairs), as<double>(G.cout), as<uint32_t>(G.chout),
+                                                        as<int64_t>(G.ckey2), as<double>(G.cval2), as<uint32_t>(G.chit2));
         }
         a.k2_nmax = G.cap_seg;
         a.k2_slot_bytes = rebuild_slot_bytes(G.cap_seg);
@@ -1723,8 +1733,9 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
                                                            as<int64_t>(G.whkey2), as<double>(G.whds2));
     if (s.cfg.contact_cache)
         k_cache_commit<<<std::max(1, ctx->num_sms), 256, 0, st>>>(g, as<int64_t>(G.cscan), as<int64_t>(G.ckey2),
-                                                                    as<double>(G.cval2), as<int64_t>(G.ckey),
-                                                                    as<double>(G.cval));
+                                                                    as<double>(G.cval2), as<uint32_t>(G.chit2),
+                                                                    as<int64_t>(G.ckey), as<double>(G.cval),
+                                                                    as<uint32_t>(G.chit));
     CKS(cudaGetLastError());
     return ZDX_OK;
 }
