@@ -116,21 +116,29 @@ __device__ __forceinline__ int64_t pairs_of(const PairArgs& a) {
     return d < a.n_pairs ? d : a.n_pairs;
 }
 __device__ __forceinline__ int64_t item_end_of(const PairArgs& a) {
-    if (!a.n_dev) return a.item_end;
-    const int64_t d = a.item_begin + *a.n_dev;
-    return d < a.item_end ? d : a.item_end;
+    int64_t r = a.item_end;
+    if (a.n_dev) {
+        const int64_t d = a.item_begin + *a.n_dev;
+        r = d < r ? d : r;
+    }
+    if (a.order_count) {
+        const int64_t c = a.item_begin + *a.order_count;
+        r = c < r ? c : r;
+    }
+    return r;
 }
 
 __global__ void k_cost_count(PairArgs a, int* buckets) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= pairs_of(a)) return;
+    if (a.cache_skip && a.cache_skip[p]) return;
     int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
     unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
                            (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
     int b = 63 - __clzll(c + 1);
     atomicAdd(buckets + (63 - b), 1);
 }
-__global__ void k_cost_scan(int* buckets) {
+__global__ void k_cost_scan(int* buckets, int* count) {
     if (threadIdx.x != 0) return;
     int run = 0;
     for (int i = 0; i < 64; ++i) {
@@ -138,10 +146,12 @@ __global__ void k_cost_scan(int* buckets) {
         buckets[64 + i] = run;
         run += c;
     }
+    if (count) *count = run;  // pairs in the order
 }
 __global__ void k_cost_scatter(PairArgs a, int* buckets, int32_t* order) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= pairs_of(a)) return;
+    if (a.cache_skip && a.cache_skip[p]) return;
     int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
     unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
                            (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
@@ -154,7 +164,7 @@ void launch_cost_order(const PairArgs& a, int32_t* order, int* buckets, cudaStre
     unsigned blocks = (unsigned)((a.n_pairs + 255) / 256);
     cudaMemsetAsync(buckets, 0, sizeof(int) * 128, s);
     k_cost_count<<<blocks, 256, 0, s>>>(a, buckets);
-    k_cost_scan<<<1, 32, 0, s>>>(buckets);
+    k_cost_scan<<<1, 32, 0, s>>>(buckets, a.order_count);
     k_cost_scatter<<<blocks, 256, 0, s>>>(a, buckets, order);
 }
 
@@ -276,9 +286,9 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
     __shared__ unsigned long long sh_base;
     __shared__ int sh_last;
     __shared__ long long sh_ftot;
-    // CACHE: smallest cull clearance, smallest far box gap (bits); no clearance; near pairs; a re-test hit
+    // CACHE: smallest cull clearance, smallest far box gap (bits); no clearance; near pairs
     __shared__ unsigned long long sh_cmin, sh_gmin;
-    __shared__ int sh_cbad, sh_nh, sh_rt;
+    __shared__ int sh_cbad, sh_nh;
     extern __shared__ __align__(16) unsigned char k1_dsm[];
     // dynamic shared memory: float boxes | keys | values (the flat path's queue aliases keys+values)
     //                        | group boxes | per-warp overlap queues
@@ -307,7 +317,6 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                 sh_gmin = dbits(__builtin_huge_val());
                 sh_cbad = 0;
                 sh_nh = 0;
-                sh_rt = 0;
             }
         }
         __syncthreads();
@@ -343,70 +352,6 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                              __longlong_as_double((long long)a.mesh_R_bits[mesh[1]])};
         auto inf = [](V3 v) { return smax3(fabs(v.x), fabs(v.y), fabs(v.z)); };
         const double pad = 1e-9 * (inf(tpos[0]) + inf(tpos[1]) + R[0] + R[1]);
-        if constexpr (CACHE) {
-            // A clearance M found at an earlier step still holds while the vertices' displacements since
-            // then add up to less than M: a vertex of body s moves by at most |x - x0| + 2 |v| |q - q0|
-            // (|R(q) v - R(q0) v| = 2 sin(theta / 2) |v| <= 2 |q - q0| |v| for unit quaternions, |v| <= R).
-            // M covers every triangle pair but the entry's near pairs, which are tested again here as the
-            // full test does (world corners, plane, strict box compare, tri_tri).  With none of them
-            // meeting, the pair has no segment, as when the certificate holds; otherwise it takes the full
-            // test below.
-            const int ci = a.cache_idx ? a.cache_idx[p] : -1;
-            if (ci >= 0) {
-                const double* e = a.cache_in + CACHE_W * (int64_t)ci;
-                double mv = 0.0;
-                for (int s2 = 0; s2 < 2; ++s2) {
-                    const double* o = e + 1 + 7 * s2;
-                    const Q4 q0 = qnormalize(Q4{o[3], o[4], o[5], o[6]});
-                    mv += norm(tpos[s2] - V3{o[0], o[1], o[2]}) + 2.0 * R[s2] * qdist(qn[s2], q0);
-                }
-                if (mv * (1.0 + 1e-9) + 8.0 * pad < e[0]) {
-                    const int nh = (int)e[CACHE_NH];
-                    const uint32_t* hin = a.cache_hin + CACHE_H * (int64_t)ci;
-                    for (int h = tid; h < nh; h += K1_THREADS) {
-                        const uint32_t code = hin[h];
-                        const int tt[2] = {(int)(code >> 16), (int)(code & 0xffffu)};
-                        V3 W[2][3], n[2];
-                        double d[2];
-                        bool ok = true;
-                        for (int s2 = 0; s2 < 2 && ok; ++s2) {
-                            const double* v = a.tris + 9 * (off[s2] + tt[s2]);
-                            for (int k = 0; k < 3; ++k) W[s2][k] = qrotate_n(qn[s2], ld3(v + 3 * k)) + tpos[s2];
-                            ok = plane_from_tri(W[s2][0], W[s2][1], W[s2][2], n[s2], d[s2]) && !(norm2(n[s2]) < 1e-30);
-                        }
-                        if (!ok) continue;  // a triangle without a plane: the full test drops it
-                        V3 lo[2], hi[2];
-                        for (int s2 = 0; s2 < 2; ++s2) {
-                            lo[s2] = V3{smin3(W[s2][0].x, W[s2][1].x, W[s2][2].x), smin3(W[s2][0].y, W[s2][1].y, W[s2][2].y),
-                                        smin3(W[s2][0].z, W[s2][1].z, W[s2][2].z)};
-                            hi[s2] = V3{smax3(W[s2][0].x, W[s2][1].x, W[s2][2].x), smax3(W[s2][0].y, W[s2][1].y, W[s2][2].y),
-                                        smax3(W[s2][0].z, W[s2][1].z, W[s2][2].z)};
-                        }
-                        const bool sep = hi[0].x < lo[1].x || lo[0].x > hi[1].x || hi[0].y < lo[1].y ||
-                                         lo[0].y > hi[1].y || hi[0].z < lo[1].z || lo[0].z > hi[1].z;
-                        V3 o0, o1;
-                        if (!sep && tri_tri(W[0], n[0], d[0], W[1], n[1], d[1], o0, o1)) sh_rt = 1;
-                    }
-                    __syncthreads();
-                    if (sh_rt == 0) {
-                        if (tid == 0) {
-                            a.pair_seg_off[p] = 0;
-                            a.pair_nseg[p] = 0;
-                            a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
-                            a.pair_status[p] = 0;
-                            atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
-                        }
-                        // the entry carries over unchanged, marked as a skip
-                        for (int k = tid; k < CACHE_W; k += K1_THREADS)
-                            a.cache_out[CACHE_W * (int64_t)p + k] = k == CACHE_SKIP ? 1.0 : e[k];
-                        for (int h = tid; h < nh; h += K1_THREADS) a.cache_hout[CACHE_H * (int64_t)p + h] = hin[h];
-                        __syncthreads();
-                        continue;
-                    }
-                }
-            }
-        }
-
         // Separation certificate along the line of centres d: every point of A lies below the largest
         // corner projection max_v (v.d) of A's triangles, every point of B above B's smallest one.  A
         // segment endpoint is on an edge of one body (seg_plane clamps t to [0, 1], src/main.cpp:545-559)
@@ -888,6 +833,97 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
         }
         __syncthreads();
     }
+}
+
+// A clearance M found at an earlier step still holds while the vertices' displacements since then add
+// up to less than M: a vertex of body s moves by at most |x - x0| + 2 |v| |q - q0| (|R(q) v - R(q0) v| =
+// 2 sin(theta / 2) |v| <= 2 |q - q0| |v| for unit quaternions, |v| <= R).  M covers every triangle pair
+// but the entry's near pairs, which are tested again as the full test does (world corners, plane,
+// strict box compare, tri_tri).  With none of them meeting, the pair has no segment, as when the
+// separation certificate holds; otherwise k_segments tests it in full.  Warp per pair, lanes over the
+// near pairs.
+__global__ void k_cache_skip(PairArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t n = pairs_of(a);
+    for (int64_t p = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); p < n; p += warps) {
+        const int ci = a.cache_idx[p];
+        bool skip = false;
+        if (ci >= 0) {
+            const double* ps = a.pose + 14 * p;
+            const V3 tpos[2] = {V3{ps[0], ps[1], ps[2]}, V3{ps[7], ps[8], ps[9]}};
+            const Q4 qn[2] = {qnormalize(Q4{ps[3], ps[4], ps[5], ps[6]}), qnormalize(Q4{ps[10], ps[11], ps[12], ps[13]})};
+            const int mesh[2] = {a.pmesh[2 * p], a.pmesh[2 * p + 1]};
+            const double R[2] = {__longlong_as_double((long long)a.mesh_R_bits[mesh[0]]),
+                                 __longlong_as_double((long long)a.mesh_R_bits[mesh[1]])};
+            auto inf = [](V3 v) { return smax3(fabs(v.x), fabs(v.y), fabs(v.z)); };
+            const double pad = 1e-9 * (inf(tpos[0]) + inf(tpos[1]) + R[0] + R[1]);
+            const double* e = a.cache_in + CACHE_W * (int64_t)ci;
+            double mv = 0.0;
+            for (int s2 = 0; s2 < 2; ++s2) {
+                const double* o = e + 1 + 7 * s2;
+                const Q4 q0 = qnormalize(Q4{o[3], o[4], o[5], o[6]});
+                mv += norm(tpos[s2] - V3{o[0], o[1], o[2]}) + 2.0 * R[s2] * qdist(qn[s2], q0);
+            }
+            if (mv * (1.0 + 1e-9) + 8.0 * pad < e[0]) {
+                const int nh = (int)e[CACHE_NH];
+                const uint32_t* hin = a.cache_hin + CACHE_H * (int64_t)ci;
+                const int64_t off[2] = {a.tri_off[mesh[0]], a.tri_off[mesh[1]]};
+                bool meet = false;
+                for (int h = lane; h < nh; h += 32) {
+                    const uint32_t code = hin[h];
+                    const int tt[2] = {(int)(code >> 16), (int)(code & 0xffffu)};
+                    V3 W[2][3], nv[2];
+                    double d[2];
+                    bool ok = true;
+                    for (int s2 = 0; s2 < 2 && ok; ++s2) {
+                        const double* v = a.tris + 9 * (off[s2] + tt[s2]);
+                        for (int k = 0; k < 3; ++k) W[s2][k] = qrotate_n(qn[s2], ld3(v + 3 * k)) + tpos[s2];
+                        ok = plane_from_tri(W[s2][0], W[s2][1], W[s2][2], nv[s2], d[s2]) && !(norm2(nv[s2]) < 1e-30);
+                    }
+                    if (!ok) continue;  // a triangle without a plane: the full test drops it
+                    V3 lo[2], hi[2];
+                    for (int s2 = 0; s2 < 2; ++s2) {
+                        lo[s2] = V3{smin3(W[s2][0].x, W[s2][1].x, W[s2][2].x), smin3(W[s2][0].y, W[s2][1].y, W[s2][2].y),
+                                    smin3(W[s2][0].z, W[s2][1].z, W[s2][2].z)};
+                        hi[s2] = V3{smax3(W[s2][0].x, W[s2][1].x, W[s2][2].x), smax3(W[s2][0].y, W[s2][1].y, W[s2][2].y),
+                                    smax3(W[s2][0].z, W[s2][1].z, W[s2][2].z)};
+                    }
+                    const bool sep = hi[0].x < lo[1].x || lo[0].x > hi[1].x || hi[0].y < lo[1].y || lo[0].y > hi[1].y ||
+                                     hi[0].z < lo[1].z || lo[0].z > hi[1].z;
+                    V3 o0, o1;
+                    if (!sep && tri_tri(W[0], nv[0], d[0], W[1], nv[1], d[1], o0, o1)) meet = true;
+                }
+                skip = !__any_sync(FULL, meet);
+                if (skip) {
+                    const int nt1 = (int)(a.tri_off[mesh[1] + 1] - off[1]);
+                    if (lane == 0) {
+                        const int64_t checks = (int64_t)a.mesh_valid[mesh[0]] * nt1;
+                        a.pair_seg_off[p] = 0;
+                        a.pair_nseg[p] = 0;
+                        a.pair_checks[p] = checks;
+                        a.pair_status[p] = 0;
+                        atomicAdd(a.checks_total, (unsigned long long)checks);
+                        // what the rebuild writes for a pair without segments
+                        a.pair_stage_off[p] = 0;
+                        a.pair_pts_stage_off[p] = 0;
+                        a.pair_ncontact[p] = 0;
+                        a.pair_npts[p] = 0;
+                        a.pair_ncomp[p] = 0;
+                        a.pair_nloop[p] = 0;
+                    }
+                    // the entry carries over unchanged, marked as a skip
+                    if (lane < CACHE_W) a.cache_out[CACHE_W * p + lane] = lane == CACHE_SKIP ? 1.0 : e[lane];
+                    for (int h = lane; h < nh; h += 32) a.cache_hout[CACHE_H * p + h] = hin[h];
+                }
+            }
+        }
+        if (lane == 0) a.cache_skip[p] = skip ? 1 : 0;
+    }
+}
+
+void launch_cache_skip(const PairArgs& a, int grid, cudaStream_t s) {
+    if (grid > 0) k_cache_skip<<<grid, 256, 0, s>>>(a);
 }
 
 void launch_segments(const PairArgs& a, int grid, cudaStream_t s) {

@@ -135,6 +135,10 @@ struct PairArgs {
     const uint32_t* cache_hin;
     uint32_t* cache_hout;
     double cache_tau;
+    // per pair, 1 when launch_cache_skip settled it from its entry (no segment); the cost order then
+    // leaves it out and writes the count of the pairs it holds to order_count (null: every pair)
+    int32_t* cache_skip;
+    int* order_count;
 };
 constexpr int CACHE_W = 18;
 constexpr int CACHE_SKIP = 15;  // entry word: skip mark
@@ -166,6 +170,10 @@ size_t tritest_slot_bytes(int cap_side, int cap_seg);
 void launch_mesh_prep(const PairArgs& a, int64_t total_tris, cudaStream_t s);
 void launch_cost_order(const PairArgs& a, int32_t* order, int* buckets, cudaStream_t s);
 void launch_segments(const PairArgs& a, int grid, cudaStream_t s);
+// The clearance cache's skips, before the cost order: a warp per pair with an entry tests its motion
+// against the clearance and its near pairs again; a pair settled so gets the outputs of a pair without
+// segments (triangle stage and rebuild), its entry carried over, and cache_skip[p] = 1.
+void launch_cache_skip(const PairArgs& a, int grid, cudaStream_t s);
 void launch_rebuild(const PairArgs& a, int warps, int warps_per_block, cudaStream_t s);
 void launch_gather(const PairArgs& a, int64_t* pair_contact_off, int64_t* pair_pts_off, double* cgeom,
                    int32_t* cinfo, double* pts, int64_t* cpt_off, int32_t* pair_stats, int64_t* ctape_off,

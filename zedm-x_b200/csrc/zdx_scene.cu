@@ -1502,6 +1502,7 @@ static int graph_alloc(zdx_ctx* ctx, Scene& s) {
     CKS(G.chit.ensure(sizeof(uint32_t) * CACHE_H * P1));
     CKS(G.chit2.ensure(sizeof(uint32_t) * CACHE_H * P1));
     CKS(G.chout.ensure(sizeof(uint32_t) * CACHE_H * P1));
+    CKS(G.cskip.ensure(sizeof(int32_t) * P1));
     CKS(cudaMemsetAsync(&as<GraphCounts>(G.g)->ncache, 0, sizeof(int64_t), ctx->stream));
     // pair kernels
     const int64_t total_tris = s.mesh_off.back();
@@ -1631,6 +1632,17 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
         CKS(cudaMemsetAsync(G.mesh_infl.p, 0, sizeof(unsigned long long) * std::max(nm, 1), st));
         a.mesh_infl_bits = as<unsigned long long>(G.mesh_infl);
         launch_mesh_prep(a, s.mesh_off.back(), st);
+        if (cache) {
+            a.cache_idx = as<int32_t>(G.cidx);
+            a.cache_in = as<double>(G.cval);
+            a.cache_out = as<double>(G.cout);
+            a.cache_hin = as<uint32_t>(G.chit);
+            a.cache_hout = as<uint32_t>(G.chout);
+            a.cache_tau = s.cfg.contact_cache_tau;
+            a.cache_skip = as<int32_t>(G.cskip);
+            a.order_count = reinterpret_cast<int*>(cnt + 8);
+            launch_cache_skip(a, std::max(1, ctx->num_sms) * 8, st);
+        }
         launch_cost_order(a, as<int32_t>(G.order), as<int>(G.buckets), st);
         a.order = as<int32_t>(G.order);
         a.item_begin = 0;
@@ -1639,14 +1651,6 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
         a.k1_slots = as<char>(G.k1_slots);
         a.seg = as<double>(G.seg_arena);
         a.seg_cap = G.segcap;
-        if (cache) {
-            a.cache_idx = as<int32_t>(G.cidx);
-            a.cache_in = as<double>(G.cval);
-            a.cache_out = as<double>(G.cout);
-            a.cache_hin = as<uint32_t>(G.chit);
-            a.cache_hout = as<uint32_t>(G.chout);
-            a.cache_tau = s.cfg.contact_cache_tau;
-        }
         launch_segments(a, G.k1_grid, st);
         if (cache) {
             // the next step's cache: this step's clearances, in pair order (the keys stay sorted)

@@ -60,7 +60,7 @@ struct SimConfig {
     int contact_cache = 1;
     // addition: the cache's near-pair margin, relative to R_A + R_B (survivor pairs with boxes closer than
     // that are tested again at each skip; the others and the culled triangles set the clearance)
-    double contact_cache_tau = 0.01;
+    double contact_cache_tau = 0.005;
 };
 
 // parse_config_file, src/main.cpp:1531-1689 (same grammar, defaults and acceptance rule).
@@ -119,7 +119,7 @@ struct GraphStep {
     DevBuf w_active, w_scan, w_pairs, w_contrib, w_valid, w_act, w_ds, w_hscan, w_scratch;
     DevBuf hkey, hds, hkey2, hds2, whkey, whds, whkey2, whds2;
     // clearance cache: sorted pair keys and entries (PairArgs::cache_*), the next step's, per-pair lookups
-    DevBuf ckey, cval, ckey2, cval2, cidx, cout, cflag, cscan, chit, chit2, chout;
+    DevBuf ckey, cval, ckey2, cval2, cidx, cout, cflag, cscan, chit, chit2, chout, cskip;
     // pair kernels' workspaces
     DevBuf tri_sph, mesh_R, mesh_valid, mesh_infl, order, buckets, pair_i64, pair_i32, counters, k1_slots, seg_arena, k2_slots,
         cstage, cistage;
@@ -129,7 +129,7 @@ struct GraphStep {
                 &bp_pairs, &bp_pstart, &rs_tmp, &scan_tmp, &tr_key, &tr_idx, &tr_key2, &tr_idx2, &tr_start, &pr_mesh,
                 &pr_pose, &pr_coff, &pr_stats, &pr_geom, &pr_info, &pr_contrib, &pr_active, &pr_ds, &pr_hscan,
                 &w_active, &w_scan, &w_pairs, &w_contrib, &w_valid, &w_act, &w_ds, &w_hscan, &w_scratch, &hkey, &hds,
-                &hkey2, &hds2, &whkey, &whds, &whkey2, &whds2, &ckey, &cval, &ckey2, &cval2, &cidx, &cout, &cflag, &chit, &chit2, &chout,
+                &hkey2, &hds2, &whkey, &whds, &whkey2, &whds2, &ckey, &cval, &ckey2, &cval2, &cidx, &cout, &cflag, &chit, &chit2, &chout, &cskip,
                 &cscan, &tri_sph, &mesh_R, &mesh_valid, &mesh_infl, &order, &buckets,
                 &pair_i64, &pair_i32, &counters, &k1_slots, &seg_arena, &k2_slots, &cstage, &cistage};
     }
