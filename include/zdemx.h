@@ -258,12 +258,12 @@ int zdx_scene_step_graph(zdx_ctx* ctx, int nsteps);
 /* Initial capacities of the graph step (0 keeps a default): candidate pairs, contacts, arena segments,
  * segments of one pair.  Growth on overflow still applies; call before the first graph step. */
 int zdx_scene_graph_reserve(zdx_ctx* ctx, int64_t pairs, int64_t contacts, int64_t segments, int seg_per_pair);
-/* The graph step's clearance cache (no reference counterpart; config key contact_cache, default 1): a
- * candidate pair whose triangle stage found no segment keeps a clearance M with the two poses and its
- * near triangle pairs (boxes closer than contact_cache_tau x (R_A + R_B)); while the vertices of the
- * two bodies have moved by at most mu_A + mu_B < M since (mu <= |x - x0| + 2 R min(|q - q0|, |q + q0|),
- * R the mesh's bounding radius) and none of the near pairs meets, the pair is known to have no segment
- * and its triangle stage is skipped.  Results are those of the step without the cache, bit for bit.
+/* The graph step's clearance cache (no reference counterpart; config key contact_cache, default 1; in
+ * scenes of 256 particles or more): a candidate pair whose triangle stage found no segment keeps a
+ * clearance M with the two poses and its near triangle pairs (boxes closer than contact_cache_tau x
+ * (R_A + R_B)); while the vertices of the two bodies have moved by at most mu_A + mu_B < M since
+ * (mu <= |x - x0| + 2 R min(|q - q0|, |q + q0|), R the mesh's bounding radius) and none of the near
+ * pairs meets, the pair is known to have no segment and its triangle stage is skipped.  Results are those of the step without the cache, bit for bit.
  * *entries: the cache's entries after the last graph step; *skipped: the pairs that step skipped. */
 int zdx_scene_graph_cache(zdx_ctx* ctx, int64_t* entries, int64_t* skipped);
 /* The whole zdem_cpu run after argument parsing (src/main.cpp:1879-2503) on CUDA device `device`:

@@ -1431,6 +1431,11 @@ __global__ void k_g_commit(GraphCounts* g, const int64_t* hscan, const int64_t* 
 
 }  // namespace
 
+// The clearance cache runs in scenes of at least this many particles: in smaller ones its kernels cost
+// more than the few pairs it could settle.
+constexpr int kCacheMinParticles = 256;
+static bool cache_on(const Scene& s) { return s.cfg.contact_cache != 0 && s.np >= kCacheMinParticles; }
+
 // Buffers at the current capacities (pointers the captured graph holds).
 static int graph_alloc(zdx_ctx* ctx, Scene& s) {
     GraphStep& G = s.gs;
@@ -1574,7 +1579,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
                                                 as<int32_t>(G.tr_idx));
     CKS(radix_sort_u32(as<uint32_t>(G.tr_key), as<int32_t>(G.tr_idx), as<uint32_t>(G.tr_key2), as<int32_t>(G.tr_idx2),
                        G.pcap, G.pbits, G.rs_tmp.p, st, npair));
-    const bool cache = s.cfg.contact_cache != 0;
+    const bool cache = cache_on(s);
     if (cache)
         k_cache_lookup<<<grid(G.pcap), 256, 0, st>>>(as<int2>(G.bp_pairs), G.pcap, npair, as<int64_t>(G.ckey), g,
                                                      as<int32_t>(G.cidx));
@@ -1735,7 +1740,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
                                                            as<int64_t>(G.hkey), as<double>(G.hds), as<int64_t>(G.hkey2),
                                                            as<double>(G.hds2), as<int64_t>(G.whkey), as<double>(G.whds),
                                                            as<int64_t>(G.whkey2), as<double>(G.whds2));
-    if (s.cfg.contact_cache)
+    if (cache_on(s))
         k_cache_commit<<<std::max(1, ctx->num_sms), 256, 0, st>>>(g, as<int64_t>(G.cscan), as<int64_t>(G.ckey2),
                                                                     as<double>(G.cval2), as<uint32_t>(G.chit2),
                                                                     as<int64_t>(G.ckey), as<double>(G.cval),

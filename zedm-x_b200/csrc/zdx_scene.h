@@ -55,8 +55,9 @@ struct SimConfig {
     // with the zdem tangential, damping and Coulomb terms
     int force_law = 0;
     double feng_k = 1e7;
-    // addition: 1 (default) lets the CUDA-graph step skip a candidate pair while a clearance it certified
-    // at an earlier step still holds (no segment either way); 0 tests every candidate pair every step
+    // addition: 1 (default) lets the CUDA-graph step of a scene of 256 particles or more skip a candidate
+    // pair while a clearance it certified at an earlier step still holds (no segment either way); 0 tests
+    // every candidate pair every step
     int contact_cache = 1;
     // addition: the cache's near-pair margin, relative to R_A + R_B (survivor pairs with boxes closer than
     // that are tested again at each skip; the others and the culled triangles set the clearance)
