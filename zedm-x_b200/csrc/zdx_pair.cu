@@ -131,7 +131,7 @@ __device__ __forceinline__ int64_t item_end_of(const PairArgs& a) {
 __global__ void k_cost_count(PairArgs a, int* buckets) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= pairs_of(a)) return;
-    if (a.cache_skip && a.cache_skip[p]) return;
+    if (a.cache_skip && a.cache_skip[p] == 1) return;
     int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
     unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
                            (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
@@ -151,7 +151,7 @@ __global__ void k_cost_scan(int* buckets, int* count) {
 __global__ void k_cost_scatter(PairArgs a, int* buckets, int32_t* order) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= pairs_of(a)) return;
-    if (a.cache_skip && a.cache_skip[p]) return;
+    if (a.cache_skip && a.cache_skip[p] == 1) return;
     int mA = a.pmesh[2 * p], mB = a.pmesh[2 * p + 1];
     unsigned long long c = (unsigned long long)(a.tri_off[mA + 1] - a.tri_off[mA]) *
                            (unsigned long long)(a.tri_off[mB + 1] - a.tri_off[mB]);
@@ -352,380 +352,434 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
                              __longlong_as_double((long long)a.mesh_R_bits[mesh[1]])};
         auto inf = [](V3 v) { return smax3(fabs(v.x), fabs(v.y), fabs(v.z)); };
         const double pad = 1e-9 * (inf(tpos[0]) + inf(tpos[1]) + R[0] + R[1]);
-        // Separation certificate along the line of centres d: every point of A lies below the largest
-        // corner projection max_v (v.d) of A's triangles, every point of B above B's smallest one.  A
-        // segment endpoint is on an edge of one body (seg_plane clamps t to [0, 1], src/main.cpp:545-559)
-        // and inside a triangle of the other up to point_in_tri's tolerance (src/main.cpp:529-543), i.e.
-        // within that mesh's inflation distance of it.  A gap wider than the larger inflation (plus
-        // rounding) means no triangle pair can yield a segment: the pair has none, as the full test finds.
-        bool slab = false;
-        V3 dslab{0.0, 0.0, 0.0};
-        if (a.mesh_infl_bits) {
-            const V3 dv = tpos[1] - tpos[0];
-            const double dl = norm(dv);
-            const double infl = smax(__longlong_as_double((long long)a.mesh_infl_bits[mesh[0]]),
-                                     __longlong_as_double((long long)a.mesh_infl_bits[mesh[1]]));
-            if (dl > 0.0 && infl < 1e300) {
-                const V3 d = dv / dl;
-                for (int s2 = 0; s2 < 2; ++s2) {
-                    const Q4 qc{qn[s2].w, -qn[s2].x, -qn[s2].y, -qn[s2].z};
-                    const V3 dloc = py ? qrotate_py_n(qc, d) : qrotate_n(qc, d);
-                    double e = s2 == 0 ? -__builtin_huge_val() : __builtin_huge_val();
-                    const double* tv = a.tris + 9 * off[s2];
-                    for (int q = tid; q < 3 * nt[s2]; q += K1_THREADS) {
-                        const double v = tv[3 * q] * dloc.x + tv[3 * q + 1] * dloc.y + tv[3 * q + 2] * dloc.z;
-                        e = s2 == 0 ? fmax(e, v) : fmin(e, v);
+        // CACHE: a pair whose entry holds (k_cache_skip) but whose near pairs meet: every triangle pair
+        // that can meet is a near pair (the others are further apart than the motion), so testing those,
+        // exactly as the full test does, gives the full test's segments.  The entry carries over.
+        bool near_only = false;
+        if constexpr (CACHE) near_only = a.cache_skip[p] == 2;
+        if (near_only) {
+            const int ci = a.cache_idx[p];
+            const double* e = a.cache_in + CACHE_W * (int64_t)ci;
+            const int nh = (int)e[CACHE_NH];
+            const uint32_t* hin = a.cache_hin + CACHE_H * (int64_t)ci;
+            K1Side& DA = S.side[0];
+            K1Side& DB = S.side[1];
+            for (int h = tid; h < nh; h += K1_THREADS) {
+                const uint32_t code = hin[h];
+                const int tt[2] = {(int)(code >> 16), (int)(code & 0xffffu)};
+                bool ok = true;
+                for (int s2 = 0; s2 < 2 && ok; ++s2) {
+                    K1Side& D = s2 == 0 ? DA : DB;
+                    const double* v = a.tris + 9 * (off[s2] + tt[s2]);
+                    V3 w[3];
+                    for (int k = 0; k < 3; ++k) w[k] = qrotate_n(qn[s2], ld3(v + 3 * k)) + tpos[s2];
+                    V3 n;
+                    double d;
+                    ok = plane_from_tri(w[0], w[1], w[2], n, d) && !(norm2(n) < 1e-30);
+                    for (int k = 0; k < 3; ++k) {
+                        D.tri[(3 * k + 0) * cap + h] = w[k].x;
+                        D.tri[(3 * k + 1) * cap + h] = w[k].y;
+                        D.tri[(3 * k + 2) * cap + h] = w[k].z;
                     }
-                    for (int o = 16; o > 0; o >>= 1) {
-                        const double y = __shfl_xor_sync(FULL, e, o);
-                        e = s2 == 0 ? fmax(e, y) : fmin(e, y);
-                    }
-                    if ((tid & 31) == 0) sh_red[s2][tid >> 5] = e;
+                    D.pl[0 * cap + h] = n.x;
+                    D.pl[1 * cap + h] = n.y;
+                    D.pl[2 * cap + h] = n.z;
+                    D.pl[3 * cap + h] = d;
+                    D.box[0 * cap + h] = smin3(w[0].x, w[1].x, w[2].x);
+                    D.box[1 * cap + h] = smin3(w[0].y, w[1].y, w[2].y);
+                    D.box[2 * cap + h] = smin3(w[0].z, w[1].z, w[2].z);
+                    D.box[3 * cap + h] = smax3(w[0].x, w[1].x, w[2].x);
+                    D.box[4 * cap + h] = smax3(w[0].y, w[1].y, w[2].y);
+                    D.box[5 * cap + h] = smax3(w[0].z, w[1].z, w[2].z);
+                    D.id[h] = tt[s2];
                 }
-                __syncthreads();
-                if (tid == 0) {
-                    double hi = -__builtin_huge_val(), lo = __builtin_huge_val();
-                    for (int w = 0; w < K1_THREADS / 32; ++w) {
-                        hi = fmax(hi, sh_red[0][w]);
-                        lo = fmin(lo, sh_red[1][w]);
-                    }
-                    const double hiA = dot(tpos[0], d) + hi, loB = dot(tpos[1], d) + lo;
-                    const double slack = infl * (1.0 + 1e-6) + 4.0 * pad;
-                    sh_sep = (hiA + slack < loB) ? 1 : 0;
-                    sh_slab[0] = hiA;
-                    sh_slab[1] = loB;
-                    sh_slab[2] = slack;
-                }
-                __syncthreads();
-                if (sh_sep && nchunk > 1) {
-                    // a split pair finishes through the joining below, with no segments from this item
-                    separated = true;
-                } else if (sh_sep) {
-                    if (tid == 0) {
-                        a.pair_seg_off[p] = 0;
-                        a.pair_nseg[p] = 0;
-                        a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
-                        a.pair_status[p] = 0;
-                        atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
-                    }
-                    if constexpr (CACHE) {
-                        // the certificate's gap along d: moved vertices shift the projections by their
-                        // displacement at most, and the slack by the change of pad (inside the allowance)
-                        double* c = a.cache_out + CACHE_W * (int64_t)p;
-                        if (tid == 0) c[0] = sh_slab[1] - sh_slab[0] - sh_slab[2];
-                        if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
-                        if (tid >= 15 && tid < CACHE_W) c[tid] = 0.0;  // not a skip, no near pairs
+                if (!ok) continue;  // a triangle without a plane: the full test drops it
+                const bool sep = DA.box[3 * cap + h] < DB.box[h] || DA.box[h] > DB.box[3 * cap + h] ||
+                                 DA.box[4 * cap + h] < DB.box[cap + h] || DA.box[cap + h] > DB.box[4 * cap + h] ||
+                                 DA.box[5 * cap + h] < DB.box[2 * cap + h] || DA.box[2 * cap + h] > DB.box[5 * cap + h];
+                if (!sep) eval_entry<NPX>(a, S, DA, DB, cap, make_int2(h, h), &sh_nseg);
+            }
+            double* c = a.cache_out + CACHE_W * (int64_t)p;
+            for (int k = tid; k < CACHE_W; k += K1_THREADS) c[k] = k == CACHE_SKIP ? 1.0 : e[k];
+            for (int h = tid; h < nh; h += K1_THREADS) a.cache_hout[CACHE_H * (int64_t)p + h] = hin[h];
+            __syncthreads();
+        }
+        if (!near_only) {
+            // Separation certificate along the line of centres d: every point of A lies below the largest
+            // corner projection max_v (v.d) of A's triangles, every point of B above B's smallest one.  A
+            // segment endpoint is on an edge of one body (seg_plane clamps t to [0, 1], src/main.cpp:545-559)
+            // and inside a triangle of the other up to point_in_tri's tolerance (src/main.cpp:529-543), i.e.
+            // within that mesh's inflation distance of it.  A gap wider than the larger inflation (plus
+            // rounding) means no triangle pair can yield a segment: the pair has none, as the full test finds.
+            bool slab = false;
+            V3 dslab{0.0, 0.0, 0.0};
+            if (a.mesh_infl_bits) {
+                const V3 dv = tpos[1] - tpos[0];
+                const double dl = norm(dv);
+                const double infl = smax(__longlong_as_double((long long)a.mesh_infl_bits[mesh[0]]),
+                                         __longlong_as_double((long long)a.mesh_infl_bits[mesh[1]]));
+                if (dl > 0.0 && infl < 1e300) {
+                    const V3 d = dv / dl;
+                    for (int s2 = 0; s2 < 2; ++s2) {
+                        const Q4 qc{qn[s2].w, -qn[s2].x, -qn[s2].y, -qn[s2].z};
+                        const V3 dloc = py ? qrotate_py_n(qc, d) : qrotate_n(qc, d);
+                        double e = s2 == 0 ? -__builtin_huge_val() : __builtin_huge_val();
+                        const double* tv = a.tris + 9 * off[s2];
+                        for (int q = tid; q < 3 * nt[s2]; q += K1_THREADS) {
+                            const double v = tv[3 * q] * dloc.x + tv[3 * q + 1] * dloc.y + tv[3 * q + 2] * dloc.z;
+                            e = s2 == 0 ? fmax(e, v) : fmin(e, v);
+                        }
+                        for (int o = 16; o > 0; o >>= 1) {
+                            const double y = __shfl_xor_sync(FULL, e, o);
+                            e = s2 == 0 ? fmax(e, y) : fmin(e, y);
+                        }
+                        if ((tid & 31) == 0) sh_red[s2][tid >> 5] = e;
                     }
                     __syncthreads();
-                    continue;
+                    if (tid == 0) {
+                        double hi = -__builtin_huge_val(), lo = __builtin_huge_val();
+                        for (int w = 0; w < K1_THREADS / 32; ++w) {
+                            hi = fmax(hi, sh_red[0][w]);
+                            lo = fmin(lo, sh_red[1][w]);
+                        }
+                        const double hiA = dot(tpos[0], d) + hi, loB = dot(tpos[1], d) + lo;
+                        const double slack = infl * (1.0 + 1e-6) + 4.0 * pad;
+                        sh_sep = (hiA + slack < loB) ? 1 : 0;
+                        sh_slab[0] = hiA;
+                        sh_slab[1] = loB;
+                        sh_slab[2] = slack;
+                    }
+                    __syncthreads();
+                    if (sh_sep && nchunk > 1) {
+                        // a split pair finishes through the joining below, with no segments from this item
+                        separated = true;
+                    } else if (sh_sep) {
+                        if (tid == 0) {
+                            a.pair_seg_off[p] = 0;
+                            a.pair_nseg[p] = 0;
+                            a.pair_checks[p] = (int64_t)a.mesh_valid[mesh[0]] * nt[1];
+                            a.pair_status[p] = 0;
+                            atomicAdd(a.checks_total, (unsigned long long)a.mesh_valid[mesh[0]] * (unsigned long long)nt[1]);
+                        }
+                        if constexpr (CACHE) {
+                            // the certificate's gap along d: moved vertices shift the projections by their
+                            // displacement at most, and the slack by the change of pad (inside the allowance)
+                            double* c = a.cache_out + CACHE_W * (int64_t)p;
+                            if (tid == 0) c[0] = sh_slab[1] - sh_slab[0] - sh_slab[2];
+                            if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
+                            if (tid >= 15 && tid < CACHE_W) c[tid] = 0.0;  // not a skip, no near pairs
+                        }
+                        __syncthreads();
+                        continue;
+                    }
+                    slab = true;
+                    dslab = d;
                 }
-                slab = true;
-                dslab = d;
             }
-        }
 
-        // Cull each side against the other body's bounding cube; keep the exact world triangles,
-        // planes and AABBs of the survivors (src/main.cpp:2064-2116).
-        //
-        // With the certificate's projections, also drop every triangle that lies wholly outside the slab
-        // where the two bodies overlap along d: an A triangle whose corners all project below
-        // lo(B.d) - slack, a B triangle whose corners all project above hi(A.d) + slack.  By the
-        // certificate's argument neither can take part in a segment.
-        double cclear = __builtin_huge_val();  // CACHE: smallest clearance of a culled triangle
-        bool cbad = false;
-        // CACHE: the culls keep every triangle within tau more of the other body, so that each triangle
-        // they drop has a clearance of at least tau (the extra survivors meet nothing: the culls are
-        // conservative either way)
-        const double tau = CACHE ? a.cache_tau * (R[0] + R[1]) : 0.0;
-        for (int s = 0; s < 2; ++s) {
-            const V3 other = tpos[1 - s];
-            const double lim = R[1 - s] + pad;
-            K1Side& D = S.side[s];
-            V3 dl{0.0, 0.0, 0.0};
-            double bound = 0.0;
-            if (slab) {
-                const Q4 qc{qn[s].w, -qn[s].x, -qn[s].y, -qn[s].z};
-                dl = py ? qrotate_py_n(qc, dslab) : qrotate_n(qc, dslab);
-                // in the mesh frame: A keeps corners reaching lo(B.d) - slack, B corners below hi(A.d) + slack
-                bound = s == 0 ? sh_slab[1] - sh_slab[2] - dot(tpos[0], dslab)
-                               : sh_slab[0] + sh_slab[2] - dot(tpos[1], dslab);
-                if constexpr (CACHE) bound = s == 0 ? bound - tau : bound + tau;
-            }
-            const int t_lo = s == 0 ? a_lo : 0, t_hi = separated ? t_lo : (s == 0 ? a_hi : nt[1]);
-            for (int t = t_lo + tid; t < t_hi; t += K1_THREADS) {
+            // Cull each side against the other body's bounding cube; keep the exact world triangles,
+            // planes and AABBs of the survivors (src/main.cpp:2064-2116).
+            //
+            // With the certificate's projections, also drop every triangle that lies wholly outside the slab
+            // where the two bodies overlap along d: an A triangle whose corners all project below
+            // lo(B.d) - slack, a B triangle whose corners all project above hi(A.d) + slack.  By the
+            // certificate's argument neither can take part in a segment.
+            double cclear = __builtin_huge_val();  // CACHE: smallest clearance of a culled triangle
+            bool cbad = false;
+            // CACHE: the culls keep every triangle within tau more of the other body, so that each triangle
+            // they drop has a clearance of at least tau (the extra survivors meet nothing: the culls are
+            // conservative either way)
+            const double tau = CACHE ? a.cache_tau * (R[0] + R[1]) : 0.0;
+            for (int s = 0; s < 2; ++s) {
+                const V3 other = tpos[1 - s];
+                const double lim = R[1 - s] + pad;
+                K1Side& D = S.side[s];
+                V3 dl{0.0, 0.0, 0.0};
+                double bound = 0.0;
                 if (slab) {
-                    const double* lv = a.tris + 9 * (off[s] + t);
-                    const double p0 = lv[0] * dl.x + lv[1] * dl.y + lv[2] * dl.z;
-                    const double p1 = lv[3] * dl.x + lv[4] * dl.y + lv[5] * dl.z;
-                    const double p2 = lv[6] * dl.x + lv[7] * dl.y + lv[8] * dl.z;
-                    if (s == 0 ? (smax3(p0, p1, p2) < bound) : (smin3(p0, p1, p2) > bound)) {
-                        // CACHE: how far the triangle sits outside the slab along d
-                        if constexpr (CACHE)
-                            cclear = fmin(cclear, (s == 0 ? bound - smax3(p0, p1, p2) : smin3(p0, p1, p2) - bound) + tau);
-                        continue;
-                    }
+                    const Q4 qc{qn[s].w, -qn[s].x, -qn[s].y, -qn[s].z};
+                    dl = py ? qrotate_py_n(qc, dslab) : qrotate_n(qc, dslab);
+                    // in the mesh frame: A keeps corners reaching lo(B.d) - slack, B corners below hi(A.d) + slack
+                    bound = s == 0 ? sh_slab[1] - sh_slab[2] - dot(tpos[0], dslab)
+                                   : sh_slab[0] + sh_slab[2] - dot(tpos[1], dslab);
+                    if constexpr (CACHE) bound = s == 0 ? bound - tau : bound + tau;
                 }
-                if (!a.per_stage) {
-                    double4 sp = a.tri_sph[off[s] + t];
-                    V3 c = V3{sp.x, sp.y, sp.z};
-                    V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];
-                    double L = sp.w + lim;
-                    double Lc = L;
-                    if constexpr (CACHE) Lc = L + tau;
-                    if (!(fabs(cw.x - other.x) <= Lc && fabs(cw.y - other.y) <= Lc && fabs(cw.z - other.z) <= Lc)) {
-                        // CACHE: how far the triangle's cube misses the other body's, on the widest axis
-                        if constexpr (CACHE)
-                            cclear = fmin(cclear, smax3(fabs(cw.x - other.x), fabs(cw.y - other.y), fabs(cw.z - other.z)) - L);
-                        continue;
-                    }
-                }
-                const double* v = a.tris + 9 * (off[s] + t);
-                V3 w[3];
-                for (int k = 0; k < 3; ++k) {
-                    V3 lv = ld3(v + 3 * k);
-                    w[k] = (py ? qrotate_py_n(qn[s], lv) : qrotate_n(qn[s], lv)) + tpos[s];
-                }
-                V3 n;
-                double d;
-                if constexpr (NPX) {
-                    // polyline.py main: the offset of plane_from_tri, the normal of tri_normals
-                    V3 np_n;
-                    if (!np::plane_from_tri(&w[0].x, &np_n.x, &d)) continue;
-                    np::tri_normal(&w[0].x, &n.x);
-                } else {
-                    if constexpr (CACHE) {
-                        // a triangle without a plane here might have one after a move: no clearance
-                        if (!plane_from_tri(w[0], w[1], w[2], n, d) || norm2(n) < 1e-30) {
-                            cbad = true;
+                const int t_lo = s == 0 ? a_lo : 0, t_hi = separated ? t_lo : (s == 0 ? a_hi : nt[1]);
+                for (int t = t_lo + tid; t < t_hi; t += K1_THREADS) {
+                    if (slab) {
+                        const double* lv = a.tris + 9 * (off[s] + t);
+                        const double p0 = lv[0] * dl.x + lv[1] * dl.y + lv[2] * dl.z;
+                        const double p1 = lv[3] * dl.x + lv[4] * dl.y + lv[5] * dl.z;
+                        const double p2 = lv[6] * dl.x + lv[7] * dl.y + lv[8] * dl.z;
+                        if (s == 0 ? (smax3(p0, p1, p2) < bound) : (smin3(p0, p1, p2) > bound)) {
+                            // CACHE: how far the triangle sits outside the slab along d
+                            if constexpr (CACHE)
+                                cclear = fmin(cclear, (s == 0 ? bound - smax3(p0, p1, p2) : smin3(p0, p1, p2) - bound) + tau);
                             continue;
                         }
-                    } else {
-                        if (!plane_from_tri(w[0], w[1], w[2], n, d)) continue;
-                        if (norm2(n) < 1e-30) continue;
                     }
+                    if (!a.per_stage) {
+                        double4 sp = a.tri_sph[off[s] + t];
+                        V3 c = V3{sp.x, sp.y, sp.z};
+                        V3 cw = (py ? qrotate_py_n(qn[s], c) : qrotate_n(qn[s], c)) + tpos[s];
+                        double L = sp.w + lim;
+                        double Lc = L;
+                        if constexpr (CACHE) Lc = L + tau;
+                        if (!(fabs(cw.x - other.x) <= Lc && fabs(cw.y - other.y) <= Lc && fabs(cw.z - other.z) <= Lc)) {
+                            // CACHE: how far the triangle's cube misses the other body's, on the widest axis
+                            if constexpr (CACHE)
+                                cclear = fmin(cclear, smax3(fabs(cw.x - other.x), fabs(cw.y - other.y), fabs(cw.z - other.z)) - L);
+                            continue;
+                        }
+                    }
+                    const double* v = a.tris + 9 * (off[s] + t);
+                    V3 w[3];
+                    for (int k = 0; k < 3; ++k) {
+                        V3 lv = ld3(v + 3 * k);
+                        w[k] = (py ? qrotate_py_n(qn[s], lv) : qrotate_n(qn[s], lv)) + tpos[s];
+                    }
+                    V3 n;
+                    double d;
+                    if constexpr (NPX) {
+                        // polyline.py main: the offset of plane_from_tri, the normal of tri_normals
+                        V3 np_n;
+                        if (!np::plane_from_tri(&w[0].x, &np_n.x, &d)) continue;
+                        np::tri_normal(&w[0].x, &n.x);
+                    } else {
+                        if constexpr (CACHE) {
+                            // a triangle without a plane here might have one after a move: no clearance
+                            if (!plane_from_tri(w[0], w[1], w[2], n, d) || norm2(n) < 1e-30) {
+                                cbad = true;
+                                continue;
+                            }
+                        } else {
+                            if (!plane_from_tri(w[0], w[1], w[2], n, d)) continue;
+                            if (norm2(n) < 1e-30) continue;
+                        }
+                    }
+                    int i = atomicAdd(&sh_n[s], 1);
+                    for (int k = 0; k < 3; ++k) {
+                        D.tri[(3 * k + 0) * cap + i] = w[k].x;
+                        D.tri[(3 * k + 1) * cap + i] = w[k].y;
+                        D.tri[(3 * k + 2) * cap + i] = w[k].z;
+                    }
+                    D.pl[0 * cap + i] = n.x;
+                    D.pl[1 * cap + i] = n.y;
+                    D.pl[2 * cap + i] = n.z;
+                    D.pl[3 * cap + i] = d;
+                    D.box[0 * cap + i] = smin3(w[0].x, w[1].x, w[2].x);
+                    D.box[1 * cap + i] = smin3(w[0].y, w[1].y, w[2].y);
+                    D.box[2 * cap + i] = smin3(w[0].z, w[1].z, w[2].z);
+                    D.box[3 * cap + i] = smax3(w[0].x, w[1].x, w[2].x);
+                    D.box[4 * cap + i] = smax3(w[0].y, w[1].y, w[2].y);
+                    D.box[5 * cap + i] = smax3(w[0].z, w[1].z, w[2].z);
+                    D.id[i] = t;
                 }
-                int i = atomicAdd(&sh_n[s], 1);
-                for (int k = 0; k < 3; ++k) {
-                    D.tri[(3 * k + 0) * cap + i] = w[k].x;
-                    D.tri[(3 * k + 1) * cap + i] = w[k].y;
-                    D.tri[(3 * k + 2) * cap + i] = w[k].z;
-                }
-                D.pl[0 * cap + i] = n.x;
-                D.pl[1 * cap + i] = n.y;
-                D.pl[2 * cap + i] = n.z;
-                D.pl[3 * cap + i] = d;
-                D.box[0 * cap + i] = smin3(w[0].x, w[1].x, w[2].x);
-                D.box[1 * cap + i] = smin3(w[0].y, w[1].y, w[2].y);
-                D.box[2 * cap + i] = smin3(w[0].z, w[1].z, w[2].z);
-                D.box[3 * cap + i] = smax3(w[0].x, w[1].x, w[2].x);
-                D.box[4 * cap + i] = smax3(w[0].y, w[1].y, w[2].y);
-                D.box[5 * cap + i] = smax3(w[0].z, w[1].z, w[2].z);
-                D.id[i] = t;
             }
-        }
-        if constexpr (CACHE) {
-            if (cclear < __builtin_huge_val()) {
-                if (cclear > 0.0) atomicMin(&sh_cmin, dbits(cclear));
-                else cbad = true;
-            }
-            if (cbad) sh_cbad = 1;
-        }
-        __syncthreads();
-        const int nA = sh_n[0], nB = sh_n[1];
-        const int64_t total = (int64_t)nA * nB;
-        const K1Side& SA = S.side[0];
-        const K1Side& SB = S.side[1];
-        // the survivors' exact boxes (component-major, stride cap) stay in the CTA's slot: the tests' gathers
-        // hit in L1, which staging them in shared memory (measured: slower) would take away
-        const double* bA = SA.box;
-        const double* bB = SB.box;
-        const int sA = cap, sB = cap;
-        if (!a.per_stage && nA > 0 && nB > 0 && nB <= K1_HCAP && total > a.flat_max) {
-            // ---- hierarchical test: B's survivors in Morton order, outward-rounded float AABBs and
-            // 32-triangle group boxes in shared memory; one warp per A triangle rejects whole groups
-            // first.  A float reject is exact (the float box contains the double one); every float
-            // overlap is re-tested with the reference's strict double compare.
-            const int N2 = next_pow2(nB);
-            const double Rb = R[1] + pad;
-            const V3 lo = tpos[1] - V3{Rb, Rb, Rb};
-            const double sc = 1024.0 / (2.0 * Rb);
-            for (int i = tid; i < N2; i += K1_THREADS) {
-                if (i < nB) {
-                    V3 c{(SB.tri[i] + SB.tri[3 * cap + i] + SB.tri[6 * cap + i]),
-                         (SB.tri[cap + i] + SB.tri[4 * cap + i] + SB.tri[7 * cap + i]),
-                         (SB.tri[2 * cap + i] + SB.tri[5 * cap + i] + SB.tri[8 * cap + i])};
-                    c = c * (1.0 / 3.0);
-                    sm_key[i] = morton3((c.x - lo.x) * sc, (c.y - lo.y) * sc, (c.z - lo.z) * sc);
-                    sm_val[i] = i;
-                } else {
-                    sm_key[i] = 0xffffffffu;
-                    sm_val[i] = -1;
+            if constexpr (CACHE) {
+                if (cclear < __builtin_huge_val()) {
+                    if (cclear > 0.0) atomicMin(&sh_cmin, dbits(cclear));
+                    else cbad = true;
                 }
+                if (cbad) sh_cbad = 1;
             }
             __syncthreads();
-            for (int kk2 = 2; kk2 <= N2; kk2 <<= 1)
-                for (int j = kk2 >> 1; j > 0; j >>= 1) {
-                    for (int i = tid; i < N2; i += K1_THREADS) {
-                        int ixj = i ^ j;
-                        if (ixj > i) {
-                            bool up = (i & kk2) == 0;
-                            uint32_t ki = sm_key[i], kj = sm_key[ixj];
-                            if ((ki > kj) == up) {
-                                sm_key[i] = kj;
-                                sm_key[ixj] = ki;
-                                int vi = sm_val[i];
-                                sm_val[i] = sm_val[ixj];
-                                sm_val[ixj] = vi;
+            const int nA = sh_n[0], nB = sh_n[1];
+            const int64_t total = (int64_t)nA * nB;
+            const K1Side& SA = S.side[0];
+            const K1Side& SB = S.side[1];
+            // the survivors' exact boxes (component-major, stride cap) stay in the CTA's slot: the tests' gathers
+            // hit in L1, which staging them in shared memory (measured: slower) would take away
+            const double* bA = SA.box;
+            const double* bB = SB.box;
+            const int sA = cap, sB = cap;
+            if (!a.per_stage && nA > 0 && nB > 0 && nB <= K1_HCAP && total > a.flat_max) {
+                // ---- hierarchical test: B's survivors in Morton order, outward-rounded float AABBs and
+                // 32-triangle group boxes in shared memory; one warp per A triangle rejects whole groups
+                // first.  A float reject is exact (the float box contains the double one); every float
+                // overlap is re-tested with the reference's strict double compare.
+                const int N2 = next_pow2(nB);
+                const double Rb = R[1] + pad;
+                const V3 lo = tpos[1] - V3{Rb, Rb, Rb};
+                const double sc = 1024.0 / (2.0 * Rb);
+                for (int i = tid; i < N2; i += K1_THREADS) {
+                    if (i < nB) {
+                        V3 c{(SB.tri[i] + SB.tri[3 * cap + i] + SB.tri[6 * cap + i]),
+                             (SB.tri[cap + i] + SB.tri[4 * cap + i] + SB.tri[7 * cap + i]),
+                             (SB.tri[2 * cap + i] + SB.tri[5 * cap + i] + SB.tri[8 * cap + i])};
+                        c = c * (1.0 / 3.0);
+                        sm_key[i] = morton3((c.x - lo.x) * sc, (c.y - lo.y) * sc, (c.z - lo.z) * sc);
+                        sm_val[i] = i;
+                    } else {
+                        sm_key[i] = 0xffffffffu;
+                        sm_val[i] = -1;
+                    }
+                }
+                __syncthreads();
+                for (int kk2 = 2; kk2 <= N2; kk2 <<= 1)
+                    for (int j = kk2 >> 1; j > 0; j >>= 1) {
+                        for (int i = tid; i < N2; i += K1_THREADS) {
+                            int ixj = i ^ j;
+                            if (ixj > i) {
+                                bool up = (i & kk2) == 0;
+                                uint32_t ki = sm_key[i], kj = sm_key[ixj];
+                                if ((ki > kj) == up) {
+                                    sm_key[i] = kj;
+                                    sm_key[ixj] = ki;
+                                    int vi = sm_val[i];
+                                    sm_val[i] = sm_val[ixj];
+                                    sm_val[ixj] = vi;
+                                }
                             }
+                        }
+                        __syncthreads();
+                    }
+                for (int m = tid; m < nB; m += K1_THREADS) {
+                    int ib = sm_val[m];
+                    for (int k = 0; k < 3; ++k) sm_box[k * K1_HCAP + m] = __double2float_rd(bB[k * sB + ib]);
+                    for (int k = 3; k < 6; ++k) sm_box[k * K1_HCAP + m] = __double2float_ru(bB[k * sB + ib]);
+                }
+                __syncthreads();
+                const int ng = (nB + 31) >> 5;
+                const int lane = tid & 31, warp = tid >> 5;
+                for (int g = warp; g < ng; g += K1_THREADS / 32) {
+                    int m = g * 32 + lane;
+                    float v[6];
+                    for (int k = 0; k < 3; ++k) v[k] = m < nB ? sm_box[k * K1_HCAP + m] : __int_as_float(0x7f800000);
+                    for (int k = 3; k < 6; ++k) v[k] = m < nB ? sm_box[k * K1_HCAP + m] : -__int_as_float(0x7f800000);
+                    for (int o = 16; o > 0; o >>= 1) {
+                        for (int k = 0; k < 3; ++k) v[k] = fminf(v[k], __shfl_xor_sync(FULL, v[k], o));
+                        for (int k = 3; k < 6; ++k) v[k] = fmaxf(v[k], __shfl_xor_sync(FULL, v[k], o));
+                    }
+                    if (lane < 6) sm_gbox[lane * (K1_HCAP / 32) + g] = v[lane];
+                }
+                __syncthreads();
+                int2* wq = sm_wq + warp * 64;
+                int wq_n = 0;
+                for (int ia = warp; ia < nA; ia += K1_THREADS / 32) {
+                    double da[6];
+                    for (int k = 0; k < 6; ++k) da[k] = bA[k * sA + ia];
+                    float fa[6];
+                    for (int k = 0; k < 3; ++k) fa[k] = __double2float_rd(da[k]);
+                    for (int k = 3; k < 6; ++k) fa[k] = __double2float_ru(da[k]);
+                    for (int gb = 0; gb < ng; gb += 32) {
+                        const int g = gb + lane;
+                        bool ov = false;
+                        if (g < ng) {
+                            const float* G = sm_gbox + g;
+                            const int gs = K1_HCAP / 32;
+                            ov = !(fa[3] < G[0] || fa[0] > G[3 * gs] || fa[4] < G[gs] || fa[1] > G[4 * gs] ||
+                                   fa[5] < G[2 * gs] || fa[2] > G[5 * gs]);
+                        }
+                        unsigned gbal = __ballot_sync(FULL, ov);
+                        while (gbal) {
+                            const int gg = gb + __ffs(gbal) - 1;
+                            gbal &= gbal - 1u;
+                            const int m = gg * 32 + lane;
+                            bool hit = false;
+                            int ib = 0;
+                            if (m < nB) {
+                                const float* Bm = sm_box + m;
+                                bool fov = !(fa[3] < Bm[0] || fa[0] > Bm[3 * K1_HCAP] || fa[4] < Bm[K1_HCAP] ||
+                                             fa[1] > Bm[4 * K1_HCAP] || fa[5] < Bm[2 * K1_HCAP] || fa[2] > Bm[5 * K1_HCAP]);
+                                if (fov) {
+                                    ib = sm_val[m];
+                                    // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
+                                    hit = !(da[3] < bB[ib] || da[0] > bB[3 * sB + ib] || da[4] < bB[sB + ib] ||
+                                            da[1] > bB[4 * sB + ib] || da[5] < bB[2 * sB + ib] || da[2] > bB[5 * sB + ib]);
+                                }
+                            }
+                            unsigned hb = __ballot_sync(FULL, hit);
+                            if (hit) wq[wq_n + __popc(hb & ((1u << lane) - 1u))] = make_int2(ia, ib);
+                            wq_n += __popc(hb);
+                            if (wq_n >= 32) {
+                                __syncwarp();
+                                for (int q = lane; q < wq_n; q += 32) eval_entry<NPX>(a, S, SA, SB, cap, wq[q], &sh_nseg);
+                                __syncwarp();
+                                wq_n = 0;
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                for (int q = lane; q < wq_n; q += 32) eval_entry<NPX>(a, S, SA, SB, cap, wq[q], &sh_nseg);
+                __syncthreads();
+            } else if (nB > 0) {
+                int ia = 0, ib = 0, dA = 0, dB = 0;
+                if (nB > 0) {
+                    ia = tid / nB;
+                    ib = tid % nB;
+                    dA = K1_THREADS / nB;
+                    dB = K1_THREADS % nB;
+                }
+                for (int64_t base = 0; base < total; base += K1_QCAP) {
+        #pragma unroll 1
+                    for (int it = 0; it < K1_ITER; ++it) {
+                        int64_t kk = base + (int64_t)it * K1_THREADS + tid;
+                        if (kk < total) {
+                            // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
+                            bool sep = bA[3 * sA + ia] < bB[0 * sB + ib] || bA[0 * sA + ia] > bB[3 * sB + ib] ||
+                                       bA[4 * sA + ia] < bB[1 * sB + ib] || bA[1 * sA + ia] > bB[4 * sB + ib] ||
+                                       bA[5 * sA + ia] < bB[2 * sB + ib] || bA[2 * sA + ia] > bB[5 * sB + ib];
+                            if (!sep) {
+                                int qi = atomicAdd(&sh_nq, 1);
+                                sh_q[qi] = make_int2(ia, ib);
+                            }
+                        }
+                        ib += dB;
+                        ia += dA;
+                        if (ib >= nB) {
+                            ib -= nB;
+                            ia++;
                         }
                     }
                     __syncthreads();
+                    const int nq = sh_nq;
+                    for (int qi = tid; qi < nq; qi += K1_THREADS) eval_entry<NPX>(a, S, SA, SB, cap, sh_q[qi], &sh_nseg);
+                    __syncthreads();
+                    if (tid == 0) sh_nq = 0;
+                    __syncthreads();
                 }
-            for (int m = tid; m < nB; m += K1_THREADS) {
-                int ib = sm_val[m];
-                for (int k = 0; k < 3; ++k) sm_box[k * K1_HCAP + m] = __double2float_rd(bB[k * sB + ib]);
-                for (int k = 3; k < 6; ++k) sm_box[k * K1_HCAP + m] = __double2float_ru(bB[k * sB + ib]);
             }
-            __syncthreads();
-            const int ng = (nB + 31) >> 5;
-            const int lane = tid & 31, warp = tid >> 5;
-            for (int g = warp; g < ng; g += K1_THREADS / 32) {
-                int m = g * 32 + lane;
-                float v[6];
-                for (int k = 0; k < 3; ++k) v[k] = m < nB ? sm_box[k * K1_HCAP + m] : __int_as_float(0x7f800000);
-                for (int k = 3; k < 6; ++k) v[k] = m < nB ? sm_box[k * K1_HCAP + m] : -__int_as_float(0x7f800000);
-                for (int o = 16; o > 0; o >>= 1) {
-                    for (int k = 0; k < 3; ++k) v[k] = fminf(v[k], __shfl_xor_sync(FULL, v[k], o));
-                    for (int k = 3; k < 6; ++k) v[k] = fmaxf(v[k], __shfl_xor_sync(FULL, v[k], o));
-                }
-                if (lane < 6) sm_gbox[lane * (K1_HCAP / 32) + g] = v[lane];
-            }
-            __syncthreads();
-            int2* wq = sm_wq + warp * 64;
-            int wq_n = 0;
-            for (int ia = warp; ia < nA; ia += K1_THREADS / 32) {
-                double da[6];
-                for (int k = 0; k < 6; ++k) da[k] = bA[k * sA + ia];
-                float fa[6];
-                for (int k = 0; k < 3; ++k) fa[k] = __double2float_rd(da[k]);
-                for (int k = 3; k < 6; ++k) fa[k] = __double2float_ru(da[k]);
-                for (int gb = 0; gb < ng; gb += 32) {
-                    const int g = gb + lane;
-                    bool ov = false;
-                    if (g < ng) {
-                        const float* G = sm_gbox + g;
-                        const int gs = K1_HCAP / 32;
-                        ov = !(fa[3] < G[0] || fa[0] > G[3 * gs] || fa[4] < G[gs] || fa[1] > G[4 * gs] ||
-                               fa[5] < G[2 * gs] || fa[2] > G[5 * gs]);
-                    }
-                    unsigned gbal = __ballot_sync(FULL, ov);
-                    while (gbal) {
-                        const int gg = gb + __ffs(gbal) - 1;
-                        gbal &= gbal - 1u;
-                        const int m = gg * 32 + lane;
-                        bool hit = false;
-                        int ib = 0;
-                        if (m < nB) {
-                            const float* Bm = sm_box + m;
-                            bool fov = !(fa[3] < Bm[0] || fa[0] > Bm[3 * K1_HCAP] || fa[4] < Bm[K1_HCAP] ||
-                                         fa[1] > Bm[4 * K1_HCAP] || fa[5] < Bm[2 * K1_HCAP] || fa[2] > Bm[5 * K1_HCAP]);
-                            if (fov) {
-                                ib = sm_val[m];
-                                // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
-                                hit = !(da[3] < bB[ib] || da[0] > bB[3 * sB + ib] || da[4] < bB[sB + ib] ||
-                                        da[1] > bB[4 * sB + ib] || da[5] < bB[2 * sB + ib] || da[2] > bB[5 * sB + ib]);
-                            }
+            if constexpr (CACHE) {
+                // the pair's clearance: none with a triangle without a plane.  Survivor pairs whose boxes are
+                // less than tau apart (those that met, and so every segment, included) become the entry's near pairs,
+                // tested again at every skip; the clearance is the smallest of the culled triangles' and of
+                // the other pairs' box gaps (the largest separation over the axes), at least tau
+                __syncthreads();
+                const bool ok = sh_cbad == 0 && !separated;
+                uint32_t* hout = a.cache_hout + CACHE_H * (int64_t)p;
+                if (ok && nA > 0 && nB > 0) {
+                    double g = __builtin_huge_val();
+                    for (int64_t q = tid; q < total; q += K1_THREADS) {
+                        const int ia = (int)(q / nB), ib = (int)(q - (int64_t)ia * nB);
+                        double gq = -__builtin_huge_val();
+                        for (int k = 0; k < 3; ++k) {
+                            gq = fmax(gq, bB[k * sB + ib] - bA[(3 + k) * sA + ia]);
+                            gq = fmax(gq, bA[k * sA + ia] - bB[(3 + k) * sB + ib]);
                         }
-                        unsigned hb = __ballot_sync(FULL, hit);
-                        if (hit) wq[wq_n + __popc(hb & ((1u << lane) - 1u))] = make_int2(ia, ib);
-                        wq_n += __popc(hb);
-                        if (wq_n >= 32) {
-                            __syncwarp();
-                            for (int q = lane; q < wq_n; q += 32) eval_entry<NPX>(a, S, SA, SB, cap, wq[q], &sh_nseg);
-                            __syncwarp();
-                            wq_n = 0;
+                        if (gq < tau) {
+                            const int ta = SA.id[ia], tb = SB.id[ib];
+                            const int h = atomicAdd(&sh_nh, 1);
+                            if (ta < 65536 && tb < 65536 && h < CACHE_H) hout[h] = (uint32_t)ta << 16 | (uint32_t)tb;
+                            else sh_cbad = 1;
+                        } else {
+                            g = fmin(g, gq);
                         }
                     }
-                }
-            }
-            __syncwarp();
-            for (int q = lane; q < wq_n; q += 32) eval_entry<NPX>(a, S, SA, SB, cap, wq[q], &sh_nseg);
-            __syncthreads();
-        } else if (nB > 0) {
-            int ia = 0, ib = 0, dA = 0, dB = 0;
-            if (nB > 0) {
-                ia = tid / nB;
-                ib = tid % nB;
-                dA = K1_THREADS / nB;
-                dB = K1_THREADS % nB;
-            }
-            for (int64_t base = 0; base < total; base += K1_QCAP) {
-    #pragma unroll 1
-                for (int it = 0; it < K1_ITER; ++it) {
-                    int64_t kk = base + (int64_t)it * K1_THREADS + tid;
-                    if (kk < total) {
-                        // the reference's AABB reject (src/main.cpp:2130-2134), strict compares
-                        bool sep = bA[3 * sA + ia] < bB[0 * sB + ib] || bA[0 * sA + ia] > bB[3 * sB + ib] ||
-                                   bA[4 * sA + ia] < bB[1 * sB + ib] || bA[1 * sA + ia] > bB[4 * sB + ib] ||
-                                   bA[5 * sA + ia] < bB[2 * sB + ib] || bA[2 * sA + ia] > bB[5 * sB + ib];
-                        if (!sep) {
-                            int qi = atomicAdd(&sh_nq, 1);
-                            sh_q[qi] = make_int2(ia, ib);
-                        }
-                    }
-                    ib += dB;
-                    ia += dA;
-                    if (ib >= nB) {
-                        ib -= nB;
-                        ia++;
-                    }
+                    if (g < __builtin_huge_val()) atomicMin(&sh_gmin, dbits(g));
                 }
                 __syncthreads();
-                const int nq = sh_nq;
-                for (int qi = tid; qi < nq; qi += K1_THREADS) eval_entry<NPX>(a, S, SA, SB, cap, sh_q[qi], &sh_nseg);
-                __syncthreads();
-                if (tid == 0) sh_nq = 0;
-                __syncthreads();
-            }
-        }
-        if constexpr (CACHE) {
-            // the pair's clearance: none with a segment or a triangle without a plane.  Survivor pairs whose
-            // boxes are less than tau apart (those that met included) become the entry's near pairs,
-            // tested again at every skip; the clearance is the smallest of the culled triangles' and of
-            // the other pairs' box gaps (the largest separation over the axes), at least tau
-            __syncthreads();
-            const bool ok = sh_nseg == 0 && sh_cbad == 0 && !separated;
-            uint32_t* hout = a.cache_hout + CACHE_H * (int64_t)p;
-            if (ok && nA > 0 && nB > 0) {
-                double g = __builtin_huge_val();
-                for (int64_t q = tid; q < total; q += K1_THREADS) {
-                    const int ia = (int)(q / nB), ib = (int)(q - (int64_t)ia * nB);
-                    double gq = -__builtin_huge_val();
-                    for (int k = 0; k < 3; ++k) {
-                        gq = fmax(gq, bB[k * sB + ib] - bA[(3 + k) * sA + ia]);
-                        gq = fmax(gq, bA[k * sA + ia] - bB[(3 + k) * sB + ib]);
-                    }
-                    if (gq < tau) {
-                        const int ta = SA.id[ia], tb = SB.id[ib];
-                        const int h = atomicAdd(&sh_nh, 1);
-                        if (ta < 65536 && tb < 65536 && h < CACHE_H) hout[h] = (uint32_t)ta << 16 | (uint32_t)tb;
-                        else sh_cbad = 1;
-                    } else {
-                        g = fmin(g, gq);
-                    }
+                double* c = a.cache_out + CACHE_W * (int64_t)p;
+                if (tid == 0) {
+                    const double m = fmin(__longlong_as_double((long long)sh_cmin), __longlong_as_double((long long)sh_gmin));
+                    c[0] = (ok && sh_cbad == 0 && m > 0.0) ? m : -1.0;
                 }
-                if (g < __builtin_huge_val()) atomicMin(&sh_gmin, dbits(g));
+                if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
+                if (tid == CACHE_SKIP) c[CACHE_SKIP] = 0.0;
+                if (tid == CACHE_NH) c[CACHE_NH] = (double)(sh_nh < CACHE_H ? sh_nh : CACHE_H);
+                if (tid > CACHE_NH && tid < CACHE_W) c[tid] = 0.0;
             }
-            __syncthreads();
-            double* c = a.cache_out + CACHE_W * (int64_t)p;
-            if (tid == 0) {
-                const double m = fmin(__longlong_as_double((long long)sh_cmin), __longlong_as_double((long long)sh_gmin));
-                c[0] = (ok && sh_cbad == 0 && m > 0.0) ? m : -1.0;
-            }
-            if (tid >= 1 && tid <= 14) c[tid] = ps[tid - 1];
-            if (tid == CACHE_SKIP) c[CACHE_SKIP] = 0.0;
-            if (tid == CACHE_NH) c[CACHE_NH] = (double)(sh_nh < CACHE_H ? sh_nh : CACHE_H);
-            if (tid > CACHE_NH && tid < CACHE_W) c[tid] = 0.0;
         }
         int ns = sh_nseg;
         int status = 0;
@@ -840,15 +894,15 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
 // 2 sin(theta / 2) |v| <= 2 |q - q0| |v| for unit quaternions, |v| <= R).  M covers every triangle pair
 // but the entry's near pairs, which are tested again as the full test does (world corners, plane,
 // strict box compare, tri_tri).  With none of them meeting, the pair has no segment, as when the
-// separation certificate holds; otherwise k_segments tests it in full.  Warp per pair, lanes over the
-// near pairs.
+// separation certificate holds; otherwise k_segments tests the near pairs alone (their segments are
+// all the pair has), or in full when the motion exceeds M.  Warp per pair, lanes over the near pairs.
 __global__ void k_cache_skip(PairArgs a) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     const int64_t n = pairs_of(a);
     for (int64_t p = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); p < n; p += warps) {
         const int ci = a.cache_idx[p];
-        bool skip = false;
+        int flag = 0;
         if (ci >= 0) {
             const double* ps = a.pose + 14 * p;
             const V3 tpos[2] = {V3{ps[0], ps[1], ps[2]}, V3{ps[7], ps[8], ps[9]}};
@@ -894,8 +948,8 @@ __global__ void k_cache_skip(PairArgs a) {
                     V3 o0, o1;
                     if (!sep && tri_tri(W[0], nv[0], d[0], W[1], nv[1], d[1], o0, o1)) meet = true;
                 }
-                skip = !__any_sync(FULL, meet);
-                if (skip) {
+                if (!__any_sync(FULL, meet)) {
+                    flag = 1;
                     const int nt1 = (int)(a.tri_off[mesh[1] + 1] - off[1]);
                     if (lane == 0) {
                         const int64_t checks = (int64_t)a.mesh_valid[mesh[0]] * nt1;
@@ -915,10 +969,12 @@ __global__ void k_cache_skip(PairArgs a) {
                     // the entry carries over unchanged, marked as a skip
                     if (lane < CACHE_W) a.cache_out[CACHE_W * p + lane] = lane == CACHE_SKIP ? 1.0 : e[lane];
                     for (int h = lane; h < nh; h += 32) a.cache_hout[CACHE_H * p + h] = hin[h];
+                } else if (nh <= a.cap_side) {
+                    flag = 2;  // k_segments tests the near pairs alone
                 }
             }
         }
-        if (lane == 0) a.cache_skip[p] = skip ? 1 : 0;
+        if (lane == 0) a.cache_skip[p] = flag;
     }
 }
 

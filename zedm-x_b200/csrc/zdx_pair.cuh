@@ -135,8 +135,9 @@ struct PairArgs {
     const uint32_t* cache_hin;
     uint32_t* cache_hout;
     double cache_tau;
-    // per pair, 1 when launch_cache_skip settled it from its entry (no segment); the cost order then
-    // leaves it out and writes the count of the pairs it holds to order_count (null: every pair)
+    // per pair, 1 when launch_cache_skip settled it from its entry (no segment; the cost order then
+    // leaves it out and writes the count of the pairs it holds to order_count, null: every pair), 2 when
+    // the entry holds but near pairs meet (k_segments tests the near pairs alone), else 0
     int32_t* cache_skip;
     int* order_count;
 };
