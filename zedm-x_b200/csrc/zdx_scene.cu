@@ -225,8 +225,13 @@ __global__ void k_pp_force(const int2* pairs, int64_t npair, const int64_t* n_de
 }
 
 // ---------------------------------------------------------------- walls
+// A candidate also needs a wall triangle whose AABB meets the particle's (k_walls' test, the same
+// arithmetic), for walls of up to kWallCandTris triangles: one without any has no contact and no history
+// to keep, so leaving it out of the list changes nothing downstream.
+constexpr int kWallCandTris = 64;
 __global__ void k_wall_cand(const double* state, const double* mat, int np, const double* wpose, const double* wrad,
-                            int nw, int32_t* cnt, const int64_t* off, int2* cand, int64_t cap) {
+                            const double* wtris, const int64_t* wtri_off, int nw, int32_t* cnt, const int64_t* off,
+                            int2* cand, int64_t cap) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
     if (off && off[i + 1] > cap) return;
@@ -237,6 +242,22 @@ __global__ void k_wall_cand(const double* state, const double* mat, int np, cons
         double dist2 = dot(d, d);
         double rsum = mat[17 * (int64_t)i + 2] + wrad[w];
         if (dist2 > rsum * rsum) continue;
+        const int64_t t0 = wtri_off[w], t1 = wtri_off[w + 1];
+        if (t1 - t0 <= kWallCandTris) {
+            const V3 xp = L3(s);
+            const double r = mat[17 * (int64_t)i + 2];
+            const V3 pmn = xp - V3{r, r, r}, pmx = xp + V3{r, r, r};
+            bool any = false;
+            for (int64_t t = t0; t < t1 && !any; ++t) {
+                const double* wt = wtris + 9 * t;
+                const V3 w0 = L3(wt), w1 = L3(wt + 3), w2 = L3(wt + 6);
+                const V3 wmn{smin3(w0.x, w1.x, w2.x), smin3(w0.y, w1.y, w2.y), smin3(w0.z, w1.z, w2.z)};
+                const V3 wmx{smax3(w0.x, w1.x, w2.x), smax3(w0.y, w1.y, w2.y), smax3(w0.z, w1.z, w2.z)};
+                any = !(pmx.x < wmn.x || pmn.x > wmx.x || pmx.y < wmn.y || pmn.y > wmx.y || pmx.z < wmn.z ||
+                        pmn.z > wmx.z);
+            }
+            if (!any) continue;
+        }
         if (off) cand[off[i] + n] = make_int2(i, w);
         n++;
     }
@@ -1125,13 +1146,15 @@ int scene_step(zdx_ctx* ctx, Scene& s) {
     CKS(s.w_scan.ensure(sizeof(int64_t) * (N1 + 1)));
     if (s.nw > 0 && np > 0) {
         CKS(s.w_active.ensure(sizeof(int32_t) * N1));
-        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad),
+                                              as<double>(s.d_wtris), as<int64_t>(s.d_wtri_off), s.nw,
                                               as<int32_t>(s.w_active), nullptr, nullptr, INT64_MAX);
         CKS(scan_counts_i32(as<int32_t>(s.w_active), np, as<int64_t>(s.w_scan), st));
         CKS(cudaMemcpyAsync(&ncand, as<int64_t>(s.w_scan) + np, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         CKS(cudaStreamSynchronize(st));
         CKS(s.w_pairs.ensure(sizeof(int2) * std::max<int64_t>(ncand, 1)));
-        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw, nullptr,
+        k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad),
+                                              as<double>(s.d_wtris), as<int64_t>(s.d_wtri_off), s.nw, nullptr,
                                               as<int64_t>(s.w_scan), as<int2>(s.w_pairs), INT64_MAX);
         ctx->launches += 3;
     } else {
@@ -1695,10 +1718,12 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
     const int64_t* ncand = &g->ncand;
     if (s.nw > 0) {
         if (!small) {
-            k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+            k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad),
+                                                  as<double>(s.d_wtris), as<int64_t>(s.d_wtri_off), s.nw,
                                                   as<int32_t>(G.w_active), nullptr, nullptr, INT64_MAX);
             CKS(scan_offsets<int32_t>(as<int32_t>(G.w_active), np, nullptr, as<int64_t>(G.w_scan), G.scan_tmp.p, st));
-            k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad), s.nw,
+            k_wall_cand<<<grid(np), 256, 0, st>>>(state, mat, np, as<double>(s.d_wpose), as<double>(s.d_wrad),
+                                                  as<double>(s.d_wtris), as<int64_t>(s.d_wtri_off), s.nw,
                                                   nullptr, as<int64_t>(G.w_scan), as<int2>(G.w_pairs), G.wcap);
         }
         k_g_take<<<1, 1, 0, st>>>(as<int64_t>(G.w_scan) + np, G.wcap, &g->ncand, &g->need_cand, flags, GRAPH_OVF_CAND);
