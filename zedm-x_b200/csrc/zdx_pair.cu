@@ -896,7 +896,8 @@ __global__ __launch_bounds__(K1_THREADS, 2) void k_segments(PairArgs a) {
 // strict box compare, tri_tri).  With none of them meeting, the pair has no segment, as when the
 // separation certificate holds; otherwise k_segments tests the near pairs alone (their segments are
 // all the pair has), or in full when the motion exceeds M.  Warp per pair, lanes over the near pairs.
-__global__ void k_cache_skip(PairArgs a) {
+// (Three blocks of 256 per SM: 80 registers with some spills, 0.8 % faster on the pour than 128.)
+__global__ __launch_bounds__(256, 3) void k_cache_skip(PairArgs a) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     const int64_t n = pairs_of(a);
