@@ -61,6 +61,8 @@ def _cases(tmp):
         "walls": (g, [part(stl)], [dict(stl=plane, pos="0 0 0", quat="1 0 0 0", scale=1, mu=0.4, restitution=0.3),
                                    dict(pos="0 0 0")]),
         "unknown_keys_and_clamp": (dict(g, colour="red", output_interval=0), [part(stl, flavour="x")], []),
+        # this library's own keys (the graph step's clearance cache), which the reference ignores
+        "cache_keys": (dict(g, contact_cache=0, contact_cache_tau=0.02), [part(stl)], []),
     }
     return cases
 
