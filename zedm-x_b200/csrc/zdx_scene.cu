@@ -1900,7 +1900,7 @@ int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps) {
     // after one start at a single step and double while every step keeps a candidate.
     int remaining = nsteps, regrow = 0;
     const bool ff_ok = free_flight_ok(s);
-    bool try_ff = ff_ok;
+    bool try_ff = ff_ok && G.ff_next;
     int chunk_cap = ff_ok ? 1 : 64;
     while (remaining > 0) {
         if (try_ff) {
@@ -1958,6 +1958,7 @@ int scene_step_graph(zdx_ctx* ctx, Scene& s, int nsteps) {
         if (!rc) rc = graph_capture(ctx, s);
         if (rc) return rc;
     }
+    G.ff_next = try_ff;
     const GraphCounts& h = *G.host;
     StepStats stats;
     stats.pairs = h.npair;

@@ -104,6 +104,7 @@ enum : int {
 // untouched and raises a flag; the host then grows the capacities, captures again and repeats it.
 struct GraphStep {
     bool active = false;       // the history lives in these buffers (not in the Scene's)
+    bool ff_next = true;       // a small scene's next call tries free flight first (its last step had no candidate)
     cudaGraphExec_t exec = nullptr;
     int64_t pcap = 0, ccap = 0, wcap = 0, segcap = 0;
     int cap_seg = 0, k2_warps = 0, k1_grid = 0, wall_warps = 0, max_wtri = 1, kernels_per_step = 0;
