@@ -902,6 +902,7 @@ int scene_upload(zdx_ctx* ctx, Scene& s) {
     CKS(s.d_whist_key.ensure(16));
     CKS(s.d_whist_ds.ensure(16));
     CKS(cudaStreamSynchronize(st));
+    if (s.pinned.empty()) s.pin_host();
     return ZDX_OK;
 }
 

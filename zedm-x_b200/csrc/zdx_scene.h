@@ -194,8 +194,27 @@ struct Scene {
     GraphStep gs;
     std::shared_ptr<OutputPipeline> out;  // asynchronous outputs, created by the first one
 
+    // The host copies a state download lands in, page-locked while the scene lives so that the copies
+    // run at DMA speed; a range that cannot be registered stays pageable (slower, same results).
+    std::vector<void*> pinned;
+    void pin_host() {
+        auto pin = [&](void* p, size_t bytes) {
+            if (p && bytes && cudaHostRegister(p, bytes, cudaHostRegisterDefault) == cudaSuccess) pinned.push_back(p);
+            else cudaGetLastError();
+        };
+        pin(state.data(), sizeof(double) * state.size());
+        pin(force.data(), sizeof(double) * force.size());
+        pin(torque.data(), sizeof(double) * torque.size());
+        pin(contact_count.data(), sizeof(int32_t) * contact_count.size());
+    }
+    void unpin_host() {
+        for (void* p : pinned) cudaHostUnregister(p);
+        pinned.clear();
+    }
+
     void release_device() {
         out.reset();  // drains the queued outputs first
+        unpin_host();
         gs.release();
         for (DevBuf* b : {&d_state, &d_mat, &d_pmesh, &d_mtris, &d_moff, &d_mme, &d_mbd, &d_mrad, &d_wtris, &d_wnorm,
                           &d_wtri_off, &d_wpose, &d_wmat, &d_wrad, &d_force, &d_torque, &d_count, &d_hist_key,
