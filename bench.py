@@ -982,13 +982,14 @@ def measure_pour(args, ctx, steps, cpu=True):
     plain_ms = _timed_steps(sc, stream, flush, 3, graph=False)
     # e2e: the graph step plus the whole state brought back to the host every step
     e2e = []
+    host = sc.state()  # the caller's buffers, filled again every step
     for k in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         sc.step_graph(1)
-        sc.state()
+        sc.state(out=host)
         e2e.append(time.perf_counter() - t1)
     np_ = sc.n
     d2h = np_ * (16 * 8 + 3 * 8 * 2 + 4)

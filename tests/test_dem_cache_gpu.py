@@ -94,3 +94,16 @@ def test_cache_with_tiny_capacities(tmp_path):
         off.step_graph(chunk)
         on.step_graph(chunk)
         _same(off, on, f"after {off.info()['steps']} steps")
+
+
+def test_state_into_caller_buffers(tmp_path):
+    """Scene.state(out=...) fills the caller's arrays with what a fresh call returns."""
+    off, on = _scenes(tmp_path, n=300, seed=4)
+    on.step_graph(5)
+    fresh = on.state()
+    buf = tuple(np.full_like(a, 7) for a in fresh)
+    got = on.state(out=buf)
+    assert all(g is b for g, b in zip(got, buf))
+    assert all(np.array_equal(g, f) for g, f in zip(got, fresh))
+    with pytest.raises(ValueError):
+        on.state(out=(np.zeros((on.n, 15)),) + buf[1:])

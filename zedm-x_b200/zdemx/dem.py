@@ -65,11 +65,21 @@ class Scene:
         _lib.check(_lib.lib().zdx_scene_info(self.ctx.handle, v.ctypes.data_as(_lib._i64p)), self.ctx.handle)
         return dict(zip(INFO_KEYS, (int(x) for x in v)))
 
-    def state(self):
-        st = np.zeros((self.n, 16))
-        f = np.zeros((self.n, 3))
-        t = np.zeros((self.n, 3))
-        c = np.zeros(self.n, np.int32)
+    def state(self, out=None):
+        """(state n x 16, force n x 3, torque n x 3, contact_count n).  out: the four arrays of an
+        earlier call to fill again instead of new ones (a loop that reads the state every step then
+        allocates nothing)."""
+        if out is None:
+            st = np.zeros((self.n, 16))
+            f = np.zeros((self.n, 3))
+            t = np.zeros((self.n, 3))
+            c = np.zeros(self.n, np.int32)
+        else:
+            st, f, t, c = out
+            for a, shape, dt in ((st, (self.n, 16), np.float64), (f, (self.n, 3), np.float64),
+                                 (t, (self.n, 3), np.float64), (c, (self.n,), np.int32)):
+                if a.shape != shape or a.dtype != dt or not a.flags["C_CONTIGUOUS"] or not a.flags["WRITEABLE"]:
+                    raise ValueError(f"state(out=...): expected a writable C-contiguous {dt.__name__} array of shape {shape}")
         _lib.check(_lib.lib().zdx_scene_get_state(self.ctx.handle, st.ctypes.data_as(_lib._dp), f.ctypes.data_as(_lib._dp),
                                                   t.ctypes.data_as(_lib._dp), c.ctypes.data_as(_lib._i32p)),
                    self.ctx.handle)
