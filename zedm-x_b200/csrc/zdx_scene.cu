@@ -1455,6 +1455,11 @@ __global__ void k_g_commit(GraphCounts* g, const int64_t* hscan, const int64_t* 
 
 }  // namespace
 
+__global__ void k_iota(int32_t* v, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int32_t)i;
+}
+
 // The clearance cache runs in scenes of at least this many particles: in smaller ones its kernels cost
 // more than the few pairs it could settle.
 constexpr int kCacheMinParticles = 256;
@@ -1555,6 +1560,24 @@ static int graph_alloc(zdx_ctx* ctx, Scene& s) {
     CKS(G.k2_slots.ensure(slot * (size_t)warps));
     CKS(G.cstage.ensure(sizeof(double) * 20 * C1));
     CKS(G.cistage.ensure(sizeof(int32_t) * 5 * C1));
+    // The meshes' per-triangle spheres, bounds and point_in_tri inflations do not change from step to
+    // step: computed here, outside the captured step.
+    {
+        PairArgs m{};
+        m.n_mesh = nm;
+        m.tris = as<double>(s.d_mtris);
+        m.tri_off = as<int64_t>(s.d_moff);
+        m.tri_sph = as<double4>(G.tri_sph);
+        m.mesh_R_bits = as<unsigned long long>(G.mesh_R);
+        m.mesh_valid = as<int>(G.mesh_valid);
+        m.mesh_infl_bits = as<unsigned long long>(G.mesh_infl);
+        CKS(cudaMemsetAsync(G.mesh_R.p, 0, sizeof(unsigned long long) * std::max(nm, 1), ctx->stream));
+        CKS(cudaMemsetAsync(G.mesh_valid.p, 0, sizeof(int) * std::max(nm, 1), ctx->stream));
+        CKS(cudaMemsetAsync(G.mesh_infl.p, 0, sizeof(unsigned long long) * std::max(nm, 1), ctx->stream));
+        launch_mesh_prep(m, total_tris, ctx->stream);
+    }
+    // the pair order of a small scene (its steps skip the cost order): the identity
+    if (s.np < kCacheMinParticles) k_iota<<<grid((int64_t)P1), 256, 0, ctx->stream>>>(as<int32_t>(G.order), (int64_t)P1);
     // activity flags are read (by the history scans) even in a step that stops early
     CKS(cudaMemsetAsync(G.pr_active.p, 0, sizeof(int32_t) * P1, ctx->stream));
     CKS(cudaMemsetAsync(G.w_act.p, 0, sizeof(int32_t) * W1, ctx->stream));
@@ -1656,11 +1679,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
         a.err = reinterpret_cast<int*>(cnt + 7);
         CKS(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 16, st));
         CKS(cudaMemsetAsync(a.pair_status, 0, sizeof(int32_t) * P1, st));
-        CKS(cudaMemsetAsync(G.mesh_R.p, 0, sizeof(unsigned long long) * std::max(nm, 1), st));
-        CKS(cudaMemsetAsync(G.mesh_valid.p, 0, sizeof(int) * std::max(nm, 1), st));
-        CKS(cudaMemsetAsync(G.mesh_infl.p, 0, sizeof(unsigned long long) * std::max(nm, 1), st));
-        a.mesh_infl_bits = as<unsigned long long>(G.mesh_infl);
-        launch_mesh_prep(a, s.mesh_off.back(), st);
+        a.mesh_infl_bits = as<unsigned long long>(G.mesh_infl);  // graph_alloc prepared the meshes
         if (cache) {
             a.cache_idx = as<int32_t>(G.cidx);
             a.cache_in = as<double>(G.cval);
@@ -1672,7 +1691,8 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
             a.order_count = reinterpret_cast<int*>(cnt + 8);
             launch_cache_skip(a, std::max(1, ctx->num_sms) * 8, st);
         }
-        launch_cost_order(a, as<int32_t>(G.order), as<int>(G.buckets), st);
+        // a small scene's few pairs take the identity order that graph_alloc wrote
+        if (s.np >= kCacheMinParticles) launch_cost_order(a, as<int32_t>(G.order), as<int>(G.buckets), st);
         a.order = as<int32_t>(G.order);
         a.item_begin = 0;
         a.item_end = G.pcap;
