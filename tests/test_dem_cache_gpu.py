@@ -1,8 +1,9 @@
 """The graph step's clearance cache (config key contact_cache, default on) against the same step without
-it: a pair skipped on a cached clearance has no segment, as the full triangle stage finds, so state,
-forces and the step log's counters agree bit for bit.  Covers pairs that close in, touch and part; poses
-moved by set_state between steps (translations and rotations larger than any clearance); and the cache
-emptied by a capacity growth."""
+it: a pair settled on a cached clearance has no segment, and a pair narrowed to its cached near pairs has
+the segments of those alone, as the full triangle stage finds, so state, forces and the step log's
+counters agree bit for bit.  Covers pairs that close in, touch and part; poses moved by set_state between
+steps (translations and rotations larger than any clearance); and the cache emptied by a capacity
+growth."""
 import numpy as np
 import pytest
 
