@@ -1402,27 +1402,33 @@ __global__ void k_cache_flags(const double* cout, int64_t cap, const int64_t* n_
     if ((threadIdx.x & 31) == 0 && b)
         atomicAdd(reinterpret_cast<unsigned long long*>(&g->cache_skipped), (unsigned long long)__popc(b));
 }
+// A warp per entry (lanes over its words, so the copies of the near-pair codes coalesce).
 __global__ void k_cache_write(const int32_t* flag, const int64_t* pos, int64_t cap, const int64_t* n_dev, const int2* pairs,
                               const double* cout, const uint32_t* hout, int64_t* ckey2, double* cval2, uint32_t* chit2) {
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (p >= dev_count(cap, n_dev) || !flag[p]) return;
-    const int64_t o = pos[p];
-    ckey2[o] = ((int64_t)pairs[p].x << 32) | (int64_t)(uint32_t)pairs[p].y;
-    for (int k = 0; k < CACHE_W; ++k) cval2[CACHE_W * o + k] = cout[CACHE_W * p + k];
-    const int nh = (int)cout[CACHE_W * p + CACHE_NH];
-    for (int h = 0; h < nh; ++h) chit2[CACHE_H * o + h] = hout[CACHE_H * p + h];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t n = dev_count(cap, n_dev);
+    for (int64_t p = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); p < n; p += warps) {
+        if (!flag[p]) continue;
+        const int64_t o = pos[p];
+        if (lane == 0) ckey2[o] = ((int64_t)pairs[p].x << 32) | (int64_t)(uint32_t)pairs[p].y;
+        if (lane < CACHE_W) cval2[CACHE_W * o + lane] = cout[CACHE_W * p + lane];
+        const int nh = (int)cout[CACHE_W * p + CACHE_NH];
+        for (int h = lane; h < nh; h += 32) chit2[CACHE_H * o + h] = hout[CACHE_H * p + h];
+    }
 }
-// with the step complete, the next step's entries become the cache
+// with the step complete, the next step's entries become the cache (a warp per entry)
 __global__ void k_cache_commit(GraphCounts* g, const int64_t* pos, const int64_t* ckey2, const double* cval2,
                                const uint32_t* chit2, int64_t* ckey, double* cval, uint32_t* chit) {
     if (g->flags) return;
+    const int lane = threadIdx.x & 31;
     const int64_t n = pos[g->npair];
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += stride) {
-        ckey[k] = ckey2[k];
-        for (int c = 0; c < CACHE_W; ++c) cval[CACHE_W * k + c] = cval2[CACHE_W * k + c];
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t k = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); k < n; k += warps) {
+        if (lane == 0) ckey[k] = ckey2[k];
+        if (lane < CACHE_W) cval[CACHE_W * k + lane] = cval2[CACHE_W * k + lane];
         const int nh = (int)cval2[CACHE_W * k + CACHE_NH];
-        for (int h = 0; h < nh; ++h) chit[CACHE_H * k + h] = chit2[CACHE_H * k + h];
+        for (int h = lane; h < nh; h += 32) chit[CACHE_H * k + h] = chit2[CACHE_H * k + h];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) g->ncache = n;
 }
@@ -1705,7 +1711,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
             // the next step's cache: this step's clearances, in pair order (the keys stay sorted)
             k_cache_flags<<<grid(G.pcap), 256, 0, st>>>(as<double>(G.cout), G.pcap, npair, as<int32_t>(G.cflag), g);
             CKS(scan_offsets<int32_t>(as<int32_t>(G.cflag), G.pcap, npair, as<int64_t>(G.cscan), G.scan_tmp.p, st));
-            k_cache_write<<<grid(G.pcap), 256, 0, st>>>(as<int32_t>(G.cflag), as<int64_t>(G.cscan), G.pcap, npair,
+            k_cache_write<<<std::max(1, ctx->num_sms) * 8, 256, 0, st>>>(as<int32_t>(G.cflag), as<int64_t>(G.cscan), G.pcap, npair,
                                                         as<int2>(G.bp_pairs), as<double>(G.cout), as<uint32_t>(G.chout),
                                                         as<int64_t>(G.ckey2), as<double>(G.cval2), as<uint32_t>(G.chit2));
         }
@@ -1787,7 +1793,7 @@ static int graph_launch_step(zdx_ctx* ctx, Scene& s) {
                                                            as<double>(G.hds2), as<int64_t>(G.whkey), as<double>(G.whds),
                                                            as<int64_t>(G.whkey2), as<double>(G.whds2));
     if (cache_on(s))
-        k_cache_commit<<<std::max(1, ctx->num_sms), 256, 0, st>>>(g, as<int64_t>(G.cscan), as<int64_t>(G.ckey2),
+        k_cache_commit<<<std::max(1, ctx->num_sms) * 8, 256, 0, st>>>(g, as<int64_t>(G.cscan), as<int64_t>(G.ckey2),
                                                                     as<double>(G.cval2), as<uint32_t>(G.chit2),
                                                                     as<int64_t>(G.ckey), as<double>(G.cval),
                                                                     as<uint32_t>(G.chit));
