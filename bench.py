@@ -525,7 +525,8 @@ def main():
     extras["independent_meshes"] = sweep_independent(args, ctx, dev, flush)
     log("independent meshes done")
     torch.cuda.empty_cache()
-    extras["dem"] = {"pour": measure_pour(args, ctx, steps=args.steps, cpu=False)}
+    # 100 timed steps (about 0.3 s): long enough for the clock sampler to see the region
+    extras["dem"] = {"pour": measure_pour(args, ctx, steps=max(args.steps, 100), cpu=False)}
     log("pour done")
     extras["dem"]["two_particles"] = measure_two(args, ctx, reps=3, extras=False)
     log("two particles done")
